@@ -1,0 +1,175 @@
+/*
+ * trn: B200-native path-space differentiable rendering, C-ABI.
+ *
+ * Drop-in replacement for the execution layer behind TensorRay's integrator
+ * and scene API (LibTensorRay/Renderer). Every function returns 0 on success
+ * and -1 on failure; trn_last_error() then describes the failure (the
+ * reference throws std::runtime_error from CUDA_CHECK/OPTIX_CHECK,
+ * LibTensorRay/Renderer/Optix.h:38-80, and pybind turns it into RuntimeError).
+ * Bulk arrays passed to trn_render_* and trn_scene_get_* are DEVICE pointers;
+ * the scene description passed to trn_scene_create is HOST memory. All work
+ * is enqueued on the caller's stream (the reference runs on stream 0 and
+ * synchronises after every kernel).
+ */
+#ifndef TRN_H_
+#define TRN_H_
+
+#include <cuda_runtime.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct trn_scene trn_scene;
+
+/* Integrator ids (TensorRay.cpp:190-222 Python classes). */
+enum {
+  TRN_PATH_TRACER = 0,     /* PathTracer (PathTracer.cpp:37-123) */
+  TRN_PRIMARY_EDGE = 1,    /* PrimaryEdgeIntegrator (BoundaryPrimary.cpp:36-181) */
+  TRN_DIRECT_EDGE = 2,     /* DirectEdgeIntegrator (BoundaryDirect.cpp:38-143) */
+  TRN_INDIRECT_EDGE = 3,   /* IndirectEdgeIntegrator (BoundaryIndirect.cpp:38-192) */
+  TRN_PIXEL_EDGE = 4       /* PixelBoundaryIntegrator (BoundaryPixel.cpp:36-159) */
+};
+
+/* BSDF description (Diffuse.h, Microfacet.h; SceneLoader.cpp:265-305). */
+typedef struct {
+  int type;            /* 0 = diffuse, 1 = microfacet */
+  int texture;         /* albedo / diffuse-reflectance texture index, -1 = constant */
+  float albedo[3];     /* constant albedo / diffuse reflectance */
+  float specular[3];   /* microfacet specular reflectance F0 */
+  float roughness;     /* microfacet roughness */
+} trn_bsdf;
+
+/* RGB float texture, texel (x, y) at data[3 * (y * width + x)]
+ * (ImageTexture, BSDF.cpp:56-98, stores the same texels channel-major). */
+typedef struct {
+  int width, height;
+  const float* data;   /* host */
+} trn_texture;
+
+/* Whole-scene description: meshes are concatenated, indices are global.
+ * Replaces Scene::ExtractGeometry / ConfigureLight inputs
+ * (Scene.cpp:46-124, 471-520). All pointers are HOST memory. */
+typedef struct {
+  int num_vertices;
+  int num_triangles;
+  int num_uvs;
+  int num_meshes;
+  int num_lights;
+  int num_bsdfs;
+  int num_textures;
+  const float* positions;        /* [V*3] raw positions (before the translation parameter) */
+  const int* indices;            /* [T*3] */
+  const float* uvs;              /* [NUV*2] or NULL */
+  const int* uv_indices;         /* [T*3] or NULL */
+  const int* vertex_mesh;        /* [V] mesh id of each vertex */
+  const int* triangle_mesh;      /* [T] mesh id of each triangle */
+  const unsigned char* mesh_smooth; /* [M] 1 = averaged vertex normals (Primitive.cpp:323-340) */
+  const int* mesh_bsdf;          /* [M] bsdf id */
+  const int* mesh_light;         /* [M] area-light id or -1 */
+  const float* mesh_translation; /* [M*3] translation parameter (Primitive::mTrans) or NULL */
+  const float* light_radiance;   /* [L*3] */
+  const trn_bsdf* bsdfs;         /* [num_bsdfs] */
+  const trn_texture* textures;   /* [num_textures] */
+} trn_scene_desc;
+
+/* Pinhole camera (Camera::Init, Camera.cpp:89-137 + BaseCamera.cpp:45-88).
+ * Matrices are row-major and act on column vectors. */
+typedef struct {
+  int width, height;
+  float pos[3];
+  float dir[3];
+  float raster_to_camera[16];
+  float view_inv[16];
+  float world_to_sample[16];
+  float sample_to_camera[16];
+  float raster_to_world[16];
+  float inv_area;
+  float plane_len_x, plane_len_y;
+} trn_camera;
+
+/* RenderOptions (Integrator.h:47-78). spp counts are per integrator;
+ * batches only bound memory in the reference and are ignored here. */
+typedef struct {
+  int seed;
+  int max_bounces;
+  int spp;        /* interior (PathTracer) */
+  int sppe;       /* primary edge */
+  int sppse0;     /* direct edge */
+  int sppse1;     /* indirect edge */
+  int sppe0;      /* pixel boundary */
+} trn_render_options;
+
+/* Sample source for one integrator call. If `samples` is non-NULL it is a
+ * device tensor of uniform floats laid out [dim][slot] with `stride` slots per
+ * dimension (Tensorf::RandomFloat SoA blocks, Tensor.h:2793-2799); otherwise
+ * samples come from the counter hash keyed by (options.seed, integrator). */
+typedef struct {
+  const float* samples;
+  long long stride;
+} trn_samples;
+
+/* Last error message of this thread ("" if none). */
+const char* trn_last_error(void);
+/* Library version string. */
+const char* trn_version(void);
+
+/* Build a camera. Replaces Camera::Init (Camera.cpp:89-103). */
+int trn_camera_init(trn_camera* out, const float pos[3], const float target[3], const float up[3],
+                    int width, int height, float fov_deg);
+
+/* Scene lifetime. Replaces Scene::Configure (Scene.cpp:522-533): create
+ * uploads the description; configure runs Primitive::Configure, face/vertex
+ * normals, light distribution, secondary edge list and the LBVH build. */
+int trn_scene_create(const trn_scene_desc* desc, trn_scene** out);
+int trn_scene_configure(trn_scene* scene, cudaStream_t stream);
+int trn_scene_destroy(trn_scene* scene);
+
+/* Parameter access (TensorRay.cpp: get_var/set_var; Primitive::mTrans,
+ * mPositionBufferRaw, BSDF texture). Device pointers. set_* marks the scene
+ * for re-configuration. */
+int trn_scene_set_translation(trn_scene* scene, const float* translation_dev, cudaStream_t stream);
+int trn_scene_set_positions(trn_scene* scene, const float* raw_positions_dev, cudaStream_t stream);
+int trn_scene_set_texels(trn_scene* scene, const float* texels_dev, cudaStream_t stream);
+
+/* Read back derived geometry for checks (device destinations). */
+int trn_scene_get_geometry(trn_scene* scene, float* pos, float* fnormal, float* area, float* vnormal,
+                           cudaStream_t stream);
+int trn_scene_counts(const trn_scene* scene, int* num_vertices, int* num_triangles, int* num_edges,
+                     long long* num_texels, int* num_meshes);
+
+/* Closest-hit ray query over the LBVH. Replaces RayIntersectOptix
+ * (Optix.h:149, Optix.cpp:252-305): out_tri = -1 on a miss. Device arrays of
+ * n rays: org/dir [n*3], tmin/tmax [n]; outputs tri [n], u/v/t [n]. */
+int trn_intersect(trn_scene* scene, int n, const float* org, const float* dir, const float* tmin,
+                  const float* tmax, int* out_tri, float* out_u, float* out_v, float* out_t,
+                  cudaStream_t stream);
+/* Occlusion query (Scene::Occluded, Scene.cpp:548-562): out_visible[i] = 1
+ * when nothing is hit inside (tmin, tmax). */
+int trn_occluded(trn_scene* scene, int n, const float* org, const float* dir, const float* tmin,
+                 const float* tmax, int* out_visible, cudaStream_t stream);
+
+/* Forward render of one integrator (Integrator::RenderC, Integrator.h:96-104,
+ * PathTracer.h:60-68). image_out [W*H*3] is overwritten. Only
+ * TRN_PATH_TRACER produces radiance; edge integrators produce their
+ * (zero-valued in the reference) primal and return 0. */
+int trn_render_fwd(trn_scene* scene, const trn_camera* camera, const trn_render_options* options,
+                   int integrator, const trn_samples* samples, float* image_out, cudaStream_t stream);
+
+/* Reverse-mode pass of one integrator (Integrator::RenderD, Integrator.h:106-121):
+ * replays the paths of the same seed/samples and accumulates dL/dparameters
+ * into the scene's gradient buffers given dL/dI [W*H*3]. */
+int trn_render_grad(trn_scene* scene, const trn_camera* camera, const trn_render_options* options,
+                    int integrator, const trn_samples* samples, const float* dLdI, cudaStream_t stream);
+
+/* Finish the geometry-chain adjoint and copy gradients out (get_grad with
+ * clear_grad, pybind_utils.h:133-142). Any destination may be NULL.
+ * d_translation [M*3], d_positions [V*3] (raw positions), d_texels [ntexel*3]. */
+int trn_scene_get_grads(trn_scene* scene, float* d_translation, float* d_positions, float* d_texels,
+                        int clear, cudaStream_t stream);
+int trn_scene_clear_grads(trn_scene* scene, cudaStream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TRN_H_ */

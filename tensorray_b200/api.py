@@ -1,0 +1,393 @@
+"""Python mirror of the reference's ``TensorRay`` module (TensorRay.cpp:48-222).
+
+Names, arguments and error behaviour follow the reference: ``Scene``,
+``RenderOptions``, ``PathTracer`` / ``PrimaryEdgeIntegrator`` /
+``DirectEdgeIntegrator`` / ``IndirectEdgeIntegrator`` /
+``PixelBoundaryIntegrator`` with ``renderC`` and ``renderD``, shapes with
+``diff_translation`` / ``diff_all_vertex_pos``, BSDFs with ``diff_texture``.
+Failures raise ``RuntimeError`` with the library's message, as pybind does for
+the reference's std::runtime_error. Device memory and streams come from
+PyTorch; all rendering runs in the native library.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import _abi
+from ._abi import (TRN_DIRECT_EDGE, TRN_INDIRECT_EDGE, TRN_PATH_TRACER, TRN_PIXEL_EDGE, TRN_PRIMARY_EDGE,
+                   TrnBsdf, TrnCamera, TrnRenderOptions, TrnSamples, TrnSceneDesc, TrnTexture, check)
+from .scenes import SceneSpec
+
+
+def _require_cuda() -> torch.device:
+    if not torch.cuda.is_available():
+        raise RuntimeError("tensorray_b200 renders on a CUDA device; none is available")
+    return torch.device("cuda", torch.cuda.current_device())
+
+
+def _stream() -> int:
+    return torch.cuda.current_stream().cuda_stream
+
+
+def _fptr(a: np.ndarray | None):
+    if a is None:
+        return None
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def _iptr(a: np.ndarray | None):
+    if a is None:
+        return None
+    return a.ctypes.data_as(C.POINTER(C.c_int))
+
+
+def env_create() -> None:
+    """Load the native library (EnvCreate, pybind_utils.h:38-53)."""
+    _abi.load()
+
+
+def env_release() -> None:
+    torch.cuda.empty_cache()
+
+
+class RenderOptions:
+    """RenderOptions (Integrator.h:47-78, bound at TensorRay.cpp:165-188)."""
+
+    def __init__(self, seed: int, max_bounces: int, spp: int, sppe: int, sppse0: int, sppse1: int, sppe0: int = 0):
+        self.seed = seed
+        self.max_bounces = max_bounces
+        self.spp = spp
+        self.sppe = sppe
+        self.sppse0 = sppse0
+        self.sppse1 = sppse1
+        self.sppe0 = sppe0
+        self.spp_batch, self.sppe_batch, self.sppse0_batch = spp, sppe, sppse0
+        self.sppse1_batch, self.sppe0_batch = sppse1, sppe0
+        self.export_deriv = False
+        self.quiet = True
+
+    def _c(self) -> TrnRenderOptions:
+        return TrnRenderOptions(int(self.seed), int(self.max_bounces), int(self.spp), int(self.sppe),
+                                int(self.sppse0), int(self.sppse1), int(self.sppe0))
+
+
+class Camera:
+    """Pinhole sensor (Camera::Init, Camera.cpp:89-103)."""
+
+    def __init__(self, pos, target, up, width: int, height: int, fov: float):
+        self.width, self.height = int(width), int(height)
+        self.pos, self.target, self.up, self.fov = tuple(pos), tuple(target), tuple(up), float(fov)
+        self.c = TrnCamera()
+        lib = _abi.load()
+        f3 = lambda v: (C.c_float * 3)(*[float(x) for x in v])
+        check(lib.trn_camera_init(C.byref(self.c), f3(pos), f3(target), f3(up), self.width, self.height,
+                                  C.c_float(self.fov)), "trn_camera_init")
+
+    def matrices(self) -> dict:
+        c = self.c
+        m = lambda a: np.array(list(a), np.float32).reshape(4, 4)
+        return {"pos": np.array(list(c.pos), np.float32), "dir": np.array(list(c.dir), np.float32),
+                "raster_to_camera": m(c.raster_to_camera), "view_inv": m(c.view_inv),
+                "world_to_sample": m(c.world_to_sample), "sample_to_camera": m(c.sample_to_camera),
+                "raster_to_world": m(c.raster_to_world), "inv_area": np.float32(c.inv_area),
+                "plane_len_x": np.float32(c.plane_len_x), "plane_len_y": np.float32(c.plane_len_y),
+                "width": c.width, "height": c.height}
+
+
+class Shape:
+    """Primitive parameters (Primitive.cpp:374-388)."""
+
+    def __init__(self, scene: "Scene", index: int, vstart: int, vcount: int, fcount: int):
+        self._scene, self.index = scene, index
+        self._vstart, self._vcount, self._fcount = vstart, vcount, fcount
+        self.requires_translation_grad = False
+        self.requires_vertex_grad = False
+
+    @property
+    def translation(self) -> torch.Tensor:
+        return self._scene._translation[self.index].clone()
+
+    @translation.setter
+    def translation(self, t) -> None:
+        self._scene._translation[self.index] = torch.as_tensor(t, dtype=torch.float32,
+                                                               device=self._scene.device).reshape(3)
+        self._scene._dirty = True
+
+    def diff_translation(self) -> None:
+        self.requires_translation_grad = True
+
+    def diff_all_vertex_pos(self) -> None:
+        self.requires_vertex_grad = True
+
+    def get_vertex_count(self) -> int:
+        return self._vcount
+
+    def get_face_count(self) -> int:
+        return self._fcount
+
+    def vertex_slice(self) -> slice:
+        return slice(self._vstart, self._vstart + self._vcount)
+
+
+class BSDF:
+    def __init__(self, scene: "Scene", index: int, texture: int):
+        self._scene, self.index, self.texture = scene, index, texture
+        self.requires_texture_grad = False
+
+    def diff_texture(self, name: str = "") -> None:
+        if self.texture < 0:
+            raise RuntimeError("BSDF has no texture to differentiate")
+        self.requires_texture_grad = True
+
+
+class Scene:
+    """Scene (Scene.h:98-130) over a native trn_scene handle."""
+
+    def __init__(self, spec: SceneSpec | None = None):
+        self.device = _require_cuda()
+        self._lib = _abi.load()
+        self._h = C.c_void_p()
+        self._dirty = True
+        self.shapes: list[Shape] = []
+        self.bsdfs: list[BSDF] = []
+        self.cameras: list[Camera] = []
+        if spec is not None:
+            self.load_spec(spec)
+
+    # -- construction -------------------------------------------------------
+    def load_spec(self, spec: SceneSpec) -> None:
+        a = spec.arrays()
+        self.spec = spec
+        self._keep = a
+        nb = len(spec.bsdfs)
+        bs = (TrnBsdf * nb)()
+        for i, b in enumerate(spec.bsdfs):
+            bs[i] = TrnBsdf(b.type, b.texture, (C.c_float * 3)(*b.albedo), (C.c_float * 3)(*b.specular),
+                            b.roughness)
+        texs = (TrnTexture * max(1, len(spec.textures)))()
+        self._tex_keep = []
+        for i, t in enumerate(spec.textures):
+            arr = np.ascontiguousarray(t, np.float32)
+            self._tex_keep.append(arr)
+            texs[i] = TrnTexture(arr.shape[1], arr.shape[0], _fptr(arr))
+        d = TrnSceneDesc()
+        d.num_vertices = len(a["positions"])
+        d.num_triangles = len(a["indices"])
+        d.num_uvs = 0 if a["uvs"] is None else len(a["uvs"])
+        d.num_meshes = len(spec.meshes)
+        d.num_lights = len(spec.lights)
+        d.num_bsdfs = nb
+        d.num_textures = len(spec.textures)
+        d.positions = _fptr(a["positions"])
+        d.indices = _iptr(a["indices"])
+        d.uvs = _fptr(a["uvs"])
+        d.uv_indices = _iptr(a["uv_indices"])
+        d.vertex_mesh = _iptr(a["vertex_mesh"])
+        d.triangle_mesh = _iptr(a["triangle_mesh"])
+        d.mesh_smooth = a["mesh_smooth"].ctypes.data_as(C.POINTER(C.c_ubyte))
+        d.mesh_bsdf = _iptr(a["mesh_bsdf"])
+        d.mesh_light = _iptr(a["mesh_light"])
+        d.mesh_translation = _fptr(a["mesh_translation"])
+        d.light_radiance = _fptr(a["light_radiance"])
+        d.bsdfs = bs
+        d.textures = texs
+        check(self._lib.trn_scene_create(C.byref(d), C.byref(self._h)), "trn_scene_create")
+        nv, nt, ne, nm = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        ntex = C.c_longlong()
+        check(self._lib.trn_scene_counts(self._h, C.byref(nv), C.byref(nt), C.byref(ne), C.byref(ntex),
+                                         C.byref(nm)), "trn_scene_counts")
+        self.num_vertices, self.num_triangles, self.num_edges = nv.value, nt.value, ne.value
+        self.num_texels, self.num_meshes = ntex.value, nm.value
+        self._translation = torch.as_tensor(a["mesh_translation"], device=self.device).clone()
+        self._raw_positions = torch.as_tensor(a["positions"], device=self.device).clone()
+        vstart = 0
+        for i, m in enumerate(spec.meshes):
+            self.shapes.append(Shape(self, i, vstart, len(m.positions), len(m.faces)))
+            vstart += len(m.positions)
+        self.bsdfs = [BSDF(self, i, b.texture) for i, b in enumerate(spec.bsdfs)]
+        self.cameras = [Camera(c.pos, c.target, c.up, c.width, c.height, c.fov) for c in spec.cameras]
+        self._dirty = True
+
+    def __del__(self):
+        try:
+            if self._h:
+                self._lib.trn_scene_destroy(self._h)
+                self._h = C.c_void_p()
+        except Exception:
+            pass
+
+    # -- parameters -----------------------------------------------------------
+    def set_vertex_positions(self, raw: torch.Tensor) -> None:
+        raw = raw.detach().to(self.device, torch.float32).contiguous().reshape(-1, 3)
+        if raw.shape[0] != self.num_vertices:
+            raise RuntimeError("vertex count mismatch")
+        self._raw_positions.copy_(raw)
+        self._dirty = True
+
+    def set_texels(self, texels: torch.Tensor) -> None:
+        t = texels.detach().to(self.device, torch.float32).contiguous()
+        if t.numel() != 3 * self.num_texels:
+            raise RuntimeError("texel count mismatch")
+        check(self._lib.trn_scene_set_texels(self._h, C.c_void_p(t.data_ptr()), C.c_void_p(_stream())),
+              "trn_scene_set_texels")
+
+    def configure(self) -> None:
+        """Scene::Configure (Scene.cpp:522-533): geometry chain + LBVH."""
+        st = C.c_void_p(_stream())
+        check(self._lib.trn_scene_set_translation(self._h, C.c_void_p(self._translation.data_ptr()), st),
+              "trn_scene_set_translation")
+        check(self._lib.trn_scene_set_positions(self._h, C.c_void_p(self._raw_positions.data_ptr()), st),
+              "trn_scene_set_positions")
+        check(self._lib.trn_scene_configure(self._h, st), "trn_scene_configure")
+        self._dirty = False
+
+    def _ensure(self) -> None:
+        if self._dirty:
+            self.configure()
+
+    def get_width(self) -> int:
+        return self.cameras[0].width
+
+    def get_height(self) -> int:
+        return self.cameras[0].height
+
+    @property
+    def handle(self):
+        return self._h
+
+    def geometry(self) -> dict:
+        self._ensure()
+        d = self.device
+        pos = torch.empty(self.num_vertices, 3, device=d)
+        fn = torch.empty(self.num_triangles, 3, device=d)
+        ar = torch.empty(self.num_triangles, device=d)
+        vn = torch.empty(self.num_vertices, 3, device=d)
+        check(self._lib.trn_scene_get_geometry(self._h, C.c_void_p(pos.data_ptr()), C.c_void_p(fn.data_ptr()),
+                                               C.c_void_p(ar.data_ptr()), C.c_void_p(vn.data_ptr()),
+                                               C.c_void_p(_stream())), "trn_scene_get_geometry")
+        return {"positions": pos, "face_normals": fn, "areas": ar, "vertex_normals": vn}
+
+    # -- gradients ---------------------------------------------------------------
+    def get_grads(self, clear: bool = True) -> dict:
+        """Finish the geometry adjoint and return dL/d(translation per mesh),
+        dL/d(raw vertex positions), dL/d(texels) (get_grad, pybind_utils.h:133-142)."""
+        d = self.device
+        gt = torch.zeros(self.num_meshes, 3, device=d)
+        gp = torch.zeros(self.num_vertices, 3, device=d)
+        gx = torch.zeros(max(1, self.num_texels), 3, device=d)
+        check(self._lib.trn_scene_get_grads(self._h, C.c_void_p(gt.data_ptr()), C.c_void_p(gp.data_ptr()),
+                                            C.c_void_p(gx.data_ptr()), int(clear), C.c_void_p(_stream())),
+              "trn_scene_get_grads")
+        return {"translation": gt, "positions": gp, "texels": gx[: self.num_texels]}
+
+    def clear_grads(self) -> None:
+        check(self._lib.trn_scene_clear_grads(self._h, C.c_void_p(_stream())), "trn_scene_clear_grads")
+
+    # -- ray queries (RayIntersectOptix replacement) -------------------------------
+    def intersect(self, org: torch.Tensor, dir: torch.Tensor, tmin: torch.Tensor, tmax: torch.Tensor):
+        self._ensure()
+        n = org.shape[0]
+        d = self.device
+        org, dir = org.contiguous().float(), dir.contiguous().float()
+        tmin, tmax = tmin.contiguous().float(), tmax.contiguous().float()
+        tri = torch.empty(n, dtype=torch.int32, device=d)
+        u, v, t = (torch.empty(n, device=d) for _ in range(3))
+        check(self._lib.trn_intersect(self._h, n, *(C.c_void_p(x.data_ptr()) for x in (org, dir, tmin, tmax, tri,
+                                                                                        u, v, t)),
+                                      C.c_void_p(_stream())), "trn_intersect")
+        return tri, u, v, t
+
+    def occluded(self, org, dir, tmin, tmax) -> torch.Tensor:
+        self._ensure()
+        n = org.shape[0]
+        vis = torch.empty(n, dtype=torch.int32, device=self.device)
+        org, dir = org.contiguous().float(), dir.contiguous().float()
+        tmin, tmax = tmin.contiguous().float(), tmax.contiguous().float()
+        check(self._lib.trn_occluded(self._h, n, *(C.c_void_p(x.data_ptr()) for x in (org, dir, tmin, tmax, vis)),
+                                     C.c_void_p(_stream())), "trn_occluded")
+        return vis
+
+
+def _samples_struct(samples: torch.Tensor | None) -> TrnSamples:
+    if samples is None:
+        return TrnSamples(None, 0)
+    if not (samples.is_cuda and samples.dtype == torch.float32 and samples.is_contiguous() and samples.dim() == 2):
+        raise RuntimeError("samples must be a contiguous float32 CUDA tensor [dims, slots]")
+    return TrnSamples(C.c_void_p(samples.data_ptr()), samples.shape[1])
+
+
+class Integrator:
+    integrator_id = TRN_PATH_TRACER
+
+    def __init__(self):
+        self.options: RenderOptions | None = None
+
+    def set_param(self, options: RenderOptions) -> None:
+        self.options = options
+
+    def _camera(self, scene: Scene, camera: Camera | None) -> Camera:
+        return camera if camera is not None else scene.cameras[0]
+
+    def renderC(self, scene: Scene, options: RenderOptions, samples: torch.Tensor | None = None,
+                camera: Camera | None = None, out: torch.Tensor | None = None) -> torch.Tensor:
+        """Forward render; returns an (H, W, 3) float32 CUDA image."""
+        scene._ensure()
+        cam = self._camera(scene, camera)
+        img = out if out is not None else torch.empty(cam.height, cam.width, 3, device=scene.device)
+        smp = _samples_struct(samples)
+        o = options._c()
+        check(scene._lib.trn_render_fwd(scene.handle, C.byref(cam.c), C.byref(o), self.integrator_id, C.byref(smp),
+                                        C.c_void_p(img.data_ptr()), C.c_void_p(_stream())), "trn_render_fwd")
+        return img
+
+    def renderD(self, scene: Scene, options: RenderOptions, dLdI: torch.Tensor,
+                samples: torch.Tensor | None = None, camera: Camera | None = None) -> torch.Tensor:
+        """Replay the integrator's paths and accumulate parameter gradients for
+        dL/dI (H, W, 3); returns the (zero) derivative image like RenderD
+        without export_deriv."""
+        scene._ensure()
+        cam = self._camera(scene, camera)
+        g = dLdI.detach().to(scene.device, torch.float32).contiguous()
+        if g.numel() != cam.width * cam.height * 3:
+            raise RuntimeError("dLdI must have H*W*3 elements")
+        smp = _samples_struct(samples)
+        o = options._c()
+        check(scene._lib.trn_render_grad(scene.handle, C.byref(cam.c), C.byref(o), self.integrator_id, C.byref(smp),
+                                         C.c_void_p(g.data_ptr()), C.c_void_p(_stream())), "trn_render_grad")
+        return torch.zeros(cam.height, cam.width, 3, device=scene.device)
+
+
+class PathTracer(Integrator):
+    integrator_id = TRN_PATH_TRACER
+
+
+class PrimaryEdgeIntegrator(Integrator):
+    integrator_id = TRN_PRIMARY_EDGE
+
+
+class DirectEdgeIntegrator(Integrator):
+    integrator_id = TRN_DIRECT_EDGE
+
+
+class IndirectEdgeIntegrator(Integrator):
+    integrator_id = TRN_INDIRECT_EDGE
+
+
+class PixelBoundaryIntegrator(Integrator):
+    integrator_id = TRN_PIXEL_EDGE
+
+
+def sample_dims(integrator_id: int, max_bounces: int) -> int:
+    """Uniform dimensions one sample slot consumes (see the sample layout in
+    the library: camera/edge draws first, then per-bounce light and BSDF draws)."""
+    D = max_bounces
+    return {TRN_PATH_TRACER: 2 + 5 * D, TRN_PRIMARY_EDGE: 2 + 5 * D, TRN_DIRECT_EDGE: 3 + 3 * D,
+            TRN_INDIRECT_EDGE: 3 + 8 * max(D - 1, 0), TRN_PIXEL_EDGE: 1 + 5 * D}[integrator_id]
+
+
+def sample_slots(integrator_id: int, width: int, height: int, spp: int) -> int:
+    n = width * height * spp
+    return n // 4 if integrator_id == TRN_PIXEL_EDGE else n

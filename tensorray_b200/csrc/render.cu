@@ -1,0 +1,1071 @@
+// Integrator kernels: the interior path tracer (forward and replaying
+// adjoint) and the primary / direct / indirect / pixel boundary terms.
+//
+// One thread owns one sample slot (one path) end to end. Where the reference
+// builds a tensor expression per stage and compacts surviving rays between
+// stages (Integrator.cpp:178-303, Ray.cpp:65-116), a path here keeps its
+// state in registers and simply stops; the per-slot sample layout replaces
+// the reference's per-call RandomFloat tensors (see SampleSource).
+#include <cstring>
+#include <string>
+#include "../../include/trn.h"
+#include "scene_impl.cuh"
+#include "shading.cuh"
+
+namespace trn {
+
+struct Params {
+  DeviceScene s;
+  CameraDesc cam;
+  SampleSource smp;
+  long long n;        // sample slots of this call
+  int D;              // max bounces
+  float inv_spp;
+  float* image;       // forward radiance accumulation [W*H*3]
+  const float* dLdI;  // [W*H*3]
+  float* g_pos;       // [V*3]
+  float* g_vn;        // [V*3]
+  float* g_tex;       // [texels*3]
+  int diff_tex;       // accumulate texture gradients
+  // edge sampling tables (primary: per camera; secondary: per scene)
+  const int* edges;
+  const float* ecdf;
+  const float* efunc;
+  int ne;
+  float eintegral;
+  int* err;
+};
+
+constexpr int kMaxDepth = 16;
+
+TRN_D F3 F3z() { return F3(0.f, 0.f, 0.f); }
+TRN_D F3 scrub(const F3& a) { return finite3(a) ? a : F3z(); }
+TRN_D void atomic_add3(float* a, const F3& g) {
+  if (g.x != 0.f) atomicAdd(a, g.x);
+  if (g.y != 0.f) atomicAdd(a + 1, g.y);
+  if (g.z != 0.f) atomicAdd(a + 2, g.z);
+}
+TRN_D F3 g_at(const Params& P, int pix) {
+  if (pix < 0) return F3z();
+  return F3(__ldg(P.dLdI + 3 * pix), __ldg(P.dLdI + 3 * pix + 1), __ldg(P.dLdI + 3 * pix + 2)) * P.inv_spp;
+}
+TRN_D F3 cam_pos(const CameraDesc& c) { return F3(c.pos[0], c.pos[1], c.pos[2]); }
+
+// AreaLight::Eval (Light.cpp:134-138): radiance when the emitter faces wi
+TRN_D F3 emitted(const DeviceScene& s, const SurfF& x, const F3& wi) {
+  if (x.emitter < 0) return F3z();
+  return dot(wi, x.ng) > 0.f ? light_radiance(s, x.emitter) : F3z();
+}
+
+// ---------------------------------------------------------------------------
+// templated path factors (differentiated by the adjoint)
+// ---------------------------------------------------------------------------
+// Next-event estimation factor of EvalRadianceDirect (Integrator.cpp:186-228),
+// excluding the incoming throughput and assuming the connection is valid.
+template <class S>
+TRN_HD V3<S> nee_factor(const BsdfDesc& b, const V3<S>& xprev, const V3<S>& x, const V3<S>& ns, const V3<S>& ng,
+                        const V3<S>& kd, const V3<S>& y, const V3<S>& nl, const S& Jl, const F3& Le, float lpdf,
+                        float mis) {
+  const V3<S> wo = -normalize(x - xprev);
+  const Frame<S> fr = make_frame(ns);
+  V3<S> wi = y - x;
+  const S d2 = dot(wi, wi);
+  const S d = sqrt_(d2);
+  wi = wi / d;
+  const S dotSh = dot(ns, wi);
+  const S G = abs_(dot(nl, -wi)) / d2;
+  const V3<S> bv = bsdf_eval(b, fr, ng, kd, wo, wi, false) * abs_(dotSh);
+  V3<S> out;
+  for (int c = 0; c < 3; c++) out[c] = bv[c] * Jl * G * Le[c] / lpdf * mis;
+  return out;
+}
+
+// BSDF-sampled continuation weight in area measure (Integrator.cpp:252-267).
+template <class S>
+TRN_HD V3<S> cont_factor(const BsdfDesc& b, const V3<S>& xprev, const V3<S>& x, const V3<S>& ns, const V3<S>& ng,
+                         const V3<S>& kd, const V3<S>& xn, const V3<S>& ngn, const S& Jn, float prev_pdf) {
+  const V3<S> wo = -normalize(x - xprev);
+  const Frame<S> fr = make_frame(ns);
+  V3<S> dir = xn - x;
+  const S dist2 = dot(dir, dir);
+  dir = dir / sqrt_(dist2);
+  const S G = abs_(dot(ngn, -dir)) / dist2;
+  const V3<S> bv = bsdf_eval(b, fr, ng, kd, wo, dir, false) * abs_(dot(ns, dir));
+  V3<S> out;
+  for (int c = 0; c < 3; c++) out[c] = bv[c] * G * Jn / prev_pdf;
+  return out;
+}
+
+// xDotN of the boundary terms: RayIntersectAD (Utils.cpp:288-297) from `org`
+// towards `target` against triangle (P0, P1, P2), then n . (w P0 + u P1 + v P2)
+// with detached vertices (BoundaryPrimary.cpp:131-145, Edge.cpp:280-291).
+template <class S>
+TRN_HD S xdotn(const V3<S>& org, const V3<S>& target, const V3<S>& P0, const V3<S>& P1, const V3<S>& P2,
+               const F3& n) {
+  const V3<S> dir = normalize(target - org);
+  const V3<S> e1 = P1 - P0, e2 = P2 - P0;
+  const V3<S> h = cross(dir, e2);
+  const S f = 1.f / dot(e1, h);
+  const V3<S> sv = org - P0;
+  const S u = f * dot(sv, h);
+  const V3<S> q = cross(sv, e1);
+  const S v = f * dot(dir, q);
+  const S w = 1.f - u - v;
+  const V3<S> u2 = vdetach(P0) * w + vdetach(P1) * u + vdetach(P2) * v;
+  return dot(lift<S>(n), u2);
+}
+
+using D3 = Dual<3>;
+TRN_D F3 contract(const V3<D3>& r, const F3& adj) {
+  F3 g;
+  for (int i = 0; i < 3; i++) g[i] = adj.x * r.x.d[i] + adj.y * r.y.d[i] + adj.z * r.z.d[i];
+  return g;
+}
+
+// ---------------------------------------------------------------------------
+// vertex records -> triangle vertices (the reparameterised PostIntersect)
+// ---------------------------------------------------------------------------
+struct VAdj { F3 p, ns, ng; float J; };
+TRN_D void vadj_zero(VAdj& a) { a.p = F3z(); a.ns = F3z(); a.ng = F3z(); a.J = 0.f; }
+
+// position = w P0 + u P1 + v P2 (detached u, v), face normal c/|c| and
+// J = A / Detach(A) with c = cross(P1 - P0, P2 - P0), shading normal
+// w n0 + u n1 + v n2 (Scene.cpp:668-730, Primitive.cpp:299-340).
+TRN_D void scatter_vertex(const Params& P, int tri, float u, float v, const VAdj& a) {
+  const DeviceScene& s = P.s;
+  int i0, i1, i2; tri_vertices(s, tri, i0, i1, i2);
+  const float w = 1.f - u - v;
+  F3 g0 = a.p * w, g1 = a.p * u, g2 = a.p * v;
+  F3 gng = a.ng;
+  if (s.smooth[tri]) {
+    if (a.ns.x != 0.f || a.ns.y != 0.f || a.ns.z != 0.f) {
+      atomic_add3(P.g_vn + 3 * i0, a.ns * w);
+      atomic_add3(P.g_vn + 3 * i1, a.ns * u);
+      atomic_add3(P.g_vn + 3 * i2, a.ns * v);
+    }
+  } else {
+    gng = gng + a.ns;
+  }
+  if (gng.x != 0.f || gng.y != 0.f || gng.z != 0.f || a.J != 0.f) {
+    const F3 p0 = load3(s.pos, i0), p1 = load3(s.pos, i1), p2 = load3(s.pos, i2);
+    const F3 e1 = p1 - p0, e2 = p2 - p0;
+    const F3 c = cross(e1, e2);
+    const float len = length(c);
+    const F3 n = c / len;
+    const float A = 0.5f * len;
+    // d|c| from J: dJ/dA = 1/A, dA/d|c| = 1/2
+    const float glen = a.J * (0.5f / A);
+    const F3 gc = (gng - n * dot(n, gng)) / len + n * glen;
+    const F3 ge1 = cross(e2, gc), ge2 = cross(gc, e1);
+    g1 = g1 + ge1; g2 = g2 + ge2; g0 = g0 - (ge1 + ge2);
+  }
+  atomic_add3(P.g_pos + 3 * i0, g0);
+  atomic_add3(P.g_pos + 3 * i1, g1);
+  atomic_add3(P.g_pos + 3 * i2, g2);
+}
+
+TRN_D void scatter_point(const Params& P, int tri, float u, float v, const F3& gp) {
+  if (gp.x == 0.f && gp.y == 0.f && gp.z == 0.f) return;
+  int i0, i1, i2; tri_vertices(P.s, tri, i0, i1, i2);
+  const float w = 1.f - u - v;
+  atomic_add3(P.g_pos + 3 * i0, gp * w);
+  atomic_add3(P.g_pos + 3 * i1, gp * u);
+  atomic_add3(P.g_pos + 3 * i2, gp * v);
+}
+
+// ---------------------------------------------------------------------------
+// one EvalRadianceDirect step for one ray (Integrator.cpp:178-303)
+// ---------------------------------------------------------------------------
+struct BounceRec {
+  // NEE
+  int ltri; float lu, lv, lpdf, lmis; int nee_ok; F3 lLe;
+  // continuation
+  float prev_pdf; float emis; F3 eLe;  // MIS weight and radiance at the next vertex
+  int next_ok;
+  int scrubbed;                        // contribution was non-finite
+};
+
+// Returns the contribution of this bounce (already NaN-scrubbed). On return
+// x/rdir/T hold the next vertex; the return flag says whether it exists.
+TRN_D bool radiance_step(const DeviceScene& s, SurfF& x, F3& rdir, F3& T, float l0, float l1, float b0, float b1,
+                         float b2, F3& contrib, BounceRec* rec) {
+  const BsdfDesc b = s.bsdfs[x.bsdf];
+  long long texel;
+  const F3 kd = bsdf_albedo(s, b, x.tu, x.tv, texel);
+  const Frame<float> fr = make_frame(x.ns);
+  const F3 wo = -rdir;
+  F3 val = F3z();
+  if (rec) { rec->nee_ok = 0; rec->next_ok = 0; rec->scrubbed = 0; }
+  LightSample ls;
+  if (light_sample(s, l0, l1, ls)) {
+    int j0, j1, j2; tri_vertices(s, ls.tri, j0, j1, j2);
+    const F3 y = bary3(ls.bu, ls.bv, load3(s.pos, j0), load3(s.pos, j1), load3(s.pos, j2));
+    const F3 nl = load3(s.fnormal, ls.tri);
+    F3 wi = y - x.p;
+    const float d2 = dot(wi, wi);
+    const float d = sqrtf(d2);
+    wi = wi / d;
+    const float dotSh = dot(x.ns, wi), dotGeo = dot(x.ng, wi);
+    const bool stable = d > kShadowEps && fabsf(dotSh) > kEdgeEps;
+    const bool noleak = dotSh * dotGeo > 0.f;
+    if (stable && noleak && !occluded(s, x.p, wi, kShadowEps, d - kShadowEps)) {
+      const F3 Le = dot(-wi, nl) > 0.f ? light_radiance(s, ls.light) : F3z();
+      const float G = fabsf(dot(nl, -wi)) / d2;
+      const float bpdf = bsdf_pdf_local(b, fr.to_local(wo), fr.to_local(wi)) * G;
+      const float mis = ls.pdf * ls.pdf / (ls.pdf * ls.pdf + bpdf * bpdf);
+      const F3 bv = bsdf_eval(b, fr, x.ng, kd, wo, wi, false) * fabsf(dotSh);
+      F3 v;
+      for (int c = 0; c < 3; c++) v[c] = T[c] * (bv[c] * 1.f * G * Le[c] / ls.pdf * mis);
+      val = val + v;
+      if (rec) {
+        rec->nee_ok = 1; rec->ltri = ls.tri; rec->lu = ls.bu; rec->lv = ls.bv; rec->lpdf = ls.pdf;
+        rec->lmis = mis; rec->lLe = Le;
+      }
+    }
+  }
+  // continuation (BSDF sampling)
+  F3 wi; float pdf;
+  bsdf_sample_only(b, fr, wo, b0, b1, b2, wi, pdf);
+  Hit h;
+  bool ok = pdf > 0.f && out_dir_valid(b, x.ns, x.ng, wi);
+  if (ok) ok = trace<false>(s, x.p, wi, kShadowEps, kRayMax, h);
+  if (!ok) {
+    contrib = scrub(val);
+    if (rec) rec->scrubbed = !finite3(val);
+    return false;
+  }
+  const SurfF xn = post_intersect(s, h.tri, h.u, h.v);
+  F3 dir = xn.p - x.p;
+  const float dist2 = dot(dir, dir);
+  dir = dir / sqrtf(dist2);
+  const float G = fabsf(dot(xn.ng, -dir)) / dist2;
+  const F3 bv = bsdf_eval(b, fr, x.ng, kd, wo, dir, false) * fabsf(dot(x.ns, dir));
+  const float prev_pdf = pdf * G;
+  F3 Tn;
+  for (int c = 0; c < 3; c++) Tn[c] = T[c] * bv[c] * G * 1.f / prev_pdf;
+  if (!(G > 0.f)) Tn = F3z();
+  float emis = 0.f;
+  F3 eLe = F3z();
+  if (xn.emitter >= 0) {
+    eLe = emitted(s, xn, -dir);
+    const float pn = light_pdf(s, xn.tri);
+    emis = prev_pdf * prev_pdf / (prev_pdf * prev_pdf + pn * pn);
+    val = val + Tn * eLe * emis;
+  }
+  contrib = scrub(val);
+  if (rec) {
+    rec->scrubbed = !finite3(val);
+    rec->prev_pdf = prev_pdf; rec->emis = emis; rec->eLe = eLe; rec->next_ok = 1;
+  }
+  x = xn; rdir = dir; T = Tn;
+  return true;
+}
+
+// ---------------------------------------------------------------------------
+// interior term: forward
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_path_fwd(Params P) {
+  const int W = P.cam.w, WH = P.cam.w * P.cam.h;
+  const F3 org = cam_pos(P.cam);
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < P.n;
+       p += (long long)gridDim.x * blockDim.x) {
+    const int pix = (int)(p % WH);
+    const F3 dir = camera_ray_dir(P.cam, pix % W, pix / W, P.smp.get(0, p), P.smp.get(1, p));
+    Hit h;
+    if (!trace<false>(P.s, org, dir, kShadowEps, kRayMax, h, P.err)) continue;
+    SurfF x = post_intersect(P.s, h.tri, h.u, h.v);
+    const float t1 = camera_factor<float>(P.cam, x.p, x.ng, 1.f);
+    F3 T(t1, t1, t1);
+    F3 rdir = normalize(x.p - org);
+    F3 L = scrub(T * emitted(P.s, x, -rdir));
+    for (int b = 0; b < P.D; b++) {
+      const int o = 2 + 5 * b;
+      F3 c;
+      const bool more = radiance_step(P.s, x, rdir, T, P.smp.get(o, p), P.smp.get(o + 1, p), P.smp.get(o + 2, p),
+                                      P.smp.get(o + 3, p), P.smp.get(o + 4, p), c, nullptr);
+      L = L + c;
+      if (!more || (T.x == 0.f && T.y == 0.f && T.z == 0.f)) break;
+    }
+    L = L * P.inv_spp;
+    atomic_add3(P.image + 3 * pix, L);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// interior term: replaying adjoint
+// ---------------------------------------------------------------------------
+// Gradient of NEE factor w.r.t. (xprev, x, ns, kd, y, nl, Jl).
+TRN_D void nee_vjp(const BsdfDesc& b, bool need_prev, bool need_kd, const F3& xprev, const F3& x, const F3& ns,
+                   const F3& ng, const F3& kd, const F3& y, const F3& nl, const F3& Le, float lpdf, float mis,
+                   const F3& adj, F3& g_prev, F3& g_x, F3& g_ns, F3& g_kd, F3& g_y, F3& g_nl, float& g_Jl) {
+  for (int grp = 0; grp < 7; grp++) {
+    if (grp == 0 && !need_prev) continue;
+    if (grp == 3 && !need_kd) continue;
+    const V3<D3> a_prev = seed3<3>(xprev, grp == 0 ? 0 : -1);
+    const V3<D3> a_x = seed3<3>(x, grp == 1 ? 0 : -1);
+    const V3<D3> a_ns = seed3<3>(ns, grp == 2 ? 0 : -1);
+    const V3<D3> a_kd = seed3<3>(kd, grp == 3 ? 0 : -1);
+    const V3<D3> a_y = seed3<3>(y, grp == 4 ? 0 : -1);
+    const V3<D3> a_nl = seed3<3>(nl, grp == 5 ? 0 : -1);
+    const D3 a_J = seed1<3>(1.f, grp == 6 ? 0 : -1);
+    const V3<D3> r = nee_factor<D3>(b, a_prev, a_x, a_ns, lift<D3>(ng), a_kd, a_y, a_nl, a_J, Le, lpdf, mis);
+    const F3 g = contract(r, adj);
+    switch (grp) {
+      case 0: g_prev = g_prev + g; break;
+      case 1: g_x = g_x + g; break;
+      case 2: g_ns = g_ns + g; break;
+      case 3: g_kd = g_kd + g; break;
+      case 4: g_y = g_y + g; break;
+      case 5: g_nl = g_nl + g; break;
+      default: g_Jl += g.x; break;
+    }
+  }
+}
+
+// Gradient of the continuation factor w.r.t. (xprev, x, ns, kd, xn, ngn, Jn).
+TRN_D void cont_vjp(const BsdfDesc& b, bool need_prev, bool need_kd, const F3& xprev, const F3& x, const F3& ns,
+                    const F3& ng, const F3& kd, const F3& xn, const F3& ngn, float prev_pdf, const F3& adj,
+                    F3& g_prev, F3& g_x, F3& g_ns, F3& g_kd, F3& g_xn, F3& g_ngn, float& g_Jn) {
+  for (int grp = 0; grp < 7; grp++) {
+    if (grp == 0 && !need_prev) continue;
+    if (grp == 3 && !need_kd) continue;
+    const V3<D3> a_prev = seed3<3>(xprev, grp == 0 ? 0 : -1);
+    const V3<D3> a_x = seed3<3>(x, grp == 1 ? 0 : -1);
+    const V3<D3> a_ns = seed3<3>(ns, grp == 2 ? 0 : -1);
+    const V3<D3> a_kd = seed3<3>(kd, grp == 3 ? 0 : -1);
+    const V3<D3> a_xn = seed3<3>(xn, grp == 4 ? 0 : -1);
+    const V3<D3> a_ngn = seed3<3>(ngn, grp == 5 ? 0 : -1);
+    const D3 a_J = seed1<3>(1.f, grp == 6 ? 0 : -1);
+    const V3<D3> r = cont_factor<D3>(b, a_prev, a_x, a_ns, lift<D3>(ng), a_kd, a_xn, a_ngn, a_J, prev_pdf);
+    const F3 g = contract(r, adj);
+    switch (grp) {
+      case 0: g_prev = g_prev + g; break;
+      case 1: g_x = g_x + g; break;
+      case 2: g_ns = g_ns + g; break;
+      case 3: g_kd = g_kd + g; break;
+      case 4: g_xn = g_xn + g; break;
+      case 5: g_ngn = g_ngn + g; break;
+      default: g_Jn += g.x; break;
+    }
+  }
+}
+
+struct VRec { int tri; float u, v; };
+
+__global__ void __launch_bounds__(128) k_path_adj(Params P) {
+  const int W = P.cam.w, WH = P.cam.w * P.cam.h;
+  const F3 org = cam_pos(P.cam);
+  const DeviceScene& s = P.s;
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < P.n;
+       p += (long long)gridDim.x * blockDim.x) {
+    const int pix = (int)(p % WH);
+    const F3 g = g_at(P, pix);
+    if (g.x == 0.f && g.y == 0.f && g.z == 0.f) continue;
+    const F3 dir = camera_ray_dir(P.cam, pix % W, pix / W, P.smp.get(0, p), P.smp.get(1, p));
+    Hit h;
+    if (!trace<false>(s, org, dir, kShadowEps, kRayMax, h, P.err)) continue;
+    // ---- forward replay, recording vertices and factor values ----
+    VRec vr[kMaxDepth + 2];
+    BounceRec br[kMaxDepth + 1];
+    bool nee_on[kMaxDepth + 2];
+    F3 Tk[kMaxDepth + 2], Nk[kMaxDepth + 2], Mk[kMaxDepth + 2], Phik[kMaxDepth + 2];
+    SurfF x = post_intersect(s, h.tri, h.u, h.v);
+    vr[1] = {h.tri, h.u, h.v};
+    const float t1 = camera_factor<float>(P.cam, x.p, x.ng, 1.f);
+    F3 T(t1, t1, t1);
+    F3 rdir = normalize(x.p - org);
+    Tk[1] = T;
+    Mk[1] = emitted(s, x, -rdir);
+    if (!finite3(T * Mk[1])) Mk[1] = F3z();
+    int K = 1;  // vertices reached
+    const int D = min(P.D, kMaxDepth);
+    for (int k = 0; k <= D + 1; k++) { nee_on[k] = false; Nk[k] = F3z(); Phik[k] = F3z(); }
+    for (int b = 0; b < D; b++) {
+      const int k = b + 1;
+      const int o = 2 + 5 * b;
+      F3 c;
+      BounceRec& R = br[k];
+      const bool more = radiance_step(s, x, rdir, T, P.smp.get(o, p), P.smp.get(o + 1, p), P.smp.get(o + 2, p),
+                                      P.smp.get(o + 3, p), P.smp.get(o + 4, p), c, &R);
+      // a scrubbed (non-finite) bounce contributes nothing and carries no gradient
+      nee_on[k] = R.nee_ok && !R.scrubbed;
+      if (!more) break;
+      vr[k + 1] = {x.tri, x.u, x.v};
+      Tk[k + 1] = T;
+      Mk[k + 1] = (R.scrubbed || R.emis == 0.f) ? F3z() : R.eLe * R.emis;
+      K = k + 1;
+      if (T.x == 0.f && T.y == 0.f && T.z == 0.f) break;
+    }
+    // ---- recompute factor values in vertex order (NEE value and phi) ----
+    // positions / normals per vertex
+    F3 xp[kMaxDepth + 2], nsv[kMaxDepth + 2], ngv[kMaxDepth + 2], kdv[kMaxDepth + 2];
+    long long texel[kMaxDepth + 2];
+    int bsdfv[kMaxDepth + 2];
+    xp[0] = org;
+    for (int k = 1; k <= K; k++) {
+      const SurfF xs = post_intersect(s, vr[k].tri, vr[k].u, vr[k].v);
+      xp[k] = xs.p; nsv[k] = xs.ns; ngv[k] = xs.ng; bsdfv[k] = xs.bsdf;
+      kdv[k] = bsdf_albedo(s, s.bsdfs[xs.bsdf], xs.tu, xs.tv, texel[k]);
+    }
+    F3 yv[kMaxDepth + 1], nlv[kMaxDepth + 1];
+    for (int k = 1; k <= K && k <= D; k++) {
+      if (!nee_on[k]) continue;
+      const BounceRec& R = br[k];
+      int j0, j1, j2; tri_vertices(s, R.ltri, j0, j1, j2);
+      yv[k] = bary3(R.lu, R.lv, load3(s.pos, j0), load3(s.pos, j1), load3(s.pos, j2));
+      nlv[k] = load3(s.fnormal, R.ltri);
+      Nk[k] = nee_factor<float>(s.bsdfs[bsdfv[k]], xp[k - 1], xp[k], nsv[k], ngv[k], kdv[k], yv[k], nlv[k], 1.f,
+                                R.lLe, R.lpdf, R.lmis);
+    }
+    for (int k = 1; k < K; k++) {
+      Phik[k] = cont_factor<float>(s.bsdfs[bsdfv[k]], xp[k - 1], xp[k], nsv[k], ngv[k], kdv[k], xp[k + 1],
+                                   ngv[k + 1], 1.f, br[k].prev_pdf);
+      // a non-finite weight is what made the forward throughput non-finite:
+      // the scrubbed contributions carry no gradient
+      if (!finite3(Phik[k])) Phik[k] = F3z();
+    }
+    // ---- reverse accumulation of the throughput adjoint ----
+    F3 a[kMaxDepth + 3];
+    a[K + 1] = F3z();
+    for (int k = K; k >= 1; k--) {
+      F3 ak = g * (Nk[k] + Mk[k]);
+      if (k < K) ak = ak + Phik[k] * a[k + 1];
+      a[k] = ak;
+    }
+    // ---- local vector-Jacobian products ----
+    VAdj va[kMaxDepth + 2];
+    for (int k = 1; k <= K; k++) vadj_zero(va[k]);
+    // primary factor T1 = G / Detach(G) * J
+    {
+      const float gam = a[1].x + a[1].y + a[1].z;
+      if (gam != 0.f && isfinite(gam)) {
+        for (int grp = 0; grp < 3; grp++) {
+          const V3<D3> dx = seed3<3>(xp[1], grp == 0 ? 0 : -1);
+          const V3<D3> dn = seed3<3>(ngv[1], grp == 1 ? 0 : -1);
+          const D3 dJ = seed1<3>(1.f, grp == 2 ? 0 : -1);
+          const D3 r = camera_factor<D3>(P.cam, dx, dn, dJ);
+          const F3 gg = F3(r.d[0], r.d[1], r.d[2]) * gam;
+          if (grp == 0) va[1].p = va[1].p + gg;
+          else if (grp == 1) va[1].ng = va[1].ng + gg;
+          else va[1].J += gg.x;
+        }
+      }
+    }
+    for (int k = 1; k <= K; k++) {
+      const BsdfDesc b = s.bsdfs[bsdfv[k]];
+      const bool need_prev = b.type != kDiffuse;
+      const bool need_kd = P.diff_tex && texel[k] >= 0;
+      F3 gkd = F3z();
+      F3 gprev = F3z();
+      if (k <= D && nee_on[k]) {
+        const F3 adj = Tk[k] * g;
+        F3 gy = F3z(), gnl = F3z();
+        float gJl = 0.f;
+        nee_vjp(b, need_prev, need_kd, xp[k - 1], xp[k], nsv[k], ngv[k], kdv[k], yv[k], nlv[k], br[k].lLe, br[k].lpdf,
+                br[k].lmis, adj, gprev, va[k].p, va[k].ns, gkd, gy, gnl, gJl);
+        VAdj la; la.p = gy; la.ns = F3z(); la.ng = gnl; la.J = gJl;
+        scatter_vertex(P, br[k].ltri, br[k].lu, br[k].lv, la);
+      }
+      if (k < K && (Phik[k].x != 0.f || Phik[k].y != 0.f || Phik[k].z != 0.f)) {
+        const F3 adj = Tk[k] * a[k + 1];
+        float gJn = 0.f;
+        cont_vjp(b, need_prev, need_kd, xp[k - 1], xp[k], nsv[k], ngv[k], kdv[k], xp[k + 1], ngv[k + 1],
+                 br[k].prev_pdf, adj, gprev, va[k].p, va[k].ns, gkd, va[k + 1].p, va[k + 1].ng, gJn);
+        va[k + 1].J += gJn;
+      }
+      if (k >= 2) va[k - 1].p = va[k - 1].p + gprev;
+      if (need_kd) atomic_add3(P.g_tex + 3 * texel[k], gkd);
+    }
+    for (int k = 1; k <= K; k++) scatter_vertex(P, vr[k].tri, vr[k].u, vr[k].v, va[k]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// EvalImportance for one ray (Integrator.cpp:75-176)
+// ---------------------------------------------------------------------------
+TRN_D bool importance_step(const DeviceScene& s, const CameraDesc& cam, SurfF& x, F3& rdir, F3& T, float b0,
+                           float b1, float b2, F3& contrib, int& pix) {
+  contrib = F3z();
+  pix = -1;
+  const BsdfDesc b = s.bsdfs[x.bsdf];
+  long long texel;
+  const F3 kd = bsdf_albedo(s, b, x.tu, x.tv, texel);
+  const Frame<float> fr = make_frame(x.ns);
+  const F3 wo = -rdir;
+  const F3 cpos = cam_pos(cam);
+  const SensorSample sds = sample_direct(cam, x.p);
+  if (sds.valid) {
+    const F3 dirc = sensor_ray_dir(cam, sds.qx, sds.qy);
+    const float dist2cam = length(x.p - cpos);
+    if (!occluded(s, cpos, dirc, kShadowEps, dist2cam - kShadowEps)) {
+      F3 val = F3z();
+      if (out_dir_valid(b, x.ns, x.ng, wo)) {
+        const F3 wi = normalize(cpos - x.p);
+        if (out_dir_valid(b, x.ns, x.ng, wi))
+          val = bsdf_eval(b, fr, x.ng, kd, wo, wi, true) * fabsf(dot(x.ns, wi));
+      }
+      contrib = scrub(T * sds.sensor_val * val);
+      pix = image_pixel(cam, sds.qx, sds.qy);
+    }
+  }
+  if (!out_dir_valid(b, x.ns, x.ng, wo)) return false;
+  F3 wi; float pdf;
+  bsdf_sample_only(b, fr, wo, b0, b1, b2, wi, pdf);
+  const F3 bv = bsdf_eval(b, fr, x.ng, kd, wo, wi, true) * fabsf(dot(x.ns, wi));
+  const F3 Tn = T * bv / pdf;
+  if (!(pdf > 0.f) || !out_dir_valid(b, x.ns, x.ng, wi)) return false;
+  Hit h;
+  if (!trace<false>(s, x.p, wi, kShadowEps, kRayMax, h)) return false;
+  x = post_intersect(s, h.tri, h.u, h.v);
+  rdir = wi;
+  T = Tn;
+  return true;
+}
+
+// scatter W * d xDotN / d(edge vertices, receiver point, far triangle)
+TRN_D void xdotn_vjp(const Params& P, float W, const F3& org, bool org_attached, int recv_tri, float ru, float rv,
+                     int va_, int vb_, float sedge, const F3& target_const, int far_tri, const F3& n) {
+  const DeviceScene& s = P.s;
+  int i0, i1, i2; tri_vertices(s, far_tri, i0, i1, i2);
+  const F3 P0 = load3(s.pos, i0), P1 = load3(s.pos, i1), P2 = load3(s.pos, i2);
+  const bool edge_attached = va_ >= 0;
+  const F3 Pa = edge_attached ? load3(s.pos, va_) : F3z();
+  const F3 Pb = edge_attached ? load3(s.pos, vb_) : F3z();
+  F3 gPa = F3z(), gPb = F3z(), gorg = F3z(), g0 = F3z(), g1 = F3z(), g2 = F3z();
+  for (int grp = 0; grp < 6; grp++) {
+    if ((grp == 0 || grp == 1) && !edge_attached) continue;
+    if (grp == 2 && !org_attached) continue;
+    const V3<D3> a = seed3<3>(Pa, grp == 0 ? 0 : -1), bb = seed3<3>(Pb, grp == 1 ? 0 : -1);
+    const V3<D3> o = seed3<3>(org, grp == 2 ? 0 : -1);
+    const V3<D3> q0 = seed3<3>(P0, grp == 3 ? 0 : -1), q1 = seed3<3>(P1, grp == 4 ? 0 : -1),
+                 q2 = seed3<3>(P2, grp == 5 ? 0 : -1);
+    V3<D3> target;
+    if (edge_attached) target = a + (bb - a) * D3(sedge);
+    else target = lift<D3>(target_const);
+    const D3 r = xdotn<D3>(o, target, q0, q1, q2, n);
+    const F3 gg = F3(r.d[0], r.d[1], r.d[2]) * W;
+    switch (grp) {
+      case 0: gPa = gg; break;
+      case 1: gPb = gg; break;
+      case 2: gorg = gg; break;
+      case 3: g0 = gg; break;
+      case 4: g1 = gg; break;
+      default: g2 = gg; break;
+    }
+  }
+  atomic_add3(P.g_pos + 3 * i0, g0);
+  atomic_add3(P.g_pos + 3 * i1, g1);
+  atomic_add3(P.g_pos + 3 * i2, g2);
+  if (edge_attached) {
+    atomic_add3(P.g_pos + 3 * va_, gPa);
+    atomic_add3(P.g_pos + 3 * vb_, gPb);
+  }
+  if (org_attached) scatter_point(P, recv_tri, ru, rv, gorg);
+}
+
+// boundary geometry term baseVal (BoundaryPrimary.cpp:115-129, Edge.cpp:258-271)
+TRN_D float base_val(float ratio, const F3& edge, const F3& d, const F3& nrm, const F3& edge2, F3& n_out) {
+  const F3 e = cross(edge, d);
+  const float sinphi = length(e);
+  const F3 proj = normalize(cross(e, nrm));
+  const float sinphi2 = length(cross(d, proj));
+  n_out = normalize(cross(nrm, proj));
+  const bool sign0 = dot(e, edge2) > 0.f;
+  const bool sign1 = dot(e, n_out) > 0.f;
+  float bv = ratio * (sinphi / sinphi2);
+  bv = bv * (sinphi > kEps ? 1.f : 0.f) * (sinphi2 > kEps ? 1.f : 0.f);
+  return bv * (sign0 == sign1 ? 1.f : -1.f);
+}
+
+// ---------------------------------------------------------------------------
+// primary boundary (BoundaryPrimary.cpp:36-181, SampleFromPrimEdges Edge.cpp:350-367)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_primary_adj(Params P) {
+  const DeviceScene& s = P.s;
+  const F3 cpos = cam_pos(P.cam);
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < P.n;
+       p += (long long)gridDim.x * blockDim.x) {
+    const float r0 = P.smp.get(0, p), r1 = P.smp.get(1, p);
+    float reuse;
+    const int e = sample_discrete(P.ecdf, P.ne, r0, reuse);
+    const int v0 = P.edges[5 * e], v1 = P.edges[5 * e + 1], v2 = P.edges[5 * e + 4];
+    const float len_e = P.efunc[e];
+    if (!(len_e > 0.f)) continue;
+    const float pmf = len_e / (P.eintegral * (float)P.ne);
+    const float pdf = pmf / len_e;
+    const F3 Pa = load3(s.pos, v0), Pb = load3(s.pos, v1), Pc = load3(s.pos, v2);
+    const F3 e1 = Pb - Pa;
+    const F3 p0 = Pa + e1 * r1;
+    const F3 edge = normalize(e1), edge2 = normalize(Pc - Pa);
+    const F3 dir = normalize(p0 - cpos);
+    Hit h;
+    if (!trace<false>(s, p0, dir, kShadowEps, kRayMax, h, P.err)) continue;
+    const F3 hitP = p0 + dir * h.t;
+    const SensorSample sds = sample_direct(P.cam, hitP);
+    if (!sds.valid) continue;
+    const F3 dirc = sensor_ray_dir(P.cam, sds.qx, sds.qy);
+    const float dist2cam = length(p0 - cpos);
+    if (occluded(s, cpos, dirc, kShadowEps, dist2cam - kShadowEps)) continue;
+    SurfF x = post_intersect(s, h.tri, h.u, h.v);
+    const float dist = length(x.p - cpos);
+    const float dist1 = length(p0 - cpos);
+    const float cos2 = fabsf(dot(x.ng, -dirc));
+    F3 n;
+    const float bval = base_val((dist / dist1), edge, dirc, x.ng, edge2, n) * cos2;
+    const int pix = image_pixel(P.cam, sds.qx, sds.qy);
+    const F3 g = g_at(P, pix);
+    if (bval == 0.f || (g.x == 0.f && g.y == 0.f && g.z == 0.f)) continue;
+    // detached radiance along the camera ray through the sensor point
+    F3 T(sds.sensor_val, sds.sensor_val, sds.sensor_val);
+    F3 rdir = dirc;
+    F3 L = scrub(T * emitted(s, x, -rdir));
+    for (int b = 0; b < P.D; b++) {
+      const int o = 2 + 5 * b;
+      F3 c;
+      const bool more = radiance_step(s, x, rdir, T, P.smp.get(o, p), P.smp.get(o + 1, p), P.smp.get(o + 2, p),
+                                      P.smp.get(o + 3, p), P.smp.get(o + 4, p), c, nullptr);
+      L = L + c;
+      if (!more || (T.x == 0.f && T.y == 0.f && T.z == 0.f)) break;
+    }
+    const F3 wv = L * (bval / pdf);
+    const float W = dot(g, wv);
+    if (W == 0.f || !isfinite(W)) continue;
+    xdotn_vjp(P, W, cpos, false, -1, 0.f, 0.f, v0, v1, r1, p0, h.tri, n);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// direct boundary (BoundaryDirect.cpp:38-143, Edge.cpp:90-144, 201-309)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_direct_adj(Params P) {
+  const DeviceScene& s = P.s;
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < P.n;
+       p += (long long)gridDim.x * blockDim.x) {
+    const float r0 = P.smp.get(0, p), r1 = P.smp.get(1, p), r2 = P.smp.get(2, p);
+    float reuse;
+    const int e = sample_discrete(P.ecdf, P.ne, r0, reuse);
+    const int v0 = P.edges[5 * e], v1 = P.edges[5 * e + 1], f0 = P.edges[5 * e + 2], f1 = P.edges[5 * e + 3],
+              v2 = P.edges[5 * e + 4];
+    const float len_e = P.efunc[e];
+    if (!(len_e > 0.f)) continue;
+    const float pdf_e = (len_e / (P.eintegral * (float)P.ne)) / len_e;
+    const F3 Pa = load3(s.pos, v0), Pb = load3(s.pos, v1), Pc = load3(s.pos, v2);
+    const F3 e1 = Pb - Pa;
+    const F3 p0 = Pa + e1 * reuse;
+    const F3 edge = normalize(e1), edge2 = normalize(Pc - Pa);
+    LightSample ls;
+    if (!light_sample(s, r1, r2, ls)) continue;
+    int j0, j1, j2; tri_vertices(s, ls.tri, j0, j1, j2);
+    const F3 p2 = bary3(ls.bu, ls.bv, load3(s.pos, j0), load3(s.pos, j1), load3(s.pos, j2));
+    const F3 nL = load3(s.fnormal, ls.tri);
+    const F3 ev = p2 - p0;
+    const float dist_sqr = dot(ev, ev);
+    const float dist = sqrtf(dist_sqr);
+    const F3 en = ev / dist;
+    const float cos_t = dot(nL, -en);
+    const F3 n0 = load3(s.fnormal, f0);
+    const F3 n1 = f1 >= 0 ? load3(s.fnormal, f1) : F3z();
+    const bool is_b = f1 < 0;
+    const float c0 = dot(en, n0), c1 = dot(en, n1);
+    const bool valid0 = fabsf(c0) > kEdgeEps;
+    const bool valid1 = (c0 > kEdgeEps && c1 < -kEdgeEps) || (c0 < -kEdgeEps && c1 > kEdgeEps);
+    const bool right = (is_b && valid0) || (!is_b && valid1);
+    if (!(right && cos_t > kEps && dist > kShadowEps)) continue;
+    const float pdf = pdf_e * ls.pdf * dist_sqr / cos_t;
+    const F3 rdir = normalize(p0 - p2);
+    Hit h0, h;
+    if (!trace<false>(s, p0, -rdir, kShadowEps, kRayMax, h0, P.err)) continue;
+    if (!trace<false>(s, p0, rdir, kShadowEps, kRayMax, h, P.err)) continue;
+    const F3 hp = p0 + (-rdir) * h0.t;
+    if (!(length(hp - p2) < kShadowEps)) continue;
+    const SurfF xl = post_intersect(s, h0.tri, h0.u, h0.v);
+    const F3 E = emitted(s, xl, rdir);
+    SurfF x = post_intersect(s, h.tri, h.u, h.v);
+    const float dl = length(p2 - x.p);
+    const float cos2 = fabsf(dot(nL, rdir));
+    const float its_t = length(x.p - p0);
+    F3 n;
+    const float bval = base_val(its_t / dl, edge, -rdir, nL, edge2, n) * cos2;
+    if (bval == 0.f || (E.x == 0.f && E.y == 0.f && E.z == 0.f)) continue;
+    const F3 ev0 = E * (bval / pdf);
+    // trace towards the sensor (EvalImportance per bounce)
+    F3 T(1.f, 1.f, 1.f);
+    F3 dirs = rdir;
+    float W = 0.f;
+    SurfF xs = x;
+    for (int b = 0; b < P.D; b++) {
+      const int o = 3 + 3 * b;
+      F3 c; int pix;
+      const bool more = importance_step(s, P.cam, xs, dirs, T, P.smp.get(o, p), P.smp.get(o + 1, p),
+                                        P.smp.get(o + 2, p), c, pix);
+      if (pix >= 0) W += dot(g_at(P, pix), ev0 * c);
+      if (!more) break;
+    }
+    if (W == 0.f || !isfinite(W)) continue;
+    xdotn_vjp(P, W, x.p, true, h.tri, h.u, h.v, v0, v1, reuse, p0, h0.tri, n);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// indirect boundary (BoundaryIndirect.cpp:38-192, Edge.cpp:146-199)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_indirect_adj(Params P) {
+  const DeviceScene& s = P.s;
+  const int D = min(P.D, kMaxDepth);
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < P.n;
+       p += (long long)gridDim.x * blockDim.x) {
+    if (D < 2) break;
+    const float r0 = P.smp.get(0, p), r1 = P.smp.get(1, p), r2 = P.smp.get(2, p);
+    float reuse;
+    const int e = sample_discrete(P.ecdf, P.ne, r0, reuse);
+    const int v0 = P.edges[5 * e], v1 = P.edges[5 * e + 1], f0 = P.edges[5 * e + 2], f1 = P.edges[5 * e + 3],
+              v2 = P.edges[5 * e + 4];
+    const float len_e = P.efunc[e];
+    if (!(len_e > 0.f)) continue;
+    const float pdf_e = (len_e / (P.eintegral * (float)P.ne)) / len_e;
+    const F3 Pa = load3(s.pos, v0), Pb = load3(s.pos, v1), Pc = load3(s.pos, v2);
+    const F3 e1 = Pb - Pa;
+    const F3 p0 = Pa + e1 * reuse;
+    const F3 edge = normalize(e1), edge2 = normalize(Pc - Pa);
+    const F3 n0 = load3(s.fnormal, f0);
+    F3 dir;
+    float pdf_d;
+    if (f1 < 0) {
+      const F3 nrm = cross(n0, edge);
+      F3 tg, bt; coordinate_system(nrm, tg, bt);
+      const float z = fminf(1.f - 2.f * r1, 1.f - kEdgeEps);
+      const float r = sqrtf(fmaxf(0.f, 1.f - z * z));
+      const float phi = 2.f * kPi * r2;
+      dir = tg * (r * cosf(phi)) + bt * (r * sinf(phi)) + nrm * z;
+      pdf_d = 0.25f / kPi;
+    } else {
+      const F3 n1 = load3(s.fnormal, f1);
+      const float phi0 = acosf(dot(n0, n1));
+      pdf_d = 0.25f / phi0;
+      const F3 zz = normalize(n0 + n1);
+      const F3 yy = normalize(cross(n0, zz));
+      const F3 xx = cross(yy, zz);
+      float phi = (r1 - 0.5f) * phi0;
+      phi = fminf(fmaxf(phi, -0.5f * phi0 + kEdgeEps), 0.5f * phi0 - kEdgeEps);
+      const F3 x1 = xx * cosf(phi) + zz * sinf(phi);
+      const bool m0 = r2 > 0.5f;
+      const float bq = 4.f * r2 - (m0 ? 3.f : 1.f);
+      const float aq = sqrtf(1.f - bq * bq) * (1.f - (m0 ? 1.f : 0.f) * 2.f);
+      dir = x1 * aq + yy * bq;
+    }
+    const float pdf = pdf_e * pdf_d;
+    Hit he, hs;
+    if (!trace<false>(s, p0, -dir, kShadowEps, kRayMax, he, P.err)) continue;
+    if (!trace<false>(s, p0, dir, kShadowEps, kRayMax, hs, P.err)) continue;
+    SurfF xe = post_intersect(s, he.tri, he.u, he.v);
+    SurfF xs = post_intersect(s, hs.tri, hs.u, hs.v);
+    const float dl = length(xe.p - xs.p);
+    const float cos2 = fabsf(dot(xe.ng, dir));
+    const float its_t = length(xs.p - p0);
+    F3 n;
+    const float bval = base_val(its_t / dl, edge, -dir, xe.ng, edge2, n) * cos2;
+    if (bval == 0.f) continue;
+    const float e0 = bval / pdf;
+    // emitter side: cumulative radiance per depth
+    F3 rad[kMaxDepth];
+    {
+      F3 T(1.f, 1.f, 1.f);
+      F3 rd = -dir;
+      SurfF xx = xe;
+      F3 cur = F3z();
+      bool alive = true;
+      for (int b = 0; b < D - 1; b++) {
+        if (alive) {
+          const int o = 3 + 5 * b;
+          F3 c;
+          alive = radiance_step(s, xx, rd, T, P.smp.get(o, p), P.smp.get(o + 1, p), P.smp.get(o + 2, p),
+                                P.smp.get(o + 3, p), P.smp.get(o + 4, p), c, nullptr);
+          cur = cur + c;
+          if (T.x == 0.f && T.y == 0.f && T.z == 0.f) alive = false;
+        }
+        rad[b] = cur;
+      }
+    }
+    // sensor side
+    float W = 0.f;
+    {
+      F3 T(1.f, 1.f, 1.f);
+      F3 rd = dir;
+      SurfF xx = xs;
+      for (int b = 0; b < D - 1; b++) {
+        const int o = 3 + 5 * (D - 1) + 3 * b;
+        F3 c; int pix;
+        const bool more = importance_step(s, P.cam, xx, rd, T, P.smp.get(o, p), P.smp.get(o + 1, p),
+                                          P.smp.get(o + 2, p), c, pix);
+        if (pix >= 0) W += dot(g_at(P, pix), rad[D - b - 2] * c) * e0;
+        if (!more) break;
+      }
+    }
+    if (W == 0.f || !isfinite(W)) continue;
+    xdotn_vjp(P, W, xs.p, true, hs.tri, hs.u, hs.v, v0, v1, reuse, p0, he.tri, n);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// pixel boundary (BoundaryPixel.cpp:36-159, Edge.cpp:377-409, Camera.cpp:433-467)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_pixel_adj(Params P) {
+  const DeviceScene& s = P.s;
+  const int W_ = P.cam.w, WH = P.cam.w * P.cam.h;
+  const F3 cpos = cam_pos(P.cam);
+  const long long nanti = P.n / 4;
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < P.n;
+       p += (long long)gridDim.x * blockDim.x) {
+    const long long slot = p % nanti;
+    const int anti = (int)(p / nanti);
+    const float r = P.smp.get(0, slot);
+    float rr;
+    if (anti == 0) rr = r;
+    else if (anti == 1) rr = r < 0.5f ? r + 0.5f : r - 0.5f;
+    else if (anti == 2) rr = r < 0.75f ? 0.75f - r : 1.75f - r;
+    else rr = r < 0.25f ? 0.25f - r : 1.25f - r;
+    const float r4 = rr * 4.f;
+    const int bi = (int)floorf(r4);
+    float ox, oy;
+    if (bi == 0) { ox = 0.f; oy = r4; }
+    else if (bi == 1) { ox = r4 - 1.f; oy = 1.f; }
+    else if (bi == 2) { ox = 1.f; oy = 3.f - r4; }
+    else { ox = 4.f - r4; oy = 0.f; }
+    const float pdfs[4] = {0.25f / (P.cam.plane_len_y * (float)P.cam.w), 0.25f / (P.cam.plane_len_x * (float)P.cam.h),
+                           0.25f / (P.cam.plane_len_y * (float)P.cam.w), 0.25f / (P.cam.plane_len_x * (float)P.cam.h)};
+    const int bsel = bi < 0 ? 0 : (bi > 3 ? 3 : bi);
+    const float pdf = pdfs[bsel];
+    const F3 dedge[4] = {F3(0.f, 1.f, 0.f), F3(1.f, 0.f, 0.f), F3(0.f, 1.f, 0.f), F3(1.f, 0.f, 0.f)};
+    const F3 dvis[4] = {F3(1.f, 0.f, 0.f), F3(0.f, -1.f, 0.f), F3(-1.f, 0.f, 0.f), F3(0.f, 1.f, 0.f)};
+    const F3 edge = normalize(xform_vector(P.cam.raster_to_world, dedge[bsel]));
+    const F3 edge2 = normalize(xform_vector(P.cam.raster_to_world, dvis[bsel]));
+    const int pixel = (int)(p % WH);
+    const F3 p0 = xform_point(P.cam.raster_to_world, F3((float)(pixel % W_) + ox, (float)(pixel / W_) + oy, 0.f));
+    const F3 dir = normalize(p0 - cpos);
+    Hit h;
+    if (!trace<false>(s, p0, dir, kShadowEps, kRayMax, h, P.err)) continue;
+    const F3 hitP = p0 + dir * h.t;
+    const SensorSample sds = sample_direct(P.cam, hitP);
+    const F3 dirc = sensor_ray_dir(P.cam, sds.qx, sds.qy);
+    SurfF x = post_intersect(s, h.tri, h.u, h.v);
+    const float dist = length(x.p - cpos);
+    const float dist1 = length(p0 - cpos);
+    const float cos2 = fabsf(dot(x.ng, -dirc));
+    F3 n;
+    // BoundaryPixel.cpp:92 reverses the sign convention
+    const float bval = -base_val(dist / dist1, edge, dirc, x.ng, edge2, n) * cos2;
+    const F3 g = g_at(P, pixel);
+    if (bval == 0.f || (g.x == 0.f && g.y == 0.f && g.z == 0.f)) continue;
+    F3 T(sds.sensor_val, sds.sensor_val, sds.sensor_val);
+    F3 rdir = dirc;
+    F3 L = scrub(T * emitted(s, x, -rdir));
+    for (int b = 0; b < P.D; b++) {
+      const int o = 1 + 5 * b;
+      F3 c;
+      const bool more = radiance_step(s, x, rdir, T, P.smp.get(o, slot), P.smp.get(o + 1, slot),
+                                      P.smp.get(o + 2, slot), P.smp.get(o + 3, slot), P.smp.get(o + 4, slot), c,
+                                      nullptr);
+      L = L + c;
+      if (!more || (T.x == 0.f && T.y == 0.f && T.z == 0.f)) break;
+    }
+    const float Wt = dot(g, L * (bval / pdf));
+    if (Wt == 0.f || !isfinite(Wt)) continue;
+    // the pixel-edge point is not a scene parameter: only the hit triangle moves
+    xdotn_vjp(P, Wt, cpos, false, -1, 0.f, 0.f, -1, -1, 0.f, p0, h.tri, n);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// primary edge list for one camera (ConstructPrimEdgeList, Edge.cpp:313-348)
+// ---------------------------------------------------------------------------
+__global__ void k_prim_edges(int ne, const int* edges, const float* pos, const float* fn, F3 cpos, float* func) {
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= ne) return;
+  const int v0 = edges[5 * e], v1 = edges[5 * e + 1], f0 = edges[5 * e + 2], f1 = edges[5 * e + 3];
+  const F3 p0 = make_f3(pos + 3 * v0);
+  const F3 ev = cpos - p0;
+  const F3 n0 = make_f3(fn + 3 * f0);
+  const F3 n1 = f1 >= 0 ? make_f3(fn + 3 * f1) : F3(0.f, 0.f, 0.f);
+  const bool ff0 = dot(ev, n0) > 0.f, ff1 = dot(ev, n1) > 0.f;
+  const bool valid = f1 < 0 || (ff0 != ff1);
+  func[e] = valid ? length(make_f3(pos + 3 * v1) - p0) : 0.f;
+}
+
+__global__ void k_cdf_single(int n, const float* func, float* cdf, float* integral_out) {
+  __shared__ double part[1024];
+  const int T = blockDim.x, tid = threadIdx.x;
+  const int chunk = (n + T - 1) / T;
+  const int a = min(n, tid * chunk), b = min(n, a + chunk);
+  double sacc = 0.0;
+  for (int i = a; i < b; i++) sacc += (double)func[i];
+  part[tid] = sacc;
+  __syncthreads();
+  if (tid == 0) { double run = 0.0; for (int i = 0; i < T; i++) { double x = part[i]; part[i] = run; run += x; } }
+  __syncthreads();
+  const float inv_size = 1.0f / (float)n;
+  double run = part[tid];
+  for (int i = a; i < b; i++) { run += (double)func[i]; cdf[i] = (float)run * inv_size; }
+  __syncthreads();
+  __shared__ float integral;
+  if (tid == 0) { integral = n > 0 ? cdf[n - 1] : 0.f; *integral_out = integral; }
+  __syncthreads();
+  if (integral > 0.f) for (int i = a; i < b; i++) cdf[i] = cdf[i] / integral;
+}
+
+__global__ void k_intersect(DeviceScene s, int n, const float* org, const float* dir, const float* tmin,
+                            const float* tmax, int* tri, float* u, float* v, float* t, int* err) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  Hit h;
+  trace<false>(s, make_f3(org + 3 * i), make_f3(dir + 3 * i), tmin[i], tmax[i], h, err);
+  tri[i] = h.tri; u[i] = h.u; v[i] = h.v; t[i] = h.t;
+}
+__global__ void k_occluded(DeviceScene s, int n, const float* org, const float* dir, const float* tmin,
+                           const float* tmax, int* vis) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  vis[i] = occluded(s, make_f3(org + 3 * i), make_f3(dir + 3 * i), tmin[i], tmax[i]) ? 0 : 1;
+}
+
+}  // namespace trn
+
+using namespace trn;
+
+namespace {
+
+int grid_for(long long n, int block) {
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  long long blocks = (n + block - 1) / block;
+  long long cap = (long long)sms * 16;
+  return (int)(blocks < cap ? (blocks < 1 ? 1 : blocks) : cap);
+}
+
+int check_common(trn_scene* s, const trn_camera* cam, const trn_render_options* o, int integrator) {
+  if (!s || !cam || !o) { set_error("null argument"); return -1; }
+  if (!s->configured) { set_error("scene is not configured (call trn_scene_configure)"); return -1; }
+  if (integrator < 0 || integrator > 4) { set_error("unknown integrator id"); return -1; }
+  if (cam->width <= 0 || cam->height <= 0) { set_error("invalid camera resolution"); return -1; }
+  if (o->max_bounces < 0 || o->max_bounces > kMaxDepth) { set_error("max_bounces must be in [0, 16]"); return -1; }
+  return 0;
+}
+
+int spp_of(const trn_render_options* o, int integrator) {
+  switch (integrator) {
+    case TRN_PATH_TRACER: return o->spp;
+    case TRN_PRIMARY_EDGE: return o->sppe;
+    case TRN_DIRECT_EDGE: return o->sppse0;
+    case TRN_INDIRECT_EDGE: return o->sppse1;
+    default: return o->sppe0;
+  }
+}
+
+Params make_params(trn_scene* s, const trn_camera* cam, const trn_render_options* o, int integrator,
+                   const trn_samples* smp) {
+  Params P;
+  P.s = s->view();
+  std::memcpy(&P.cam, cam, sizeof(CameraDesc));
+  const int spp = spp_of(o, integrator);
+  P.n = (long long)cam->width * cam->height * spp;
+  P.D = o->max_bounces;
+  P.inv_spp = spp > 0 ? 1.0f / (float)spp : 0.f;
+  P.smp.table = smp ? smp->samples : nullptr;
+  P.smp.stride = smp && smp->samples ? smp->stride : 0;
+  P.smp.seed = (uint32_t)o->seed;
+  P.smp.term = (uint32_t)integrator;
+  P.image = nullptr; P.dLdI = nullptr;
+  P.g_pos = s->g_pos; P.g_vn = s->g_vnormal; P.g_tex = s->g_texels; P.diff_tex = s->ntexel > 0;
+  P.edges = s->edges; P.ecdf = s->sec_cdf; P.efunc = s->sec_func; P.ne = s->ne; P.eintegral = 0.f;
+  P.err = s->err;
+  return P;
+}
+
+}  // namespace
+
+extern "C" {
+
+int trn_render_fwd(trn_scene* s, const trn_camera* cam, const trn_render_options* o, int integrator,
+                   const trn_samples* smp, float* image, cudaStream_t st) {
+  if (check_common(s, cam, o, integrator)) return -1;
+  if (!image) { set_error("trn_render_fwd: null image"); return -1; }
+  TRN_CUDA_TRY(cudaMemsetAsync(image, 0, sizeof(float) * 3 * cam->width * cam->height, st));
+  if (integrator != TRN_PATH_TRACER) return 0;  // edge terms have no primal image
+  Params P = make_params(s, cam, o, integrator, smp);
+  if (P.n == 0) return 0;
+  if (P.smp.table && P.smp.stride < P.n) { set_error("trn_render_fwd: sample table too small"); return -1; }
+  P.image = image;
+  k_path_fwd<<<grid_for(P.n, 128), 128, 0, st>>>(P);
+  TRN_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+int trn_render_grad(trn_scene* s, const trn_camera* cam, const trn_render_options* o, int integrator,
+                    const trn_samples* smp, const float* dLdI, cudaStream_t st) {
+  if (check_common(s, cam, o, integrator)) return -1;
+  if (!dLdI) { set_error("trn_render_grad: null dLdI"); return -1; }
+  Params P = make_params(s, cam, o, integrator, smp);
+  if (P.n == 0) return 0;
+  const long long slots = integrator == TRN_PIXEL_EDGE ? P.n / 4 : P.n;
+  if (P.smp.table && P.smp.stride < slots) { set_error("trn_render_grad: sample table too small"); return -1; }
+  if (integrator == TRN_PIXEL_EDGE && (P.n % 4) != 0) { set_error("pixel boundary needs W*H*spp divisible by 4"); return -1; }
+  P.dLdI = dLdI;
+  s->grads_finalized = false;
+  float* tmp = nullptr;
+  float* integral_dev = nullptr;
+  if (integrator == TRN_PRIMARY_EDGE) {
+    // per-camera silhouette list (ConstructPrimEdgeList)
+    if (s->ne == 0) return 0;
+    TRN_CUDA_TRY(cudaMallocAsync((void**)&tmp, sizeof(float) * (2 * (size_t)s->ne + 1), st));
+    float* func = tmp;
+    float* cdf = tmp + s->ne;
+    integral_dev = tmp + 2 * (size_t)s->ne;
+    const F3 cpos(cam->pos[0], cam->pos[1], cam->pos[2]);
+    k_prim_edges<<<(s->ne + 255) / 256, 256, 0, st>>>(s->ne, s->edges, s->pos, s->fnormal, cpos, func);
+    k_cdf_single<<<1, 1024, 0, st>>>(s->ne, func, cdf, integral_dev);
+    float integral = 0.f;
+    TRN_CUDA_TRY(cudaMemcpyAsync(&integral, integral_dev, sizeof(float), cudaMemcpyDeviceToHost, st));
+    TRN_CUDA_TRY(cudaStreamSynchronize(st));
+    if (!(integral > 0.f)) { cudaFreeAsync(tmp, st); return 0; }
+    P.ecdf = cdf; P.efunc = func; P.eintegral = integral;
+  } else if (integrator == TRN_DIRECT_EDGE || integrator == TRN_INDIRECT_EDGE) {
+    if (s->ne == 0) return 0;
+    float integral = 0.f;
+    TRN_CUDA_TRY(cudaMemcpyAsync(&integral, s->sec_integral_dev, sizeof(float), cudaMemcpyDeviceToHost, st));
+    TRN_CUDA_TRY(cudaStreamSynchronize(st));
+    if (!(integral > 0.f)) return 0;
+    P.eintegral = integral;
+  }
+  const int g = grid_for(P.n, 128);
+  switch (integrator) {
+    case TRN_PATH_TRACER: k_path_adj<<<g, 128, 0, st>>>(P); break;
+    case TRN_PRIMARY_EDGE: k_primary_adj<<<g, 128, 0, st>>>(P); break;
+    case TRN_DIRECT_EDGE: k_direct_adj<<<g, 128, 0, st>>>(P); break;
+    case TRN_INDIRECT_EDGE: k_indirect_adj<<<g, 128, 0, st>>>(P); break;
+    default: k_pixel_adj<<<g, 128, 0, st>>>(P); break;
+  }
+  TRN_CUDA_TRY(cudaGetLastError());
+  if (tmp) TRN_CUDA_TRY(cudaFreeAsync(tmp, st));
+  return 0;
+}
+
+int trn_intersect(trn_scene* s, int n, const float* org, const float* dir, const float* tmin, const float* tmax,
+                  int* tri, float* u, float* v, float* t, cudaStream_t st) {
+  if (!s || !s->configured) { set_error("trn_intersect: scene not configured"); return -1; }
+  if (n <= 0) return 0;
+  if (!org || !dir || !tmin || !tmax || !tri || !u || !v || !t) { set_error("trn_intersect: null argument"); return -1; }
+  k_intersect<<<(n + 127) / 128, 128, 0, st>>>(s->view(), n, org, dir, tmin, tmax, tri, u, v, t, s->err);
+  TRN_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+int trn_occluded(trn_scene* s, int n, const float* org, const float* dir, const float* tmin, const float* tmax,
+                 int* vis, cudaStream_t st) {
+  if (!s || !s->configured) { set_error("trn_occluded: scene not configured"); return -1; }
+  if (n <= 0) return 0;
+  if (!org || !dir || !tmin || !tmax || !vis) { set_error("trn_occluded: null argument"); return -1; }
+  k_occluded<<<(n + 127) / 128, 128, 0, st>>>(s->view(), n, org, dir, tmin, tmax, vis);
+  TRN_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,95 @@
+// Host-side scene object shared by scene.cu (build, configure, gradients) and
+// render.cu (integrators). Not part of the public C-ABI.
+#pragma once
+#include <string>
+#include <vector>
+#include "scene_types.cuh"
+
+struct trn_scene {
+  // ---- sizes -----------------------------------------------------------------
+  int nv = 0, nt = 0, nuv = 0, nmesh = 0, nlight = 0, nbsdf = 0, ntex = 0, ne = 0;
+  long long ntexel = 0;
+  // ---- parameters (device) ---------------------------------------------------
+  float* raw_pos = nullptr;       // [V][3] positions before the mesh translation
+  float* translation = nullptr;   // [M][3] per-mesh translation parameter
+  float* texels = nullptr;        // [ntexel][3]
+  // ---- derived geometry (device) --------------------------------------------
+  float* pos = nullptr;           // [V][3]
+  int* idx = nullptr;             // [T][3]
+  float* fnormal = nullptr;       // [T][3]
+  float* area = nullptr;          // [T]
+  float* vnormal = nullptr;       // [V][3]
+  unsigned char* smooth = nullptr;// [T]
+  float* uv = nullptr;            // [NUV][2]
+  int* uvidx = nullptr;           // [T][3]
+  int* bsdf_id = nullptr;         // [T]
+  int* emitter_id = nullptr;      // [T]
+  int* vert_mesh = nullptr;       // [V]
+  int* vf_off = nullptr;          // [V+1] vertex -> incident faces (CSR)
+  int* vf_list = nullptr;         // [3T]
+  // merged light
+  int n_emit = 0;
+  int* emit_tris = nullptr;
+  int* tri_to_emit = nullptr;
+  float* light_func = nullptr;
+  float* light_cdf = nullptr;
+  float* light_radiance = nullptr;
+  float* light_integral_dev = nullptr;
+  float light_lum[64];
+  std::vector<float> h_light_radiance;
+  // materials
+  trn::BsdfDesc* bsdfs = nullptr;
+  trn::TexDesc* texs = nullptr;
+  std::vector<trn::BsdfDesc> h_bsdfs;
+  std::vector<trn::TexDesc> h_texs;
+  // edges (ObjMesh::processEdges, ObjMesh.cpp:584-632): v0 v1 f0 f1 v2
+  int* edges = nullptr;           // [E][5]
+  float* sec_func = nullptr;      // [E] length if the edge is a secondary edge else 0
+  float* sec_cdf = nullptr;       // [E]
+  float* sec_integral_dev = nullptr;
+  // acceleration structure
+  trn::BvhNode* nodes = nullptr;  // [T-1]
+  float4* tri_verts = nullptr;    // [T][3]
+  int* parent = nullptr;          // [2T-1]
+  int* flags = nullptr;           // [T-1]
+  unsigned long long* keys = nullptr;     // [T]
+  unsigned long long* keys_alt = nullptr; // [T]
+  void* sort_tmp = nullptr;
+  size_t sort_tmp_bytes = 0;
+  float* bounds = nullptr;        // [6]
+  // ---- gradients (device) ------------------------------------------------------
+  float* g_pos = nullptr;         // [V][3] dL/d(world position)
+  float* g_vnormal = nullptr;     // [V][3] dL/d(vertex normal)
+  float* g_texels = nullptr;      // [ntexel][3]
+  float* g_translation = nullptr; // [M][3]
+  int* err = nullptr;             // device error word
+  float h_light_integral = 0.f;
+  bool configured = false;
+  bool grads_finalized = true;
+
+  trn::DeviceScene view() const {
+    trn::DeviceScene s;
+    s.nv = nv; s.nt = nt;
+    s.pos = pos; s.idx = idx; s.fnormal = fnormal; s.area = area; s.vnormal = vnormal;
+    s.smooth = smooth; s.uv = uv; s.uvidx = uvidx; s.bsdf_id = bsdf_id; s.emitter_id = emitter_id;
+    s.n_emit = n_emit; s.emit_tris = emit_tris; s.tri_to_emit = tri_to_emit;
+    s.light_func = light_func; s.light_cdf = light_cdf; s.light_integral = h_light_integral;
+    s.light_radiance = light_radiance;
+    s.n_bsdf = nbsdf; s.bsdfs = bsdfs; s.texs = texs; s.texels = texels;
+    s.nodes = nodes; s.tri_verts = tri_verts; s.root_is_leaf = nt == 1;
+    return s;
+  }
+};
+
+namespace trn {
+void set_error(const std::string& msg);
+}
+
+#define TRN_CUDA_TRY(expr)                                                        \
+  do {                                                                            \
+    cudaError_t _e = (expr);                                                      \
+    if (_e != cudaSuccess) {                                                      \
+      trn::set_error(std::string(#expr) + ": " + cudaGetErrorString(_e));        \
+      return -1;                                                                  \
+    }                                                                             \
+  } while (0)

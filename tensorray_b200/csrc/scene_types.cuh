@@ -1,0 +1,91 @@
+// Device-side views of the scene, camera and render options.
+//
+// HBM layout (all arrays are device pointers owned by the trn_scene handle):
+//   pos        [V][3] f32  world-space vertex positions (Primitive::Configure
+//                          output, Primitive.cpp:193 TransformPoints)
+//   idx        [T][3] i32  position indices (TriangleMesh::mIndexPosBuffer)
+//   fnormal    [T][3] f32  unit face normals   (Primitive.cpp:299-321)
+//   area       [T]    f32  triangle areas      (Primitive.cpp:316)
+//   vnormal    [V][3] f32  averaged vertex normals (Primitive.cpp:323-340)
+//   smooth     [T]    u8   shading-normal flag (mUseSmoothShadingBuffer)
+//   uv/uvidx   [NUV][2], [T][3]  texture coordinates (Scene.cpp:687-697)
+//   bsdf_id    [T]    i32  material per triangle (mSbtIndexBuffer)
+//   emitter_id [T]    i32  area-light id or -1 (mEmitterIDBuffer)
+//   tri_verts  [T][12] f32 leaf-ordered triangle vertices for traversal:
+//                          (P0.xyz, tri_id) (P1.xyz, 0) (P2.xyz, 0)
+//   nodes      [T-1]  BvhNode  binary LBVH, child boxes stored in the parent
+#pragma once
+#include "common.cuh"
+
+namespace trn {
+
+enum BsdfType : int { kDiffuse = 0, kMicrofacet = 1 };
+
+struct BsdfDesc {
+  int type;          // BsdfType
+  int tex;           // texture index for the (diffuse) albedo, -1 = constant
+  float albedo[3];   // Diffuse albedo / Microfacet diffuse reflectance
+  float spec[3];     // Microfacet specular reflectance (F0)
+  float roughness;   // Microfacet roughness (Microfacet.cpp:51 alpha = r^2)
+};
+
+struct TexDesc {
+  int w, h;
+  long long offset;  // texel offset into the texel array (RGB triples)
+};
+
+struct alignas(16) BvhNode {
+  // child 0 box (lo, hi), child 1 box (lo, hi), children (>=0 node, <0 ~leaf)
+  float4 a;  // l0x l0y l0z h0x
+  float4 b;  // h0y h0z l1x l1y
+  float4 c;  // l1z h1x h1y h1z
+  int4 d;    // c0 c1 - -
+};
+
+struct DeviceScene {
+  int nv, nt;
+  const float* pos;
+  const int* idx;
+  const float* fnormal;
+  const float* area;
+  const float* vnormal;
+  const unsigned char* smooth;
+  const float* uv;
+  const int* uvidx;
+  const int* bsdf_id;
+  const int* emitter_id;
+  // merged area light (Scene::ConfigureLight, Scene.cpp:471-520)
+  int n_emit;                 // emitter triangles
+  const int* emit_tris;       // [n_emit] global triangle ids
+  const int* tri_to_emit;     // [T] index into emit_tris or -1
+  const float* light_func;    // [n_emit] luminance * area (detached)
+  const float* light_cdf;     // [n_emit] normalised inclusive CDF
+  float light_integral;       // Distribution1D::mIntegralVal
+  const float* light_radiance;// [n_lights][3]
+  // materials
+  int n_bsdf;
+  const BsdfDesc* bsdfs;
+  const TexDesc* texs;
+  const float* texels;        // [sum w*h][3]
+  // acceleration structure
+  const BvhNode* nodes;
+  const float4* tri_verts;    // [T][3] float4
+  int root_is_leaf;
+};
+
+// Pinhole camera (Camera.cpp:89-137, BaseCamera.cpp:45-88). Matrices are
+// row-major 4x4 acting on column vectors (M * v).
+struct CameraDesc {
+  int w, h;
+  float pos[3];
+  float dir[3];
+  float raster_to_camera[16];
+  float view_inv[16];
+  float world_to_sample[16];
+  float sample_to_camera[16];
+  float raster_to_world[16];
+  float inv_area;            // Camera::mInvArea
+  float plane_len_x, plane_len_y;
+};
+
+}  // namespace trn
