@@ -1,0 +1,395 @@
+#!/usr/bin/env python
+"""Benchmark: grad path-samples/sec of render + gradient on one B200 per rank.
+
+Workload (default): the 100K-triangle config -- a sphere displaced by 3-octave
+value noise, GGX microfacet (roughness 0.3) with a 512x512 albedo texture,
+ground quad and quad light, 512x512 pixels, 64 spp per term, depth 5, all
+boundary terms (primary, direct, indirect, pixel), gradients w.r.t. every
+vertex position and the texture. One step = parameter upload to the scene +
+Scene::Configure (geometry chain + LBVH rebuild) + PathTracer.renderC +
+dL/dI of 0.5*|I - I_target|^2 + renderD of all five integrators + the
+geometry adjoint. A grad path-sample is one sample slot processed forward +
+adjoint by one integrator: W*H*spp per enabled term.
+
+With --gpus N (torchrun) every rank renders its own seeds of the same view
+and the gradient buffers are summed with one NCCL all-reduce (weak scaling).
+--impl reference times the CPU oracle (the port of the reference path) on a
+bounded sample of the same workload on this host's cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+import torch  # noqa: E402
+
+# algorithmic bytes per counted unit (the roofline model of the path):
+# closest-hit query = 32 B ray + 16 B hit + 48 B hit-triangle fetch; shadow
+# query = 32 B + 4 B + 48 B; smooth-shaded vertex +36 B normals +12 B normal
+# indices; textured vertex +24 B uv +12 B uv indices +12 B texel; light
+# sample = 4 B per CDF probe + 48 B emitter triangle; one vertex gradient
+# update = 12 B read-modify-write (24 B); texel update 24 B; pixel access 12 B.
+B_CLOSEST, B_SHADOW, B_SMOOTH, B_TEX, B_LIGHT_TRI = 96, 84, 48, 48, 48
+B_VSCATTER, B_NSCATTER, B_TSCATTER, B_PIXEL = 24, 24, 24, 12
+CNT_NAMES = ["closest", "shadow", "shade", "smooth", "tex", "light", "vscatter", "nscatter", "tscatter", "pixel"]
+
+
+def algorithmic_bytes(c: dict, n_emit: int) -> int:
+    light = 4 * max(1, math.ceil(math.log2(max(n_emit, 2)))) + B_LIGHT_TRI
+    return (c["closest"] * B_CLOSEST + c["shadow"] * B_SHADOW + c["smooth"] * B_SMOOTH + c["tex"] * B_TEX +
+            c["light"] * light + c["vscatter"] * B_VSCATTER + c["nscatter"] * B_NSCATTER +
+            c["tscatter"] * B_TSCATTER + c["pixel"] * B_PIXEL)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="trn", choices=["trn", "reference"])
+    ap.add_argument("--res", type=int, default=512)
+    ap.add_argument("--spp", type=int, default=64)
+    ap.add_argument("--depth", type=int, default=5)
+    ap.add_argument("--tris", type=int, default=100_000)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--quick", action="store_true", help="small smoke-sized run")
+    return ap.parse_args()
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+
+    def start(self):
+        os.makedirs(os.path.dirname(self.path), exist_ok=True)
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}",
+                 "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait()
+        self.f.close()
+        sm, smax, reasons = [], [], set()
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax.append(float(p[2]))
+            except ValueError:
+                continue
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            for nm, v in zip(names, p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def workload_name(a) -> str:
+    return (f"displaced sphere {a.tris // 1000}K tris, GGX r=0.3 + 512^2 texture, {a.res}x{a.res}, "
+            f"{a.spp} spp x 5 terms (interior+primary+direct+indirect+pixel), depth {a.depth}, "
+            f"grads: all vertex positions + texels")
+
+
+# ---------------------------------------------------------------------------
+# reference arm: the CPU oracle on a bounded sample
+# ---------------------------------------------------------------------------
+def cpu_oracle_rate(a, budget_s: float = 20.0, res: int = 8, spp: int = 1):
+    from oracle import tr_oracle as O
+    from tensorray_b200 import api, scenes
+    torch.set_num_threads(os.cpu_count() or 1)
+    spec = scenes.config2_scene(res, res, tris=a.tris)
+    sc = O.OracleScene(spec, requires_grad=("positions", "texels"))
+    c = spec.cameras[0]
+    cam = O.camera_matrices(c.pos, c.target, c.up, c.width, c.height, c.fov)
+    D = a.depth
+    units = 0
+    t0 = time.perf_counter()
+    it = 0
+    while True:
+        target = torch.zeros(res * res, 3)
+        for integ in range(5):
+            smp = O.hash_table(it, integ, api.sample_dims(integ, D), api.sample_slots(integ, res, res, spp))
+            dLdI = target + 0.5
+            O.grads(sc, cam, integ, spp, D, smp, dLdI)
+            units += res * res * spp
+        it += 1
+        if time.perf_counter() - t0 > budget_s or it >= 50:
+            break
+    dt = time.perf_counter() - t0
+    return units / dt, units, dt, torch.get_num_threads()
+
+
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    steps = []
+    tot_units = 0
+    t_all = 0.0
+    for _ in range(a.warmup):
+        cpu_oracle_rate(a, budget_s=2.0)
+    for _ in range(a.steps):
+        rate, units, dt, cores = cpu_oracle_rate(a, budget_s=10.0)
+        steps.append(dt)
+        tot_units += units
+        t_all += dt
+    value = tot_units / t_all
+    sample = f"{tot_units // a.steps} grad path-samples per step: 8x8 px, 1 spp per term, 5 terms, same scene"
+    line = {"metric": "grad path-samples/sec", "value": value, "unit": "grad path-samples/s",
+            "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * t_all / a.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded procedural scene)", "impl": "reference",
+            "config": {"workload": workload_name(a), "sample": sample},
+            "cpu_baseline": {"value": value, "unit": "grad path-samples/s", "cores": torch.get_num_threads(),
+                             "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "grad path-samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# trn arm
+# ---------------------------------------------------------------------------
+def main():
+    a = parse()
+    if a.quick:
+        a.res, a.spp, a.tris = 128, 4, 20_000
+    if a.impl == "reference":
+        return run_reference(a)
+    import torch.distributed as dist
+    from tensorray_b200 import api, scenes
+    from tensorray_b200 import autograd as tra
+    from tensorray_b200 import _abi
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    lib = _abi.load()
+
+    spec = scenes.config2_scene(a.res, a.res, tris=a.tris)
+    scene = api.Scene(spec)
+    scene.configure()
+    sphere = scene.shapes[0]
+    D = a.depth
+    base_seed = 1000 * rank
+    opts = api.RenderOptions(base_seed, D, a.spp, a.spp, a.spp, a.spp, a.spp)
+    integrators = [api.PathTracer(), api.PrimaryEdgeIntegrator(), api.DirectEdgeIntegrator(),
+                   api.IndirectEdgeIntegrator(), api.PixelBoundaryIntegrator()]
+    kernel_names = ["k_path_fwd", "k_path_adj", "k_primary_adj", "k_direct_adj", "k_indirect_adj", "k_pixel_adj"]
+    units_per_step = a.res * a.res * a.spp * 5
+    V0 = scene._raw_positions.clone()
+    tex0 = torch.as_tensor(np.ascontiguousarray(spec.textures[0]), device=dev).reshape(-1, 3).clone()
+    # target: same view rendered with perturbed geometry
+    g = torch.Generator(device="cpu").manual_seed(7)
+    Vt = V0.clone()
+    sl = sphere.vertex_slice()
+    Vt[sl] += (torch.randn(Vt[sl].shape, generator=g) * 0.01).to(dev)
+    scene.set_vertex_positions(Vt)
+    scene.configure()
+    target = integrators[0].renderC(scene, api.RenderOptions(12345, D, a.spp, 0, 0, 0, 0)).clone()
+    scene.set_vertex_positions(V0)
+    scene.configure()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > 126 MB L2
+    stream = torch.cuda.current_stream()
+
+    def step(ev=None):
+        # parameter update -> Scene::Configure
+        scene.set_vertex_positions(V0)
+        scene.set_texels(tex0)
+        scene.configure()
+        if ev: ev["fwd"][0].record(stream)
+        img = integrators[0].renderC(scene, opts)
+        if ev: ev["fwd"][1].record(stream)
+        dLdI = img - target
+        scene.clear_grads()
+        for i, it in enumerate(integrators):
+            if ev: ev[kernel_names[i + 1]][0].record(stream)
+            it.renderD(scene, opts, dLdI)
+            if ev: ev[kernel_names[i + 1]][1].record(stream)
+        gr = scene.get_grads(clear=True)
+        if world > 1:
+            flat = torch.cat([gr["positions"].reshape(-1), gr["texels"].reshape(-1)])
+            dist.all_reduce(flat)
+        return gr
+
+    for _ in range(a.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    ev_keys = ["fwd"] + kernel_names[1:]
+    per_kernel = {k: [] for k in ev_keys}
+    clocks = Clocks(local)
+    clocks.start()
+    launches0 = lib.trn_kernel_launches()
+    total_ms = 0.0
+    for s in range(a.steps):
+        if world > 1:
+            dist.barrier()
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev = {k: (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for k in ev_keys}
+        e0.record(stream)
+        step(ev)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        total_ms += e0.elapsed_time(e1)
+        for k in ev_keys:
+            per_kernel[k].append(ev[k][0].elapsed_time(ev[k][1]))
+    launches = lib.trn_kernel_launches() - launches0
+    clk = clocks.stop()
+    ms = torch.tensor([total_ms / a.steps], device=dev)
+    if world > 1:
+        dist.all_reduce(ms, op=dist.ReduceOp.MAX)
+    ms_per_step = float(ms)
+    value = units_per_step * world / (ms_per_step / 1e3)
+
+    # ---- e2e: through the autograd.Function with host buffers ----
+    e2e = None
+    if not a.no_e2e:
+        ctx = tra.RenderContext(scene, opts)
+        Vh = V0.cpu().pin_memory()
+        th = tex0.cpu().pin_memory()
+        gVh = torch.empty_like(Vh).pin_memory()
+        gth = torch.empty_like(th).pin_memory()
+        lossh = torch.empty(1).pin_memory()
+
+        def e2e_step():
+            V = Vh.to(dev, non_blocking=True).requires_grad_(True)
+            T = th.to(dev, non_blocking=True).requires_grad_(True)
+            img = tra.render(V, T, ctx)
+            loss = 0.5 * ((img - target) ** 2).sum()
+            loss.backward()
+            gv, gt = V.grad, T.grad
+            if world > 1:
+                flat = torch.cat([gv.reshape(-1), gt.reshape(-1)])
+                dist.all_reduce(flat)
+            gVh.copy_(gv, non_blocking=True)
+            gth.copy_(gt, non_blocking=True)
+            lossh.copy_(loss.detach().reshape(1), non_blocking=True)
+
+        for _ in range(a.warmup):
+            e2e_step()
+        torch.cuda.synchronize()
+        tot = 0.0
+        for _ in range(a.steps):
+            if world > 1:
+                dist.barrier()
+            flush.zero_()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            e2e_step()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            tot += e0.elapsed_time(e1)
+        t = torch.tensor([tot / a.steps], device=dev)
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e = {"value": units_per_step * world / (float(t) / 1e3), "unit": "grad path-samples/s",
+               "h2d_bytes_per_step": int(Vh.numel() * 4 + th.numel() * 4),
+               "d2h_bytes_per_step": int(gVh.numel() * 4 + gth.numel() * 4 + 4),
+               "ms_per_step": float(t)}
+
+    # ---- roofline of the dominant kernel: counters from one instrumented step ----
+    lib.trn_stats_enable(scene.handle, 1)
+    import ctypes as C
+    buf = (C.c_ulonglong * 16)()
+    lib.trn_stats_read(scene.handle, buf, 1, C.c_void_p(stream.cuda_stream))
+    counts = {}
+    scene.set_vertex_positions(V0)
+    scene.configure()
+    img = integrators[0].renderC(scene, opts)
+    lib.trn_stats_read(scene.handle, buf, 1, C.c_void_p(stream.cuda_stream))
+    counts["fwd"] = dict(zip(CNT_NAMES, list(buf)[:10]))
+    dLdI = img - target
+    for i, it in enumerate(integrators):
+        it.renderD(scene, opts, dLdI)
+        lib.trn_stats_read(scene.handle, buf, 1, C.c_void_p(stream.cuda_stream))
+        counts[kernel_names[i + 1]] = dict(zip(CNT_NAMES, list(buf)[:10]))
+    scene.get_grads(clear=True)
+    lib.trn_stats_enable(scene.handle, 0)
+    avg = {k: sum(v) / len(v) for k, v in per_kernel.items()}
+    dom = max(avg, key=avg.get)
+    n_emit = 2
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    per_kernel_roof = {}
+    for k in ev_keys:
+        by = algorithmic_bytes(counts[k], n_emit)
+        per_kernel_roof[k] = {"ms": avg[k], "alg_bytes": by, "gbs": by / (avg[k] / 1e3) / 1e9,
+                              "counts": counts[k]}
+    ach = per_kernel_roof[dom]["gbs"]
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        try:
+            traffic = json.load(open(tpath)).get(dom.replace("fwd", "k_path_fwd"))
+        except Exception:
+            traffic = None
+    roofline = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                "traffic": traffic, "kernel": dom if dom != "fwd" else "k_path_fwd",
+                "peak_source": peak_src}
+
+    cpu = None
+    if rank == 0 and world == 1:
+        rate, units, dt, cores = cpu_oracle_rate(a, budget_s=15.0)
+        cpu = {"value": rate, "unit": "grad path-samples/s", "cores": cores, "kind": "port",
+               "sample": f"{units} grad path-samples in {dt:.1f}s: 8x8 px, 1 spp per term, 5 terms, same scene"}
+
+    if rank == 0:
+        line = {
+            "metric": "grad path-samples/sec", "value": value, "unit": "grad path-samples/s", "n_gpus": world,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
+            "config": {"workload": workload_name(a), "global_batch_samples": units_per_step * world,
+                       "res": a.res, "spp_per_term": a.spp, "depth": D, "triangles": scene.num_triangles,
+                       "l2": "flushed between timed steps (256 MB write)", "parallelism": f"seeds x{world}"},
+            "e2e": e2e, "gpu_launches": int(launches), "clocks": clk, "roofline": roofline,
+            "kernels": {k: {"ms": v["ms"], "GB/s": v["gbs"]} for k, v in per_kernel_roof.items()},
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -109,6 +109,39 @@ typedef struct {
   long long stride;
 } trn_samples;
 
+/* Launch shape of the persistent integrator kernels (0 = library default):
+ * threads per block, resident blocks per SM, and sample slots each lane takes
+ * per fetch from the work queue. Chosen by the autotuner
+ * (tensorray_b200/autotune.py). */
+typedef struct {
+  int block;
+  int blocks_per_sm;
+  int chunk;
+} trn_launch;
+
+/* One camera view of a batched render (the reference renders one view per
+ * call and loops over views in Python, pyTensorRay/renderer_multi_view.py:53-61).
+ * pixel_offset: first pixel of this view in the concatenated image / dL/dI
+ * buffers (-1 = right after the previous view). slot_offset shifts the
+ * view's hash-sampler slots (a render split into spp chunks uses disjoint
+ * slots per chunk); weight scales contributions (0 = 1/spp). grad_*: device
+ * gradient destinations of this view ([V*3], [V*3], [texels*3]); NULL = the
+ * scene's own buffers. */
+typedef struct {
+  trn_camera camera;
+  int spp;
+  int seed;
+  long long pixel_offset;
+  long long slot_offset;
+  float weight;
+  int reserved;
+  float* grad_positions;
+  float* grad_vertex_normals;
+  float* grad_texels;
+} trn_view;
+
+typedef struct trn_viewset trn_viewset;
+
 /* Last error message of this thread ("" if none). */
 const char* trn_last_error(void);
 /* Library version string. */
@@ -162,12 +195,46 @@ int trn_render_fwd(trn_scene* scene, const trn_camera* camera, const trn_render_
 int trn_render_grad(trn_scene* scene, const trn_camera* camera, const trn_render_options* options,
                     int integrator, const trn_samples* samples, const float* dLdI, cudaStream_t stream);
 
+/* Batched multi-view rendering: all views of a view set in one persistent
+ * launch per integrator, images concatenated [npix*3]. The per-view spp of
+ * trn_view applies to the integrator being rendered; options supplies
+ * max_bounces and the seed. */
+int trn_viewset_create(trn_scene* scene, int nviews, const trn_view* views, trn_viewset** out);
+int trn_viewset_destroy(trn_viewset* views);
+int trn_viewset_num_pixels(const trn_viewset* views, long long* npix);
+int trn_render_views_fwd(trn_scene* scene, trn_viewset* views, const trn_render_options* options, int integrator,
+                         const trn_samples* samples, const trn_launch* launch, float* images, cudaStream_t stream);
+int trn_render_views_grad(trn_scene* scene, trn_viewset* views, const trn_render_options* options, int integrator,
+                          const trn_samples* samples, const trn_launch* launch, const float* dLdI,
+                          cudaStream_t stream);
+/* Per-view image loss 0.5*|I - T|^2 (pyTensorRay/loss.py:34-38) into loss[nviews]
+ * and dL/dI = I - T into dLdI (either may be NULL). */
+int trn_views_loss(trn_viewset* views, const float* images, const float* targets, float* dLdI, float* loss,
+                   cudaStream_t stream);
+
 /* Finish the geometry-chain adjoint and copy gradients out (get_grad with
  * clear_grad, pybind_utils.h:133-142). Any destination may be NULL.
  * d_translation [M*3], d_positions [V*3] (raw positions), d_texels [ntexel*3]. */
 int trn_scene_get_grads(trn_scene* scene, float* d_translation, float* d_positions, float* d_texels,
                         int clear, cudaStream_t stream);
 int trn_scene_clear_grads(trn_scene* scene, cudaStream_t stream);
+/* Geometry-chain adjoint for caller-owned gradient buffers (per-request
+ * gradients of the serving loop): folds grad_vertex_normals [V*3] into
+ * grad_positions [V*3] (and zeroes it), and writes d_translation [M*3]. */
+int trn_scene_finalize_grads(trn_scene* scene, float* grad_positions, float* grad_vertex_normals,
+                             float* d_translation, cudaStream_t stream);
+
+/* Instrumentation (the reference counts JIT launches per pass with
+ * KernelLaunchCounter, Tensor.h:1526-1547, printed at PathTracer.cpp:114).
+ * trn_kernel_launches: kernels this library has launched since load.
+ * trn_stats_enable / trn_stats_read: per-scene device work counters of the
+ * integrator kernels, 16 x u64: closest-hit queries, shadow queries, shading
+ * vertices, smooth-shaded vertices, textured vertices, light samples,
+ * position-gradient vertex updates, normal-gradient vertex updates, texel
+ * gradient updates, pixel accesses (rest reserved). */
+unsigned long long trn_kernel_launches(void);
+int trn_stats_enable(trn_scene* scene, int on);
+int trn_stats_read(trn_scene* scene, unsigned long long* out16, int reset, cudaStream_t stream);
 
 #ifdef __cplusplus
 }

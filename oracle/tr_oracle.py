@@ -70,9 +70,12 @@ def hash_uniform(seed: int, term: int, dim: int, slots: np.ndarray) -> np.ndarra
     return ((k + np.float32(0.5)) * np.float32(1.0 / 8388608.0)).astype(np.float32)
 
 
-def hash_table(seed: int, term: int, dims: int, slots: int) -> torch.Tensor:
+def hash_table(seed: int, term: int, dims: int, slots: int, view_seed: int = 0, view: int = 0) -> torch.Tensor:
+    """The library's hash sampler for one view: the stream seed folds the
+    render seed with the view's seed and index."""
+    stream = (seed * 1000003 + (view_seed * 7919 + view)) & 0xFFFFFFFF
     idx = np.arange(slots, dtype=np.uint64)
-    return torch.from_numpy(np.stack([hash_uniform(seed, term, d, idx) for d in range(dims)]))
+    return torch.from_numpy(np.stack([hash_uniform(stream, term, d, idx) for d in range(dims)]))
 
 
 def uniform_table(seed: int, dims: int, slots: int) -> torch.Tensor:
@@ -411,11 +414,13 @@ class OracleScene:
         return tri >= 0
 
 
-def intersect_brute(P0, P1, P2, org, dir, tmin, tmax, chunk=512):
+def intersect_brute(P0, P1, P2, org, dir, tmin, tmax, chunk=None):
     """Watertight ray/triangle test (Woop, Benthin, Wald, JCGT 2013) against
     every triangle; closest hit = lexicographic min of (t, triangle id)."""
     n = org.shape[0]
     T = P0.shape[0]
+    if chunk is None:
+        chunk = max(1, min(512, (1 << 22) // max(T, 1)))
     out_tri = torch.full((n,), -1, dtype=torch.long)
     out_u, out_v, out_t = torch.zeros(n), torch.zeros(n), torch.full((n,), -1.0)
     if n == 0:

@@ -62,6 +62,16 @@ class TrnSamples(C.Structure):
     _fields_ = [("samples", C.c_void_p), ("stride", C.c_longlong)]
 
 
+class TrnLaunch(C.Structure):
+    _fields_ = [("block", C.c_int), ("blocks_per_sm", C.c_int), ("chunk", C.c_int)]
+
+
+class TrnView(C.Structure):
+    _fields_ = [("camera", TrnCamera), ("spp", C.c_int), ("seed", C.c_int), ("pixel_offset", C.c_longlong),
+                ("slot_offset", C.c_longlong), ("weight", C.c_float), ("reserved", C.c_int),
+                ("grad_positions", C.c_void_p), ("grad_vertex_normals", C.c_void_p), ("grad_texels", C.c_void_p)]
+
+
 _SIGNATURES = {
     "trn_last_error": (C.c_char_p, []),
     "trn_version": (C.c_char_p, []),
@@ -86,6 +96,18 @@ _SIGNATURES = {
                                   C.POINTER(TrnSamples), C.c_void_p, C.c_void_p]),
     "trn_scene_get_grads": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
     "trn_scene_clear_grads": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "trn_viewset_create": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(TrnView), C.POINTER(C.c_void_p)]),
+    "trn_viewset_destroy": (C.c_int, [C.c_void_p]),
+    "trn_viewset_num_pixels": (C.c_int, [C.c_void_p, C.POINTER(C.c_longlong)]),
+    "trn_render_views_fwd": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(TrnRenderOptions), C.c_int,
+                                       C.POINTER(TrnSamples), C.POINTER(TrnLaunch), C.c_void_p, C.c_void_p]),
+    "trn_render_views_grad": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(TrnRenderOptions), C.c_int,
+                                        C.POINTER(TrnSamples), C.POINTER(TrnLaunch), C.c_void_p, C.c_void_p]),
+    "trn_views_loss": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "trn_scene_finalize_grads": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "trn_kernel_launches": (C.c_ulonglong, []),
+    "trn_stats_enable": (C.c_int, [C.c_void_p, C.c_int]),
+    "trn_stats_read": (C.c_int, [C.c_void_p, C.POINTER(C.c_ulonglong), C.c_int, C.c_void_p]),
 }
 
 _lib = None

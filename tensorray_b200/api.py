@@ -18,7 +18,8 @@ import torch
 
 from . import _abi
 from ._abi import (TRN_DIRECT_EDGE, TRN_INDIRECT_EDGE, TRN_PATH_TRACER, TRN_PIXEL_EDGE, TRN_PRIMARY_EDGE,
-                   TrnBsdf, TrnCamera, TrnRenderOptions, TrnSamples, TrnSceneDesc, TrnTexture, check)
+                   TrnBsdf, TrnCamera, TrnLaunch, TrnRenderOptions, TrnSamples, TrnSceneDesc, TrnTexture, TrnView,
+                   check)
 from .scenes import SceneSpec
 
 
@@ -391,3 +392,87 @@ def sample_dims(integrator_id: int, max_bounces: int) -> int:
 def sample_slots(integrator_id: int, width: int, height: int, spp: int) -> int:
     n = width * height * spp
     return n // 4 if integrator_id == TRN_PIXEL_EDGE else n
+
+
+class ViewSet:
+    """Many camera views rendered by one persistent launch per integrator.
+
+    Replaces the reference's Python loop over cameras
+    (pyTensorRay/renderer_multi_view.py:53-61): images of all views are
+    concatenated [npix, 3]; per-view spp and seeds are part of the set."""
+
+    def __init__(self, scene: Scene, cameras: list, spps: list, seeds: list | None = None):
+        n = len(cameras)
+        if n == 0 or len(spps) != n:
+            raise RuntimeError("ViewSet needs one spp per camera")
+        seeds = seeds if seeds is not None else list(range(n))
+        arr = (TrnView * n)()
+        for i, (c, sp, sd) in enumerate(zip(cameras, spps, seeds)):
+            arr[i] = TrnView(c.c, int(sp), int(sd), -1, 0, 0.0, 0, None, None, None)
+        self.scene = scene
+        self.cameras = list(cameras)
+        self.spps = [int(x) for x in spps]
+        self._h = C.c_void_p()
+        check(scene._lib.trn_viewset_create(scene.handle, n, arr, C.byref(self._h)), "trn_viewset_create")
+        npix = C.c_longlong()
+        check(scene._lib.trn_viewset_num_pixels(self._h, C.byref(npix)), "trn_viewset_num_pixels")
+        self.npix = npix.value
+        self.offsets = []
+        off = 0
+        for c in cameras:
+            self.offsets.append(off)
+            off += c.width * c.height
+
+    def __del__(self):
+        try:
+            if self._h:
+                self.scene._lib.trn_viewset_destroy(self._h)
+                self._h = C.c_void_p()
+        except Exception:
+            pass
+
+    def slots(self, integrator_id: int) -> int:
+        n = sum(c.width * c.height * s for c, s in zip(self.cameras, self.spps))
+        return n // 4 if integrator_id == TRN_PIXEL_EDGE else n
+
+    def render(self, integrator_id: int, options: RenderOptions, samples=None, launch: TrnLaunch | None = None,
+               out: torch.Tensor | None = None) -> torch.Tensor:
+        self.scene._ensure()
+        img = out if out is not None else torch.empty(self.npix, 3, device=self.scene.device)
+        smp = _samples_struct(samples)
+        o = options._c()
+        check(self.scene._lib.trn_render_views_fwd(self.scene.handle, self._h, C.byref(o), integrator_id,
+                                                   C.byref(smp), C.byref(launch) if launch else None,
+                                                   C.c_void_p(img.data_ptr()), C.c_void_p(_stream())),
+              "trn_render_views_fwd")
+        return img
+
+    def render_grad(self, integrator_id: int, options: RenderOptions, dLdI: torch.Tensor, samples=None,
+                    launch: TrnLaunch | None = None) -> None:
+        self.scene._ensure()
+        g = dLdI.contiguous()
+        if g.numel() != 3 * self.npix:
+            raise RuntimeError("dLdI must have npix*3 elements")
+        smp = _samples_struct(samples)
+        o = options._c()
+        check(self.scene._lib.trn_render_views_grad(self.scene.handle, self._h, C.byref(o), integrator_id,
+                                                    C.byref(smp), C.byref(launch) if launch else None,
+                                                    C.c_void_p(g.data_ptr()), C.c_void_p(_stream())),
+              "trn_render_views_grad")
+
+    def loss(self, images: torch.Tensor, targets: torch.Tensor, dLdI: torch.Tensor | None = None):
+        """Per-view 0.5*|I - T|^2 and dL/dI (one launch for all views)."""
+        loss = torch.empty(len(self.cameras), device=self.scene.device)
+        check(self.scene._lib.trn_views_loss(self._h, C.c_void_p(images.data_ptr()), C.c_void_p(targets.data_ptr()),
+                                             C.c_void_p(dLdI.data_ptr()) if dLdI is not None else None,
+                                             C.c_void_p(loss.data_ptr()), C.c_void_p(_stream())), "trn_views_loss")
+        return loss
+
+    def view_image(self, images: torch.Tensor, v: int) -> torch.Tensor:
+        c = self.cameras[v]
+        o = self.offsets[v]
+        return images[o:o + c.width * c.height].reshape(c.height, c.width, 3)
+
+
+def launch_config(block: int = 0, blocks_per_sm: int = 0, chunk: int = 0) -> TrnLaunch:
+    return TrnLaunch(int(block), int(blocks_per_sm), int(chunk))

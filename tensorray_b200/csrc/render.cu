@@ -6,8 +6,10 @@
 // stages (Integrator.cpp:178-303, Ray.cpp:65-116), a path here keeps its
 // state in registers and simply stops; the per-slot sample layout replaces
 // the reference's per-call RandomFloat tensors (see SampleSource).
+#include <algorithm>
 #include <cstring>
 #include <string>
+#include <vector>
 #include "../../include/trn.h"
 #include "scene_impl.cuh"
 #include "shading.cuh"
@@ -16,27 +18,59 @@ namespace trn {
 
 struct Params {
   DeviceScene s;
-  CameraDesc cam;
-  SampleSource smp;
-  long long n;        // sample slots of this call
-  int D;              // max bounces
-  float inv_spp;
-  float* image;       // forward radiance accumulation [W*H*3]
-  const float* dLdI;  // [W*H*3]
-  float* g_pos;       // [V*3]
-  float* g_vn;        // [V*3]
-  float* g_tex;       // [texels*3]
-  int diff_tex;       // accumulate texture gradients
-  // edge sampling tables (primary: per camera; secondary: per scene)
+  const ViewDesc* views;     // [nviews] cameras, slot ranges, pixel offsets
+  const long long* vbegin;   // [nviews] first path slot of each view
+  int nviews;
+  long long total;           // path slots of this launch (all views)
+  unsigned long long* work;  // work-distribution counter (zeroed before launch)
+  int chunk;                 // slots per lane per work fetch
+  const float* table;        // sample table [dim][total-slot] or nullptr (hash)
+  long long stride;
+  uint32_t term;             // integrator id (hash stream)
+  uint32_t seed;             // RenderOptions::mRndSeed
+  int D;                     // max bounces
+  float* image;              // forward radiance accumulation [pixels*3]
+  const float* dLdI;         // [pixels*3]
+  float* g_pos;              // [V*3]
+  float* g_vn;               // [V*3]
+  float* g_tex;              // [texels*3]
+  int diff_tex;              // accumulate texture gradients
+  // secondary edge sampling table (per scene); primary tables live in the views
   const int* edges;
   const float* ecdf;
   const float* efunc;
+  const float* eint;
   int ne;
-  float eintegral;
   int* err;
+  unsigned long long* stats;  // optional work counters (see Cnt), nullptr = off
 };
 
 constexpr int kMaxDepth = 16;
+
+// Per-thread work counters behind the roofline's algorithmic-byte model:
+// ray queries, shading vertices, light samples, gradient scatters, pixels.
+enum { kCntClosest = 0, kCntShadow, kCntShade, kCntSmooth, kCntTex, kCntLight, kCntVScatter, kCntNScatter,
+       kCntTScatter, kCntPixel, kCntNum };
+struct Cnt {
+  unsigned v[kCntNum];
+  TRN_D Cnt() {
+#pragma unroll
+    for (int i = 0; i < kCntNum; i++) v[i] = 0u;
+  }
+};
+TRN_D void flush_cnt(const Cnt& c, unsigned long long* stats) {
+  if (!stats) return;
+#pragma unroll
+  for (int i = 0; i < kCntNum; i++) {
+    const unsigned x = __reduce_add_sync(0xffffffffu, c.v[i]);
+    if ((threadIdx.x & 31) == 0 && x) atomicAdd(stats + i, (unsigned long long)x);
+  }
+}
+TRN_D void count_shade(Cnt& c, const DeviceScene& s, const SurfF& x) {
+  c.v[kCntShade]++;
+  if (s.smooth[x.tri]) c.v[kCntSmooth]++;
+  if (s.bsdfs[x.bsdf].tex >= 0) c.v[kCntTex]++;
+}
 
 TRN_D F3 F3z() { return F3(0.f, 0.f, 0.f); }
 TRN_D F3 scrub(const F3& a) { return finite3(a) ? a : F3z(); }
@@ -45,9 +79,78 @@ TRN_D void atomic_add3(float* a, const F3& g) {
   if (g.y != 0.f) atomicAdd(a + 1, g.y);
   if (g.z != 0.f) atomicAdd(a + 2, g.z);
 }
-TRN_D F3 g_at(const Params& P, int pix) {
+
+// Per-warp staging area for aggregated scatters (one per block, 8 warps max).
+TRN_D float* warp_scratch() {
+  __shared__ float buf[8 * 32 * 3];
+  return buf + (threadIdx.x >> 5) * 96;
+}
+
+// Warp-aggregated scatter-add of a float3 into base[3*idx]: lanes of the
+// converged warp that target the same index first sum in shared memory, then
+// one lane per distinct index issues the global atomics. Replaces the plain
+// per-element atomicAdd of IndexedWriteKernel (TensorKernels.cuh:177-209),
+// which serialises when many paths hit the same few vertices (quads, lights).
+TRN_D void agg_add3(float* base, long long idx, const F3& g) {
+  const unsigned active = __activemask();
+  const int lane = threadIdx.x & 31;
+  const unsigned peers = __match_any_sync(active, idx);
+  const int leader = __ffs(peers) - 1;
+  float* w = warp_scratch();
+  if (lane == leader) { w[3 * lane] = g.x; w[3 * lane + 1] = g.y; w[3 * lane + 2] = g.z; }
+  __syncwarp(active);
+  if (lane != leader) {
+    atomicAdd(w + 3 * leader, g.x); atomicAdd(w + 3 * leader + 1, g.y); atomicAdd(w + 3 * leader + 2, g.z);
+  }
+  __syncwarp(active);
+  if (lane == leader) atomic_add3(base + 3 * idx, F3(w[3 * lane], w[3 * lane + 1], w[3 * lane + 2]));
+  __syncwarp(active);
+}
+TRN_D F3 g_at(const Params& P, const ViewDesc& V, int pix) {
   if (pix < 0) return F3z();
-  return F3(__ldg(P.dLdI + 3 * pix), __ldg(P.dLdI + 3 * pix + 1), __ldg(P.dLdI + 3 * pix + 2)) * P.inv_spp;
+  const float* d = P.dLdI + 3 * (V.pix_off + pix);
+  return F3(__ldg(d), __ldg(d + 1), __ldg(d + 2)) * V.inv_spp;
+}
+
+// the view owning global slot g (last view whose first slot is <= g)
+TRN_D const ViewDesc& view_of(const Params& P, long long g) {
+  int lo = 0, hi = P.nviews - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(P.vbegin + mid) <= g) lo = mid; else hi = mid - 1;
+  }
+  return P.views[lo];
+}
+
+// Uniform sample `dim` of one slot: the table is indexed by the launch-global
+// slot, the hash by (view seed, term, dim, view-local slot).
+struct PathSmp {
+  const Params* P;
+  uint32_t seed;
+  long long gslot, lslot;
+  TRN_D float operator()(int dim) const {
+    if (P->table) return __ldg(P->table + (long long)dim * P->stride + gslot);
+    return hash_uniform(P->seed * 1000003u + seed, P->term, (uint32_t)dim, (uint32_t)lslot);
+  }
+};
+
+// Persistent work loop: each warp fetches 32*chunk consecutive slots from a
+// global counter, so uneven views and path lengths balance across SMs.
+template <class F>
+TRN_D void for_each_slot(const Params& P, F&& body) {
+  const int lane = threadIdx.x & 31;
+  const long long step = 32LL * P.chunk;
+  for (;;) {
+    unsigned long long start = 0;
+    if (lane == 0) start = atomicAdd(P.work, (unsigned long long)step);
+    start = __shfl_sync(0xffffffffu, start, 0);
+    if ((long long)start >= P.total) break;
+    for (int j = 0; j < P.chunk; j++) {
+      const long long g = (long long)start + 32LL * j + lane;
+      if (g < P.total) body(g);
+    }
+    __syncwarp();
+  }
 }
 TRN_D F3 cam_pos(const CameraDesc& c) { return F3(c.pos[0], c.pos[1], c.pos[2]); }
 
@@ -131,18 +234,18 @@ TRN_D void vadj_zero(VAdj& a) { a.p = F3z(); a.ns = F3z(); a.ng = F3z(); a.J = 0
 // position = w P0 + u P1 + v P2 (detached u, v), face normal c/|c| and
 // J = A / Detach(A) with c = cross(P1 - P0, P2 - P0), shading normal
 // w n0 + u n1 + v n2 (Scene.cpp:668-730, Primitive.cpp:299-340).
-TRN_D void scatter_vertex(const Params& P, int tri, float u, float v, const VAdj& a) {
+TRN_D void scatter_vertex(const Params& P, const ViewDesc& V, int tri, float u, float v, const VAdj& a, Cnt& cnt) {
   const DeviceScene& s = P.s;
+  cnt.v[kCntVScatter] += 3;
   int i0, i1, i2; tri_vertices(s, tri, i0, i1, i2);
   const float w = 1.f - u - v;
   F3 g0 = a.p * w, g1 = a.p * u, g2 = a.p * v;
   F3 gng = a.ng;
   if (s.smooth[tri]) {
-    if (a.ns.x != 0.f || a.ns.y != 0.f || a.ns.z != 0.f) {
-      atomic_add3(P.g_vn + 3 * i0, a.ns * w);
-      atomic_add3(P.g_vn + 3 * i1, a.ns * u);
-      atomic_add3(P.g_vn + 3 * i2, a.ns * v);
-    }
+    cnt.v[kCntNScatter] += 3;
+    agg_add3(V.gvn, i0, a.ns * w);
+    agg_add3(V.gvn, i1, a.ns * u);
+    agg_add3(V.gvn, i2, a.ns * v);
   } else {
     gng = gng + a.ns;
   }
@@ -159,18 +262,18 @@ TRN_D void scatter_vertex(const Params& P, int tri, float u, float v, const VAdj
     const F3 ge1 = cross(e2, gc), ge2 = cross(gc, e1);
     g1 = g1 + ge1; g2 = g2 + ge2; g0 = g0 - (ge1 + ge2);
   }
-  atomic_add3(P.g_pos + 3 * i0, g0);
-  atomic_add3(P.g_pos + 3 * i1, g1);
-  atomic_add3(P.g_pos + 3 * i2, g2);
+  agg_add3(V.gpos, i0, g0);
+  agg_add3(V.gpos, i1, g1);
+  agg_add3(V.gpos, i2, g2);
 }
 
-TRN_D void scatter_point(const Params& P, int tri, float u, float v, const F3& gp) {
-  if (gp.x == 0.f && gp.y == 0.f && gp.z == 0.f) return;
+TRN_D void scatter_point(const Params& P, const ViewDesc& V, int tri, float u, float v, const F3& gp, Cnt& cnt) {
+  cnt.v[kCntVScatter] += 3;
   int i0, i1, i2; tri_vertices(P.s, tri, i0, i1, i2);
   const float w = 1.f - u - v;
-  atomic_add3(P.g_pos + 3 * i0, gp * w);
-  atomic_add3(P.g_pos + 3 * i1, gp * u);
-  atomic_add3(P.g_pos + 3 * i2, gp * v);
+  agg_add3(V.gpos, i0, gp * w);
+  agg_add3(V.gpos, i1, gp * u);
+  agg_add3(V.gpos, i2, gp * v);
 }
 
 // ---------------------------------------------------------------------------
@@ -188,8 +291,9 @@ struct BounceRec {
 // Returns the contribution of this bounce (already NaN-scrubbed). On return
 // x/rdir/T hold the next vertex; the return flag says whether it exists.
 TRN_D bool radiance_step(const DeviceScene& s, SurfF& x, F3& rdir, F3& T, float l0, float l1, float b0, float b1,
-                         float b2, F3& contrib, BounceRec* rec) {
+                         float b2, F3& contrib, BounceRec* rec, Cnt& cnt) {
   const BsdfDesc b = s.bsdfs[x.bsdf];
+  count_shade(cnt, s, x);
   long long texel;
   const F3 kd = bsdf_albedo(s, b, x.tu, x.tv, texel);
   const Frame<float> fr = make_frame(x.ns);
@@ -198,6 +302,7 @@ TRN_D bool radiance_step(const DeviceScene& s, SurfF& x, F3& rdir, F3& T, float 
   if (rec) { rec->nee_ok = 0; rec->next_ok = 0; rec->scrubbed = 0; }
   LightSample ls;
   if (light_sample(s, l0, l1, ls)) {
+    cnt.v[kCntLight]++;
     int j0, j1, j2; tri_vertices(s, ls.tri, j0, j1, j2);
     const F3 y = bary3(ls.bu, ls.bv, load3(s.pos, j0), load3(s.pos, j1), load3(s.pos, j2));
     const F3 nl = load3(s.fnormal, ls.tri);
@@ -208,6 +313,7 @@ TRN_D bool radiance_step(const DeviceScene& s, SurfF& x, F3& rdir, F3& T, float 
     const float dotSh = dot(x.ns, wi), dotGeo = dot(x.ng, wi);
     const bool stable = d > kShadowEps && fabsf(dotSh) > kEdgeEps;
     const bool noleak = dotSh * dotGeo > 0.f;
+    if (stable && noleak) cnt.v[kCntShadow]++;
     if (stable && noleak && !occluded(s, x.p, wi, kShadowEps, d - kShadowEps)) {
       const F3 Le = dot(-wi, nl) > 0.f ? light_radiance(s, ls.light) : F3z();
       const float G = fabsf(dot(nl, -wi)) / d2;
@@ -228,7 +334,7 @@ TRN_D bool radiance_step(const DeviceScene& s, SurfF& x, F3& rdir, F3& T, float 
   bsdf_sample_only(b, fr, wo, b0, b1, b2, wi, pdf);
   Hit h;
   bool ok = pdf > 0.f && out_dir_valid(b, x.ns, x.ng, wi);
-  if (ok) ok = trace<false>(s, x.p, wi, kShadowEps, kRayMax, h);
+  if (ok) { cnt.v[kCntClosest]++; ok = trace<false>(s, x.p, wi, kShadowEps, kRayMax, h); }
   if (!ok) {
     contrib = scrub(val);
     if (rec) rec->scrubbed = !finite3(val);
@@ -264,31 +370,38 @@ TRN_D bool radiance_step(const DeviceScene& s, SurfF& x, F3& rdir, F3& T, float 
 // ---------------------------------------------------------------------------
 // interior term: forward
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128) k_path_fwd(Params P) {
-  const int W = P.cam.w, WH = P.cam.w * P.cam.h;
-  const F3 org = cam_pos(P.cam);
-  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < P.n;
-       p += (long long)gridDim.x * blockDim.x) {
+__global__ void __launch_bounds__(256) k_path_fwd(Params P) {
+  Cnt cnt;
+  for_each_slot(P, [&](long long gslot) {
+    const ViewDesc& V = view_of(P, gslot);
+    const long long p = gslot - V.begin;
+    const CameraDesc& cam = V.cam;
+    const PathSmp S{&P, V.seed, gslot, p + V.slot_off};
+    const int W = cam.w, WH = cam.w * cam.h;
+    const F3 org = cam_pos(cam);
     const int pix = (int)(p % WH);
-    const F3 dir = camera_ray_dir(P.cam, pix % W, pix / W, P.smp.get(0, p), P.smp.get(1, p));
+    const F3 dir = camera_ray_dir(cam, pix % W, pix / W, S(0), S(1));
     Hit h;
-    if (!trace<false>(P.s, org, dir, kShadowEps, kRayMax, h, P.err)) continue;
+    cnt.v[kCntClosest]++;
+    if (!trace<false>(P.s, org, dir, kShadowEps, kRayMax, h, P.err)) return;
     SurfF x = post_intersect(P.s, h.tri, h.u, h.v);
-    const float t1 = camera_factor<float>(P.cam, x.p, x.ng, 1.f);
+    const float t1 = camera_factor<float>(cam, x.p, x.ng, 1.f);
     F3 T(t1, t1, t1);
     F3 rdir = normalize(x.p - org);
     F3 L = scrub(T * emitted(P.s, x, -rdir));
     for (int b = 0; b < P.D; b++) {
       const int o = 2 + 5 * b;
       F3 c;
-      const bool more = radiance_step(P.s, x, rdir, T, P.smp.get(o, p), P.smp.get(o + 1, p), P.smp.get(o + 2, p),
-                                      P.smp.get(o + 3, p), P.smp.get(o + 4, p), c, nullptr);
+      const bool more = radiance_step(P.s, x, rdir, T, S(o), S(o + 1), S(o + 2),
+                                      S(o + 3), S(o + 4), c, nullptr, cnt);
       L = L + c;
       if (!more || (T.x == 0.f && T.y == 0.f && T.z == 0.f)) break;
     }
-    L = L * P.inv_spp;
-    atomic_add3(P.image + 3 * pix, L);
-  }
+    L = L * V.inv_spp;
+    cnt.v[kCntPixel]++;
+    atomic_add3(P.image + 3 * (V.pix_off + pix), L);
+  });
+  flush_cnt(cnt, P.stats);
 }
 
 // ---------------------------------------------------------------------------
@@ -352,18 +465,24 @@ TRN_D void cont_vjp(const BsdfDesc& b, bool need_prev, bool need_kd, const F3& x
 
 struct VRec { int tri; float u, v; };
 
-__global__ void __launch_bounds__(128) k_path_adj(Params P) {
-  const int W = P.cam.w, WH = P.cam.w * P.cam.h;
-  const F3 org = cam_pos(P.cam);
+__global__ void __launch_bounds__(256) k_path_adj(Params P) {
   const DeviceScene& s = P.s;
-  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < P.n;
-       p += (long long)gridDim.x * blockDim.x) {
+  Cnt cnt;
+  for_each_slot(P, [&](long long gslot) {
+    const ViewDesc& V = view_of(P, gslot);
+    const long long p = gslot - V.begin;
+    const CameraDesc& cam = V.cam;
+    const PathSmp S{&P, V.seed, gslot, p + V.slot_off};
+    const int W = cam.w, WH = cam.w * cam.h;
+    const F3 org = cam_pos(cam);
     const int pix = (int)(p % WH);
-    const F3 g = g_at(P, pix);
-    if (g.x == 0.f && g.y == 0.f && g.z == 0.f) continue;
-    const F3 dir = camera_ray_dir(P.cam, pix % W, pix / W, P.smp.get(0, p), P.smp.get(1, p));
+    cnt.v[kCntPixel]++;
+    const F3 g = g_at(P, V, pix);
+    if (g.x == 0.f && g.y == 0.f && g.z == 0.f) return;
+    const F3 dir = camera_ray_dir(cam, pix % W, pix / W, S(0), S(1));
     Hit h;
-    if (!trace<false>(s, org, dir, kShadowEps, kRayMax, h, P.err)) continue;
+    cnt.v[kCntClosest]++;
+    if (!trace<false>(s, org, dir, kShadowEps, kRayMax, h, P.err)) return;
     // ---- forward replay, recording vertices and factor values ----
     VRec vr[kMaxDepth + 2];
     BounceRec br[kMaxDepth + 1];
@@ -371,7 +490,7 @@ __global__ void __launch_bounds__(128) k_path_adj(Params P) {
     F3 Tk[kMaxDepth + 2], Nk[kMaxDepth + 2], Mk[kMaxDepth + 2], Phik[kMaxDepth + 2];
     SurfF x = post_intersect(s, h.tri, h.u, h.v);
     vr[1] = {h.tri, h.u, h.v};
-    const float t1 = camera_factor<float>(P.cam, x.p, x.ng, 1.f);
+    const float t1 = camera_factor<float>(cam, x.p, x.ng, 1.f);
     F3 T(t1, t1, t1);
     F3 rdir = normalize(x.p - org);
     Tk[1] = T;
@@ -385,8 +504,8 @@ __global__ void __launch_bounds__(128) k_path_adj(Params P) {
       const int o = 2 + 5 * b;
       F3 c;
       BounceRec& R = br[k];
-      const bool more = radiance_step(s, x, rdir, T, P.smp.get(o, p), P.smp.get(o + 1, p), P.smp.get(o + 2, p),
-                                      P.smp.get(o + 3, p), P.smp.get(o + 4, p), c, &R);
+      const bool more = radiance_step(s, x, rdir, T, S(o), S(o + 1), S(o + 2),
+                                      S(o + 3), S(o + 4), c, &R, cnt);
       // a scrubbed (non-finite) bounce contributes nothing and carries no gradient
       nee_on[k] = R.nee_ok && !R.scrubbed;
       if (!more) break;
@@ -443,7 +562,7 @@ __global__ void __launch_bounds__(128) k_path_adj(Params P) {
           const V3<D3> dx = seed3<3>(xp[1], grp == 0 ? 0 : -1);
           const V3<D3> dn = seed3<3>(ngv[1], grp == 1 ? 0 : -1);
           const D3 dJ = seed1<3>(1.f, grp == 2 ? 0 : -1);
-          const D3 r = camera_factor<D3>(P.cam, dx, dn, dJ);
+          const D3 r = camera_factor<D3>(cam, dx, dn, dJ);
           const F3 gg = F3(r.d[0], r.d[1], r.d[2]) * gam;
           if (grp == 0) va[1].p = va[1].p + gg;
           else if (grp == 1) va[1].ng = va[1].ng + gg;
@@ -464,7 +583,7 @@ __global__ void __launch_bounds__(128) k_path_adj(Params P) {
         nee_vjp(b, need_prev, need_kd, xp[k - 1], xp[k], nsv[k], ngv[k], kdv[k], yv[k], nlv[k], br[k].lLe, br[k].lpdf,
                 br[k].lmis, adj, gprev, va[k].p, va[k].ns, gkd, gy, gnl, gJl);
         VAdj la; la.p = gy; la.ns = F3z(); la.ng = gnl; la.J = gJl;
-        scatter_vertex(P, br[k].ltri, br[k].lu, br[k].lv, la);
+        scatter_vertex(P, V, br[k].ltri, br[k].lu, br[k].lv, la, cnt);
       }
       if (k < K && (Phik[k].x != 0.f || Phik[k].y != 0.f || Phik[k].z != 0.f)) {
         const F3 adj = Tk[k] * a[k + 1];
@@ -474,20 +593,22 @@ __global__ void __launch_bounds__(128) k_path_adj(Params P) {
         va[k + 1].J += gJn;
       }
       if (k >= 2) va[k - 1].p = va[k - 1].p + gprev;
-      if (need_kd) atomic_add3(P.g_tex + 3 * texel[k], gkd);
+      if (need_kd) { cnt.v[kCntTScatter]++; agg_add3(V.gtex, texel[k], gkd); }
     }
-    for (int k = 1; k <= K; k++) scatter_vertex(P, vr[k].tri, vr[k].u, vr[k].v, va[k]);
-  }
+    for (int k = 1; k <= K; k++) scatter_vertex(P, V, vr[k].tri, vr[k].u, vr[k].v, va[k], cnt);
+  });
+  flush_cnt(cnt, P.stats);
 }
 
 // ---------------------------------------------------------------------------
 // EvalImportance for one ray (Integrator.cpp:75-176)
 // ---------------------------------------------------------------------------
 TRN_D bool importance_step(const DeviceScene& s, const CameraDesc& cam, SurfF& x, F3& rdir, F3& T, float b0,
-                           float b1, float b2, F3& contrib, int& pix) {
+                           float b1, float b2, F3& contrib, int& pix, Cnt& cnt) {
   contrib = F3z();
   pix = -1;
   const BsdfDesc b = s.bsdfs[x.bsdf];
+  count_shade(cnt, s, x);
   long long texel;
   const F3 kd = bsdf_albedo(s, b, x.tu, x.tv, texel);
   const Frame<float> fr = make_frame(x.ns);
@@ -497,6 +618,7 @@ TRN_D bool importance_step(const DeviceScene& s, const CameraDesc& cam, SurfF& x
   if (sds.valid) {
     const F3 dirc = sensor_ray_dir(cam, sds.qx, sds.qy);
     const float dist2cam = length(x.p - cpos);
+    cnt.v[kCntShadow]++;
     if (!occluded(s, cpos, dirc, kShadowEps, dist2cam - kShadowEps)) {
       F3 val = F3z();
       if (out_dir_valid(b, x.ns, x.ng, wo)) {
@@ -515,6 +637,7 @@ TRN_D bool importance_step(const DeviceScene& s, const CameraDesc& cam, SurfF& x
   const F3 Tn = T * bv / pdf;
   if (!(pdf > 0.f) || !out_dir_valid(b, x.ns, x.ng, wi)) return false;
   Hit h;
+  cnt.v[kCntClosest]++;
   if (!trace<false>(s, x.p, wi, kShadowEps, kRayMax, h)) return false;
   x = post_intersect(s, h.tri, h.u, h.v);
   rdir = wi;
@@ -523,9 +646,10 @@ TRN_D bool importance_step(const DeviceScene& s, const CameraDesc& cam, SurfF& x
 }
 
 // scatter W * d xDotN / d(edge vertices, receiver point, far triangle)
-TRN_D void xdotn_vjp(const Params& P, float W, const F3& org, bool org_attached, int recv_tri, float ru, float rv,
-                     int va_, int vb_, float sedge, const F3& target_const, int far_tri, const F3& n) {
+TRN_D void xdotn_vjp(const Params& P, const ViewDesc& V, float W, const F3& org, bool org_attached, int recv_tri, float ru, float rv,
+                     int va_, int vb_, float sedge, const F3& target_const, int far_tri, const F3& n, Cnt& cnt) {
   const DeviceScene& s = P.s;
+  cnt.v[kCntVScatter] += 3 + (va_ >= 0 ? 2 : 0);
   int i0, i1, i2; tri_vertices(s, far_tri, i0, i1, i2);
   const F3 P0 = load3(s.pos, i0), P1 = load3(s.pos, i1), P2 = load3(s.pos, i2);
   const bool edge_attached = va_ >= 0;
@@ -553,14 +677,14 @@ TRN_D void xdotn_vjp(const Params& P, float W, const F3& org, bool org_attached,
       default: g2 = gg; break;
     }
   }
-  atomic_add3(P.g_pos + 3 * i0, g0);
-  atomic_add3(P.g_pos + 3 * i1, g1);
-  atomic_add3(P.g_pos + 3 * i2, g2);
+  agg_add3(V.gpos, i0, g0);
+  agg_add3(V.gpos, i1, g1);
+  agg_add3(V.gpos, i2, g2);
   if (edge_attached) {
-    atomic_add3(P.g_pos + 3 * va_, gPa);
-    atomic_add3(P.g_pos + 3 * vb_, gPb);
+    agg_add3(V.gpos, va_, gPa);
+    agg_add3(V.gpos, vb_, gPb);
   }
-  if (org_attached) scatter_point(P, recv_tri, ru, rv, gorg);
+  if (org_attached) scatter_point(P, V, recv_tri, ru, rv, gorg, cnt);
 }
 
 // boundary geometry term baseVal (BoundaryPrimary.cpp:115-129, Edge.cpp:258-271)
@@ -580,18 +704,24 @@ TRN_D float base_val(float ratio, const F3& edge, const F3& d, const F3& nrm, co
 // ---------------------------------------------------------------------------
 // primary boundary (BoundaryPrimary.cpp:36-181, SampleFromPrimEdges Edge.cpp:350-367)
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128) k_primary_adj(Params P) {
+__global__ void __launch_bounds__(256) k_primary_adj(Params P) {
   const DeviceScene& s = P.s;
-  const F3 cpos = cam_pos(P.cam);
-  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < P.n;
-       p += (long long)gridDim.x * blockDim.x) {
-    const float r0 = P.smp.get(0, p), r1 = P.smp.get(1, p);
+  Cnt cnt;
+  for_each_slot(P, [&](long long gslot) {
+    const ViewDesc& V = view_of(P, gslot);
+    const long long p = gslot - V.begin;
+    const CameraDesc& cam = V.cam;
+    const PathSmp S{&P, V.seed, gslot, p + V.slot_off};
+    const F3 cpos = cam_pos(cam);
+    const float r0 = S(0), r1 = S(1);
     float reuse;
-    const int e = sample_discrete(P.ecdf, P.ne, r0, reuse);
+    const float integral = __ldg(V.pint);
+    if (!(integral > 0.f)) return;
+    const int e = sample_discrete(V.pcdf, P.ne, r0, reuse);
     const int v0 = P.edges[5 * e], v1 = P.edges[5 * e + 1], v2 = P.edges[5 * e + 4];
-    const float len_e = P.efunc[e];
-    if (!(len_e > 0.f)) continue;
-    const float pmf = len_e / (P.eintegral * (float)P.ne);
+    const float len_e = V.pfunc[e];
+    if (!(len_e > 0.f)) return;
+    const float pmf = len_e / (integral * (float)P.ne);
     const float pdf = pmf / len_e;
     const F3 Pa = load3(s.pos, v0), Pb = load3(s.pos, v1), Pc = load3(s.pos, v2);
     const F3 e1 = Pb - Pa;
@@ -599,22 +729,24 @@ __global__ void __launch_bounds__(128) k_primary_adj(Params P) {
     const F3 edge = normalize(e1), edge2 = normalize(Pc - Pa);
     const F3 dir = normalize(p0 - cpos);
     Hit h;
-    if (!trace<false>(s, p0, dir, kShadowEps, kRayMax, h, P.err)) continue;
+    cnt.v[kCntClosest]++;
+    if (!trace<false>(s, p0, dir, kShadowEps, kRayMax, h, P.err)) return;
     const F3 hitP = p0 + dir * h.t;
-    const SensorSample sds = sample_direct(P.cam, hitP);
-    if (!sds.valid) continue;
-    const F3 dirc = sensor_ray_dir(P.cam, sds.qx, sds.qy);
+    const SensorSample sds = sample_direct(cam, hitP);
+    if (!sds.valid) return;
+    const F3 dirc = sensor_ray_dir(cam, sds.qx, sds.qy);
     const float dist2cam = length(p0 - cpos);
-    if (occluded(s, cpos, dirc, kShadowEps, dist2cam - kShadowEps)) continue;
+    cnt.v[kCntShadow]++;
+    if (occluded(s, cpos, dirc, kShadowEps, dist2cam - kShadowEps)) return;
     SurfF x = post_intersect(s, h.tri, h.u, h.v);
     const float dist = length(x.p - cpos);
     const float dist1 = length(p0 - cpos);
     const float cos2 = fabsf(dot(x.ng, -dirc));
     F3 n;
     const float bval = base_val((dist / dist1), edge, dirc, x.ng, edge2, n) * cos2;
-    const int pix = image_pixel(P.cam, sds.qx, sds.qy);
-    const F3 g = g_at(P, pix);
-    if (bval == 0.f || (g.x == 0.f && g.y == 0.f && g.z == 0.f)) continue;
+    const int pix = image_pixel(cam, sds.qx, sds.qy);
+    const F3 g = g_at(P, V, pix);
+    if (bval == 0.f || (g.x == 0.f && g.y == 0.f && g.z == 0.f)) return;
     // detached radiance along the camera ray through the sensor point
     F3 T(sds.sensor_val, sds.sensor_val, sds.sensor_val);
     F3 rdir = dirc;
@@ -622,39 +754,46 @@ __global__ void __launch_bounds__(128) k_primary_adj(Params P) {
     for (int b = 0; b < P.D; b++) {
       const int o = 2 + 5 * b;
       F3 c;
-      const bool more = radiance_step(s, x, rdir, T, P.smp.get(o, p), P.smp.get(o + 1, p), P.smp.get(o + 2, p),
-                                      P.smp.get(o + 3, p), P.smp.get(o + 4, p), c, nullptr);
+      const bool more = radiance_step(s, x, rdir, T, S(o), S(o + 1), S(o + 2),
+                                      S(o + 3), S(o + 4), c, nullptr, cnt);
       L = L + c;
       if (!more || (T.x == 0.f && T.y == 0.f && T.z == 0.f)) break;
     }
     const F3 wv = L * (bval / pdf);
     const float W = dot(g, wv);
-    if (W == 0.f || !isfinite(W)) continue;
-    xdotn_vjp(P, W, cpos, false, -1, 0.f, 0.f, v0, v1, r1, p0, h.tri, n);
-  }
+    if (W == 0.f || !isfinite(W)) return;
+    xdotn_vjp(P, V, W, cpos, false, -1, 0.f, 0.f, v0, v1, r1, p0, h.tri, n, cnt);
+  });
+  flush_cnt(cnt, P.stats);
 }
 
 // ---------------------------------------------------------------------------
 // direct boundary (BoundaryDirect.cpp:38-143, Edge.cpp:90-144, 201-309)
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128) k_direct_adj(Params P) {
+__global__ void __launch_bounds__(256) k_direct_adj(Params P) {
   const DeviceScene& s = P.s;
-  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < P.n;
-       p += (long long)gridDim.x * blockDim.x) {
-    const float r0 = P.smp.get(0, p), r1 = P.smp.get(1, p), r2 = P.smp.get(2, p);
+  Cnt cnt;
+  for_each_slot(P, [&](long long gslot) {
+    const ViewDesc& V = view_of(P, gslot);
+    const long long p = gslot - V.begin;
+    const CameraDesc& cam = V.cam;
+    const PathSmp S{&P, V.seed, gslot, p + V.slot_off};
+    const float r0 = S(0), r1 = S(1), r2 = S(2);
     float reuse;
+    const float integral = __ldg(P.eint);
+    if (!(integral > 0.f)) return;
     const int e = sample_discrete(P.ecdf, P.ne, r0, reuse);
     const int v0 = P.edges[5 * e], v1 = P.edges[5 * e + 1], f0 = P.edges[5 * e + 2], f1 = P.edges[5 * e + 3],
               v2 = P.edges[5 * e + 4];
     const float len_e = P.efunc[e];
-    if (!(len_e > 0.f)) continue;
-    const float pdf_e = (len_e / (P.eintegral * (float)P.ne)) / len_e;
+    if (!(len_e > 0.f)) return;
+    const float pdf_e = (len_e / (integral * (float)P.ne)) / len_e;
     const F3 Pa = load3(s.pos, v0), Pb = load3(s.pos, v1), Pc = load3(s.pos, v2);
     const F3 e1 = Pb - Pa;
     const F3 p0 = Pa + e1 * reuse;
     const F3 edge = normalize(e1), edge2 = normalize(Pc - Pa);
     LightSample ls;
-    if (!light_sample(s, r1, r2, ls)) continue;
+    if (!light_sample(s, r1, r2, ls)) return;
     int j0, j1, j2; tri_vertices(s, ls.tri, j0, j1, j2);
     const F3 p2 = bary3(ls.bu, ls.bv, load3(s.pos, j0), load3(s.pos, j1), load3(s.pos, j2));
     const F3 nL = load3(s.fnormal, ls.tri);
@@ -670,14 +809,16 @@ __global__ void __launch_bounds__(128) k_direct_adj(Params P) {
     const bool valid0 = fabsf(c0) > kEdgeEps;
     const bool valid1 = (c0 > kEdgeEps && c1 < -kEdgeEps) || (c0 < -kEdgeEps && c1 > kEdgeEps);
     const bool right = (is_b && valid0) || (!is_b && valid1);
-    if (!(right && cos_t > kEps && dist > kShadowEps)) continue;
+    if (!(right && cos_t > kEps && dist > kShadowEps)) return;
     const float pdf = pdf_e * ls.pdf * dist_sqr / cos_t;
     const F3 rdir = normalize(p0 - p2);
     Hit h0, h;
-    if (!trace<false>(s, p0, -rdir, kShadowEps, kRayMax, h0, P.err)) continue;
-    if (!trace<false>(s, p0, rdir, kShadowEps, kRayMax, h, P.err)) continue;
+    cnt.v[kCntClosest] += 2;
+    cnt.v[kCntLight]++;
+    if (!trace<false>(s, p0, -rdir, kShadowEps, kRayMax, h0, P.err)) return;
+    if (!trace<false>(s, p0, rdir, kShadowEps, kRayMax, h, P.err)) return;
     const F3 hp = p0 + (-rdir) * h0.t;
-    if (!(length(hp - p2) < kShadowEps)) continue;
+    if (!(length(hp - p2) < kShadowEps)) return;
     const SurfF xl = post_intersect(s, h0.tri, h0.u, h0.v);
     const F3 E = emitted(s, xl, rdir);
     SurfF x = post_intersect(s, h.tri, h.u, h.v);
@@ -686,7 +827,7 @@ __global__ void __launch_bounds__(128) k_direct_adj(Params P) {
     const float its_t = length(x.p - p0);
     F3 n;
     const float bval = base_val(its_t / dl, edge, -rdir, nL, edge2, n) * cos2;
-    if (bval == 0.f || (E.x == 0.f && E.y == 0.f && E.z == 0.f)) continue;
+    if (bval == 0.f || (E.x == 0.f && E.y == 0.f && E.z == 0.f)) return;
     const F3 ev0 = E * (bval / pdf);
     // trace towards the sensor (EvalImportance per bounce)
     F3 T(1.f, 1.f, 1.f);
@@ -696,33 +837,39 @@ __global__ void __launch_bounds__(128) k_direct_adj(Params P) {
     for (int b = 0; b < P.D; b++) {
       const int o = 3 + 3 * b;
       F3 c; int pix;
-      const bool more = importance_step(s, P.cam, xs, dirs, T, P.smp.get(o, p), P.smp.get(o + 1, p),
-                                        P.smp.get(o + 2, p), c, pix);
-      if (pix >= 0) W += dot(g_at(P, pix), ev0 * c);
+      const bool more = importance_step(s, cam, xs, dirs, T, S(o), S(o + 1),
+                                        S(o + 2), c, pix, cnt);
+      if (pix >= 0) W += dot(g_at(P, V, pix), ev0 * c);
       if (!more) break;
     }
-    if (W == 0.f || !isfinite(W)) continue;
-    xdotn_vjp(P, W, x.p, true, h.tri, h.u, h.v, v0, v1, reuse, p0, h0.tri, n);
-  }
+    if (W == 0.f || !isfinite(W)) return;
+    xdotn_vjp(P, V, W, x.p, true, h.tri, h.u, h.v, v0, v1, reuse, p0, h0.tri, n, cnt);
+  });
+  flush_cnt(cnt, P.stats);
 }
 
 // ---------------------------------------------------------------------------
 // indirect boundary (BoundaryIndirect.cpp:38-192, Edge.cpp:146-199)
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128) k_indirect_adj(Params P) {
+__global__ void __launch_bounds__(256) k_indirect_adj(Params P) {
   const DeviceScene& s = P.s;
   const int D = min(P.D, kMaxDepth);
-  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < P.n;
-       p += (long long)gridDim.x * blockDim.x) {
-    if (D < 2) break;
-    const float r0 = P.smp.get(0, p), r1 = P.smp.get(1, p), r2 = P.smp.get(2, p);
+  Cnt cnt;
+  if (D >= 2) for_each_slot(P, [&](long long g) {
+    const ViewDesc& V = view_of(P, g);
+    const long long p = g - V.begin;
+    const CameraDesc& cam = V.cam;
+    const PathSmp S{&P, V.seed, g, p};
+    const float r0 = S(0), r1 = S(1), r2 = S(2);
     float reuse;
+    const float integral = __ldg(P.eint);
+    if (!(integral > 0.f)) return;
     const int e = sample_discrete(P.ecdf, P.ne, r0, reuse);
     const int v0 = P.edges[5 * e], v1 = P.edges[5 * e + 1], f0 = P.edges[5 * e + 2], f1 = P.edges[5 * e + 3],
               v2 = P.edges[5 * e + 4];
     const float len_e = P.efunc[e];
-    if (!(len_e > 0.f)) continue;
-    const float pdf_e = (len_e / (P.eintegral * (float)P.ne)) / len_e;
+    if (!(len_e > 0.f)) return;
+    const float pdf_e = (len_e / (integral * (float)P.ne)) / len_e;
     const F3 Pa = load3(s.pos, v0), Pb = load3(s.pos, v1), Pc = load3(s.pos, v2);
     const F3 e1 = Pb - Pa;
     const F3 p0 = Pa + e1 * reuse;
@@ -755,8 +902,9 @@ __global__ void __launch_bounds__(128) k_indirect_adj(Params P) {
     }
     const float pdf = pdf_e * pdf_d;
     Hit he, hs;
-    if (!trace<false>(s, p0, -dir, kShadowEps, kRayMax, he, P.err)) continue;
-    if (!trace<false>(s, p0, dir, kShadowEps, kRayMax, hs, P.err)) continue;
+    cnt.v[kCntClosest] += 2;
+    if (!trace<false>(s, p0, -dir, kShadowEps, kRayMax, he, P.err)) return;
+    if (!trace<false>(s, p0, dir, kShadowEps, kRayMax, hs, P.err)) return;
     SurfF xe = post_intersect(s, he.tri, he.u, he.v);
     SurfF xs = post_intersect(s, hs.tri, hs.u, hs.v);
     const float dl = length(xe.p - xs.p);
@@ -764,7 +912,7 @@ __global__ void __launch_bounds__(128) k_indirect_adj(Params P) {
     const float its_t = length(xs.p - p0);
     F3 n;
     const float bval = base_val(its_t / dl, edge, -dir, xe.ng, edge2, n) * cos2;
-    if (bval == 0.f) continue;
+    if (bval == 0.f) return;
     const float e0 = bval / pdf;
     // emitter side: cumulative radiance per depth
     F3 rad[kMaxDepth];
@@ -778,8 +926,8 @@ __global__ void __launch_bounds__(128) k_indirect_adj(Params P) {
         if (alive) {
           const int o = 3 + 5 * b;
           F3 c;
-          alive = radiance_step(s, xx, rd, T, P.smp.get(o, p), P.smp.get(o + 1, p), P.smp.get(o + 2, p),
-                                P.smp.get(o + 3, p), P.smp.get(o + 4, p), c, nullptr);
+          alive = radiance_step(s, xx, rd, T, S(o), S(o + 1), S(o + 2),
+                                S(o + 3), S(o + 4), c, nullptr, cnt);
           cur = cur + c;
           if (T.x == 0.f && T.y == 0.f && T.z == 0.f) alive = false;
         }
@@ -795,30 +943,36 @@ __global__ void __launch_bounds__(128) k_indirect_adj(Params P) {
       for (int b = 0; b < D - 1; b++) {
         const int o = 3 + 5 * (D - 1) + 3 * b;
         F3 c; int pix;
-        const bool more = importance_step(s, P.cam, xx, rd, T, P.smp.get(o, p), P.smp.get(o + 1, p),
-                                          P.smp.get(o + 2, p), c, pix);
-        if (pix >= 0) W += dot(g_at(P, pix), rad[D - b - 2] * c) * e0;
+        const bool more = importance_step(s, cam, xx, rd, T, S(o), S(o + 1),
+                                          S(o + 2), c, pix, cnt);
+        if (pix >= 0) W += dot(g_at(P, V, pix), rad[D - b - 2] * c) * e0;
         if (!more) break;
       }
     }
-    if (W == 0.f || !isfinite(W)) continue;
-    xdotn_vjp(P, W, xs.p, true, hs.tri, hs.u, hs.v, v0, v1, reuse, p0, he.tri, n);
-  }
+    if (W == 0.f || !isfinite(W)) return;
+    xdotn_vjp(P, V, W, xs.p, true, hs.tri, hs.u, hs.v, v0, v1, reuse, p0, he.tri, n, cnt);
+  });
+  flush_cnt(cnt, P.stats);
 }
 
 // ---------------------------------------------------------------------------
 // pixel boundary (BoundaryPixel.cpp:36-159, Edge.cpp:377-409, Camera.cpp:433-467)
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128) k_pixel_adj(Params P) {
+__global__ void __launch_bounds__(256) k_pixel_adj(Params P) {
   const DeviceScene& s = P.s;
-  const int W_ = P.cam.w, WH = P.cam.w * P.cam.h;
-  const F3 cpos = cam_pos(P.cam);
-  const long long nanti = P.n / 4;
-  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < P.n;
-       p += (long long)gridDim.x * blockDim.x) {
+  Cnt cnt;
+  for_each_slot(P, [&](long long gslot) {
+    const ViewDesc& V = view_of(P, gslot);
+    const long long p = gslot - V.begin;
+    const CameraDesc& cam = V.cam;
+    const int W_ = cam.w, WH = cam.w * cam.h;
+    const F3 cpos = cam_pos(cam);
+    const long long nanti = V.n / 4;
     const long long slot = p % nanti;
     const int anti = (int)(p / nanti);
-    const float r = P.smp.get(0, slot);
+    // the 4 antithetic copies of a slot share its samples (BoundaryPixel.cpp:135-138)
+    const PathSmp S{&P, V.seed, V.begin / 4 + slot, slot + V.slot_off};
+    const float r = S(0);
     float rr;
     if (anti == 0) rr = r;
     else if (anti == 1) rr = r < 0.5f ? r + 0.5f : r - 0.5f;
@@ -831,22 +985,23 @@ __global__ void __launch_bounds__(128) k_pixel_adj(Params P) {
     else if (bi == 1) { ox = r4 - 1.f; oy = 1.f; }
     else if (bi == 2) { ox = 1.f; oy = 3.f - r4; }
     else { ox = 4.f - r4; oy = 0.f; }
-    const float pdfs[4] = {0.25f / (P.cam.plane_len_y * (float)P.cam.w), 0.25f / (P.cam.plane_len_x * (float)P.cam.h),
-                           0.25f / (P.cam.plane_len_y * (float)P.cam.w), 0.25f / (P.cam.plane_len_x * (float)P.cam.h)};
+    const float pdfs[4] = {0.25f / (cam.plane_len_y * (float)cam.w), 0.25f / (cam.plane_len_x * (float)cam.h),
+                           0.25f / (cam.plane_len_y * (float)cam.w), 0.25f / (cam.plane_len_x * (float)cam.h)};
     const int bsel = bi < 0 ? 0 : (bi > 3 ? 3 : bi);
     const float pdf = pdfs[bsel];
     const F3 dedge[4] = {F3(0.f, 1.f, 0.f), F3(1.f, 0.f, 0.f), F3(0.f, 1.f, 0.f), F3(1.f, 0.f, 0.f)};
     const F3 dvis[4] = {F3(1.f, 0.f, 0.f), F3(0.f, -1.f, 0.f), F3(-1.f, 0.f, 0.f), F3(0.f, 1.f, 0.f)};
-    const F3 edge = normalize(xform_vector(P.cam.raster_to_world, dedge[bsel]));
-    const F3 edge2 = normalize(xform_vector(P.cam.raster_to_world, dvis[bsel]));
+    const F3 edge = normalize(xform_vector(cam.raster_to_world, dedge[bsel]));
+    const F3 edge2 = normalize(xform_vector(cam.raster_to_world, dvis[bsel]));
     const int pixel = (int)(p % WH);
-    const F3 p0 = xform_point(P.cam.raster_to_world, F3((float)(pixel % W_) + ox, (float)(pixel / W_) + oy, 0.f));
+    const F3 p0 = xform_point(cam.raster_to_world, F3((float)(pixel % W_) + ox, (float)(pixel / W_) + oy, 0.f));
     const F3 dir = normalize(p0 - cpos);
     Hit h;
-    if (!trace<false>(s, p0, dir, kShadowEps, kRayMax, h, P.err)) continue;
+    cnt.v[kCntClosest]++;
+    if (!trace<false>(s, p0, dir, kShadowEps, kRayMax, h, P.err)) return;
     const F3 hitP = p0 + dir * h.t;
-    const SensorSample sds = sample_direct(P.cam, hitP);
-    const F3 dirc = sensor_ray_dir(P.cam, sds.qx, sds.qy);
+    const SensorSample sds = sample_direct(cam, hitP);
+    const F3 dirc = sensor_ray_dir(cam, sds.qx, sds.qy);
     SurfF x = post_intersect(s, h.tri, h.u, h.v);
     const float dist = length(x.p - cpos);
     const float dist1 = length(p0 - cpos);
@@ -854,33 +1009,38 @@ __global__ void __launch_bounds__(128) k_pixel_adj(Params P) {
     F3 n;
     // BoundaryPixel.cpp:92 reverses the sign convention
     const float bval = -base_val(dist / dist1, edge, dirc, x.ng, edge2, n) * cos2;
-    const F3 g = g_at(P, pixel);
-    if (bval == 0.f || (g.x == 0.f && g.y == 0.f && g.z == 0.f)) continue;
+    const F3 g = g_at(P, V, pixel);
+    if (bval == 0.f || (g.x == 0.f && g.y == 0.f && g.z == 0.f)) return;
     F3 T(sds.sensor_val, sds.sensor_val, sds.sensor_val);
     F3 rdir = dirc;
     F3 L = scrub(T * emitted(s, x, -rdir));
     for (int b = 0; b < P.D; b++) {
       const int o = 1 + 5 * b;
       F3 c;
-      const bool more = radiance_step(s, x, rdir, T, P.smp.get(o, slot), P.smp.get(o + 1, slot),
-                                      P.smp.get(o + 2, slot), P.smp.get(o + 3, slot), P.smp.get(o + 4, slot), c,
-                                      nullptr);
+      const bool more = radiance_step(s, x, rdir, T, S(o), S(o + 1),
+                                      S(o + 2), S(o + 3), S(o + 4), c,
+                                      nullptr, cnt);
       L = L + c;
       if (!more || (T.x == 0.f && T.y == 0.f && T.z == 0.f)) break;
     }
     const float Wt = dot(g, L * (bval / pdf));
-    if (Wt == 0.f || !isfinite(Wt)) continue;
+    if (Wt == 0.f || !isfinite(Wt)) return;
     // the pixel-edge point is not a scene parameter: only the hit triangle moves
-    xdotn_vjp(P, Wt, cpos, false, -1, 0.f, 0.f, -1, -1, 0.f, p0, h.tri, n);
-  }
+    xdotn_vjp(P, V, Wt, cpos, false, -1, 0.f, 0.f, -1, -1, 0.f, p0, h.tri, n, cnt);
+  });
+  flush_cnt(cnt, P.stats);
 }
 
 // ---------------------------------------------------------------------------
 // primary edge list for one camera (ConstructPrimEdgeList, Edge.cpp:313-348)
 // ---------------------------------------------------------------------------
-__global__ void k_prim_edges(int ne, const int* edges, const float* pos, const float* fn, F3 cpos, float* func) {
-  int e = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void k_prim_edges_views(int ne, const int* edges, const float* pos, const float* fn,
+                                   const ViewDesc* views, float* func_all) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  const int v = blockIdx.y;
   if (e >= ne) return;
+  const CameraDesc& c = views[v].cam;
+  const F3 cpos(c.pos[0], c.pos[1], c.pos[2]);
   const int v0 = edges[5 * e], v1 = edges[5 * e + 1], f0 = edges[5 * e + 2], f1 = edges[5 * e + 3];
   const F3 p0 = make_f3(pos + 3 * v0);
   const F3 ev = cpos - p0;
@@ -888,11 +1048,16 @@ __global__ void k_prim_edges(int ne, const int* edges, const float* pos, const f
   const F3 n1 = f1 >= 0 ? make_f3(fn + 3 * f1) : F3(0.f, 0.f, 0.f);
   const bool ff0 = dot(ev, n0) > 0.f, ff1 = dot(ev, n1) > 0.f;
   const bool valid = f1 < 0 || (ff0 != ff1);
-  func[e] = valid ? length(make_f3(pos + 3 * v1) - p0) : 0.f;
+  func_all[(long long)v * ne + e] = valid ? length(make_f3(pos + 3 * v1) - p0) : 0.f;
 }
 
-__global__ void k_cdf_single(int n, const float* func, float* cdf, float* integral_out) {
+// Distribution1D::SetFunction for one block per view (prefix sums in double)
+__global__ void k_cdf_views(int n, const float* func_all, float* cdf_all, float* integral_all) {
   __shared__ double part[1024];
+  __shared__ float integral;
+  const int v = blockIdx.x;
+  const float* func = func_all + (long long)v * n;
+  float* cdf = cdf_all + (long long)v * n;
   const int T = blockDim.x, tid = threadIdx.x;
   const int chunk = (n + T - 1) / T;
   const int a = min(n, tid * chunk), b = min(n, a + chunk);
@@ -906,10 +1071,35 @@ __global__ void k_cdf_single(int n, const float* func, float* cdf, float* integr
   double run = part[tid];
   for (int i = a; i < b; i++) { run += (double)func[i]; cdf[i] = (float)run * inv_size; }
   __syncthreads();
-  __shared__ float integral;
-  if (tid == 0) { integral = n > 0 ? cdf[n - 1] : 0.f; *integral_out = integral; }
+  if (tid == 0) { integral = n > 0 ? cdf[n - 1] : 0.f; integral_all[v] = integral; }
   __syncthreads();
   if (integral > 0.f) for (int i = a; i < b; i++) cdf[i] = cdf[i] / integral;
+}
+
+// 0.5 |I - T|^2 per view and dL/dI = I - T (pyTensorRay/loss.py:34-38)
+__global__ void k_view_loss(long long npix, const ViewDesc* views, const long long* pbegin, int nviews,
+                            const float* img, const float* tgt, float* dLdI, float* loss) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  float l = 0.f;
+  int v = -1;
+  if (i < npix) {
+    int lo = 0, hi = nviews - 1;
+    while (lo < hi) { const int mid = (lo + hi + 1) >> 1; if (pbegin[mid] <= i) lo = mid; else hi = mid - 1; }
+    v = lo;
+    for (int c = 0; c < 3; c++) {
+      const float d = img[3 * i + c] - tgt[3 * i + c];
+      if (dLdI) dLdI[3 * i + c] = d;
+      l += 0.5f * d * d;
+    }
+  }
+  // warp-aggregate per view
+  const unsigned m = __match_any_sync(0xffffffffu, v);
+  float sum = 0.f;
+  for (int k = 0; k < 32; k++) {
+    const float y = __shfl_sync(0xffffffffu, l, k);
+    if (m & (1u << k)) sum += y;
+  }
+  if (v >= 0 && (int)(threadIdx.x & 31) == __ffs(m) - 1 && loss) atomicAdd(loss + v, sum);
 }
 
 __global__ void k_intersect(DeviceScene s, int n, const float* org, const float* dir, const float* tmin,
@@ -931,21 +1121,39 @@ __global__ void k_occluded(DeviceScene s, int n, const float* org, const float* 
 
 using namespace trn;
 
+// A set of camera views rendered by one launch per integrator: the device view
+// table plus per-view silhouette-edge workspace.
+struct trn_viewset {
+  trn_scene* scene = nullptr;
+  int nviews = 0;
+  long long npix = 0;
+  std::vector<trn_view> h_views;
+  std::vector<long long> h_pbegin;
+  ViewDesc* views = nullptr;      // device [nviews]
+  long long* vbegin = nullptr;    // device [nviews], rewritten per integrator (spp differs)
+  long long* pbegin = nullptr;    // device [nviews] first pixel of each view
+  float* pfunc = nullptr;         // device [nviews][E]
+  float* pcdf = nullptr;          // device [nviews][E]
+  float* pint = nullptr;          // device [nviews]
+  unsigned long long* work = nullptr;
+  int ne = 0;
+  // slot layout currently uploaded: spp multiplier and per-view spp
+  int uploaded_key = -2;
+  long long total = 0;
+};
+
 namespace {
 
-int grid_for(long long n, int block) {
-  int dev = 0, sms = 148;
-  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  long long blocks = (n + block - 1) / block;
-  long long cap = (long long)sms * 16;
-  return (int)(blocks < cap ? (blocks < 1 ? 1 : blocks) : cap);
+int sms() {
+  int dev = 0, n = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+  return n;
 }
 
-int check_common(trn_scene* s, const trn_camera* cam, const trn_render_options* o, int integrator) {
-  if (!s || !cam || !o) { set_error("null argument"); return -1; }
+int check_common(trn_scene* s, const trn_render_options* o, int integrator) {
+  if (!s || !o) { set_error("null argument"); return -1; }
   if (!s->configured) { set_error("scene is not configured (call trn_scene_configure)"); return -1; }
   if (integrator < 0 || integrator > 4) { set_error("unknown integrator id"); return -1; }
-  if (cam->width <= 0 || cam->height <= 0) { set_error("invalid camera resolution"); return -1; }
   if (o->max_bounces < 0 || o->max_bounces > kMaxDepth) { set_error("max_bounces must be in [0, 16]"); return -1; }
   return 0;
 }
@@ -960,92 +1168,285 @@ int spp_of(const trn_render_options* o, int integrator) {
   }
 }
 
-Params make_params(trn_scene* s, const trn_camera* cam, const trn_render_options* o, int integrator,
-                   const trn_samples* smp) {
+// Upload the view table for one integrator: per-view spp comes from the view
+// (spp_override < 0) or from the options (single-view calls).
+int upload_views(trn_viewset* vs, const trn_render_options* o, int integrator, int spp_override, long long& total,
+                 cudaStream_t st) {
+  (void)o;
+  float* s_gpos = vs->scene->g_pos;
+  float* s_gvn = vs->scene->g_vnormal;
+  float* s_gtex = vs->scene->g_texels;
+  const int key = spp_override;  // the layout only depends on the per-view spp
+  if (vs->uploaded_key == key && key != -2) {
+    total = vs->total;
+    if (integrator == TRN_PIXEL_EDGE)
+      for (int v = 0; v < vs->nviews; v++) {
+        const int spp = spp_override >= 0 ? spp_override : vs->h_views[v].spp;
+        if (((long long)vs->h_views[v].camera.width * vs->h_views[v].camera.height * spp) % 4 != 0) {
+          set_error("pixel boundary needs W*H*spp divisible by 4");
+          return -1;
+        }
+      }
+    return 0;
+  }
+  std::vector<ViewDesc> d(vs->nviews);
+  std::vector<long long> begin(vs->nviews);
+  total = 0;
+  for (int v = 0; v < vs->nviews; v++) {
+    const trn_view& hv = vs->h_views[v];
+    const int spp = spp_override >= 0 ? spp_override : hv.spp;
+    if (spp < 0) { set_error("negative spp"); return -1; }
+    std::memcpy(&d[v].cam, &hv.camera, sizeof(CameraDesc));
+    d[v].begin = total;
+    d[v].n = (long long)hv.camera.width * hv.camera.height * spp;
+    if (integrator == TRN_PIXEL_EDGE && (d[v].n % 4) != 0) {
+      set_error("pixel boundary needs W*H*spp divisible by 4");
+      return -1;
+    }
+    d[v].pix_off = vs->h_pbegin[v];
+    d[v].inv_spp = hv.weight > 0.f ? hv.weight : (spp > 0 ? 1.0f / (float)spp : 0.f);
+    d[v].slot_off = hv.slot_offset;
+    d[v].gpos = hv.grad_positions ? hv.grad_positions : s_gpos;
+    d[v].gvn = hv.grad_vertex_normals ? hv.grad_vertex_normals : s_gvn;
+    d[v].gtex = hv.grad_texels ? hv.grad_texels : s_gtex;
+    d[v].seed = (uint32_t)hv.seed * 7919u + (uint32_t)v;
+    d[v].spp = spp;
+    d[v].pad_ = 0;
+    d[v].pfunc = vs->pfunc ? vs->pfunc + (long long)v * vs->ne : nullptr;
+    d[v].pcdf = vs->pcdf ? vs->pcdf + (long long)v * vs->ne : nullptr;
+    d[v].pint = vs->pint ? vs->pint + v : nullptr;
+    begin[v] = total;
+    total += d[v].n;
+  }
+  TRN_CUDA_TRY(cudaMemcpyAsync(vs->views, d.data(), sizeof(ViewDesc) * vs->nviews, cudaMemcpyHostToDevice, st));
+  TRN_CUDA_TRY(cudaMemcpyAsync(vs->vbegin, begin.data(), sizeof(long long) * vs->nviews, cudaMemcpyHostToDevice, st));
+  // the host vectors must outlive the async copies
+  TRN_CUDA_TRY(cudaStreamSynchronize(st));
+  vs->uploaded_key = key;
+  vs->total = total;
+  return 0;
+}
+
+Params base_params(trn_scene* s, trn_viewset* vs, const trn_render_options* o, int integrator,
+                   const trn_samples* smp, const trn_launch* ln, long long total) {
   Params P;
   P.s = s->view();
-  std::memcpy(&P.cam, cam, sizeof(CameraDesc));
-  const int spp = spp_of(o, integrator);
-  P.n = (long long)cam->width * cam->height * spp;
+  P.views = vs->views;
+  P.vbegin = vs->vbegin;
+  P.nviews = vs->nviews;
+  P.total = total;
+  P.work = vs->work;
+  P.chunk = (ln && ln->chunk > 0) ? ln->chunk : 1;
+  P.table = smp ? smp->samples : nullptr;
+  P.stride = smp && smp->samples ? smp->stride : 0;
+  P.term = (uint32_t)integrator;
+  P.seed = (uint32_t)o->seed;
   P.D = o->max_bounces;
-  P.inv_spp = spp > 0 ? 1.0f / (float)spp : 0.f;
-  P.smp.table = smp ? smp->samples : nullptr;
-  P.smp.stride = smp && smp->samples ? smp->stride : 0;
-  P.smp.seed = (uint32_t)o->seed;
-  P.smp.term = (uint32_t)integrator;
-  P.image = nullptr; P.dLdI = nullptr;
+  P.image = nullptr;
+  P.dLdI = nullptr;
   P.g_pos = s->g_pos; P.g_vn = s->g_vnormal; P.g_tex = s->g_texels; P.diff_tex = s->ntexel > 0;
-  P.edges = s->edges; P.ecdf = s->sec_cdf; P.efunc = s->sec_func; P.ne = s->ne; P.eintegral = 0.f;
+  P.edges = s->edges; P.ecdf = s->sec_cdf; P.efunc = s->sec_func; P.eint = s->sec_integral_dev; P.ne = s->ne;
   P.err = s->err;
+  P.stats = s->stats_on ? s->stats : nullptr;
   return P;
+}
+
+void launch_dims(const trn_launch* ln, long long total, int& grid, int& block) {
+  block = (ln && ln->block > 0) ? ln->block : 128;
+  const int per_sm = (ln && ln->blocks_per_sm > 0) ? ln->blocks_per_sm : 1024 / block;
+  const long long chunk = (ln && ln->chunk > 0) ? ln->chunk : 1;
+  long long want = (long long)sms() * per_sm;
+  const long long need = (total + 32 * chunk - 1) / (32 * chunk) * 32 / block + 1;
+  grid = (int)std::max<long long>(1, std::min(want, need));
+}
+
+int validate_launch(const trn_launch* ln) {
+  if (!ln) return 0;
+  if (ln->block != 0 && (ln->block < 32 || ln->block > 256 || ln->block % 32 != 0)) {
+    set_error("launch block must be a multiple of 32 in [32, 256]");
+    return -1;
+  }
+  if (ln->blocks_per_sm < 0 || ln->blocks_per_sm > 64 || ln->chunk < 0 || ln->chunk > 64) {
+    set_error("launch blocks_per_sm must be in [0, 64] and chunk in [0, 64]");
+    return -1;
+  }
+  return 0;
+}
+
+template <class K>
+void launch(K kernel, const trn_launch* ln, long long total, const Params& P, cudaStream_t st) {
+  int grid, block;
+  launch_dims(ln, total, grid, block);
+  kernel<<<grid, block, 0, st>>>(P);
+  count_launch(1);
+}
+
+int render_views(trn_scene* s, trn_viewset* vs, const trn_render_options* o, int integrator,
+                 const trn_samples* smp, const trn_launch* ln, int spp_override, float* image, const float* dLdI,
+                 cudaStream_t st) {
+  if (check_common(s, o, integrator)) return -1;
+  if (!vs || vs->nviews <= 0) { set_error("empty view set"); return -1; }
+  if (validate_launch(ln)) return -1;
+  long long total = 0;
+  if (upload_views(vs, o, integrator, spp_override, total, st)) return -1;
+  Params P = base_params(s, vs, o, integrator, smp, ln, total);
+  const long long slots = integrator == TRN_PIXEL_EDGE ? total / 4 : total;
+  if (P.table && P.stride < slots) { set_error("sample table too small"); return -1; }
+  if (image) {
+    TRN_CUDA_TRY(cudaMemsetAsync(image, 0, sizeof(float) * 3 * vs->npix, st));
+    if (integrator != TRN_PATH_TRACER || total == 0) return 0;  // edge terms have no primal image
+    P.image = image;
+    TRN_CUDA_TRY(cudaMemsetAsync(vs->work, 0, sizeof(unsigned long long), st));
+    launch(k_path_fwd, ln, total, P, st);
+    TRN_CUDA_TRY(cudaGetLastError());
+    return 0;
+  }
+  if (total == 0) return 0;
+  P.dLdI = dLdI;
+  s->grads_finalized = false;
+  if (integrator == TRN_PRIMARY_EDGE) {
+    if (s->ne == 0) return 0;
+    dim3 g((s->ne + 255) / 256, vs->nviews);
+    k_prim_edges_views<<<g, 256, 0, st>>>(s->ne, s->edges, s->pos, s->fnormal, vs->views, vs->pfunc);
+    k_cdf_views<<<vs->nviews, 1024, 0, st>>>(s->ne, vs->pfunc, vs->pcdf, vs->pint);
+    count_launch(2);
+  } else if ((integrator == TRN_DIRECT_EDGE || integrator == TRN_INDIRECT_EDGE) && s->ne == 0) {
+    return 0;
+  }
+  TRN_CUDA_TRY(cudaMemsetAsync(vs->work, 0, sizeof(unsigned long long), st));
+  switch (integrator) {
+    case TRN_PATH_TRACER: launch(k_path_adj, ln, total, P, st); break;
+    case TRN_PRIMARY_EDGE: launch(k_primary_adj, ln, total, P, st); break;
+    case TRN_DIRECT_EDGE: launch(k_direct_adj, ln, total, P, st); break;
+    case TRN_INDIRECT_EDGE: launch(k_indirect_adj, ln, total, P, st); break;
+    default: launch(k_pixel_adj, ln, total, P, st); break;
+  }
+  TRN_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+int single_view(trn_scene* s, const trn_camera* cam, trn_viewset** out) {
+  if (!cam) { set_error("null camera"); return -1; }
+  trn_view v;
+  std::memset(&v, 0, sizeof(v));
+  std::memcpy(&v.camera, cam, sizeof(trn_camera));
+  return trn_viewset_create(s, 1, &v, out);
 }
 
 }  // namespace
 
 extern "C" {
 
-int trn_render_fwd(trn_scene* s, const trn_camera* cam, const trn_render_options* o, int integrator,
-                   const trn_samples* smp, float* image, cudaStream_t st) {
-  if (check_common(s, cam, o, integrator)) return -1;
-  if (!image) { set_error("trn_render_fwd: null image"); return -1; }
-  TRN_CUDA_TRY(cudaMemsetAsync(image, 0, sizeof(float) * 3 * cam->width * cam->height, st));
-  if (integrator != TRN_PATH_TRACER) return 0;  // edge terms have no primal image
-  Params P = make_params(s, cam, o, integrator, smp);
-  if (P.n == 0) return 0;
-  if (P.smp.table && P.smp.stride < P.n) { set_error("trn_render_fwd: sample table too small"); return -1; }
-  P.image = image;
-  k_path_fwd<<<grid_for(P.n, 128), 128, 0, st>>>(P);
+int trn_viewset_create(trn_scene* s, int nviews, const trn_view* views, trn_viewset** out) {
+  if (!s || !views || !out || nviews <= 0) { set_error("trn_viewset_create: invalid arguments"); return -1; }
+  *out = nullptr;
+  trn_viewset* vs = new trn_viewset();
+  vs->scene = s;
+  vs->nviews = nviews;
+  vs->h_views.assign(views, views + nviews);
+  vs->ne = s->ne;
+  long long pix = 0;
+  for (int v = 0; v < nviews; v++) {
+    const trn_view& hv = views[v];
+    if (hv.camera.width <= 0 || hv.camera.height <= 0) {
+      set_error("trn_viewset_create: invalid camera resolution");
+      delete vs;
+      return -1;
+    }
+    const long long off = hv.pixel_offset >= 0 ? hv.pixel_offset : pix;
+    vs->h_pbegin.push_back(off);
+    pix = std::max(pix, off + (long long)hv.camera.width * hv.camera.height);
+  }
+  for (int v = 1; v < nviews; v++)
+    if (vs->h_pbegin[v] < vs->h_pbegin[v - 1]) {
+      set_error("trn_viewset_create: pixel offsets must be non-decreasing");
+      delete vs;
+      return -1;
+    }
+  vs->npix = pix;
+  auto fail = [&](const char* what) {
+    set_error(std::string("trn_viewset_create: ") + what);
+    trn_viewset_destroy(vs);
+    return -1;
+  };
+  if (cudaMalloc(&vs->views, sizeof(ViewDesc) * nviews) != cudaSuccess) return fail("out of memory");
+  if (cudaMalloc(&vs->vbegin, sizeof(long long) * nviews) != cudaSuccess) return fail("out of memory");
+  if (cudaMalloc(&vs->pbegin, sizeof(long long) * nviews) != cudaSuccess) return fail("out of memory");
+  if (cudaMalloc(&vs->work, sizeof(unsigned long long)) != cudaSuccess) return fail("out of memory");
+  if (cudaMemcpy(vs->pbegin, vs->h_pbegin.data(), sizeof(long long) * nviews, cudaMemcpyHostToDevice) != cudaSuccess)
+    return fail("copy failed");
+  if (s->ne > 0) {
+    const size_t n = (size_t)nviews * s->ne;
+    if (cudaMalloc(&vs->pfunc, sizeof(float) * n) != cudaSuccess) return fail("out of memory");
+    if (cudaMalloc(&vs->pcdf, sizeof(float) * n) != cudaSuccess) return fail("out of memory");
+  }
+  if (cudaMalloc(&vs->pint, sizeof(float) * nviews) != cudaSuccess) return fail("out of memory");
+  cudaMemset(vs->pint, 0, sizeof(float) * nviews);
+  *out = vs;
+  return 0;
+}
+
+int trn_viewset_destroy(trn_viewset* vs) {
+  if (!vs) return 0;
+  void* ptrs[] = {vs->views, vs->vbegin, vs->pbegin, vs->pfunc, vs->pcdf, vs->pint, vs->work};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  delete vs;
+  return 0;
+}
+
+int trn_viewset_num_pixels(const trn_viewset* vs, long long* npix) {
+  if (!vs || !npix) { set_error("trn_viewset_num_pixels: null argument"); return -1; }
+  *npix = vs->npix;
+  return 0;
+}
+
+int trn_render_views_fwd(trn_scene* s, trn_viewset* vs, const trn_render_options* o, int integrator,
+                         const trn_samples* smp, const trn_launch* ln, float* images, cudaStream_t st) {
+  if (!images) { set_error("trn_render_views_fwd: null image"); return -1; }
+  return render_views(s, vs, o, integrator, smp, ln, -1, images, nullptr, st);
+}
+
+int trn_render_views_grad(trn_scene* s, trn_viewset* vs, const trn_render_options* o, int integrator,
+                          const trn_samples* smp, const trn_launch* ln, const float* dLdI, cudaStream_t st) {
+  if (!dLdI) { set_error("trn_render_views_grad: null dLdI"); return -1; }
+  return render_views(s, vs, o, integrator, smp, ln, -1, nullptr, dLdI, st);
+}
+
+int trn_views_loss(trn_viewset* vs, const float* images, const float* targets, float* dLdI, float* loss,
+                   cudaStream_t st) {
+  if (!vs || !images || !targets) { set_error("trn_views_loss: null argument"); return -1; }
+  if (loss) TRN_CUDA_TRY(cudaMemsetAsync(loss, 0, sizeof(float) * vs->nviews, st));
+  const long long n = vs->npix;
+  k_view_loss<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, vs->views, vs->pbegin, vs->nviews, images, targets,
+                                                          dLdI, loss);
+  count_launch(1);
   TRN_CUDA_TRY(cudaGetLastError());
   return 0;
 }
 
+int trn_render_fwd(trn_scene* s, const trn_camera* cam, const trn_render_options* o, int integrator,
+                   const trn_samples* smp, float* image, cudaStream_t st) {
+  if (check_common(s, o, integrator)) return -1;
+  if (!image) { set_error("trn_render_fwd: null image"); return -1; }
+  trn_viewset* vs = nullptr;
+  if (single_view(s, cam, &vs)) return -1;
+  const int rc = render_views(s, vs, o, integrator, smp, nullptr, spp_of(o, integrator), image, nullptr, st);
+  cudaStreamSynchronize(st);
+  trn_viewset_destroy(vs);
+  return rc;
+}
+
 int trn_render_grad(trn_scene* s, const trn_camera* cam, const trn_render_options* o, int integrator,
                     const trn_samples* smp, const float* dLdI, cudaStream_t st) {
-  if (check_common(s, cam, o, integrator)) return -1;
+  if (check_common(s, o, integrator)) return -1;
   if (!dLdI) { set_error("trn_render_grad: null dLdI"); return -1; }
-  Params P = make_params(s, cam, o, integrator, smp);
-  if (P.n == 0) return 0;
-  const long long slots = integrator == TRN_PIXEL_EDGE ? P.n / 4 : P.n;
-  if (P.smp.table && P.smp.stride < slots) { set_error("trn_render_grad: sample table too small"); return -1; }
-  if (integrator == TRN_PIXEL_EDGE && (P.n % 4) != 0) { set_error("pixel boundary needs W*H*spp divisible by 4"); return -1; }
-  P.dLdI = dLdI;
-  s->grads_finalized = false;
-  float* tmp = nullptr;
-  float* integral_dev = nullptr;
-  if (integrator == TRN_PRIMARY_EDGE) {
-    // per-camera silhouette list (ConstructPrimEdgeList)
-    if (s->ne == 0) return 0;
-    TRN_CUDA_TRY(cudaMallocAsync((void**)&tmp, sizeof(float) * (2 * (size_t)s->ne + 1), st));
-    float* func = tmp;
-    float* cdf = tmp + s->ne;
-    integral_dev = tmp + 2 * (size_t)s->ne;
-    const F3 cpos(cam->pos[0], cam->pos[1], cam->pos[2]);
-    k_prim_edges<<<(s->ne + 255) / 256, 256, 0, st>>>(s->ne, s->edges, s->pos, s->fnormal, cpos, func);
-    k_cdf_single<<<1, 1024, 0, st>>>(s->ne, func, cdf, integral_dev);
-    float integral = 0.f;
-    TRN_CUDA_TRY(cudaMemcpyAsync(&integral, integral_dev, sizeof(float), cudaMemcpyDeviceToHost, st));
-    TRN_CUDA_TRY(cudaStreamSynchronize(st));
-    if (!(integral > 0.f)) { cudaFreeAsync(tmp, st); return 0; }
-    P.ecdf = cdf; P.efunc = func; P.eintegral = integral;
-  } else if (integrator == TRN_DIRECT_EDGE || integrator == TRN_INDIRECT_EDGE) {
-    if (s->ne == 0) return 0;
-    float integral = 0.f;
-    TRN_CUDA_TRY(cudaMemcpyAsync(&integral, s->sec_integral_dev, sizeof(float), cudaMemcpyDeviceToHost, st));
-    TRN_CUDA_TRY(cudaStreamSynchronize(st));
-    if (!(integral > 0.f)) return 0;
-    P.eintegral = integral;
-  }
-  const int g = grid_for(P.n, 128);
-  switch (integrator) {
-    case TRN_PATH_TRACER: k_path_adj<<<g, 128, 0, st>>>(P); break;
-    case TRN_PRIMARY_EDGE: k_primary_adj<<<g, 128, 0, st>>>(P); break;
-    case TRN_DIRECT_EDGE: k_direct_adj<<<g, 128, 0, st>>>(P); break;
-    case TRN_INDIRECT_EDGE: k_indirect_adj<<<g, 128, 0, st>>>(P); break;
-    default: k_pixel_adj<<<g, 128, 0, st>>>(P); break;
-  }
-  TRN_CUDA_TRY(cudaGetLastError());
-  if (tmp) TRN_CUDA_TRY(cudaFreeAsync(tmp, st));
-  return 0;
+  trn_viewset* vs = nullptr;
+  if (single_view(s, cam, &vs)) return -1;
+  const int rc = render_views(s, vs, o, integrator, smp, nullptr, spp_of(o, integrator), nullptr, dLdI, st);
+  cudaStreamSynchronize(st);
+  trn_viewset_destroy(vs);
+  return rc;
 }
 
 int trn_intersect(trn_scene* s, int n, const float* org, const float* dir, const float* tmin, const float* tmax,
@@ -1054,6 +1455,7 @@ int trn_intersect(trn_scene* s, int n, const float* org, const float* dir, const
   if (n <= 0) return 0;
   if (!org || !dir || !tmin || !tmax || !tri || !u || !v || !t) { set_error("trn_intersect: null argument"); return -1; }
   k_intersect<<<(n + 127) / 128, 128, 0, st>>>(s->view(), n, org, dir, tmin, tmax, tri, u, v, t, s->err);
+  count_launch(1);
   TRN_CUDA_TRY(cudaGetLastError());
   return 0;
 }
@@ -1064,6 +1466,7 @@ int trn_occluded(trn_scene* s, int n, const float* org, const float* dir, const 
   if (n <= 0) return 0;
   if (!org || !dir || !tmin || !tmax || !vis) { set_error("trn_occluded: null argument"); return -1; }
   k_occluded<<<(n + 127) / 128, 128, 0, st>>>(s->view(), n, org, dir, tmin, tmax, vis);
+  count_launch(1);
   TRN_CUDA_TRY(cudaGetLastError());
   return 0;
 }

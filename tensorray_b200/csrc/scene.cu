@@ -13,6 +13,7 @@
 #include <cub/cub.cuh>
 #include <algorithm>
 #include <cstring>
+#include <atomic>
 #include <mutex>
 #include <numeric>
 #include <string>
@@ -26,6 +27,8 @@ namespace trn {
 
 static thread_local std::string g_err;
 void set_error(const std::string& msg) { g_err = msg; }
+static std::atomic<unsigned long long> g_launches{0};
+void count_launch(int n) { g_launches.fetch_add((unsigned long long)n, std::memory_order_relaxed); }
 
 static_assert(sizeof(trn_camera) == sizeof(CameraDesc), "camera layout");
 static_assert(sizeof(trn_bsdf) == sizeof(BsdfDesc), "bsdf layout");
@@ -630,7 +633,8 @@ int trn_scene_create(const trn_scene_desc* d, trn_scene** out) {
       dev_alloc_copy(&s->g_vnormal, (const float*)nullptr, 3 * (size_t)nv) ||
       dev_alloc_copy(&s->g_texels, (const float*)nullptr, std::max<size_t>(3, 3 * (size_t)ntexel)) ||
       dev_alloc_copy(&s->g_translation, (const float*)nullptr, 3 * (size_t)nm) ||
-      dev_alloc_copy(&s->err, (const int*)nullptr, 1))
+      dev_alloc_copy(&s->err, (const int*)nullptr, 1) ||
+      dev_alloc_copy(&s->stats, (const unsigned long long*)nullptr, 16))
     return fail();
   if (d->uvs && d->uv_indices && d->num_uvs > 0) {
     s->nuv = d->num_uvs;
@@ -655,7 +659,8 @@ int trn_scene_destroy(trn_scene* s) {
                   s->emit_tris, s->tri_to_emit, s->light_func, s->light_cdf, s->light_radiance,
                   s->light_integral_dev, s->bsdfs, s->texs, s->edges, s->sec_func, s->sec_cdf,
                   s->sec_integral_dev, s->nodes, s->tri_verts, s->parent, s->flags, s->keys, s->keys_alt,
-                  s->sort_tmp, s->bounds, s->g_pos, s->g_vnormal, s->g_texels, s->g_translation, s->err};
+                  s->sort_tmp, s->bounds, s->g_pos, s->g_vnormal, s->g_texels, s->g_translation, s->err,
+                  s->stats};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   delete s;
@@ -668,6 +673,7 @@ int trn_scene_configure(trn_scene* s, cudaStream_t st) {
   k_transform<<<nblk(nv), 256, 0, st>>>(nv, s->raw_pos, s->vert_mesh, s->translation, s->pos);
   k_face<<<nblk(nt), 256, 0, st>>>(nt, s->pos, s->idx, s->fnormal, s->area);
   k_vnormal<<<nblk(nv), 256, 0, st>>>(nv, s->vf_off, s->vf_list, s->fnormal, s->vnormal);
+  count_launch(3);
   // merged light distribution
   if (s->n_emit > 0) {
     float* lum_dev = nullptr;
@@ -676,19 +682,20 @@ int trn_scene_configure(trn_scene* s, cudaStream_t st) {
     k_light_func<<<nblk(s->n_emit), 256, 0, st>>>(s->n_emit, s->emit_tris, s->emitter_id, lum_dev, s->area,
                                                    s->light_func);
     k_cdf<<<1, 1024, 0, st>>>(s->n_emit, s->light_func, s->light_cdf, s->light_integral_dev);
+    count_launch(2);
     TRN_CUDA_TRY(cudaFreeAsync(lum_dev, st));
-    TRN_CUDA_TRY(cudaMemcpyAsync(&s->h_light_integral, s->light_integral_dev, sizeof(float),
-                                 cudaMemcpyDeviceToHost, st));
   }
   // secondary edge list
   if (s->ne > 0) {
     k_sec_edges<<<nblk(s->ne), 256, 0, st>>>(s->ne, s->edges, s->pos, s->fnormal, s->sec_func);
     k_cdf<<<1, 1024, 0, st>>>(s->ne, s->sec_func, s->sec_cdf, s->sec_integral_dev);
+    count_launch(2);
   }
   // LBVH
   k_bounds_init<<<1, 32, 0, st>>>((unsigned int*)s->bounds);
   k_bounds<<<nblk(nt), 256, 0, st>>>(nt, s->pos, s->idx, (unsigned int*)s->bounds);
   k_morton<<<nblk(nt), 256, 0, st>>>(nt, s->pos, s->idx, (const unsigned int*)s->bounds, s->keys);
+  count_launch(4);  // bounds init, bounds, morton, and the radix sort counted as one
   size_t bytes = s->sort_tmp_bytes;
   if (cub::DeviceRadixSort::SortKeys(s->sort_tmp, bytes, s->keys, s->keys_alt, nt, 0, 64, st) != cudaSuccess) {
     set_error("trn_scene_configure: radix sort failed");
@@ -697,8 +704,10 @@ int trn_scene_configure(trn_scene* s, cudaStream_t st) {
   if (nt > 1) {
     TRN_CUDA_TRY(cudaMemsetAsync(s->flags, 0, sizeof(int) * (nt - 1), st));
     k_karras<<<nblk(nt - 1), 256, 0, st>>>(nt, s->keys_alt, s->nodes, s->parent);
+    count_launch(1);
   }
   k_refit<<<nblk(nt), 256, 0, st>>>(nt, s->keys_alt, s->pos, s->idx, s->nodes, s->parent, s->flags, s->tri_verts);
+  count_launch(1);
   TRN_CUDA_TRY(cudaGetLastError());
   TRN_CUDA_TRY(cudaStreamSynchronize(st));
   s->configured = true;
@@ -743,6 +752,41 @@ int trn_scene_counts(const trn_scene* s, int* nv, int* nt, int* ne, long long* n
   return 0;
 }
 
+unsigned long long trn_kernel_launches(void) { return g_launches.load(); }
+
+int trn_scene_finalize_grads(trn_scene* s, float* gpos, float* gvn, float* d_translation, cudaStream_t st) {
+  if (!s || !gpos || !gvn) { set_error("trn_scene_finalize_grads: null argument"); return -1; }
+  const int nv = s->nv, nt = s->nt;
+  float* g_sum = nullptr;
+  TRN_CUDA_TRY(cudaMallocAsync((void**)&g_sum, sizeof(float) * 3 * nv, st));
+  k_vnormal_adj<<<nblk(nv), 256, 0, st>>>(nv, s->vf_off, s->vf_list, s->fnormal, gvn, g_sum);
+  k_face_adj<<<nblk(nt), 256, 0, st>>>(nt, s->pos, s->idx, g_sum, gpos);
+  count_launch(2);
+  TRN_CUDA_TRY(cudaFreeAsync(g_sum, st));
+  TRN_CUDA_TRY(cudaMemsetAsync(gvn, 0, sizeof(float) * 3 * nv, st));
+  if (d_translation) {
+    TRN_CUDA_TRY(cudaMemsetAsync(d_translation, 0, sizeof(float) * 3 * s->nmesh, st));
+    k_translation_adj<<<nblk(nv), 256, 0, st>>>(nv, s->vert_mesh, gpos, d_translation);
+    count_launch(1);
+  }
+  TRN_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+int trn_stats_enable(trn_scene* s, int on) {
+  if (!s) { set_error("trn_stats_enable: null scene"); return -1; }
+  s->stats_on = on != 0;
+  return 0;
+}
+
+int trn_stats_read(trn_scene* s, unsigned long long* out, int reset, cudaStream_t st) {
+  if (!s || !out) { set_error("trn_stats_read: null argument"); return -1; }
+  TRN_CUDA_TRY(cudaMemcpyAsync(out, s->stats, sizeof(unsigned long long) * 16, cudaMemcpyDeviceToHost, st));
+  TRN_CUDA_TRY(cudaStreamSynchronize(st));
+  if (reset) TRN_CUDA_TRY(cudaMemsetAsync(s->stats, 0, sizeof(unsigned long long) * 16, st));
+  return 0;
+}
+
 int trn_scene_clear_grads(trn_scene* s, cudaStream_t st) {
   if (!s) { set_error("trn_scene_clear_grads: null scene"); return -1; }
   TRN_CUDA_TRY(cudaMemsetAsync(s->g_pos, 0, sizeof(float) * 3 * s->nv, st));
@@ -767,6 +811,7 @@ int trn_scene_get_grads(trn_scene* s, float* d_translation, float* d_positions, 
     TRN_CUDA_TRY(cudaMemsetAsync(s->g_vnormal, 0, sizeof(float) * 3 * nv, st));
     TRN_CUDA_TRY(cudaMemsetAsync(s->g_translation, 0, sizeof(float) * 3 * s->nmesh, st));
     k_translation_adj<<<nblk(nv), 256, 0, st>>>(nv, s->vert_mesh, s->g_pos, s->g_translation);
+    count_launch(3);
     TRN_CUDA_TRY(cudaGetLastError());
     s->grads_finalized = true;
   }

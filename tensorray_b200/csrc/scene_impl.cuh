@@ -63,6 +63,8 @@ struct trn_scene {
   float* g_texels = nullptr;      // [ntexel][3]
   float* g_translation = nullptr; // [M][3]
   int* err = nullptr;             // device error word
+  unsigned long long* stats = nullptr;  // [16] work counters of the integrator kernels
+  bool stats_on = false;
   float h_light_integral = 0.f;
   bool configured = false;
   bool grads_finalized = true;
@@ -73,7 +75,7 @@ struct trn_scene {
     s.pos = pos; s.idx = idx; s.fnormal = fnormal; s.area = area; s.vnormal = vnormal;
     s.smooth = smooth; s.uv = uv; s.uvidx = uvidx; s.bsdf_id = bsdf_id; s.emitter_id = emitter_id;
     s.n_emit = n_emit; s.emit_tris = emit_tris; s.tri_to_emit = tri_to_emit;
-    s.light_func = light_func; s.light_cdf = light_cdf; s.light_integral = h_light_integral;
+    s.light_func = light_func; s.light_cdf = light_cdf; s.light_integral = light_integral_dev;
     s.light_radiance = light_radiance;
     s.n_bsdf = nbsdf; s.bsdfs = bsdfs; s.texs = texs; s.texels = texels;
     s.nodes = nodes; s.tri_verts = tri_verts; s.root_is_leaf = nt == 1;
@@ -83,6 +85,7 @@ struct trn_scene {
 
 namespace trn {
 void set_error(const std::string& msg);
+void count_launch(int n = 1);  // host-side count of this library's kernel launches
 }
 
 #define TRN_CUDA_TRY(expr)                                                        \

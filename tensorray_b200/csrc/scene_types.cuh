@@ -60,7 +60,7 @@ struct DeviceScene {
   const int* tri_to_emit;     // [T] index into emit_tris or -1
   const float* light_func;    // [n_emit] luminance * area (detached)
   const float* light_cdf;     // [n_emit] normalised inclusive CDF
-  float light_integral;       // Distribution1D::mIntegralVal
+  const float* light_integral;  // Distribution1D::mIntegralVal (device scalar)
   const float* light_radiance;// [n_lights][3]
   // materials
   int n_bsdf;
@@ -86,6 +86,28 @@ struct CameraDesc {
   float raster_to_world[16];
   float inv_area;            // Camera::mInvArea
   float plane_len_x, plane_len_y;
+};
+
+// One camera view of a batched launch. Path slots of all views are
+// concatenated: view v owns slots [begin, begin + n) with n = W*H*spp, and
+// its pixels start at pix_off in the image / dL/dI buffers.
+struct ViewDesc {
+  CameraDesc cam;
+  long long begin;
+  long long n;
+  long long pix_off;
+  long long slot_off;  // added to the view-local slot of the hash sampler
+  float inv_spp;       // contribution weight (1/spp of the whole render)
+  uint32_t seed;
+  int spp;
+  int pad_;
+  float* gpos;         // gradient destinations of this view
+  float* gvn;
+  float* gtex;
+  // silhouette-edge distribution of this view (ConstructPrimEdgeList)
+  const float* pfunc;
+  const float* pcdf;
+  const float* pint;
 };
 
 }  // namespace trn

@@ -304,7 +304,7 @@ TRN_D bool light_sample(const DeviceScene& s, float s0, float s1, LightSample& l
   if (s.n_emit <= 0) return false;
   float reuse;
   const int e = sample_discrete(s.light_cdf, s.n_emit, s0, reuse);
-  const float pmf = s.light_func[e] / (s.light_integral * (float)s.n_emit);
+  const float pmf = s.light_func[e] / (__ldg(s.light_integral) * (float)s.n_emit);
   const float t = sqrtf(reuse);
   ls.bu = 1.f - t;
   ls.bv = t * s1;
@@ -318,7 +318,7 @@ TRN_D bool light_sample(const DeviceScene& s, float s0, float s1, LightSample& l
 TRN_D float light_pdf(const DeviceScene& s, int tri) {
   const int e = s.tri_to_emit[tri];
   if (e < 0) return 0.f;
-  const float pmf = s.light_func[e] / (s.light_integral * (float)s.n_emit);
+  const float pmf = s.light_func[e] / (__ldg(s.light_integral) * (float)s.n_emit);
   return pmf / s.area[tri];
 }
 

@@ -1,0 +1,86 @@
+"""Batched multi-view launches equal the per-view calls they replace
+(pyTensorRay/renderer_multi_view.py:53-61 loops over views one at a time)."""
+import pytest
+import torch
+
+from oracle import tr_oracle as O
+from tensorray_b200 import api, scenes
+from tests.helpers import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+D = 3
+
+
+@pytest.fixture(scope="module")
+def setup(built_lib):
+    spec = scenes.config1_scene(32, 32)
+    scene = api.Scene(spec)
+    scene.configure()
+    cams = [api.Camera(c.pos, c.target, c.up, c.width, c.height, c.fov)
+            for c in scenes.fibonacci_cameras(5, 4.0, [16, 24, 32], seed=3)]
+    spps = [2, 4, 2, 4, 2]
+    return scene, cams, spps
+
+
+def _tables(integ, cams, spps, seed):
+    per = [O.uniform_table(seed + 17 * i, api.sample_dims(integ, D), api.sample_slots(integ, c.width, c.height, s))
+           for i, (c, s) in enumerate(zip(cams, spps))]
+    return per, torch.cat(per, 1).contiguous()
+
+
+def test_batched_forward_equals_per_view(setup):
+    scene, cams, spps = setup
+    vs = api.ViewSet(scene, cams, spps)
+    per, cat = _tables(0, cams, spps, 1)
+    opts = api.RenderOptions(0, D, 0, 0, 0, 0, 0)
+    img = vs.render(0, opts, samples=cat.cuda())
+    for v, (c, s) in enumerate(zip(cams, spps)):
+        o = api.RenderOptions(0, D, s, 0, 0, 0, 0)
+        ref = api.PathTracer().renderC(scene, o, samples=per[v].cuda(), camera=c)
+        torch.testing.assert_close(vs.view_image(img, v), ref, rtol=1e-5, atol=1e-6)
+
+
+@pytest.mark.parametrize("integ", [0, 1, 2, 3, 4])
+def test_batched_grads_equal_sum_of_per_view(setup, integ):
+    scene, cams, spps = setup
+    vs = api.ViewSet(scene, cams, spps)
+    per, cat = _tables(integ, cams, spps, 5)
+    g = torch.Generator().manual_seed(1)
+    dLdI = (torch.rand(vs.npix, 3, generator=g) - 0.3).cuda()
+    opts = api.RenderOptions(0, D, 0, 0, 0, 0, 0)
+    scene.clear_grads()
+    vs.render_grad(integ, opts, dLdI, samples=cat.cuda())
+    gb = scene.get_grads()["positions"].clone()
+    scene.clear_grads()
+    cls = [api.PathTracer, api.PrimaryEdgeIntegrator, api.DirectEdgeIntegrator, api.IndirectEdgeIntegrator,
+           api.PixelBoundaryIntegrator][integ]
+    for v, (c, s) in enumerate(zip(cams, spps)):
+        o = api.RenderOptions(0, D, s, s, s, s, s)
+        cls().renderD(scene, o, vs.view_image(dLdI, v), samples=per[v].cuda(), camera=c)
+    gs = scene.get_grads()["positions"]
+    assert float(gs.abs().sum()) > 0
+    assert rel_l2(gb.cpu(), gs.cpu()) < 1e-5
+
+
+def test_view_loss_matches_torch(setup):
+    scene, cams, spps = setup
+    vs = api.ViewSet(scene, cams, spps)
+    img = torch.rand(vs.npix, 3, device="cuda")
+    tgt = torch.rand(vs.npix, 3, device="cuda")
+    d = torch.empty_like(img)
+    loss = vs.loss(img, tgt, d)
+    torch.testing.assert_close(d, img - tgt)
+    for v in range(len(cams)):
+        ref = 0.5 * ((vs.view_image(img, v) - vs.view_image(tgt, v)) ** 2).sum()
+        torch.testing.assert_close(loss[v], ref, rtol=1e-4, atol=1e-4)
+
+
+def test_launch_configs_give_same_image(setup):
+    scene, cams, spps = setup
+    vs = api.ViewSet(scene, cams, spps)
+    opts = api.RenderOptions(4, D, 0, 0, 0, 0, 0)
+    ref = vs.render(0, opts)
+    for blk, per_sm, chunk in [(64, 8, 1), (256, 4, 4), (128, 16, 2)]:
+        img = vs.render(0, opts, launch=api.launch_config(blk, per_sm, chunk))
+        torch.testing.assert_close(img, ref, rtol=1e-5, atol=1e-6)
