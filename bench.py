@@ -63,6 +63,10 @@ def parse():
     ap.add_argument("--tris", type=int, default=100_000)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--quick", action="store_true", help="small smoke-sized run")
+    ap.add_argument("--requests", type=int, default=48, help="serve workload: number of requests")
+    ap.add_argument("--workload", default="single", choices=["single", "views", "serve"],
+                    help="single: the 100K-triangle single-view config; views: 32 batched views "
+                         "of the icosphere scene against the plain per-view form")
     return ap.parse_args()
 
 
@@ -182,6 +186,10 @@ def main():
         a.res, a.spp, a.tris = 128, 4, 20_000
     if a.impl == "reference":
         return run_reference(a)
+    if a.workload == "views":
+        return run_views(a)
+    if a.workload == "serve":
+        return run_serve(a)
     import torch.distributed as dist
     from tensorray_b200 import api, scenes
     from tensorray_b200 import autograd as tra
@@ -202,7 +210,8 @@ def main():
     scene.configure()
     sphere = scene.shapes[0]
     D = a.depth
-    base_seed = 1000 * rank
+    from tensorray_b200 import dist as trd
+    base_seed = trd.rank_seed(0, rank)
     opts = api.RenderOptions(base_seed, D, a.spp, a.spp, a.spp, a.spp, a.spp)
     integrators = [api.PathTracer(), api.PrimaryEdgeIntegrator(), api.DirectEdgeIntegrator(),
                    api.IndirectEdgeIntegrator(), api.PixelBoundaryIntegrator()]
@@ -238,10 +247,7 @@ def main():
             it.renderD(scene, opts, dLdI)
             if ev: ev[kernel_names[i + 1]][1].record(stream)
         gr = scene.get_grads(clear=True)
-        if world > 1:
-            flat = torch.cat([gr["positions"].reshape(-1), gr["texels"].reshape(-1)])
-            dist.all_reduce(flat)
-        return gr
+        return trd.allreduce_grads(gr)
 
     for _ in range(a.warmup):
         step()
@@ -389,6 +395,205 @@ def main():
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# batched multi-view workload: one graph-captured launch per integrator for
+# all views vs the same kernels launched one view at a time
+# ---------------------------------------------------------------------------
+def run_views(a):
+    from tensorray_b200 import api, autotune, scenes
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    rng = np.random.default_rng(0)
+    nviews = 8 if a.quick else 32
+    res_choices = [64, 96] if a.quick else [128, 256, 384, 512]
+    spec = scenes.config1_scene(256, 256)
+    scene = api.Scene(spec)
+    scene.configure()
+    cams_spec = scenes.fibonacci_cameras(nviews, 4.0, res_choices, seed=1)
+    cams = [api.Camera(c.pos, c.target, c.up, c.width, c.height, c.fov) for c in cams_spec]
+    spps = [int(x) for x in rng.choice([8, 16, 32, 64] if not a.quick else [4, 8], size=nviews)]
+    D = 3
+    terms = [api.TRN_PATH_TRACER, api.TRN_PRIMARY_EDGE, api.TRN_DIRECT_EDGE]
+    vs = api.ViewSet(scene, cams, spps)
+    opts = api.RenderOptions(1, D, 0, 0, 0, 0, 0)
+    # targets: the same views with the sphere shifted
+    scene.shapes[0].translation = torch.tensor([0.05, -0.03, 0.02])
+    scene.configure()
+    targets = vs.render(api.TRN_PATH_TRACER, api.RenderOptions(77, D, 0, 0, 0, 0, 0)).clone()
+    scene.shapes[0].translation = torch.zeros(3)
+    scene.configure()
+    units = sum(c.width * c.height * s for c, s in zip(cams, spps)) * len(terms)
+    # autotuned launch shapes
+    ln_f = autotune.tune_forward(vs, opts)
+    ln_g = {t: autotune.tune(vs, t, opts) for t in terms}
+    img = torch.empty(vs.npix, 3, device=scene.device)
+    dLdI = torch.empty(vs.npix, 3, device=scene.device)
+
+    def batched_step():
+        vs.render(api.TRN_PATH_TRACER, opts, launch=ln_f, out=img)
+        loss = vs.loss(img, targets, dLdI)
+        for t in terms:
+            vs.render_grad(t, opts, dLdI, launch=ln_g[t])
+        g = scene.get_grads(clear=True)
+        return loss, g["positions"]
+
+    # plain form: one view set per view, same kernels, launched view by view
+    singles = [api.ViewSet(scene, [c], [s], seeds=[i]) for i, (c, s) in enumerate(zip(cams, spps))]
+    tgt_v = [vs.view_image(targets, i).reshape(-1, 3).contiguous() for i in range(nviews)]
+
+    def plain_step():
+        losses = []
+        for i, sv in enumerate(singles):
+            im = sv.render(api.TRN_PATH_TRACER, opts)
+            d = torch.empty_like(im)
+            losses.append(sv.loss(im, tgt_v[i], d))
+            for t in terms:
+                sv.render_grad(t, opts, d)
+        g = scene.get_grads(clear=True)
+        return losses, g["positions"]
+
+    for _ in range(a.warmup):
+        batched_step()
+        plain_step()
+    torch.cuda.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        batched_step()
+    torch.cuda.current_stream().wait_stream(s)
+    torch.cuda.synchronize()
+    with torch.cuda.graph(graph):
+        out_loss, out_grad = batched_step()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=scene.device)
+
+    def timed(fn):
+        tot = 0.0
+        for _ in range(a.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            tot += e0.elapsed_time(e1)
+        return tot / a.steps
+
+    for _ in range(a.warmup):
+        graph.replay()
+    ms_batched = timed(graph.replay)
+    ms_plain = timed(plain_step)
+    # the graph-captured step computes what the eager batched step computes
+    graph.replay()
+    torch.cuda.synchronize()
+    g_graph = out_grad.clone()
+    _, g_eager = batched_step()
+    rel = float((g_graph - g_eager).norm() / g_eager.norm().clamp_min(1e-30))
+    line = {"metric": "grad path-samples/sec", "value": units / (ms_batched / 1e3), "unit": "grad path-samples/s",
+            "n_gpus": 1, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_batched, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
+            "config": {"workload": f"{nviews} views of the 1280-tri icosphere scene, res {res_choices}, "
+                                   f"spp {sorted(set(spps))}, depth {D}, interior+primary+direct, one "
+                                   "graph-captured launch per integrator",
+                       "views": nviews, "samples_per_step": units},
+            "plain_per_view": {"value": units / (ms_plain / 1e3), "ms_per_step": ms_plain},
+            "batched_over_plain": ms_plain / ms_batched,
+            "graph_vs_eager_grad_rel_l2": rel,
+            "launch": {"fwd": [ln_f.block, ln_f.blocks_per_sm, ln_f.chunk],
+                       **{str(t): [ln_g[t].block, ln_g[t].blocks_per_sm, ln_g[t].chunk] for t in terms}}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# served workload: Poisson arrivals of render+gradient requests over four
+# resident scenes, continuous batching vs one request at a time
+# ---------------------------------------------------------------------------
+def run_serve(a):
+    from tensorray_b200 import api, scenes, serve
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    rng = np.random.default_rng(0)
+    sizes = {"s1k": 1_000, "s50k": 50_000, "s300k": 300_000, "s1m": 1_000_000}
+    if a.quick:
+        sizes = {"s1k": 1_000, "s20k": 20_000}
+    world = {k: api.Scene(scenes.served_scene(n, seed=i)) for i, (k, n) in enumerate(sizes.items())}
+    for sc in world.values():
+        sc.configure()
+    names = list(world)
+    nreq = a.requests if not a.quick else 12
+    rate = 200.0
+    gaps = rng.exponential(1.0 / rate, size=nreq)
+    arrivals = np.cumsum(gaps) - gaps[0]
+    rmax = 256 if a.quick else 1024
+
+    def make(i):
+        name = names[int(rng.integers(len(names)))]
+        u = rng.normal(size=3)
+        u /= np.linalg.norm(u)
+        pos = tuple(float(x) for x in 4.0 * u)
+        up = (0.0, 1.0, 0.0) if abs(u[1]) < 0.99 else (1.0, 0.0, 0.0)
+        res = int(rng.integers(128, rmax + 1))
+        spp = int(rng.integers(4, 65))
+        depth = int(rng.integers(3, 7))
+        cam = api.Camera(pos, (0.0, 0.0, 0.0), up, res, res, 45.0)
+        tgt = torch.zeros(res * res, 3, device="cuda")
+        return serve.RenderRequest(name, cam, spp, depth, tgt, seed=i)
+
+    reqs = [make(i) for i in range(nreq)]
+    budget = 120e9
+    # warm up every scene's kernels
+    warm = serve.Server(world, hbm_budget_bytes=budget)
+    for name in names:
+        cam = api.Camera((0.0, 0.0, 4.0), (0.0, 0.0, 0.0), (0.0, 1.0, 0.0), 64, 64, 45.0)
+        warm.submit(serve.RenderRequest(name, cam, 8, 3, torch.zeros(64 * 64, 3, device="cuda"), seed=999))
+    while not warm.idle():
+        warm.step()
+    torch.cuda.synchronize()
+    clocks = Clocks(torch.cuda.current_device())
+    clocks.start()
+    srv = serve.Server(world, hbm_budget_bytes=budget, chunk_spp=8)
+    t0 = time.perf_counter()
+    stats = srv.run(reqs, list(arrivals))
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    clk = clocks.stop()
+    lat = [r.latency for r in stats.completed]
+    samples = sum(r.samples() for r in stats.completed)
+    # plain: one request at a time through the single-view API, no batching
+    plain_lat = []
+    t1 = time.perf_counter()
+    tq = 0.0
+    for r, at in zip(reqs, arrivals):
+        start = max(at, tq)
+        sc = world[r.scene]
+        e0 = time.perf_counter()
+        opts = api.RenderOptions(r.seed, r.depth, r.spp, r.spp, r.spp, 0, 0)
+        img = api.PathTracer().renderC(sc, opts, camera=r.camera)
+        d = img.reshape(-1, 3) - r.target
+        sc.clear_grads()
+        for it in (api.PathTracer(), api.PrimaryEdgeIntegrator(), api.DirectEdgeIntegrator()):
+            it.renderD(sc, opts, d.reshape(img.shape), camera=r.camera)
+        sc.get_grads()
+        torch.cuda.synchronize()
+        dur = time.perf_counter() - e0
+        tq = start + dur
+        plain_lat.append(tq - at)
+    plain_wall = time.perf_counter() - t1
+    line = {"metric": "grad path-samples/sec", "value": samples / wall, "unit": "grad path-samples/s", "n_gpus": 1,
+            "steps": 1, "warmup": 1, "ms_per_step": 1e3 * wall, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scenes, Poisson arrivals)",
+            "config": {"workload": f"{nreq} render+gradient requests at {rate:.0f} req/s over scenes "
+                                   f"{list(sizes.values())} tris, res 128-{rmax}^2, spp 4-64, depth 3-6, "
+                                   "interior+primary+direct, continuous batching, 120 GB budget"},
+            "requests_per_s": len(stats.completed) / wall,
+            "latency_s": {"p50": serve.percentile(lat, 50), "p99": serve.percentile(lat, 99),
+                          "mean": float(np.mean(lat))},
+            "plain_one_at_a_time": {"requests_per_s": nreq / plain_wall, "value": samples / plain_wall,
+                                    "latency_s": {"p50": serve.percentile(plain_lat, 50),
+                                                  "p99": serve.percentile(plain_lat, 99)}},
+            "peak_request_bytes": stats.peak_bytes, "iterations": stats.iterations, "clocks": clk}
+    print(json.dumps(line), flush=True)
 
 
 if __name__ == "__main__":

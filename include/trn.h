@@ -126,7 +126,9 @@ typedef struct {
  * view's hash-sampler slots (a render split into spp chunks uses disjoint
  * slots per chunk); weight scales contributions (0 = 1/spp). grad_*: device
  * gradient destinations of this view ([V*3], [V*3], [texels*3]); NULL = the
- * scene's own buffers. */
+ * scene's own buffers. image / dLdI: per-view buffers (a request of a serving
+ * loop); a NULL call buffer in trn_render_views_fwd/grad then means "use the
+ * per-view buffers". */
 typedef struct {
   trn_camera camera;
   int spp;
@@ -134,10 +136,12 @@ typedef struct {
   long long pixel_offset;
   long long slot_offset;
   float weight;
-  int reserved;
+  int max_bounces;          /* 0 = options.max_bounces */
   float* grad_positions;
   float* grad_vertex_normals;
   float* grad_texels;
+  float* image;             /* own image [W*H*3] (accumulated, not cleared); NULL = the call's buffer */
+  const float* dLdI;        /* own dL/dI [W*H*3]; NULL = the call's buffer */
 } trn_view;
 
 typedef struct trn_viewset trn_viewset;
@@ -201,6 +205,9 @@ int trn_render_grad(trn_scene* scene, const trn_camera* camera, const trn_render
  * max_bounces and the seed. */
 int trn_viewset_create(trn_scene* scene, int nviews, const trn_view* views, trn_viewset** out);
 int trn_viewset_destroy(trn_viewset* views);
+/* Replace the views of a set (storage grows as needed; a serving loop
+ * re-uses one set per scene and phase). */
+int trn_viewset_update(trn_viewset* views, int nviews, const trn_view* view_array);
 int trn_viewset_num_pixels(const trn_viewset* views, long long* npix);
 int trn_render_views_fwd(trn_scene* scene, trn_viewset* views, const trn_render_options* options, int integrator,
                          const trn_samples* samples, const trn_launch* launch, float* images, cudaStream_t stream);

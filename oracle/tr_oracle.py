@@ -70,10 +70,10 @@ def hash_uniform(seed: int, term: int, dim: int, slots: np.ndarray) -> np.ndarra
     return ((k + np.float32(0.5)) * np.float32(1.0 / 8388608.0)).astype(np.float32)
 
 
-def hash_table(seed: int, term: int, dims: int, slots: int, view_seed: int = 0, view: int = 0) -> torch.Tensor:
+def hash_table(seed: int, term: int, dims: int, slots: int, view_seed: int = 0) -> torch.Tensor:
     """The library's hash sampler for one view: the stream seed folds the
-    render seed with the view's seed and index."""
-    stream = (seed * 1000003 + (view_seed * 7919 + view)) & 0xFFFFFFFF
+    render seed with the view's own seed."""
+    stream = (seed * 1000003 + view_seed) & 0xFFFFFFFF
     idx = np.arange(slots, dtype=np.uint64)
     return torch.from_numpy(np.stack([hash_uniform(stream, term, d, idx) for d in range(dims)]))
 

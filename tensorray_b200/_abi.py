@@ -68,8 +68,9 @@ class TrnLaunch(C.Structure):
 
 class TrnView(C.Structure):
     _fields_ = [("camera", TrnCamera), ("spp", C.c_int), ("seed", C.c_int), ("pixel_offset", C.c_longlong),
-                ("slot_offset", C.c_longlong), ("weight", C.c_float), ("reserved", C.c_int),
-                ("grad_positions", C.c_void_p), ("grad_vertex_normals", C.c_void_p), ("grad_texels", C.c_void_p)]
+                ("slot_offset", C.c_longlong), ("weight", C.c_float), ("max_bounces", C.c_int),
+                ("grad_positions", C.c_void_p), ("grad_vertex_normals", C.c_void_p), ("grad_texels", C.c_void_p),
+                ("image", C.c_void_p), ("dLdI", C.c_void_p)]
 
 
 _SIGNATURES = {
@@ -98,6 +99,7 @@ _SIGNATURES = {
     "trn_scene_clear_grads": (C.c_int, [C.c_void_p, C.c_void_p]),
     "trn_viewset_create": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(TrnView), C.POINTER(C.c_void_p)]),
     "trn_viewset_destroy": (C.c_int, [C.c_void_p]),
+    "trn_viewset_update": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(TrnView)]),
     "trn_viewset_num_pixels": (C.c_int, [C.c_void_p, C.POINTER(C.c_longlong)]),
     "trn_render_views_fwd": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(TrnRenderOptions), C.c_int,
                                        C.POINTER(TrnSamples), C.POINTER(TrnLaunch), C.c_void_p, C.c_void_p]),

@@ -287,6 +287,14 @@ class Scene:
     def clear_grads(self) -> None:
         check(self._lib.trn_scene_clear_grads(self._h, C.c_void_p(_stream())), "trn_scene_clear_grads")
 
+    def finalize_grads(self, grad_positions: torch.Tensor, grad_vertex_normals: torch.Tensor,
+                       d_translation: torch.Tensor | None = None) -> None:
+        """Geometry adjoint for caller-owned gradient buffers (one request)."""
+        check(self._lib.trn_scene_finalize_grads(self._h, C.c_void_p(grad_positions.data_ptr()),
+                                                 C.c_void_p(grad_vertex_normals.data_ptr()),
+                                                 C.c_void_p(d_translation.data_ptr()) if d_translation is not None
+                                                 else None, C.c_void_p(_stream())), "trn_scene_finalize_grads")
+
     # -- ray queries (RayIntersectOptix replacement) -------------------------------
     def intersect(self, org: torch.Tensor, dir: torch.Tensor, tmin: torch.Tensor, tmax: torch.Tensor):
         self._ensure()
@@ -401,14 +409,18 @@ class ViewSet:
     (pyTensorRay/renderer_multi_view.py:53-61): images of all views are
     concatenated [npix, 3]; per-view spp and seeds are part of the set."""
 
-    def __init__(self, scene: Scene, cameras: list, spps: list, seeds: list | None = None):
+    def __init__(self, scene: Scene, cameras: list, spps: list, seeds: list | None = None, views=None):
         n = len(cameras)
         if n == 0 or len(spps) != n:
             raise RuntimeError("ViewSet needs one spp per camera")
         seeds = seeds if seeds is not None else list(range(n))
-        arr = (TrnView * n)()
-        for i, (c, sp, sd) in enumerate(zip(cameras, spps, seeds)):
-            arr[i] = TrnView(c.c, int(sp), int(sd), -1, 0, 0.0, 0, None, None, None)
+        if views is None:
+            arr = (TrnView * n)()
+            for i, (c, sp, sd) in enumerate(zip(cameras, spps, seeds)):
+                arr[i] = TrnView(c.c, int(sp), int(sd), -1, 0, 0.0, 0, None, None, None, None, None)
+        else:
+            arr = views
+        self._arr = arr
         self.scene = scene
         self.cameras = list(cameras)
         self.spps = [int(x) for x in spps]
@@ -431,6 +443,16 @@ class ViewSet:
         except Exception:
             pass
 
+    def update(self, cameras: list, spps: list, views) -> None:
+        """Replace the views (serving loop); `views` is a ctypes TrnView array."""
+        self._arr = views
+        check(self.scene._lib.trn_viewset_update(self._h, len(cameras), views), "trn_viewset_update")
+        npix = C.c_longlong()
+        check(self.scene._lib.trn_viewset_num_pixels(self._h, C.byref(npix)), "trn_viewset_num_pixels")
+        self.npix = npix.value
+        self.cameras = list(cameras)
+        self.spps = [int(x) for x in spps]
+
     def slots(self, integrator_id: int) -> int:
         n = sum(c.width * c.height * s for c, s in zip(self.cameras, self.spps))
         return n // 4 if integrator_id == TRN_PIXEL_EDGE else n
@@ -438,27 +460,28 @@ class ViewSet:
     def render(self, integrator_id: int, options: RenderOptions, samples=None, launch: TrnLaunch | None = None,
                out: torch.Tensor | None = None) -> torch.Tensor:
         self.scene._ensure()
-        img = out if out is not None else torch.empty(self.npix, 3, device=self.scene.device)
+        per_view = out is False  # views carry their own image buffers (accumulate)
+        img = None if per_view else (out if out is not None else torch.empty(self.npix, 3, device=self.scene.device))
         smp = _samples_struct(samples)
         o = options._c()
         check(self.scene._lib.trn_render_views_fwd(self.scene.handle, self._h, C.byref(o), integrator_id,
                                                    C.byref(smp), C.byref(launch) if launch else None,
-                                                   C.c_void_p(img.data_ptr()), C.c_void_p(_stream())),
-              "trn_render_views_fwd")
+                                                   C.c_void_p(img.data_ptr()) if img is not None else None,
+                                                   C.c_void_p(_stream())), "trn_render_views_fwd")
         return img
 
     def render_grad(self, integrator_id: int, options: RenderOptions, dLdI: torch.Tensor, samples=None,
                     launch: TrnLaunch | None = None) -> None:
         self.scene._ensure()
-        g = dLdI.contiguous()
-        if g.numel() != 3 * self.npix:
+        g = None if dLdI is None else dLdI.contiguous()
+        if g is not None and g.numel() != 3 * self.npix:
             raise RuntimeError("dLdI must have npix*3 elements")
         smp = _samples_struct(samples)
         o = options._c()
         check(self.scene._lib.trn_render_views_grad(self.scene.handle, self._h, C.byref(o), integrator_id,
                                                     C.byref(smp), C.byref(launch) if launch else None,
-                                                    C.c_void_p(g.data_ptr()), C.c_void_p(_stream())),
-              "trn_render_views_grad")
+                                                    C.c_void_p(g.data_ptr()) if g is not None else None,
+                                                    C.c_void_p(_stream())), "trn_render_views_grad")
 
     def loss(self, images: torch.Tensor, targets: torch.Tensor, dLdI: torch.Tensor | None = None):
         """Per-view 0.5*|I - T|^2 and dL/dI (one launch for all views)."""

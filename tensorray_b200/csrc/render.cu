@@ -29,8 +29,6 @@ struct Params {
   uint32_t term;             // integrator id (hash stream)
   uint32_t seed;             // RenderOptions::mRndSeed
   int D;                     // max bounces
-  float* image;              // forward radiance accumulation [pixels*3]
-  const float* dLdI;         // [pixels*3]
   float* g_pos;              // [V*3]
   float* g_vn;               // [V*3]
   float* g_tex;              // [texels*3]
@@ -108,7 +106,7 @@ TRN_D void agg_add3(float* base, long long idx, const F3& g) {
 }
 TRN_D F3 g_at(const Params& P, const ViewDesc& V, int pix) {
   if (pix < 0) return F3z();
-  const float* d = P.dLdI + 3 * (V.pix_off + pix);
+  const float* d = V.dLdI + 3 * pix;
   return F3(__ldg(d), __ldg(d + 1), __ldg(d + 2)) * V.inv_spp;
 }
 
@@ -367,40 +365,90 @@ TRN_D bool radiance_step(const DeviceScene& s, SurfF& x, F3& rdir, F3& T, float 
   return true;
 }
 
+
+// Per-warp compaction of the work queue: lanes keep pulling sample slots (one
+// warp-aggregated atomic per round) until each holds a slot that survives the
+// cheap `setup` phase (primary hit, valid edge sample, visible, ...); then the
+// warp runs the expensive `body` (path tracing + adjoint) together. Rejected
+// samples therefore never hold a lane hostage while others trace long paths.
+template <class State, class Setup, class Body>
+TRN_D void for_each_valid(const Params& P, Setup&& setup, Body&& body) {
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;
+  State st;
+  bool have = false, done = false;
+  for (;;) {
+    for (;;) {
+      const unsigned need = __ballot_sync(0xffffffffu, !have && !done);
+      if (!need) break;
+      const int leader = __ffs(need) - 1;
+      unsigned long long base = 0;
+      if (lane == leader) base = atomicAdd(P.work, (unsigned long long)__popc(need));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      if (!have && !done) {
+        const long long g = (long long)base + __popc(need & lt);
+        if (g >= P.total) done = true;
+        else have = setup(g, st);
+      }
+    }
+    if (!__any_sync(0xffffffffu, have)) break;
+    if (have) { body(st); have = false; }
+    __syncwarp();
+  }
+}
+
 // ---------------------------------------------------------------------------
 // interior term: forward
 // ---------------------------------------------------------------------------
+struct FwdState {
+  const ViewDesc* V;
+  long long gslot, p;
+  int pix;
+  SurfF x;
+  F3 T, rdir, L;
+};
+
 __global__ void __launch_bounds__(256) k_path_fwd(Params P) {
   Cnt cnt;
-  for_each_slot(P, [&](long long gslot) {
-    const ViewDesc& V = view_of(P, gslot);
-    const long long p = gslot - V.begin;
-    const CameraDesc& cam = V.cam;
-    const PathSmp S{&P, V.seed, gslot, p + V.slot_off};
-    const int W = cam.w, WH = cam.w * cam.h;
-    const F3 org = cam_pos(cam);
-    const int pix = (int)(p % WH);
-    const F3 dir = camera_ray_dir(cam, pix % W, pix / W, S(0), S(1));
-    Hit h;
-    cnt.v[kCntClosest]++;
-    if (!trace<false>(P.s, org, dir, kShadowEps, kRayMax, h, P.err)) return;
-    SurfF x = post_intersect(P.s, h.tri, h.u, h.v);
-    const float t1 = camera_factor<float>(cam, x.p, x.ng, 1.f);
-    F3 T(t1, t1, t1);
-    F3 rdir = normalize(x.p - org);
-    F3 L = scrub(T * emitted(P.s, x, -rdir));
-    for (int b = 0; b < P.D; b++) {
-      const int o = 2 + 5 * b;
-      F3 c;
-      const bool more = radiance_step(P.s, x, rdir, T, S(o), S(o + 1), S(o + 2),
-                                      S(o + 3), S(o + 4), c, nullptr, cnt);
-      L = L + c;
-      if (!more || (T.x == 0.f && T.y == 0.f && T.z == 0.f)) break;
-    }
-    L = L * V.inv_spp;
-    cnt.v[kCntPixel]++;
-    atomic_add3(P.image + 3 * (V.pix_off + pix), L);
-  });
+  stage_top(P.s);
+  for_each_valid<FwdState>(P,
+    [&](long long gslot, FwdState& st) -> bool {
+      const ViewDesc& V = view_of(P, gslot);
+      const long long p = gslot - V.begin;
+      const CameraDesc& cam = V.cam;
+      const PathSmp S{&P, V.seed, gslot, p + V.slot_off};
+      const int W = cam.w, WH = cam.w * cam.h;
+      const F3 org = cam_pos(cam);
+      const int pix = (int)(p % WH);
+      const F3 dir = camera_ray_dir(cam, pix % W, pix / W, S(0), S(1));
+      Hit h;
+      cnt.v[kCntClosest]++;
+      if (!trace<false>(P.s, org, dir, kShadowEps, kRayMax, h, P.err)) return false;
+      st.V = &V; st.gslot = gslot; st.p = p; st.pix = pix;
+      st.x = post_intersect(P.s, h.tri, h.u, h.v);
+      const float t1 = camera_factor<float>(cam, st.x.p, st.x.ng, 1.f);
+      st.T = F3(t1, t1, t1);
+      st.rdir = normalize(st.x.p - org);
+      st.L = scrub(st.T * emitted(P.s, st.x, -st.rdir));
+      return true;
+    },
+    [&](FwdState& st) {
+      const ViewDesc& V = *st.V;
+      const PathSmp S{&P, V.seed, st.gslot, st.p + V.slot_off};
+      SurfF x = st.x;
+      F3 T = st.T, rdir = st.rdir, L = st.L;
+      for (int b = 0; b < V.D; b++) {
+        const int o = 2 + 5 * b;
+        F3 c;
+        const bool more = radiance_step(P.s, x, rdir, T, S(o), S(o + 1), S(o + 2), S(o + 3), S(o + 4), c, nullptr,
+                                        cnt);
+        L = L + c;
+        if (!more || (T.x == 0.f && T.y == 0.f && T.z == 0.f)) break;
+      }
+      L = L * V.inv_spp;
+      cnt.v[kCntPixel]++;
+      atomic_add3(V.image + 3 * st.pix, L);
+    });
   flush_cnt(cnt, P.stats);
 }
 
@@ -465,24 +513,42 @@ TRN_D void cont_vjp(const BsdfDesc& b, bool need_prev, bool need_kd, const F3& x
 
 struct VRec { int tri; float u, v; };
 
+struct AdjState {
+  const ViewDesc* V;
+  long long gslot, p;
+  int pix;
+  F3 g;
+  Hit h;
+};
+
 __global__ void __launch_bounds__(256) k_path_adj(Params P) {
   const DeviceScene& s = P.s;
   Cnt cnt;
-  for_each_slot(P, [&](long long gslot) {
-    const ViewDesc& V = view_of(P, gslot);
-    const long long p = gslot - V.begin;
+  stage_top(P.s);
+  for_each_valid<AdjState>(P,
+    [&](long long gslot, AdjState& st) -> bool {
+      const ViewDesc& V = view_of(P, gslot);
+      const long long p = gslot - V.begin;
+      const CameraDesc& cam = V.cam;
+      const PathSmp S{&P, V.seed, gslot, p + V.slot_off};
+      const int W = cam.w, WH = cam.w * cam.h;
+      const int pix = (int)(p % WH);
+      cnt.v[kCntPixel]++;
+      const F3 g = g_at(P, V, pix);
+      if (g.x == 0.f && g.y == 0.f && g.z == 0.f) return false;
+      const F3 dir = camera_ray_dir(cam, pix % W, pix / W, S(0), S(1));
+      cnt.v[kCntClosest]++;
+      if (!trace<false>(s, cam_pos(cam), dir, kShadowEps, kRayMax, st.h, P.err)) return false;
+      st.V = &V; st.gslot = gslot; st.p = p; st.pix = pix; st.g = g;
+      return true;
+    },
+    [&](AdjState& st) {
+    const ViewDesc& V = *st.V;
     const CameraDesc& cam = V.cam;
-    const PathSmp S{&P, V.seed, gslot, p + V.slot_off};
-    const int W = cam.w, WH = cam.w * cam.h;
+    const PathSmp S{&P, V.seed, st.gslot, st.p + V.slot_off};
     const F3 org = cam_pos(cam);
-    const int pix = (int)(p % WH);
-    cnt.v[kCntPixel]++;
-    const F3 g = g_at(P, V, pix);
-    if (g.x == 0.f && g.y == 0.f && g.z == 0.f) return;
-    const F3 dir = camera_ray_dir(cam, pix % W, pix / W, S(0), S(1));
-    Hit h;
-    cnt.v[kCntClosest]++;
-    if (!trace<false>(s, org, dir, kShadowEps, kRayMax, h, P.err)) return;
+    const F3 g = st.g;
+    const Hit h = st.h;
     // ---- forward replay, recording vertices and factor values ----
     VRec vr[kMaxDepth + 2];
     BounceRec br[kMaxDepth + 1];
@@ -497,7 +563,7 @@ __global__ void __launch_bounds__(256) k_path_adj(Params P) {
     Mk[1] = emitted(s, x, -rdir);
     if (!finite3(T * Mk[1])) Mk[1] = F3z();
     int K = 1;  // vertices reached
-    const int D = min(P.D, kMaxDepth);
+    const int D = min(V.D, kMaxDepth);
     for (int k = 0; k <= D + 1; k++) { nee_on[k] = false; Nk[k] = F3z(); Phik[k] = F3z(); }
     for (int b = 0; b < D; b++) {
       const int k = b + 1;
@@ -596,7 +662,7 @@ __global__ void __launch_bounds__(256) k_path_adj(Params P) {
       if (need_kd) { cnt.v[kCntTScatter]++; agg_add3(V.gtex, texel[k], gkd); }
     }
     for (int k = 1; k <= K; k++) scatter_vertex(P, V, vr[k].tri, vr[k].u, vr[k].v, va[k], cnt);
-  });
+    });
   flush_cnt(cnt, P.stats);
 }
 
@@ -704,66 +770,93 @@ TRN_D float base_val(float ratio, const F3& edge, const F3& d, const F3& nrm, co
 // ---------------------------------------------------------------------------
 // primary boundary (BoundaryPrimary.cpp:36-181, SampleFromPrimEdges Edge.cpp:350-367)
 // ---------------------------------------------------------------------------
+struct EdgeState {
+  const ViewDesc* V;
+  long long gslot, p;
+  SurfF x;         // receiving surface (sensor side for direct/indirect)
+  SurfF xe;        // emitter-side surface (indirect)
+  F3 rdir;         // incoming direction at x
+  F3 T0;           // start throughput / emitted radiance scale
+  F3 p0;           // edge point
+  F3 n;            // detached xDotN normal
+  float w0;        // Detach(baseVal / pdf) factor
+  float sedge;     // edge parameter of p0
+  int v0, v1;      // edge vertices (-1: not a scene parameter)
+  int far_tri;     // triangle intersected by RayIntersectAD
+  int pix;         // primary / pixel: pixel of the sensor point
+  F3 g;
+};
+
 __global__ void __launch_bounds__(256) k_primary_adj(Params P) {
   const DeviceScene& s = P.s;
   Cnt cnt;
-  for_each_slot(P, [&](long long gslot) {
-    const ViewDesc& V = view_of(P, gslot);
-    const long long p = gslot - V.begin;
-    const CameraDesc& cam = V.cam;
-    const PathSmp S{&P, V.seed, gslot, p + V.slot_off};
-    const F3 cpos = cam_pos(cam);
-    const float r0 = S(0), r1 = S(1);
-    float reuse;
-    const float integral = __ldg(V.pint);
-    if (!(integral > 0.f)) return;
-    const int e = sample_discrete(V.pcdf, P.ne, r0, reuse);
-    const int v0 = P.edges[5 * e], v1 = P.edges[5 * e + 1], v2 = P.edges[5 * e + 4];
-    const float len_e = V.pfunc[e];
-    if (!(len_e > 0.f)) return;
-    const float pmf = len_e / (integral * (float)P.ne);
-    const float pdf = pmf / len_e;
-    const F3 Pa = load3(s.pos, v0), Pb = load3(s.pos, v1), Pc = load3(s.pos, v2);
-    const F3 e1 = Pb - Pa;
-    const F3 p0 = Pa + e1 * r1;
-    const F3 edge = normalize(e1), edge2 = normalize(Pc - Pa);
-    const F3 dir = normalize(p0 - cpos);
-    Hit h;
-    cnt.v[kCntClosest]++;
-    if (!trace<false>(s, p0, dir, kShadowEps, kRayMax, h, P.err)) return;
-    const F3 hitP = p0 + dir * h.t;
-    const SensorSample sds = sample_direct(cam, hitP);
-    if (!sds.valid) return;
-    const F3 dirc = sensor_ray_dir(cam, sds.qx, sds.qy);
-    const float dist2cam = length(p0 - cpos);
-    cnt.v[kCntShadow]++;
-    if (occluded(s, cpos, dirc, kShadowEps, dist2cam - kShadowEps)) return;
-    SurfF x = post_intersect(s, h.tri, h.u, h.v);
-    const float dist = length(x.p - cpos);
-    const float dist1 = length(p0 - cpos);
-    const float cos2 = fabsf(dot(x.ng, -dirc));
-    F3 n;
-    const float bval = base_val((dist / dist1), edge, dirc, x.ng, edge2, n) * cos2;
-    const int pix = image_pixel(cam, sds.qx, sds.qy);
-    const F3 g = g_at(P, V, pix);
-    if (bval == 0.f || (g.x == 0.f && g.y == 0.f && g.z == 0.f)) return;
-    // detached radiance along the camera ray through the sensor point
-    F3 T(sds.sensor_val, sds.sensor_val, sds.sensor_val);
-    F3 rdir = dirc;
-    F3 L = scrub(T * emitted(s, x, -rdir));
-    for (int b = 0; b < P.D; b++) {
-      const int o = 2 + 5 * b;
-      F3 c;
-      const bool more = radiance_step(s, x, rdir, T, S(o), S(o + 1), S(o + 2),
-                                      S(o + 3), S(o + 4), c, nullptr, cnt);
-      L = L + c;
-      if (!more || (T.x == 0.f && T.y == 0.f && T.z == 0.f)) break;
-    }
-    const F3 wv = L * (bval / pdf);
-    const float W = dot(g, wv);
-    if (W == 0.f || !isfinite(W)) return;
-    xdotn_vjp(P, V, W, cpos, false, -1, 0.f, 0.f, v0, v1, r1, p0, h.tri, n, cnt);
-  });
+  stage_top(P.s);
+  for_each_valid<EdgeState>(P,
+    [&](long long gslot, EdgeState& st) -> bool {
+      const ViewDesc& V = view_of(P, gslot);
+      const long long p = gslot - V.begin;
+      const CameraDesc& cam = V.cam;
+      const PathSmp S{&P, V.seed, gslot, p + V.slot_off};
+      const F3 cpos = cam_pos(cam);
+      const float r0 = S(0), r1 = S(1);
+      float reuse;
+      const float integral = __ldg(V.pint);
+      if (!(integral > 0.f)) return false;
+      const int e = sample_discrete(V.pcdf, P.ne, r0, reuse);
+      const int v0 = P.edges[5 * e], v1 = P.edges[5 * e + 1], v2 = P.edges[5 * e + 4];
+      const float len_e = V.pfunc[e];
+      if (!(len_e > 0.f)) return false;
+      const float pmf = len_e / (integral * (float)P.ne);
+      const float pdf = pmf / len_e;
+      const F3 Pa = load3(s.pos, v0), Pb = load3(s.pos, v1), Pc = load3(s.pos, v2);
+      const F3 e1 = Pb - Pa;
+      const F3 p0 = Pa + e1 * r1;
+      const F3 edge = normalize(e1), edge2 = normalize(Pc - Pa);
+      const F3 dir = normalize(p0 - cpos);
+      Hit h;
+      cnt.v[kCntClosest]++;
+      if (!trace<false>(s, p0, dir, kShadowEps, kRayMax, h, P.err)) return false;
+      const F3 hitP = p0 + dir * h.t;
+      const SensorSample sds = sample_direct(cam, hitP);
+      if (!sds.valid) return false;
+      const F3 dirc = sensor_ray_dir(cam, sds.qx, sds.qy);
+      const float dist2cam = length(p0 - cpos);
+      cnt.v[kCntShadow]++;
+      if (occluded(s, cpos, dirc, kShadowEps, dist2cam - kShadowEps)) return false;
+      const SurfF x = post_intersect(s, h.tri, h.u, h.v);
+      const float dist = length(x.p - cpos);
+      const float dist1 = length(p0 - cpos);
+      const float cos2 = fabsf(dot(x.ng, -dirc));
+      F3 n;
+      const float bval = base_val((dist / dist1), edge, dirc, x.ng, edge2, n) * cos2;
+      const int pix = image_pixel(cam, sds.qx, sds.qy);
+      const F3 g = g_at(P, V, pix);
+      if (bval == 0.f || (g.x == 0.f && g.y == 0.f && g.z == 0.f)) return false;
+      st.V = &V; st.gslot = gslot; st.p = p; st.x = x; st.rdir = dirc;
+      st.T0 = F3(sds.sensor_val, sds.sensor_val, sds.sensor_val);
+      st.p0 = p0; st.n = n; st.w0 = bval / pdf; st.sedge = r1; st.v0 = v0; st.v1 = v1; st.far_tri = h.tri;
+      st.pix = pix; st.g = g;
+      return true;
+    },
+    [&](EdgeState& st) {
+      const ViewDesc& V = *st.V;
+      const PathSmp S{&P, V.seed, st.gslot, st.p + V.slot_off};
+      // detached radiance along the camera ray through the sensor point
+      SurfF x = st.x;
+      F3 T = st.T0, rdir = st.rdir;
+      F3 L = scrub(T * emitted(s, x, -rdir));
+      for (int b = 0; b < V.D; b++) {
+        const int o = 2 + 5 * b;
+        F3 c;
+        const bool more = radiance_step(s, x, rdir, T, S(o), S(o + 1), S(o + 2), S(o + 3), S(o + 4), c, nullptr,
+                                        cnt);
+        L = L + c;
+        if (!more || (T.x == 0.f && T.y == 0.f && T.z == 0.f)) break;
+      }
+      const float W = dot(st.g, L * st.w0);
+      if (W == 0.f || !isfinite(W)) return;
+      xdotn_vjp(P, V, W, cam_pos(V.cam), false, -1, 0.f, 0.f, st.v0, st.v1, st.sedge, st.p0, st.far_tri, st.n, cnt);
+    });
   flush_cnt(cnt, P.stats);
 }
 
@@ -773,78 +866,86 @@ __global__ void __launch_bounds__(256) k_primary_adj(Params P) {
 __global__ void __launch_bounds__(256) k_direct_adj(Params P) {
   const DeviceScene& s = P.s;
   Cnt cnt;
-  for_each_slot(P, [&](long long gslot) {
-    const ViewDesc& V = view_of(P, gslot);
-    const long long p = gslot - V.begin;
-    const CameraDesc& cam = V.cam;
-    const PathSmp S{&P, V.seed, gslot, p + V.slot_off};
-    const float r0 = S(0), r1 = S(1), r2 = S(2);
-    float reuse;
-    const float integral = __ldg(P.eint);
-    if (!(integral > 0.f)) return;
-    const int e = sample_discrete(P.ecdf, P.ne, r0, reuse);
-    const int v0 = P.edges[5 * e], v1 = P.edges[5 * e + 1], f0 = P.edges[5 * e + 2], f1 = P.edges[5 * e + 3],
-              v2 = P.edges[5 * e + 4];
-    const float len_e = P.efunc[e];
-    if (!(len_e > 0.f)) return;
-    const float pdf_e = (len_e / (integral * (float)P.ne)) / len_e;
-    const F3 Pa = load3(s.pos, v0), Pb = load3(s.pos, v1), Pc = load3(s.pos, v2);
-    const F3 e1 = Pb - Pa;
-    const F3 p0 = Pa + e1 * reuse;
-    const F3 edge = normalize(e1), edge2 = normalize(Pc - Pa);
-    LightSample ls;
-    if (!light_sample(s, r1, r2, ls)) return;
-    int j0, j1, j2; tri_vertices(s, ls.tri, j0, j1, j2);
-    const F3 p2 = bary3(ls.bu, ls.bv, load3(s.pos, j0), load3(s.pos, j1), load3(s.pos, j2));
-    const F3 nL = load3(s.fnormal, ls.tri);
-    const F3 ev = p2 - p0;
-    const float dist_sqr = dot(ev, ev);
-    const float dist = sqrtf(dist_sqr);
-    const F3 en = ev / dist;
-    const float cos_t = dot(nL, -en);
-    const F3 n0 = load3(s.fnormal, f0);
-    const F3 n1 = f1 >= 0 ? load3(s.fnormal, f1) : F3z();
-    const bool is_b = f1 < 0;
-    const float c0 = dot(en, n0), c1 = dot(en, n1);
-    const bool valid0 = fabsf(c0) > kEdgeEps;
-    const bool valid1 = (c0 > kEdgeEps && c1 < -kEdgeEps) || (c0 < -kEdgeEps && c1 > kEdgeEps);
-    const bool right = (is_b && valid0) || (!is_b && valid1);
-    if (!(right && cos_t > kEps && dist > kShadowEps)) return;
-    const float pdf = pdf_e * ls.pdf * dist_sqr / cos_t;
-    const F3 rdir = normalize(p0 - p2);
-    Hit h0, h;
-    cnt.v[kCntClosest] += 2;
-    cnt.v[kCntLight]++;
-    if (!trace<false>(s, p0, -rdir, kShadowEps, kRayMax, h0, P.err)) return;
-    if (!trace<false>(s, p0, rdir, kShadowEps, kRayMax, h, P.err)) return;
-    const F3 hp = p0 + (-rdir) * h0.t;
-    if (!(length(hp - p2) < kShadowEps)) return;
-    const SurfF xl = post_intersect(s, h0.tri, h0.u, h0.v);
-    const F3 E = emitted(s, xl, rdir);
-    SurfF x = post_intersect(s, h.tri, h.u, h.v);
-    const float dl = length(p2 - x.p);
-    const float cos2 = fabsf(dot(nL, rdir));
-    const float its_t = length(x.p - p0);
-    F3 n;
-    const float bval = base_val(its_t / dl, edge, -rdir, nL, edge2, n) * cos2;
-    if (bval == 0.f || (E.x == 0.f && E.y == 0.f && E.z == 0.f)) return;
-    const F3 ev0 = E * (bval / pdf);
-    // trace towards the sensor (EvalImportance per bounce)
-    F3 T(1.f, 1.f, 1.f);
-    F3 dirs = rdir;
-    float W = 0.f;
-    SurfF xs = x;
-    for (int b = 0; b < P.D; b++) {
-      const int o = 3 + 3 * b;
-      F3 c; int pix;
-      const bool more = importance_step(s, cam, xs, dirs, T, S(o), S(o + 1),
-                                        S(o + 2), c, pix, cnt);
-      if (pix >= 0) W += dot(g_at(P, V, pix), ev0 * c);
-      if (!more) break;
-    }
-    if (W == 0.f || !isfinite(W)) return;
-    xdotn_vjp(P, V, W, x.p, true, h.tri, h.u, h.v, v0, v1, reuse, p0, h0.tri, n, cnt);
-  });
+  stage_top(P.s);
+  for_each_valid<EdgeState>(P,
+    [&](long long gslot, EdgeState& st) -> bool {
+      const ViewDesc& V = view_of(P, gslot);
+      const long long p = gslot - V.begin;
+      const PathSmp S{&P, V.seed, gslot, p + V.slot_off};
+      const float r0 = S(0), r1 = S(1), r2 = S(2);
+      float reuse;
+      const float integral = __ldg(P.eint);
+      if (!(integral > 0.f)) return false;
+      const int e = sample_discrete(P.ecdf, P.ne, r0, reuse);
+      const int v0 = P.edges[5 * e], v1 = P.edges[5 * e + 1], f0 = P.edges[5 * e + 2], f1 = P.edges[5 * e + 3],
+                v2 = P.edges[5 * e + 4];
+      const float len_e = P.efunc[e];
+      if (!(len_e > 0.f)) return false;
+      const float pdf_e = (len_e / (integral * (float)P.ne)) / len_e;
+      const F3 Pa = load3(s.pos, v0), Pb = load3(s.pos, v1), Pc = load3(s.pos, v2);
+      const F3 e1 = Pb - Pa;
+      const F3 p0 = Pa + e1 * reuse;
+      const F3 edge = normalize(e1), edge2 = normalize(Pc - Pa);
+      LightSample ls;
+      if (!light_sample(s, r1, r2, ls)) return false;
+      int j0, j1, j2; tri_vertices(s, ls.tri, j0, j1, j2);
+      const F3 p2 = bary3(ls.bu, ls.bv, load3(s.pos, j0), load3(s.pos, j1), load3(s.pos, j2));
+      const F3 nL = load3(s.fnormal, ls.tri);
+      const F3 ev = p2 - p0;
+      const float dist_sqr = dot(ev, ev);
+      const float dist = sqrtf(dist_sqr);
+      const F3 en = ev / dist;
+      const float cos_t = dot(nL, -en);
+      const F3 n0 = load3(s.fnormal, f0);
+      const F3 n1 = f1 >= 0 ? load3(s.fnormal, f1) : F3z();
+      const bool is_b = f1 < 0;
+      const float c0 = dot(en, n0), c1 = dot(en, n1);
+      const bool valid0 = fabsf(c0) > kEdgeEps;
+      const bool valid1 = (c0 > kEdgeEps && c1 < -kEdgeEps) || (c0 < -kEdgeEps && c1 > kEdgeEps);
+      const bool right = (is_b && valid0) || (!is_b && valid1);
+      if (!(right && cos_t > kEps && dist > kShadowEps)) return false;
+      const float pdf = pdf_e * ls.pdf * dist_sqr / cos_t;
+      const F3 rdir = normalize(p0 - p2);
+      Hit h0, h;
+      cnt.v[kCntClosest] += 2;
+      cnt.v[kCntLight]++;
+      if (!trace<false>(s, p0, -rdir, kShadowEps, kRayMax, h0, P.err)) return false;
+      if (!trace<false>(s, p0, rdir, kShadowEps, kRayMax, h, P.err)) return false;
+      const F3 hp = p0 + (-rdir) * h0.t;
+      if (!(length(hp - p2) < kShadowEps)) return false;
+      const SurfF xl = post_intersect(s, h0.tri, h0.u, h0.v);
+      const F3 E = emitted(s, xl, rdir);
+      const SurfF x = post_intersect(s, h.tri, h.u, h.v);
+      const float dl = length(p2 - x.p);
+      const float cos2 = fabsf(dot(nL, rdir));
+      const float its_t = length(x.p - p0);
+      F3 n;
+      const float bval = base_val(its_t / dl, edge, -rdir, nL, edge2, n) * cos2;
+      if (bval == 0.f || (E.x == 0.f && E.y == 0.f && E.z == 0.f)) return false;
+      st.V = &V; st.gslot = gslot; st.p = p; st.x = x; st.rdir = rdir; st.T0 = E; st.p0 = p0; st.n = n;
+      st.w0 = bval / pdf; st.sedge = reuse; st.v0 = v0; st.v1 = v1; st.far_tri = h0.tri;
+      return true;
+    },
+    [&](EdgeState& st) {
+      const ViewDesc& V = *st.V;
+      const PathSmp S{&P, V.seed, st.gslot, st.p + V.slot_off};
+      const F3 ev0 = st.T0 * st.w0;
+      // trace towards the sensor (EvalImportance per bounce)
+      F3 T(1.f, 1.f, 1.f);
+      F3 dirs = st.rdir;
+      float W = 0.f;
+      SurfF xs = st.x;
+      for (int b = 0; b < V.D; b++) {
+        const int o = 3 + 3 * b;
+        F3 c; int pix;
+        const bool more = importance_step(s, V.cam, xs, dirs, T, S(o), S(o + 1), S(o + 2), c, pix, cnt);
+        if (pix >= 0) W += dot(g_at(P, V, pix), ev0 * c);
+        if (!more) break;
+      }
+      if (W == 0.f || !isfinite(W)) return;
+      xdotn_vjp(P, V, W, st.x.p, true, st.x.tri, st.x.u, st.x.v, st.v0, st.v1, st.sedge, st.p0, st.far_tri, st.n,
+                cnt);
+    });
   flush_cnt(cnt, P.stats);
 }
 
@@ -853,105 +954,112 @@ __global__ void __launch_bounds__(256) k_direct_adj(Params P) {
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_indirect_adj(Params P) {
   const DeviceScene& s = P.s;
-  const int D = min(P.D, kMaxDepth);
   Cnt cnt;
-  if (D >= 2) for_each_slot(P, [&](long long g) {
-    const ViewDesc& V = view_of(P, g);
-    const long long p = g - V.begin;
-    const CameraDesc& cam = V.cam;
-    const PathSmp S{&P, V.seed, g, p};
-    const float r0 = S(0), r1 = S(1), r2 = S(2);
-    float reuse;
-    const float integral = __ldg(P.eint);
-    if (!(integral > 0.f)) return;
-    const int e = sample_discrete(P.ecdf, P.ne, r0, reuse);
-    const int v0 = P.edges[5 * e], v1 = P.edges[5 * e + 1], f0 = P.edges[5 * e + 2], f1 = P.edges[5 * e + 3],
-              v2 = P.edges[5 * e + 4];
-    const float len_e = P.efunc[e];
-    if (!(len_e > 0.f)) return;
-    const float pdf_e = (len_e / (integral * (float)P.ne)) / len_e;
-    const F3 Pa = load3(s.pos, v0), Pb = load3(s.pos, v1), Pc = load3(s.pos, v2);
-    const F3 e1 = Pb - Pa;
-    const F3 p0 = Pa + e1 * reuse;
-    const F3 edge = normalize(e1), edge2 = normalize(Pc - Pa);
-    const F3 n0 = load3(s.fnormal, f0);
-    F3 dir;
-    float pdf_d;
-    if (f1 < 0) {
-      const F3 nrm = cross(n0, edge);
-      F3 tg, bt; coordinate_system(nrm, tg, bt);
-      const float z = fminf(1.f - 2.f * r1, 1.f - kEdgeEps);
-      const float r = sqrtf(fmaxf(0.f, 1.f - z * z));
-      const float phi = 2.f * kPi * r2;
-      dir = tg * (r * cosf(phi)) + bt * (r * sinf(phi)) + nrm * z;
-      pdf_d = 0.25f / kPi;
-    } else {
-      const F3 n1 = load3(s.fnormal, f1);
-      const float phi0 = acosf(dot(n0, n1));
-      pdf_d = 0.25f / phi0;
-      const F3 zz = normalize(n0 + n1);
-      const F3 yy = normalize(cross(n0, zz));
-      const F3 xx = cross(yy, zz);
-      float phi = (r1 - 0.5f) * phi0;
-      phi = fminf(fmaxf(phi, -0.5f * phi0 + kEdgeEps), 0.5f * phi0 - kEdgeEps);
-      const F3 x1 = xx * cosf(phi) + zz * sinf(phi);
-      const bool m0 = r2 > 0.5f;
-      const float bq = 4.f * r2 - (m0 ? 3.f : 1.f);
-      const float aq = sqrtf(1.f - bq * bq) * (1.f - (m0 ? 1.f : 0.f) * 2.f);
-      dir = x1 * aq + yy * bq;
-    }
-    const float pdf = pdf_e * pdf_d;
-    Hit he, hs;
-    cnt.v[kCntClosest] += 2;
-    if (!trace<false>(s, p0, -dir, kShadowEps, kRayMax, he, P.err)) return;
-    if (!trace<false>(s, p0, dir, kShadowEps, kRayMax, hs, P.err)) return;
-    SurfF xe = post_intersect(s, he.tri, he.u, he.v);
-    SurfF xs = post_intersect(s, hs.tri, hs.u, hs.v);
-    const float dl = length(xe.p - xs.p);
-    const float cos2 = fabsf(dot(xe.ng, dir));
-    const float its_t = length(xs.p - p0);
-    F3 n;
-    const float bval = base_val(its_t / dl, edge, -dir, xe.ng, edge2, n) * cos2;
-    if (bval == 0.f) return;
-    const float e0 = bval / pdf;
-    // emitter side: cumulative radiance per depth
-    F3 rad[kMaxDepth];
-    {
-      F3 T(1.f, 1.f, 1.f);
-      F3 rd = -dir;
-      SurfF xx = xe;
-      F3 cur = F3z();
-      bool alive = true;
-      for (int b = 0; b < D - 1; b++) {
-        if (alive) {
-          const int o = 3 + 5 * b;
-          F3 c;
-          alive = radiance_step(s, xx, rd, T, S(o), S(o + 1), S(o + 2),
-                                S(o + 3), S(o + 4), c, nullptr, cnt);
-          cur = cur + c;
-          if (T.x == 0.f && T.y == 0.f && T.z == 0.f) alive = false;
+  stage_top(P.s);
+  for_each_valid<EdgeState>(P,
+    [&](long long gslot, EdgeState& st) -> bool {
+      const ViewDesc& V = view_of(P, gslot);
+      const long long p = gslot - V.begin;
+      if (V.D < 2) return false;
+      const PathSmp S{&P, V.seed, gslot, p + V.slot_off};
+      const float r0 = S(0), r1 = S(1), r2 = S(2);
+      float reuse;
+      const float integral = __ldg(P.eint);
+      if (!(integral > 0.f)) return false;
+      const int e = sample_discrete(P.ecdf, P.ne, r0, reuse);
+      const int v0 = P.edges[5 * e], v1 = P.edges[5 * e + 1], f0 = P.edges[5 * e + 2], f1 = P.edges[5 * e + 3],
+                v2 = P.edges[5 * e + 4];
+      const float len_e = P.efunc[e];
+      if (!(len_e > 0.f)) return false;
+      const float pdf_e = (len_e / (integral * (float)P.ne)) / len_e;
+      const F3 Pa = load3(s.pos, v0), Pb = load3(s.pos, v1), Pc = load3(s.pos, v2);
+      const F3 e1 = Pb - Pa;
+      const F3 p0 = Pa + e1 * reuse;
+      const F3 edge = normalize(e1), edge2 = normalize(Pc - Pa);
+      const F3 n0 = load3(s.fnormal, f0);
+      F3 dir;
+      float pdf_d;
+      if (f1 < 0) {
+        const F3 nrm = cross(n0, edge);
+        F3 tg, bt; coordinate_system(nrm, tg, bt);
+        const float z = fminf(1.f - 2.f * r1, 1.f - kEdgeEps);
+        const float r = sqrtf(fmaxf(0.f, 1.f - z * z));
+        const float phi = 2.f * kPi * r2;
+        dir = tg * (r * cosf(phi)) + bt * (r * sinf(phi)) + nrm * z;
+        pdf_d = 0.25f / kPi;
+      } else {
+        const F3 n1 = load3(s.fnormal, f1);
+        const float phi0 = acosf(dot(n0, n1));
+        pdf_d = 0.25f / phi0;
+        const F3 zz = normalize(n0 + n1);
+        const F3 yy = normalize(cross(n0, zz));
+        const F3 xx = cross(yy, zz);
+        float phi = (r1 - 0.5f) * phi0;
+        phi = fminf(fmaxf(phi, -0.5f * phi0 + kEdgeEps), 0.5f * phi0 - kEdgeEps);
+        const F3 x1 = xx * cosf(phi) + zz * sinf(phi);
+        const bool m0 = r2 > 0.5f;
+        const float bq = 4.f * r2 - (m0 ? 3.f : 1.f);
+        const float aq = sqrtf(1.f - bq * bq) * (1.f - (m0 ? 1.f : 0.f) * 2.f);
+        dir = x1 * aq + yy * bq;
+      }
+      const float pdf = pdf_e * pdf_d;
+      Hit he, hs;
+      cnt.v[kCntClosest] += 2;
+      if (!trace<false>(s, p0, -dir, kShadowEps, kRayMax, he, P.err)) return false;
+      if (!trace<false>(s, p0, dir, kShadowEps, kRayMax, hs, P.err)) return false;
+      const SurfF xe = post_intersect(s, he.tri, he.u, he.v);
+      const SurfF xs = post_intersect(s, hs.tri, hs.u, hs.v);
+      const float dl = length(xe.p - xs.p);
+      const float cos2 = fabsf(dot(xe.ng, dir));
+      const float its_t = length(xs.p - p0);
+      F3 n;
+      const float bval = base_val(its_t / dl, edge, -dir, xe.ng, edge2, n) * cos2;
+      if (bval == 0.f) return false;
+      st.V = &V; st.gslot = gslot; st.p = p; st.x = xs; st.xe = xe; st.rdir = dir; st.p0 = p0; st.n = n;
+      st.w0 = bval / pdf; st.sedge = reuse; st.v0 = v0; st.v1 = v1; st.far_tri = he.tri;
+      return true;
+    },
+    [&](EdgeState& st) {
+      const ViewDesc& V = *st.V;
+      const int D = min(V.D, kMaxDepth);
+      const PathSmp S{&P, V.seed, st.gslot, st.p + V.slot_off};
+      // emitter side: cumulative radiance per depth
+      F3 rad[kMaxDepth];
+      {
+        F3 T(1.f, 1.f, 1.f);
+        F3 rd = -st.rdir;
+        SurfF xx = st.xe;
+        F3 cur = F3z();
+        bool alive = true;
+        for (int b = 0; b < D - 1; b++) {
+          if (alive) {
+            const int o = 3 + 5 * b;
+            F3 c;
+            alive = radiance_step(s, xx, rd, T, S(o), S(o + 1), S(o + 2), S(o + 3), S(o + 4), c, nullptr, cnt);
+            cur = cur + c;
+            if (T.x == 0.f && T.y == 0.f && T.z == 0.f) alive = false;
+          }
+          rad[b] = cur;
         }
-        rad[b] = cur;
       }
-    }
-    // sensor side
-    float W = 0.f;
-    {
-      F3 T(1.f, 1.f, 1.f);
-      F3 rd = dir;
-      SurfF xx = xs;
-      for (int b = 0; b < D - 1; b++) {
-        const int o = 3 + 5 * (D - 1) + 3 * b;
-        F3 c; int pix;
-        const bool more = importance_step(s, cam, xx, rd, T, S(o), S(o + 1),
-                                          S(o + 2), c, pix, cnt);
-        if (pix >= 0) W += dot(g_at(P, V, pix), rad[D - b - 2] * c) * e0;
-        if (!more) break;
+      // sensor side, paired by depth (BoundaryIndirect.cpp:158-175)
+      float W = 0.f;
+      {
+        F3 T(1.f, 1.f, 1.f);
+        F3 rd = st.rdir;
+        SurfF xx = st.x;
+        for (int b = 0; b < D - 1; b++) {
+          const int o = 3 + 5 * (D - 1) + 3 * b;
+          F3 c; int pix;
+          const bool more = importance_step(s, V.cam, xx, rd, T, S(o), S(o + 1), S(o + 2), c, pix, cnt);
+          if (pix >= 0) W += dot(g_at(P, V, pix), rad[D - b - 2] * c) * st.w0;
+          if (!more) break;
+        }
       }
-    }
-    if (W == 0.f || !isfinite(W)) return;
-    xdotn_vjp(P, V, W, xs.p, true, hs.tri, hs.u, hs.v, v0, v1, reuse, p0, he.tri, n, cnt);
-  });
+      if (W == 0.f || !isfinite(W)) return;
+      xdotn_vjp(P, V, W, st.x.p, true, st.x.tri, st.x.u, st.x.v, st.v0, st.v1, st.sedge, st.p0, st.far_tri, st.n,
+                cnt);
+    });
   flush_cnt(cnt, P.stats);
 }
 
@@ -961,73 +1069,81 @@ __global__ void __launch_bounds__(256) k_indirect_adj(Params P) {
 __global__ void __launch_bounds__(256) k_pixel_adj(Params P) {
   const DeviceScene& s = P.s;
   Cnt cnt;
-  for_each_slot(P, [&](long long gslot) {
-    const ViewDesc& V = view_of(P, gslot);
-    const long long p = gslot - V.begin;
-    const CameraDesc& cam = V.cam;
-    const int W_ = cam.w, WH = cam.w * cam.h;
-    const F3 cpos = cam_pos(cam);
-    const long long nanti = V.n / 4;
-    const long long slot = p % nanti;
-    const int anti = (int)(p / nanti);
-    // the 4 antithetic copies of a slot share its samples (BoundaryPixel.cpp:135-138)
-    const PathSmp S{&P, V.seed, V.begin / 4 + slot, slot + V.slot_off};
-    const float r = S(0);
-    float rr;
-    if (anti == 0) rr = r;
-    else if (anti == 1) rr = r < 0.5f ? r + 0.5f : r - 0.5f;
-    else if (anti == 2) rr = r < 0.75f ? 0.75f - r : 1.75f - r;
-    else rr = r < 0.25f ? 0.25f - r : 1.25f - r;
-    const float r4 = rr * 4.f;
-    const int bi = (int)floorf(r4);
-    float ox, oy;
-    if (bi == 0) { ox = 0.f; oy = r4; }
-    else if (bi == 1) { ox = r4 - 1.f; oy = 1.f; }
-    else if (bi == 2) { ox = 1.f; oy = 3.f - r4; }
-    else { ox = 4.f - r4; oy = 0.f; }
-    const float pdfs[4] = {0.25f / (cam.plane_len_y * (float)cam.w), 0.25f / (cam.plane_len_x * (float)cam.h),
-                           0.25f / (cam.plane_len_y * (float)cam.w), 0.25f / (cam.plane_len_x * (float)cam.h)};
-    const int bsel = bi < 0 ? 0 : (bi > 3 ? 3 : bi);
-    const float pdf = pdfs[bsel];
-    const F3 dedge[4] = {F3(0.f, 1.f, 0.f), F3(1.f, 0.f, 0.f), F3(0.f, 1.f, 0.f), F3(1.f, 0.f, 0.f)};
-    const F3 dvis[4] = {F3(1.f, 0.f, 0.f), F3(0.f, -1.f, 0.f), F3(-1.f, 0.f, 0.f), F3(0.f, 1.f, 0.f)};
-    const F3 edge = normalize(xform_vector(cam.raster_to_world, dedge[bsel]));
-    const F3 edge2 = normalize(xform_vector(cam.raster_to_world, dvis[bsel]));
-    const int pixel = (int)(p % WH);
-    const F3 p0 = xform_point(cam.raster_to_world, F3((float)(pixel % W_) + ox, (float)(pixel / W_) + oy, 0.f));
-    const F3 dir = normalize(p0 - cpos);
-    Hit h;
-    cnt.v[kCntClosest]++;
-    if (!trace<false>(s, p0, dir, kShadowEps, kRayMax, h, P.err)) return;
-    const F3 hitP = p0 + dir * h.t;
-    const SensorSample sds = sample_direct(cam, hitP);
-    const F3 dirc = sensor_ray_dir(cam, sds.qx, sds.qy);
-    SurfF x = post_intersect(s, h.tri, h.u, h.v);
-    const float dist = length(x.p - cpos);
-    const float dist1 = length(p0 - cpos);
-    const float cos2 = fabsf(dot(x.ng, -dirc));
-    F3 n;
-    // BoundaryPixel.cpp:92 reverses the sign convention
-    const float bval = -base_val(dist / dist1, edge, dirc, x.ng, edge2, n) * cos2;
-    const F3 g = g_at(P, V, pixel);
-    if (bval == 0.f || (g.x == 0.f && g.y == 0.f && g.z == 0.f)) return;
-    F3 T(sds.sensor_val, sds.sensor_val, sds.sensor_val);
-    F3 rdir = dirc;
-    F3 L = scrub(T * emitted(s, x, -rdir));
-    for (int b = 0; b < P.D; b++) {
-      const int o = 1 + 5 * b;
-      F3 c;
-      const bool more = radiance_step(s, x, rdir, T, S(o), S(o + 1),
-                                      S(o + 2), S(o + 3), S(o + 4), c,
-                                      nullptr, cnt);
-      L = L + c;
-      if (!more || (T.x == 0.f && T.y == 0.f && T.z == 0.f)) break;
-    }
-    const float Wt = dot(g, L * (bval / pdf));
-    if (Wt == 0.f || !isfinite(Wt)) return;
-    // the pixel-edge point is not a scene parameter: only the hit triangle moves
-    xdotn_vjp(P, V, Wt, cpos, false, -1, 0.f, 0.f, -1, -1, 0.f, p0, h.tri, n, cnt);
-  });
+  stage_top(P.s);
+  for_each_valid<EdgeState>(P,
+    [&](long long gslot, EdgeState& st) -> bool {
+      const ViewDesc& V = view_of(P, gslot);
+      const long long p = gslot - V.begin;
+      const CameraDesc& cam = V.cam;
+      const int W_ = cam.w, WH = cam.w * cam.h;
+      const F3 cpos = cam_pos(cam);
+      const long long nanti = V.n / 4;
+      const long long slot = p % nanti;
+      const int anti = (int)(p / nanti);
+      // the 4 antithetic copies of a slot share its samples (BoundaryPixel.cpp:135-138)
+      const PathSmp S{&P, V.seed, V.begin / 4 + slot, slot + V.slot_off};
+      const float r = S(0);
+      float rr;
+      if (anti == 0) rr = r;
+      else if (anti == 1) rr = r < 0.5f ? r + 0.5f : r - 0.5f;
+      else if (anti == 2) rr = r < 0.75f ? 0.75f - r : 1.75f - r;
+      else rr = r < 0.25f ? 0.25f - r : 1.25f - r;
+      const float r4 = rr * 4.f;
+      const int bi = (int)floorf(r4);
+      float ox, oy;
+      if (bi == 0) { ox = 0.f; oy = r4; }
+      else if (bi == 1) { ox = r4 - 1.f; oy = 1.f; }
+      else if (bi == 2) { ox = 1.f; oy = 3.f - r4; }
+      else { ox = 4.f - r4; oy = 0.f; }
+      const int bsel = bi < 0 ? 0 : (bi > 3 ? 3 : bi);
+      const float pdf = (bsel & 1) ? 0.25f / (cam.plane_len_x * (float)cam.h) : 0.25f / (cam.plane_len_y * (float)cam.w);
+      const F3 dedge = (bsel & 1) ? F3(1.f, 0.f, 0.f) : F3(0.f, 1.f, 0.f);
+      const F3 dvis = bsel == 0 ? F3(1.f, 0.f, 0.f) : (bsel == 1 ? F3(0.f, -1.f, 0.f)
+                                                    : (bsel == 2 ? F3(-1.f, 0.f, 0.f) : F3(0.f, 1.f, 0.f)));
+      const F3 edge = normalize(xform_vector(cam.raster_to_world, dedge));
+      const F3 edge2 = normalize(xform_vector(cam.raster_to_world, dvis));
+      const int pixel = (int)(p % WH);
+      const F3 p0 = xform_point(cam.raster_to_world, F3((float)(pixel % W_) + ox, (float)(pixel / W_) + oy, 0.f));
+      const F3 dir = normalize(p0 - cpos);
+      Hit h;
+      cnt.v[kCntClosest]++;
+      if (!trace<false>(s, p0, dir, kShadowEps, kRayMax, h, P.err)) return false;
+      const F3 hitP = p0 + dir * h.t;
+      const SensorSample sds = sample_direct(cam, hitP);
+      const F3 dirc = sensor_ray_dir(cam, sds.qx, sds.qy);
+      const SurfF x = post_intersect(s, h.tri, h.u, h.v);
+      const float dist = length(x.p - cpos);
+      const float dist1 = length(p0 - cpos);
+      const float cos2 = fabsf(dot(x.ng, -dirc));
+      F3 n;
+      // BoundaryPixel.cpp:92 reverses the sign convention
+      const float bval = -base_val(dist / dist1, edge, dirc, x.ng, edge2, n) * cos2;
+      const F3 g = g_at(P, V, pixel);
+      if (bval == 0.f || (g.x == 0.f && g.y == 0.f && g.z == 0.f)) return false;
+      st.V = &V; st.gslot = V.begin / 4 + slot; st.p = slot; st.x = x; st.rdir = dirc;
+      st.T0 = F3(sds.sensor_val, sds.sensor_val, sds.sensor_val);
+      st.p0 = p0; st.n = n; st.w0 = bval / pdf; st.far_tri = h.tri; st.g = g;
+      return true;
+    },
+    [&](EdgeState& st) {
+      const ViewDesc& V = *st.V;
+      const PathSmp S{&P, V.seed, st.gslot, st.p + V.slot_off};
+      SurfF x = st.x;
+      F3 T = st.T0, rdir = st.rdir;
+      F3 L = scrub(T * emitted(s, x, -rdir));
+      for (int b = 0; b < V.D; b++) {
+        const int o = 1 + 5 * b;
+        F3 c;
+        const bool more = radiance_step(s, x, rdir, T, S(o), S(o + 1), S(o + 2), S(o + 3), S(o + 4), c, nullptr,
+                                        cnt);
+        L = L + c;
+        if (!more || (T.x == 0.f && T.y == 0.f && T.z == 0.f)) break;
+      }
+      const float Wt = dot(st.g, L * st.w0);
+      if (Wt == 0.f || !isfinite(Wt)) return;
+      // the pixel-edge point is not a scene parameter: only the hit triangle moves
+      xdotn_vjp(P, V, Wt, cam_pos(V.cam), false, -1, 0.f, 0.f, -1, -1, 0.f, st.p0, st.far_tri, st.n, cnt);
+    });
   flush_cnt(cnt, P.stats);
 }
 
@@ -1104,6 +1220,7 @@ __global__ void k_view_loss(long long npix, const ViewDesc* views, const long lo
 
 __global__ void k_intersect(DeviceScene s, int n, const float* org, const float* dir, const float* tmin,
                             const float* tmax, int* tri, float* u, float* v, float* t, int* err) {
+  stage_top(s);
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   Hit h;
@@ -1112,6 +1229,7 @@ __global__ void k_intersect(DeviceScene s, int n, const float* org, const float*
 }
 __global__ void k_occluded(DeviceScene s, int n, const float* org, const float* dir, const float* tmin,
                            const float* tmax, int* vis) {
+  stage_top(s);
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   vis[i] = occluded(s, make_f3(org + 3 * i), make_f3(dir + 3 * i), tmin[i], tmax[i]) ? 0 : 1;
@@ -1126,6 +1244,11 @@ using namespace trn;
 struct trn_viewset {
   trn_scene* scene = nullptr;
   int nviews = 0;
+  int cap = 0;                    // allocated view capacity
+  ViewDesc* h_stage = nullptr;    // pinned staging of the view table
+  long long* h_stage_begin = nullptr;
+  cudaEvent_t copy_done = nullptr;
+  bool pbegin_dirty = true;
   long long npix = 0;
   std::vector<trn_view> h_views;
   std::vector<long long> h_pbegin;
@@ -1140,6 +1263,12 @@ struct trn_viewset {
   // slot layout currently uploaded: spp multiplier and per-view spp
   int uploaded_key = -2;
   long long total = 0;
+  // image / dL/dI base buffers of the uploaded table (views without their own)
+  float* cur_image = nullptr;
+  const float* cur_dLdI = nullptr;
+  int cur_depth = -1;
+  float* want_image = nullptr;
+  const float* want_dLdI = nullptr;
 };
 
 namespace {
@@ -1176,8 +1305,9 @@ int upload_views(trn_viewset* vs, const trn_render_options* o, int integrator, i
   float* s_gpos = vs->scene->g_pos;
   float* s_gvn = vs->scene->g_vnormal;
   float* s_gtex = vs->scene->g_texels;
-  const int key = spp_override;  // the layout only depends on the per-view spp
-  if (vs->uploaded_key == key && key != -2) {
+  const int key = spp_override;  // the layout depends on the per-view spp, buffers and depth
+  if (vs->uploaded_key == key && key != -2 && vs->cur_image == vs->want_image && vs->cur_dLdI == vs->want_dLdI &&
+      vs->cur_depth == o->max_bounces) {
     total = vs->total;
     if (integrator == TRN_PIXEL_EDGE)
       for (int v = 0; v < vs->nviews; v++) {
@@ -1189,8 +1319,12 @@ int upload_views(trn_viewset* vs, const trn_render_options* o, int integrator, i
       }
     return 0;
   }
-  std::vector<ViewDesc> d(vs->nviews);
-  std::vector<long long> begin(vs->nviews);
+  vs->cur_image = vs->want_image;
+  vs->cur_dLdI = vs->want_dLdI;
+  vs->cur_depth = o->max_bounces;
+  if (vs->copy_done) cudaEventSynchronize(vs->copy_done);  // previous upload has left the staging buffer
+  ViewDesc* d = vs->h_stage;
+  long long* begin = vs->h_stage_begin;
   total = 0;
   for (int v = 0; v < vs->nviews; v++) {
     const trn_view& hv = vs->h_views[v];
@@ -1206,10 +1340,13 @@ int upload_views(trn_viewset* vs, const trn_render_options* o, int integrator, i
     d[v].pix_off = vs->h_pbegin[v];
     d[v].inv_spp = hv.weight > 0.f ? hv.weight : (spp > 0 ? 1.0f / (float)spp : 0.f);
     d[v].slot_off = hv.slot_offset;
+    d[v].D = hv.max_bounces > 0 ? std::min(hv.max_bounces, (int)kMaxDepth) : o->max_bounces;
+    d[v].image = hv.image ? hv.image : (vs->cur_image ? vs->cur_image + 3 * vs->h_pbegin[v] : nullptr);
+    d[v].dLdI = hv.dLdI ? hv.dLdI : (vs->cur_dLdI ? vs->cur_dLdI + 3 * vs->h_pbegin[v] : nullptr);
     d[v].gpos = hv.grad_positions ? hv.grad_positions : s_gpos;
     d[v].gvn = hv.grad_vertex_normals ? hv.grad_vertex_normals : s_gvn;
     d[v].gtex = hv.grad_texels ? hv.grad_texels : s_gtex;
-    d[v].seed = (uint32_t)hv.seed * 7919u + (uint32_t)v;
+    d[v].seed = (uint32_t)hv.seed;  // independent of the view's position in the set
     d[v].spp = spp;
     d[v].pad_ = 0;
     d[v].pfunc = vs->pfunc ? vs->pfunc + (long long)v * vs->ne : nullptr;
@@ -1218,10 +1355,9 @@ int upload_views(trn_viewset* vs, const trn_render_options* o, int integrator, i
     begin[v] = total;
     total += d[v].n;
   }
-  TRN_CUDA_TRY(cudaMemcpyAsync(vs->views, d.data(), sizeof(ViewDesc) * vs->nviews, cudaMemcpyHostToDevice, st));
-  TRN_CUDA_TRY(cudaMemcpyAsync(vs->vbegin, begin.data(), sizeof(long long) * vs->nviews, cudaMemcpyHostToDevice, st));
-  // the host vectors must outlive the async copies
-  TRN_CUDA_TRY(cudaStreamSynchronize(st));
+  TRN_CUDA_TRY(cudaMemcpyAsync(vs->views, d, sizeof(ViewDesc) * vs->nviews, cudaMemcpyHostToDevice, st));
+  TRN_CUDA_TRY(cudaMemcpyAsync(vs->vbegin, begin, sizeof(long long) * vs->nviews, cudaMemcpyHostToDevice, st));
+  TRN_CUDA_TRY(cudaEventRecord(vs->copy_done, st));
   vs->uploaded_key = key;
   vs->total = total;
   return 0;
@@ -1242,8 +1378,6 @@ Params base_params(trn_scene* s, trn_viewset* vs, const trn_render_options* o, i
   P.term = (uint32_t)integrator;
   P.seed = (uint32_t)o->seed;
   P.D = o->max_bounces;
-  P.image = nullptr;
-  P.dLdI = nullptr;
   P.g_pos = s->g_pos; P.g_vn = s->g_vnormal; P.g_tex = s->g_texels; P.diff_tex = s->ntexel > 0;
   P.edges = s->edges; P.ecdf = s->sec_cdf; P.efunc = s->sec_func; P.eint = s->sec_integral_dev; P.ne = s->ne;
   P.err = s->err;
@@ -1282,27 +1416,28 @@ void launch(K kernel, const trn_launch* ln, long long total, const Params& P, cu
 }
 
 int render_views(trn_scene* s, trn_viewset* vs, const trn_render_options* o, int integrator,
-                 const trn_samples* smp, const trn_launch* ln, int spp_override, float* image, const float* dLdI,
-                 cudaStream_t st) {
+                 const trn_samples* smp, const trn_launch* ln, int spp_override, bool forward, float* image,
+                 const float* dLdI, cudaStream_t st) {
   if (check_common(s, o, integrator)) return -1;
   if (!vs || vs->nviews <= 0) { set_error("empty view set"); return -1; }
   if (validate_launch(ln)) return -1;
   long long total = 0;
+  vs->want_image = forward ? image : nullptr;
+  vs->want_dLdI = forward ? nullptr : dLdI;
   if (upload_views(vs, o, integrator, spp_override, total, st)) return -1;
   Params P = base_params(s, vs, o, integrator, smp, ln, total);
   const long long slots = integrator == TRN_PIXEL_EDGE ? total / 4 : total;
   if (P.table && P.stride < slots) { set_error("sample table too small"); return -1; }
-  if (image) {
-    TRN_CUDA_TRY(cudaMemsetAsync(image, 0, sizeof(float) * 3 * vs->npix, st));
+  if (forward) {
+    // a call buffer is cleared; views with their own image accumulate into it
+    if (image) TRN_CUDA_TRY(cudaMemsetAsync(image, 0, sizeof(float) * 3 * vs->npix, st));
     if (integrator != TRN_PATH_TRACER || total == 0) return 0;  // edge terms have no primal image
-    P.image = image;
     TRN_CUDA_TRY(cudaMemsetAsync(vs->work, 0, sizeof(unsigned long long), st));
     launch(k_path_fwd, ln, total, P, st);
     TRN_CUDA_TRY(cudaGetLastError());
     return 0;
   }
   if (total == 0) return 0;
-  P.dLdI = dLdI;
   s->grads_finalized = false;
   if (integrator == TRN_PRIMARY_EDGE) {
     if (s->ne == 0) return 0;
@@ -1325,6 +1460,66 @@ int render_views(trn_scene* s, trn_viewset* vs, const trn_render_options* o, int
   return 0;
 }
 
+// (Re)define the views of a set. Device arrays grow to the largest view count
+// seen; the per-view silhouette workspace is E floats x 2 per view.
+int set_views(trn_viewset* vs, int nviews, const trn_view* views) {
+  std::vector<long long> pb;
+  long long pix = 0;
+  for (int v = 0; v < nviews; v++) {
+    const trn_view& hv = views[v];
+    if (hv.camera.width <= 0 || hv.camera.height <= 0 || hv.spp < 0 || hv.max_bounces < 0 ||
+        hv.max_bounces > kMaxDepth) {
+      set_error("viewset: invalid view (resolution, spp or max_bounces)");
+      return -1;
+    }
+    const long long off = hv.pixel_offset >= 0 ? hv.pixel_offset : pix;
+    if (!pb.empty() && off < pb.back()) { set_error("viewset: pixel offsets must be non-decreasing"); return -1; }
+    pb.push_back(off);
+    pix = std::max(pix, off + (long long)hv.camera.width * hv.camera.height);
+  }
+  if (vs->copy_done) cudaEventSynchronize(vs->copy_done);  // staging buffers are free again
+  if (nviews > vs->cap) {
+    void* old[] = {vs->views, vs->vbegin, vs->pbegin, vs->pfunc, vs->pcdf, vs->pint};
+    for (void* q : old) if (q) cudaFree(q);
+    if (vs->h_stage) cudaFreeHost(vs->h_stage);
+    if (vs->h_stage_begin) cudaFreeHost(vs->h_stage_begin);
+    vs->views = nullptr; vs->vbegin = vs->pbegin = nullptr; vs->pfunc = vs->pcdf = vs->pint = nullptr;
+    vs->h_stage = nullptr; vs->h_stage_begin = nullptr;
+    const int cap = std::max(nviews, 2 * vs->cap);
+    bool ok = cudaMalloc(&vs->views, sizeof(ViewDesc) * cap) == cudaSuccess &&
+              cudaMalloc(&vs->vbegin, sizeof(long long) * cap) == cudaSuccess &&
+              cudaMalloc(&vs->pbegin, sizeof(long long) * cap) == cudaSuccess &&
+              cudaMalloc(&vs->pint, sizeof(float) * cap) == cudaSuccess &&
+              cudaMallocHost(&vs->h_stage, sizeof(ViewDesc) * cap) == cudaSuccess &&
+              cudaMallocHost(&vs->h_stage_begin, sizeof(long long) * 2 * cap) == cudaSuccess;
+    if (ok && vs->ne > 0)
+      ok = cudaMalloc(&vs->pfunc, sizeof(float) * (size_t)cap * vs->ne) == cudaSuccess &&
+           cudaMalloc(&vs->pcdf, sizeof(float) * (size_t)cap * vs->ne) == cudaSuccess;
+    if (!ok) { set_error("viewset: out of memory"); vs->cap = 0; return -1; }
+    cudaMemset(vs->pint, 0, sizeof(float) * cap);
+    vs->cap = cap;
+  }
+  vs->nviews = nviews;
+  vs->h_views.assign(views, views + nviews);
+  vs->h_pbegin = pb;
+  vs->npix = pix;
+  vs->uploaded_key = -2;
+  vs->pbegin_dirty = true;
+  return 0;
+}
+
+// upload the per-view pixel offsets (used by the loss kernel) when they changed
+int upload_pbegin(trn_viewset* vs, cudaStream_t st) {
+  if (!vs->pbegin_dirty) return 0;
+  if (vs->copy_done) cudaEventSynchronize(vs->copy_done);
+  long long* stage = vs->h_stage_begin + vs->cap;
+  std::memcpy(stage, vs->h_pbegin.data(), sizeof(long long) * vs->nviews);
+  TRN_CUDA_TRY(cudaMemcpyAsync(vs->pbegin, stage, sizeof(long long) * vs->nviews, cudaMemcpyHostToDevice, st));
+  TRN_CUDA_TRY(cudaEventRecord(vs->copy_done, st));
+  vs->pbegin_dirty = false;
+  return 0;
+}
+
 int single_view(trn_scene* s, const trn_camera* cam, trn_viewset** out) {
   if (!cam) { set_error("null camera"); return -1; }
   trn_view v;
@@ -1342,55 +1537,32 @@ int trn_viewset_create(trn_scene* s, int nviews, const trn_view* views, trn_view
   *out = nullptr;
   trn_viewset* vs = new trn_viewset();
   vs->scene = s;
-  vs->nviews = nviews;
-  vs->h_views.assign(views, views + nviews);
   vs->ne = s->ne;
-  long long pix = 0;
-  for (int v = 0; v < nviews; v++) {
-    const trn_view& hv = views[v];
-    if (hv.camera.width <= 0 || hv.camera.height <= 0) {
-      set_error("trn_viewset_create: invalid camera resolution");
-      delete vs;
-      return -1;
-    }
-    const long long off = hv.pixel_offset >= 0 ? hv.pixel_offset : pix;
-    vs->h_pbegin.push_back(off);
-    pix = std::max(pix, off + (long long)hv.camera.width * hv.camera.height);
-  }
-  for (int v = 1; v < nviews; v++)
-    if (vs->h_pbegin[v] < vs->h_pbegin[v - 1]) {
-      set_error("trn_viewset_create: pixel offsets must be non-decreasing");
-      delete vs;
-      return -1;
-    }
-  vs->npix = pix;
-  auto fail = [&](const char* what) {
-    set_error(std::string("trn_viewset_create: ") + what);
+  if (cudaMalloc(&vs->work, sizeof(unsigned long long)) != cudaSuccess ||
+      cudaEventCreateWithFlags(&vs->copy_done, cudaEventDisableTiming) != cudaSuccess) {
+    set_error("trn_viewset_create: out of memory");
     trn_viewset_destroy(vs);
     return -1;
-  };
-  if (cudaMalloc(&vs->views, sizeof(ViewDesc) * nviews) != cudaSuccess) return fail("out of memory");
-  if (cudaMalloc(&vs->vbegin, sizeof(long long) * nviews) != cudaSuccess) return fail("out of memory");
-  if (cudaMalloc(&vs->pbegin, sizeof(long long) * nviews) != cudaSuccess) return fail("out of memory");
-  if (cudaMalloc(&vs->work, sizeof(unsigned long long)) != cudaSuccess) return fail("out of memory");
-  if (cudaMemcpy(vs->pbegin, vs->h_pbegin.data(), sizeof(long long) * nviews, cudaMemcpyHostToDevice) != cudaSuccess)
-    return fail("copy failed");
-  if (s->ne > 0) {
-    const size_t n = (size_t)nviews * s->ne;
-    if (cudaMalloc(&vs->pfunc, sizeof(float) * n) != cudaSuccess) return fail("out of memory");
-    if (cudaMalloc(&vs->pcdf, sizeof(float) * n) != cudaSuccess) return fail("out of memory");
   }
-  if (cudaMalloc(&vs->pint, sizeof(float) * nviews) != cudaSuccess) return fail("out of memory");
-  cudaMemset(vs->pint, 0, sizeof(float) * nviews);
+  if (set_views(vs, nviews, views)) { trn_viewset_destroy(vs); return -1; }
   *out = vs;
   return 0;
 }
 
+int trn_viewset_update(trn_viewset* vs, int nviews, const trn_view* views) {
+  if (!vs || !views || nviews <= 0) { set_error("trn_viewset_update: invalid arguments"); return -1; }
+  return set_views(vs, nviews, views);
+}
+
 int trn_viewset_destroy(trn_viewset* vs) {
   if (!vs) return 0;
+  if (vs->copy_done) cudaEventSynchronize(vs->copy_done);
   void* ptrs[] = {vs->views, vs->vbegin, vs->pbegin, vs->pfunc, vs->pcdf, vs->pint, vs->work};
   for (void* p : ptrs)
     if (p) cudaFree(p);
+  if (vs->h_stage) cudaFreeHost(vs->h_stage);
+  if (vs->h_stage_begin) cudaFreeHost(vs->h_stage_begin);
+  if (vs->copy_done) cudaEventDestroy(vs->copy_done);
   delete vs;
   return 0;
 }
@@ -1403,19 +1575,24 @@ int trn_viewset_num_pixels(const trn_viewset* vs, long long* npix) {
 
 int trn_render_views_fwd(trn_scene* s, trn_viewset* vs, const trn_render_options* o, int integrator,
                          const trn_samples* smp, const trn_launch* ln, float* images, cudaStream_t st) {
-  if (!images) { set_error("trn_render_views_fwd: null image"); return -1; }
-  return render_views(s, vs, o, integrator, smp, ln, -1, images, nullptr, st);
+  if (!images)
+    for (const trn_view& v : vs->h_views)
+      if (!v.image) { set_error("trn_render_views_fwd: no image buffer for a view"); return -1; }
+  return render_views(s, vs, o, integrator, smp, ln, -1, true, images, nullptr, st);
 }
 
 int trn_render_views_grad(trn_scene* s, trn_viewset* vs, const trn_render_options* o, int integrator,
                           const trn_samples* smp, const trn_launch* ln, const float* dLdI, cudaStream_t st) {
-  if (!dLdI) { set_error("trn_render_views_grad: null dLdI"); return -1; }
-  return render_views(s, vs, o, integrator, smp, ln, -1, nullptr, dLdI, st);
+  if (!dLdI)
+    for (const trn_view& v : vs->h_views)
+      if (!v.dLdI) { set_error("trn_render_views_grad: no dL/dI buffer for a view"); return -1; }
+  return render_views(s, vs, o, integrator, smp, ln, -1, false, nullptr, dLdI, st);
 }
 
 int trn_views_loss(trn_viewset* vs, const float* images, const float* targets, float* dLdI, float* loss,
                    cudaStream_t st) {
   if (!vs || !images || !targets) { set_error("trn_views_loss: null argument"); return -1; }
+  if (upload_pbegin(vs, st)) return -1;
   if (loss) TRN_CUDA_TRY(cudaMemsetAsync(loss, 0, sizeof(float) * vs->nviews, st));
   const long long n = vs->npix;
   k_view_loss<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, vs->views, vs->pbegin, vs->nviews, images, targets,
@@ -1431,7 +1608,7 @@ int trn_render_fwd(trn_scene* s, const trn_camera* cam, const trn_render_options
   if (!image) { set_error("trn_render_fwd: null image"); return -1; }
   trn_viewset* vs = nullptr;
   if (single_view(s, cam, &vs)) return -1;
-  const int rc = render_views(s, vs, o, integrator, smp, nullptr, spp_of(o, integrator), image, nullptr, st);
+  const int rc = render_views(s, vs, o, integrator, smp, nullptr, spp_of(o, integrator), true, image, nullptr, st);
   cudaStreamSynchronize(st);
   trn_viewset_destroy(vs);
   return rc;
@@ -1443,7 +1620,7 @@ int trn_render_grad(trn_scene* s, const trn_camera* cam, const trn_render_option
   if (!dLdI) { set_error("trn_render_grad: null dLdI"); return -1; }
   trn_viewset* vs = nullptr;
   if (single_view(s, cam, &vs)) return -1;
-  const int rc = render_views(s, vs, o, integrator, smp, nullptr, spp_of(o, integrator), nullptr, dLdI, st);
+  const int rc = render_views(s, vs, o, integrator, smp, nullptr, spp_of(o, integrator), false, nullptr, dLdI, st);
   cudaStreamSynchronize(st);
   trn_viewset_destroy(vs);
   return rc;

@@ -281,6 +281,117 @@ __global__ void k_refit(int n, const unsigned long long* keys, const float* pos,
   }
 }
 
+
+// ---------------------------------------------------------------------------
+// collapse the binary LBVH into the 8-wide quantised BVH (top-down, one
+// level of wide nodes per launch). Each wide node takes the two children of
+// its binary node and repeatedly opens the internal child with the largest
+// surface area until it holds 8 children or only leaves.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float box_area(const float* lo, const float* hi) {
+  const float dx = fmaxf(hi[0] - lo[0], 0.f), dy = fmaxf(hi[1] - lo[1], 0.f), dz = fmaxf(hi[2] - lo[2], 0.f);
+  return dx * dy + dy * dz + dz * dx;
+}
+
+__device__ __forceinline__ void child_box(const BvhNode& n, int side, float* lo, float* hi) {
+  const float* a = reinterpret_cast<const float*>(&n);
+  const int o = side ? 6 : 0;
+  lo[0] = a[o]; lo[1] = a[o + 1]; lo[2] = a[o + 2];
+  hi[0] = a[o + 3]; hi[1] = a[o + 4]; hi[2] = a[o + 5];
+}
+
+__device__ __forceinline__ float qdecode(int q, float scale, float origin) {
+  return __fmaf_rn((float)q, scale, origin);
+}
+
+__global__ void k_collapse(int n_in, const int2* in, int2* out, int* counters, const BvhNode* nodes,
+                           const float4* tri_verts, WNode* wnodes, float4* wtri) {
+  const int item = blockIdx.x * blockDim.x + threadIdx.x;
+  if (item >= n_in) return;
+  const int b = in[item].x, w = in[item].y;
+  int cid[8];
+  float clo[8][3], chi[8][3];
+  const BvhNode nb = nodes[b];
+  cid[0] = nb.d.x; child_box(nb, 0, clo[0], chi[0]);
+  cid[1] = nb.d.y; child_box(nb, 1, clo[1], chi[1]);
+  int n = 2;
+  while (n < 8) {
+    int best = -1;
+    float best_a = -1.f;
+    for (int i = 0; i < n; i++)
+      if (cid[i] >= 0) {
+        const float a = box_area(clo[i], chi[i]);
+        if (a > best_a) { best_a = a; best = i; }
+      }
+    if (best < 0) break;
+    const BvhNode c = nodes[cid[best]];
+    cid[best] = c.d.x; child_box(c, 0, clo[best], chi[best]);
+    cid[n] = c.d.y; child_box(c, 1, clo[n], chi[n]);
+    n++;
+  }
+  int ni = 0, nl = 0;
+  for (int i = 0; i < n; i++) (cid[i] >= 0 ? ni : nl)++;
+  const int child_base = ni ? atomicAdd(&counters[0], ni) : 0;
+  const int tri_base = nl ? atomicAdd(&counters[1], nl) : 0;
+  const int qbase = ni ? atomicAdd(&counters[2], ni) : 0;
+  WNode wn;
+  float lo[3] = {3.4e38f, 3.4e38f, 3.4e38f}, hi[3] = {-3.4e38f, -3.4e38f, -3.4e38f};
+  for (int i = 0; i < n; i++)
+    for (int k = 0; k < 3; k++) { lo[k] = fminf(lo[k], clo[i][k]); hi[k] = fmaxf(hi[k], chi[i][k]); }
+  float scale[3];
+  unsigned char ebias[3];
+  for (int k = 0; k < 3; k++) {
+    const float ext = hi[k] - lo[k];
+    int e = -100;
+    if (ext > 0.f) {
+      int ee;
+      const float m = frexpf(ext / 255.f, &ee);
+      e = (m == 0.5f) ? ee - 1 : ee;
+      while (ldexpf(255.f, e) < ext) e++;
+    }
+    e = max(-126, min(127, e));
+    ebias[k] = (unsigned char)(e + 127);
+    scale[k] = __uint_as_float((unsigned)(e + 127) << 23);
+  }
+  wn.ox = lo[0]; wn.oy = lo[1]; wn.oz = lo[2];
+  wn.ex = ebias[0]; wn.ey = ebias[1]; wn.ez = ebias[2];
+  wn.nchild = (unsigned char)n;
+  wn.child_base = child_base;
+  wn.tri_base = tri_base;
+  int ii = 0, il = 0;
+  for (int i = 0; i < 8; i++) {
+    if (i >= n) {
+      wn.meta[i] = 0;
+      for (int k = 0; k < 3; k++) { wn.qlo[k][i] = 255; wn.qhi[k][i] = 0; }
+      continue;
+    }
+    for (int k = 0; k < 3; k++) {
+      int ql = (int)floorf((clo[i][k] - lo[k]) / scale[k]);
+      int qh = (int)ceilf((chi[i][k] - lo[k]) / scale[k]);
+      ql = max(0, min(255, ql));
+      qh = max(0, min(255, qh));
+      while (ql > 0 && qdecode(ql, scale[k], lo[k]) > clo[i][k]) ql--;
+      while (qh < 255 && qdecode(qh, scale[k], lo[k]) < chi[i][k]) qh++;
+      wn.qlo[k][i] = (unsigned char)ql;
+      wn.qhi[k][i] = (unsigned char)qh;
+    }
+    if (cid[i] >= 0) {
+      wn.meta[i] = (unsigned char)(0x80 | ii);
+      out[qbase + ii] = make_int2(cid[i], child_base + ii);
+      ii++;
+    } else {
+      const int leaf = ~cid[i];
+      wn.meta[i] = (unsigned char)(0xC0 | il);
+      const int slot = tri_base + il;
+      wtri[3 * slot + 0] = tri_verts[3 * leaf + 0];
+      wtri[3 * slot + 1] = tri_verts[3 * leaf + 1];
+      wtri[3 * slot + 2] = tri_verts[3 * leaf + 2];
+      il++;
+    }
+  }
+  wnodes[w] = wn;
+}
+
 // ---------------------------------------------------------------------------
 // geometry-chain adjoint
 // ---------------------------------------------------------------------------
@@ -629,6 +740,10 @@ int trn_scene_create(const trn_scene_desc* d, trn_scene** out) {
       dev_alloc_copy(&s->keys, (const unsigned long long*)nullptr, (size_t)nt) ||
       dev_alloc_copy(&s->keys_alt, (const unsigned long long*)nullptr, (size_t)nt) ||
       dev_alloc_copy(&s->bounds, (const float*)nullptr, 6) ||
+      dev_alloc_copy(&s->wnodes, (const WNode*)nullptr, std::max(1, nt)) ||
+      dev_alloc_copy(&s->wtri, (const float4*)nullptr, 3 * (size_t)nt) ||
+      dev_alloc_copy(&s->wqueue, (const int*)nullptr, 4 * (size_t)std::max(1, nt)) ||
+      dev_alloc_copy(&s->wcount, (const int*)nullptr, 4) ||
       dev_alloc_copy(&s->g_pos, (const float*)nullptr, 3 * (size_t)nv) ||
       dev_alloc_copy(&s->g_vnormal, (const float*)nullptr, 3 * (size_t)nv) ||
       dev_alloc_copy(&s->g_texels, (const float*)nullptr, std::max<size_t>(3, 3 * (size_t)ntexel)) ||
@@ -660,7 +775,7 @@ int trn_scene_destroy(trn_scene* s) {
                   s->light_integral_dev, s->bsdfs, s->texs, s->edges, s->sec_func, s->sec_cdf,
                   s->sec_integral_dev, s->nodes, s->tri_verts, s->parent, s->flags, s->keys, s->keys_alt,
                   s->sort_tmp, s->bounds, s->g_pos, s->g_vnormal, s->g_texels, s->g_translation, s->err,
-                  s->stats};
+                  s->stats, s->wnodes, s->wtri, s->wqueue, s->wcount};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   delete s;
@@ -708,6 +823,30 @@ int trn_scene_configure(trn_scene* s, cudaStream_t st) {
   }
   k_refit<<<nblk(nt), 256, 0, st>>>(nt, s->keys_alt, s->pos, s->idx, s->nodes, s->parent, s->flags, s->tri_verts);
   count_launch(1);
+  // 8-wide quantised BVH
+  s->n_wnodes = 0;
+  if (nt > 1) {
+    int2* qa = reinterpret_cast<int2*>(s->wqueue);
+    int2* qb = qa + nt;
+    const int init[4] = {1, 0, 0, 0};
+    const int2 root = make_int2(0, 0);
+    TRN_CUDA_TRY(cudaMemcpyAsync(s->wcount, init, sizeof(init), cudaMemcpyHostToDevice, st));
+    TRN_CUDA_TRY(cudaMemcpyAsync(qa, &root, sizeof(int2), cudaMemcpyHostToDevice, st));
+    int n_in = 1;
+    int levels = 0;
+    while (n_in > 0) {
+      TRN_CUDA_TRY(cudaMemsetAsync(s->wcount + 2, 0, sizeof(int), st));
+      k_collapse<<<nblk(n_in, 128), 128, 0, st>>>(n_in, qa, qb, s->wcount, s->nodes, s->tri_verts, s->wnodes, s->wtri);
+      count_launch(1);
+      int c[4];
+      TRN_CUDA_TRY(cudaMemcpyAsync(c, s->wcount, sizeof(c), cudaMemcpyDeviceToHost, st));
+      TRN_CUDA_TRY(cudaStreamSynchronize(st));
+      n_in = c[2];
+      s->n_wnodes = c[0];
+      std::swap(qa, qb);
+      if (++levels > 64) { set_error("trn_scene_configure: wide BVH collapse did not terminate"); return -1; }
+    }
+  }
   TRN_CUDA_TRY(cudaGetLastError());
   TRN_CUDA_TRY(cudaStreamSynchronize(st));
   s->configured = true;

@@ -57,6 +57,11 @@ struct trn_scene {
   void* sort_tmp = nullptr;
   size_t sort_tmp_bytes = 0;
   float* bounds = nullptr;        // [6]
+  trn::WNode* wnodes = nullptr;   // [<= T] 8-wide nodes
+  float4* wtri = nullptr;         // [T][3]
+  int* wqueue = nullptr;          // [2][T] (binary node, wide node) work pairs
+  int* wcount = nullptr;          // [4] counters
+  int n_wnodes = 0;
   // ---- gradients (device) ------------------------------------------------------
   float* g_pos = nullptr;         // [V][3] dL/d(world position)
   float* g_vnormal = nullptr;     // [V][3] dL/d(vertex normal)
@@ -79,6 +84,7 @@ struct trn_scene {
     s.light_radiance = light_radiance;
     s.n_bsdf = nbsdf; s.bsdfs = bsdfs; s.texs = texs; s.texels = texels;
     s.nodes = nodes; s.tri_verts = tri_verts; s.root_is_leaf = nt == 1;
+    s.wnodes = wnodes; s.wtri = wtri; s.n_wnodes = n_wnodes;
     return s;
   }
 };

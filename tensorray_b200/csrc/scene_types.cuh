@@ -42,6 +42,24 @@ struct alignas(16) BvhNode {
   int4 d;    // c0 c1 - -
 };
 
+// 8-wide BVH node with quantised child boxes (80 bytes). Child boxes are
+// stored as 8-bit offsets from `origin` in units of a per-axis power of two,
+// rounded outwards, so decoding is conservative. Internal children of a node
+// are stored contiguously from child_base, leaf triangles from tri_base;
+// meta[i]: bit 7 = slot used, bit 6 = leaf, bits 0-5 = offset from the base.
+struct alignas(16) WNode {
+  float ox, oy, oz;
+  unsigned char ex, ey, ez, nchild;  // biased exponents (IEEE bias 127)
+  int child_base;
+  int tri_base;
+  unsigned char meta[8];
+  unsigned char qlo[3][8];
+  unsigned char qhi[3][8];
+};
+static_assert(sizeof(WNode) == 80, "WNode must be 80 bytes");
+
+constexpr int kTopNodes = 73;  // root + 8 + 64 wide nodes staged in shared memory
+
 struct DeviceScene {
   int nv, nt;
   const float* pos;
@@ -69,7 +87,10 @@ struct DeviceScene {
   const float* texels;        // [sum w*h][3]
   // acceleration structure
   const BvhNode* nodes;
-  const float4* tri_verts;    // [T][3] float4
+  const float4* tri_verts;    // [T][3] float4 (binary-leaf order)
+  const WNode* wnodes;        // 8-wide quantised BVH
+  const float4* wtri;         // [T][3] float4 in wide-leaf order
+  int n_wnodes;
   int root_is_leaf;
 };
 
@@ -101,6 +122,10 @@ struct ViewDesc {
   uint32_t seed;
   int spp;
   int pad_;
+  float* image;        // forward radiance of this view [W*H*3] (accumulated)
+  const float* dLdI;   // dL/dI of this view [W*H*3]
+  int D;               // max bounces of this view
+  int pad2_;
   float* gpos;         // gradient destinations of this view
   float* gvn;
   float* gtex;

@@ -109,6 +109,102 @@ TRN_D void leaf_tri(const DeviceScene& s, int leaf, F3& p0, F3& p1, F3& p2, int&
   tri = __float_as_int(a.w);
 }
 
+
+// ---- 8-wide quantised BVH -------------------------------------------------
+// Top levels (root, its children, grandchildren: kTopNodes nodes) are staged
+// in shared memory once per block by stage_top(); deeper nodes are read with
+// 16-byte read-only loads.
+TRN_D WNode* top_nodes() {
+  __shared__ WNode top[kTopNodes];
+  return top;
+}
+
+// every kernel that traces rays calls this once before its work loop
+TRN_D void stage_top(const DeviceScene& s) {
+  const int n = min(s.n_wnodes, kTopNodes);
+  const uint4* src = reinterpret_cast<const uint4*>(s.wnodes);
+  uint4* dst = reinterpret_cast<uint4*>(top_nodes());
+  for (int i = threadIdx.x; i < n * 5; i += blockDim.x) dst[i] = __ldg(src + i);
+  __syncthreads();
+}
+
+TRN_D void load_wnode(const DeviceScene& s, int idx, WNode& n) {
+  uint4* d = reinterpret_cast<uint4*>(&n);
+  if (idx < kTopNodes) {
+    const uint4* src = reinterpret_cast<const uint4*>(top_nodes() + idx);
+#pragma unroll
+    for (int i = 0; i < 5; i++) d[i] = src[i];
+  } else {
+    const uint4* src = reinterpret_cast<const uint4*>(s.wnodes + idx);
+#pragma unroll
+    for (int i = 0; i < 5; i++) d[i] = __ldg(src + i);
+  }
+}
+
+template <bool ANY>
+TRN_D bool trace_wide(const DeviceScene& s, const RayPre& r, float tmin, float tmax, Hit& hit, int* err) {
+  float best_t = tmax;
+  int best_tri = 0x7fffffff;
+  bool found = false;
+  int2 stack[kStackSize];  // (node, tnear bits)
+  int sp = 0;
+  int cur = 0;
+  for (;;) {
+    WNode n;
+    load_wnode(s, cur, n);
+    const float sx = __uint_as_float((unsigned)n.ex << 23);
+    const float sy = __uint_as_float((unsigned)n.ey << 23);
+    const float sz = __uint_as_float((unsigned)n.ez << 23);
+    int next = -1;
+    float next_t = 0.f;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      const unsigned m = n.meta[i];
+      if (!(m & 0x80u)) continue;
+      const float lx = __fmaf_rn((float)n.qlo[0][i], sx, n.ox), hx = __fmaf_rn((float)n.qhi[0][i], sx, n.ox);
+      const float ly = __fmaf_rn((float)n.qlo[1][i], sy, n.oy), hy = __fmaf_rn((float)n.qhi[1][i], sy, n.oy);
+      const float lz = __fmaf_rn((float)n.qlo[2][i], sz, n.oz), hz = __fmaf_rn((float)n.qhi[2][i], sz, n.oz);
+      float tn;
+      if (!slab(r, lx, ly, lz, hx, hy, hz, tmin, best_t, tn)) continue;
+      if (m & 0x40u) {
+        const int slot = n.tri_base + (int)(m & 0x3fu);
+        const float4 a = __ldg(&s.wtri[3 * slot + 0]);
+        const float4 b = __ldg(&s.wtri[3 * slot + 1]);
+        const float4 c = __ldg(&s.wtri[3 * slot + 2]);
+        const int tri = __float_as_int(a.w);
+        float t, u, v;
+        if (intersect_tri(r, F3(a.x, a.y, a.z), F3(b.x, b.y, b.z), F3(c.x, c.y, c.z), tmin, tmax, t, u, v)) {
+          if (ANY) { hit.tri = tri; hit.t = t; hit.u = u; hit.v = v; return true; }
+          if (t < best_t || (t == best_t && tri < best_tri)) {
+            best_t = t; best_tri = tri; hit.u = u; hit.v = v; found = true;
+          }
+        }
+      } else {
+        const int child = n.child_base + (int)(m & 0x3fu);
+        if (next < 0) { next = child; next_t = tn; }
+        else {
+          // keep the nearer child to descend into, push the other
+          int pushc = child; float pusht = tn;
+          if (tn < next_t) { pushc = next; pusht = next_t; next = child; next_t = tn; }
+          if (sp < kStackSize) stack[sp++] = make_int2(pushc, __float_as_int(pusht));
+          else if (err) atomicExch(err, 1);
+        }
+      }
+    }
+    if (next >= 0) { cur = next; continue; }
+    // pop the next node whose box is still in front of the closest hit
+    bool got = false;
+    while (sp > 0) {
+      const int2 e = stack[--sp];
+      if (__int_as_float(e.y) <= best_t * 1.0000004f) { cur = e.x; got = true; break; }
+    }
+    if (!got) break;
+  }
+  if (ANY) return false;
+  if (found) { hit.tri = best_tri; hit.t = best_t; }
+  return found;
+}
+
 // Closest hit (ANY == false) or occlusion (ANY == true). Returns true on hit.
 template <bool ANY>
 TRN_D bool trace(const DeviceScene& s, const F3& o, const F3& d, float tmin, float tmax, Hit& hit,
@@ -116,6 +212,7 @@ TRN_D bool trace(const DeviceScene& s, const F3& o, const F3& d, float tmin, flo
   hit.tri = -1; hit.u = 0.f; hit.v = 0.f; hit.t = -1.f;
   if (s.nt <= 0) return false;
   const RayPre r = ray_setup(o, d);
+  if (s.n_wnodes > 0) return trace_wide<ANY>(s, r, tmin, tmax, hit, err);
   float best_t = tmax;
   int best_tri = 0x7fffffff;
   bool found = false;

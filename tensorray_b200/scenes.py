@@ -273,6 +273,22 @@ def config2_scene(width: int = 512, height: int = 512, tris: int = 100_000, seed
     return spec
 
 
+def served_scene(tris: int, seed: int = 0) -> SceneSpec:
+    """A diffuse displaced sphere of about `tris` triangles over the ground
+    quad, lit by the quad light (the resident scenes of the serving workload)."""
+    spec = SceneSpec()
+    spec.bsdfs = [BsdfSpec(DIFFUSE, (0.7, 0.7, 0.7)), BsdfSpec(DIFFUSE, (0.5, 0.5, 0.5))]
+    if tris <= 2000:
+        P, F = icosphere(3, 1.0)
+        spec.meshes.append(MeshSpec(P, F, bsdf=0, smooth=True))
+    else:
+        P, F, uv, uvf = displaced_uv_sphere(tris, 1.0, 0.1, seed)
+        spec.meshes.append(MeshSpec(P, F, bsdf=0, smooth=True))
+    _ground_and_light(spec, 1)
+    spec.cameras = [CameraSpec((0.0, 0.0, 4.0), (0.0, 0.0, 0.0), (0.0, 1.0, 0.0), 256, 256, 45.0)]
+    return spec
+
+
 def fibonacci_cameras(n: int, radius: float, resolutions, seed: int = 0):
     """`n` poses on a Fibonacci sphere looking at the origin; resolutions are
     drawn from `resolutions` with a seeded generator."""

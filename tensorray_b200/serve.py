@@ -1,0 +1,248 @@
+"""Continuous-batching render + gradient server.
+
+Requests (scene, camera, spp, depth, target image) arrive over time. The
+server keeps every scene's BVH, geometry and textures resident, admits a
+request when its device buffers fit in the HBM budget, and advances all
+admitted requests together. Each iteration issues, per scene, one batched
+launch for the next forward chunk of every request still rendering and one
+batched launch per gradient term for every request in its gradient phase:
+iteration-level continuous batching, so a request that arrives while others
+are on the GPU joins at the next iteration instead of waiting for them to
+finish. Every scene has its own CUDA stream, so launches of different scenes
+overlap on the device. A request's samples depend only on its own seed and
+chunk offsets, never on the batch it shares, so its result is the same alone
+and in the mix (up to float atomic ordering).
+
+The reference has no serving mode; its closest pattern is the per-view loop
+of pyTensorRay/renderer_multi_view.py:53-61.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import time
+from collections import deque
+from dataclasses import dataclass, field
+
+import torch
+
+from . import api
+from ._abi import TRN_DIRECT_EDGE, TRN_PATH_TRACER, TRN_PRIMARY_EDGE, TrnView
+
+PHASE_FWD, PHASE_GRAD, PHASE_FINISH, PHASE_DONE = 0, 1, 2, 3
+
+
+@dataclass
+class RenderRequest:
+    scene: str
+    camera: api.Camera
+    spp: int
+    depth: int
+    target: torch.Tensor                      # (H*W, 3) on the device
+    seed: int = 0
+    terms: tuple = (TRN_PATH_TRACER, TRN_PRIMARY_EDGE, TRN_DIRECT_EDGE)
+    arrival: float | None = None
+    rid: int = -1
+    # results / state (filled by the server)
+    image: torch.Tensor | None = None
+    dLdI: torch.Tensor | None = None
+    grad_positions: torch.Tensor | None = None
+    grad_vertex_normals: torch.Tensor | None = None
+    loss: torch.Tensor | None = None
+    phase: int = PHASE_FWD
+    chunk: int = 0
+    nbytes: int = 0
+    t_admit: float | None = None
+    t_done: float | None = None
+    done_event: object = None
+
+    @property
+    def latency(self) -> float | None:
+        return None if self.t_done is None else self.t_done - self.arrival
+
+    def samples(self) -> int:
+        return self.camera.width * self.camera.height * self.spp * len(self.terms)
+
+
+@dataclass
+class ServerStats:
+    completed: list = field(default_factory=list)
+    peak_bytes: int = 0
+    iterations: int = 0
+
+
+class Server:
+    def __init__(self, scenes: dict, hbm_budget_bytes: float = 120e9, chunk_spp: int = 8, max_active: int = 256,
+                 clock=time.perf_counter):
+        self.scenes = scenes
+        self.budget = int(hbm_budget_bytes)
+        self.chunk_spp = chunk_spp
+        self.max_active = max_active
+        self.clock = clock
+        self.streams = {k: torch.cuda.Stream() for k in scenes}
+        self.vsets: dict = {}
+        self.pending: deque = deque()
+        self.active: list = []
+        self.used = 0
+        self.stats = ServerStats()
+        self._next_id = 0
+        for sc in scenes.values():
+            sc._ensure()
+
+    # -- memory model --------------------------------------------------------------
+    def request_bytes(self, req: RenderRequest) -> int:
+        sc = self.scenes[req.scene]
+        npix = req.camera.width * req.camera.height
+        # image + dL/dI + two gradient buffers + this view's silhouette workspace
+        return 4 * (2 * 3 * npix + 2 * 3 * sc.num_vertices + 2 * sc.num_edges + 1)
+
+    # -- API --------------------------------------------------------------------------
+    def submit(self, req: RenderRequest) -> RenderRequest:
+        if req.arrival is None:
+            req.arrival = self.clock()
+        req.rid = self._next_id
+        self._next_id += 1
+        req.nbytes = self.request_bytes(req)
+        if req.nbytes > self.budget:
+            raise RuntimeError(f"request {req.rid} needs {req.nbytes} bytes, above the HBM budget {self.budget}")
+        self.pending.append(req)
+        return req
+
+    def idle(self) -> bool:
+        return not self.pending and not self.active
+
+    def step(self) -> None:
+        """One scheduling iteration: admit, launch one chunk per request, retire."""
+        self._admit()
+        for name, sc in self.scenes.items():
+            reqs = [r for r in self.active if r.scene == name]
+            if not reqs:
+                continue
+            with torch.cuda.stream(self.streams[name]):
+                self._forward(name, sc, [r for r in reqs if r.phase == PHASE_FWD])
+                self._gradient(name, sc, [r for r in reqs if r.phase == PHASE_GRAD])
+        self._retire()
+        self.stats.iterations += 1
+
+    def run(self, requests: list, arrival_times: list | None = None) -> ServerStats:
+        """Feed requests at their (relative) arrival times and serve until all
+        are done. Returns the completed requests with latencies."""
+        t0 = self.clock()
+        order = list(zip(arrival_times or [0.0] * len(requests), requests))
+        order.sort(key=lambda x: x[0])
+        i = 0
+        while i < len(order) or not self.idle():
+            now = self.clock() - t0
+            while i < len(order) and order[i][0] <= now:
+                order[i][1].arrival = t0 + order[i][0]
+                self.submit(order[i][1])
+                i += 1
+            if self.idle():
+                time.sleep(max(0.0, min(0.001, order[i][0] - now)) if i < len(order) else 0.0)
+                continue
+            self.step()
+        return self.stats
+
+    # -- internals ----------------------------------------------------------------------
+    def _admit(self) -> None:
+        while self.pending and len(self.active) < self.max_active:
+            req = self.pending[0]
+            if self.used + req.nbytes > self.budget:
+                break
+            self.pending.popleft()
+            sc = self.scenes[req.scene]
+            npix = req.camera.width * req.camera.height
+            with torch.cuda.stream(self.streams[req.scene]):
+                d = sc.device
+                req.image = torch.zeros(npix, 3, device=d)
+                req.dLdI = torch.empty(npix, 3, device=d)
+                req.grad_positions = torch.zeros(sc.num_vertices, 3, device=d)
+                req.grad_vertex_normals = torch.zeros(sc.num_vertices, 3, device=d)
+            req.phase, req.chunk = PHASE_FWD, 0
+            req.t_admit = self.clock()
+            self.used += req.nbytes
+            self.stats.peak_bytes = max(self.stats.peak_bytes, self.used)
+            self.active.append(req)
+
+    def _nchunks(self, req: RenderRequest) -> int:
+        return (req.spp + self.chunk_spp - 1) // self.chunk_spp
+
+    def _views(self, reqs: list, grad: bool):
+        arr = (TrnView * len(reqs))()
+        spps = []
+        for i, r in enumerate(reqs):
+            c = r.camera
+            k0 = r.chunk * self.chunk_spp
+            spp = min(self.chunk_spp, r.spp - k0)
+            spps.append(spp)
+            arr[i] = TrnView(c.c, spp, int(r.seed), -1, k0 * c.width * c.height, 1.0 / r.spp, int(r.depth),
+                             C.c_void_p(r.grad_positions.data_ptr()) if grad else None,
+                             C.c_void_p(r.grad_vertex_normals.data_ptr()) if grad else None, None,
+                             None if grad else C.c_void_p(r.image.data_ptr()),
+                             C.c_void_p(r.dLdI.data_ptr()) if grad else None)
+        return arr, spps
+
+    def _viewset(self, name: str, phase: int, reqs: list, arr, spps):
+        key = (name, phase)
+        cams = [r.camera for r in reqs]
+        vs = self.vsets.get(key)
+        if vs is None:
+            vs = api.ViewSet(self.scenes[name], cams, spps, views=arr)
+            self.vsets[key] = vs
+        else:
+            vs.update(cams, spps, arr)
+        return vs
+
+    def _forward(self, name: str, sc: api.Scene, reqs: list) -> None:
+        if not reqs:
+            return
+        arr, spps = self._views(reqs, grad=False)
+        vs = self._viewset(name, PHASE_FWD, reqs, arr, spps)
+        vs.render(TRN_PATH_TRACER, api.RenderOptions(0, 0, 0, 0, 0, 0, 0), out=False)
+        for r in reqs:
+            r.chunk += 1
+            if r.chunk >= self._nchunks(r):
+                # loss 0.5 |I - T|^2 and dL/dI (pyTensorRay/loss.py:34-38)
+                torch.sub(r.image, r.target, out=r.dLdI)
+                r.loss = 0.5 * (r.dLdI * r.dLdI).sum()
+                r.phase, r.chunk = PHASE_GRAD, 0
+
+    def _gradient(self, name: str, sc: api.Scene, reqs: list) -> None:
+        if not reqs:
+            return
+        groups: dict = {}
+        for r in reqs:
+            groups.setdefault(tuple(r.terms), []).append(r)
+        for gi, (terms, grp) in enumerate(sorted(groups.items())):
+            arr, spps = self._views(grp, grad=True)
+            vs = self._viewset(name, (PHASE_GRAD, gi), grp, arr, spps)
+            for t in terms:
+                vs.render_grad(t, api.RenderOptions(0, 0, 0, 0, 0, 0, 0), None)
+        for r in reqs:
+            r.chunk += 1
+            if r.chunk >= self._nchunks(r):
+                sc.finalize_grads(r.grad_positions, r.grad_vertex_normals)
+                r.done_event = torch.cuda.Event()
+                r.done_event.record()
+                r.phase = PHASE_FINISH
+
+    def _retire(self) -> None:
+        keep = []
+        for r in self.active:
+            if r.phase == PHASE_FINISH and r.done_event.query():
+                r.t_done = self.clock()
+                r.phase = PHASE_DONE
+                self.used -= r.nbytes
+                r.dLdI = None
+                r.grad_vertex_normals = None
+                self.stats.completed.append(r)
+            else:
+                keep.append(r)
+        self.active = keep
+
+
+def percentile(xs: list, q: float) -> float:
+    if not xs:
+        return float("nan")
+    ys = sorted(xs)
+    k = min(len(ys) - 1, max(0, int(round(q / 100.0 * (len(ys) - 1)))))
+    return ys[k]
