@@ -62,6 +62,7 @@ def parse():
     ap.add_argument("--depth", type=int, default=5)
     ap.add_argument("--tris", type=int, default=100_000)
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--quick", action="store_true", help="small smoke-sized run")
     ap.add_argument("--requests", type=int, default=48, help="serve workload: number of requests")
     ap.add_argument("--workload", default="single", choices=["single", "views", "serve"],
@@ -374,7 +375,7 @@ def main():
                 "peak_source": peak_src}
 
     cpu = None
-    if rank == 0 and world == 1:
+    if rank == 0 and world == 1 and not a.no_cpu:
         rate, units, dt, cores = cpu_oracle_rate(a, budget_s=15.0)
         cpu = {"value": rate, "unit": "grad path-samples/s", "cores": cores, "kind": "port",
                "sample": f"{units} grad path-samples in {dt:.1f}s: 8x8 px, 1 spp per term, 5 terms, same scene"}

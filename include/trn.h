@@ -161,6 +161,10 @@ int trn_camera_init(trn_camera* out, const float pos[3], const float target[3], 
 int trn_scene_create(const trn_scene_desc* desc, trn_scene** out);
 int trn_scene_configure(trn_scene* scene, cudaStream_t stream);
 int trn_scene_destroy(trn_scene* scene);
+/* Re-run the geometry chain for new parameters and refit the LBVH boxes
+ * without rebuilding its topology (Scene::Update / UpdateAccelerationStructure,
+ * Scene.cpp:368-469, 535-546). Falls back to trn_scene_configure the first time. */
+int trn_scene_refit(trn_scene* scene, cudaStream_t stream);
 
 /* Parameter access (TensorRay.cpp: get_var/set_var; Primitive::mTrans,
  * mPositionBufferRaw, BSDF texture). Device pointers. set_* marks the scene

@@ -10,7 +10,7 @@ import ctypes as C
 import os
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "_lib", "libtrn.so")
+LIB_PATH = os.environ.get("TRN_LIB") or os.path.join(_HERE, "_lib", "libtrn.so")
 
 TRN_PATH_TRACER = 0
 TRN_PRIMARY_EDGE = 1
@@ -81,6 +81,7 @@ _SIGNATURES = {
     "trn_scene_create": (C.c_int, [C.POINTER(TrnSceneDesc), C.POINTER(C.c_void_p)]),
     "trn_scene_configure": (C.c_int, [C.c_void_p, C.c_void_p]),
     "trn_scene_destroy": (C.c_int, [C.c_void_p]),
+    "trn_scene_refit": (C.c_int, [C.c_void_p, C.c_void_p]),
     "trn_scene_set_translation": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "trn_scene_set_positions": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "trn_scene_set_texels": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),

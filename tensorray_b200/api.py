@@ -235,14 +235,18 @@ class Scene:
         check(self._lib.trn_scene_set_texels(self._h, C.c_void_p(t.data_ptr()), C.c_void_p(_stream())),
               "trn_scene_set_texels")
 
-    def configure(self) -> None:
-        """Scene::Configure (Scene.cpp:522-533): geometry chain + LBVH."""
+    def configure(self, refit: bool = False) -> None:
+        """Scene::Configure (Scene.cpp:522-533): geometry chain + LBVH build, or
+        with refit=True Scene::Update: geometry chain + LBVH refit."""
         st = C.c_void_p(_stream())
         check(self._lib.trn_scene_set_translation(self._h, C.c_void_p(self._translation.data_ptr()), st),
               "trn_scene_set_translation")
         check(self._lib.trn_scene_set_positions(self._h, C.c_void_p(self._raw_positions.data_ptr()), st),
               "trn_scene_set_positions")
-        check(self._lib.trn_scene_configure(self._h, st), "trn_scene_configure")
+        if refit:
+            check(self._lib.trn_scene_refit(self._h, st), "trn_scene_refit")
+        else:
+            check(self._lib.trn_scene_configure(self._h, st), "trn_scene_configure")
         self._dirty = False
 
     def _ensure(self) -> None:

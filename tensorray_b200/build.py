@@ -43,31 +43,34 @@ def _stale() -> bool:
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    """Compile every CUDA source into one shared library; returns its path."""
-    if not force and not _stale():
+def build(force: bool = False, verbose: bool = False, out: str | None = None, defines=()) -> str:
+    """Compile every CUDA source into one shared library; returns its path.
+    `out` and `defines` build an alternative variant elsewhere."""
+    target = out or LIB
+    if not force and out is None and not _stale():
         return LIB
-    os.makedirs(LIBDIR, exist_ok=True)
+    libdir = os.path.dirname(target)
+    os.makedirs(libdir, exist_ok=True)
     objs = []
     for src in SOURCES:
-        obj = os.path.join(LIBDIR, src.replace(".cu", ".o"))
-        cmd = [_nvcc(), *NVCC_FLAGS, "-c", os.path.join(CSRC, src), "-o", obj]
+        obj = os.path.join(libdir, src.replace(".cu", ".o"))
+        cmd = [_nvcc(), *NVCC_FLAGS, *[f"-D{d}" for d in defines], "-c", os.path.join(CSRC, src), "-o", obj]
         res = subprocess.run(cmd, capture_output=True, text=True)
         if verbose or res.returncode != 0:
             sys.stderr.write(res.stdout + res.stderr)
         if res.returncode != 0:
             raise RuntimeError(f"nvcc failed for {src}")
         objs.append(obj)
-    tmp = LIB + ".tmp"
+    tmp = target + ".tmp"
     cmd = [_nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a", *objs, "-o", tmp, "-lcudart"]
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
         sys.stderr.write(res.stdout + res.stderr)
         raise RuntimeError("nvcc link failed")
-    os.replace(tmp, LIB)
+    os.replace(tmp, target)
     for o in objs:
         os.remove(o)
-    return LIB
+    return target
 
 
 if __name__ == "__main__":

@@ -28,6 +28,8 @@ struct Params {
   long long stride;
   uint32_t term;             // integrator id (hash stream)
   uint32_t seed;             // RenderOptions::mRndSeed
+  float* image;              // call image buffer (views without their own)
+  const float* dLdI;         // call dL/dI buffer (views without their own)
   int D;                     // max bounces
   float* g_pos;              // [V*3]
   float* g_vn;               // [V*3]
@@ -106,7 +108,7 @@ TRN_D void agg_add3(float* base, long long idx, const F3& g) {
 }
 TRN_D F3 g_at(const Params& P, const ViewDesc& V, int pix) {
   if (pix < 0) return F3z();
-  const float* d = V.dLdI + 3 * pix;
+  const float* d = (V.dLdI ? V.dLdI : P.dLdI + 3 * V.pix_off) + 3 * pix;
   return F3(__ldg(d), __ldg(d + 1), __ldg(d + 2)) * V.inv_spp;
 }
 
@@ -371,8 +373,20 @@ TRN_D bool radiance_step(const DeviceScene& s, SurfF& x, F3& rdir, F3& T, float 
 // cheap `setup` phase (primary hit, valid edge sample, visible, ...); then the
 // warp runs the expensive `body` (path tracing + adjoint) together. Rejected
 // samples therefore never hold a lane hostage while others trace long paths.
+#ifndef TRN_COMPACT
+#define TRN_COMPACT 1
+#endif
+
 template <class State, class Setup, class Body>
 TRN_D void for_each_valid(const Params& P, Setup&& setup, Body&& body) {
+#if !TRN_COMPACT
+  // lockstep variant: each warp takes 32 consecutive slots per round
+  for_each_slot(P, [&](long long g) {
+    State st;
+    if (setup(g, st)) body(st);
+  });
+  return;
+#endif
   const int lane = threadIdx.x & 31;
   const unsigned lt = (1u << lane) - 1u;
   State st;
@@ -447,7 +461,7 @@ __global__ void __launch_bounds__(256) k_path_fwd(Params P) {
       }
       L = L * V.inv_spp;
       cnt.v[kCntPixel]++;
-      atomic_add3(V.image + 3 * st.pix, L);
+      atomic_add3((V.image ? V.image : P.image + 3 * V.pix_off) + 3 * st.pix, L);
     });
   flush_cnt(cnt, P.stats);
 }
@@ -521,6 +535,7 @@ struct AdjState {
   Hit h;
 };
 
+template <int MAXD>
 __global__ void __launch_bounds__(256) k_path_adj(Params P) {
   const DeviceScene& s = P.s;
   Cnt cnt;
@@ -550,10 +565,10 @@ __global__ void __launch_bounds__(256) k_path_adj(Params P) {
     const F3 g = st.g;
     const Hit h = st.h;
     // ---- forward replay, recording vertices and factor values ----
-    VRec vr[kMaxDepth + 2];
-    BounceRec br[kMaxDepth + 1];
-    bool nee_on[kMaxDepth + 2];
-    F3 Tk[kMaxDepth + 2], Nk[kMaxDepth + 2], Mk[kMaxDepth + 2], Phik[kMaxDepth + 2];
+    VRec vr[MAXD + 2];
+    BounceRec br[MAXD + 1];
+    bool nee_on[MAXD + 2];
+    F3 Tk[MAXD + 2], Mk[MAXD + 2];
     SurfF x = post_intersect(s, h.tri, h.u, h.v);
     vr[1] = {h.tri, h.u, h.v};
     const float t1 = camera_factor<float>(cam, x.p, x.ng, 1.f);
@@ -563,8 +578,8 @@ __global__ void __launch_bounds__(256) k_path_adj(Params P) {
     Mk[1] = emitted(s, x, -rdir);
     if (!finite3(T * Mk[1])) Mk[1] = F3z();
     int K = 1;  // vertices reached
-    const int D = min(V.D, kMaxDepth);
-    for (int k = 0; k <= D + 1; k++) { nee_on[k] = false; Nk[k] = F3z(); Phik[k] = F3z(); }
+    const int D = min(V.D, MAXD);
+    for (int k = 0; k <= D + 1; k++) nee_on[k] = false;
     for (int b = 0; b < D; b++) {
       const int k = b + 1;
       const int o = 2 + 5 * b;
@@ -581,87 +596,82 @@ __global__ void __launch_bounds__(256) k_path_adj(Params P) {
       K = k + 1;
       if (T.x == 0.f && T.y == 0.f && T.z == 0.f) break;
     }
-    // ---- recompute factor values in vertex order (NEE value and phi) ----
-    // positions / normals per vertex
-    F3 xp[kMaxDepth + 2], nsv[kMaxDepth + 2], ngv[kMaxDepth + 2], kdv[kMaxDepth + 2];
-    long long texel[kMaxDepth + 2];
-    int bsdfv[kMaxDepth + 2];
-    xp[0] = org;
-    for (int k = 1; k <= K; k++) {
+    // ---- reverse pass: a_k = g*(N_k + M_k) + phi_k * a_{k+1}, one vertex window at a time ----
+    struct VG { F3 p, ns, ng, kd; long long texel; int bsdf; };
+    auto load_vg = [&](int k) {
+      VG r;
       const SurfF xs = post_intersect(s, vr[k].tri, vr[k].u, vr[k].v);
-      xp[k] = xs.p; nsv[k] = xs.ns; ngv[k] = xs.ng; bsdfv[k] = xs.bsdf;
-      kdv[k] = bsdf_albedo(s, s.bsdfs[xs.bsdf], xs.tu, xs.tv, texel[k]);
-    }
-    F3 yv[kMaxDepth + 1], nlv[kMaxDepth + 1];
-    for (int k = 1; k <= K && k <= D; k++) {
-      if (!nee_on[k]) continue;
-      const BounceRec& R = br[k];
-      int j0, j1, j2; tri_vertices(s, R.ltri, j0, j1, j2);
-      yv[k] = bary3(R.lu, R.lv, load3(s.pos, j0), load3(s.pos, j1), load3(s.pos, j2));
-      nlv[k] = load3(s.fnormal, R.ltri);
-      Nk[k] = nee_factor<float>(s.bsdfs[bsdfv[k]], xp[k - 1], xp[k], nsv[k], ngv[k], kdv[k], yv[k], nlv[k], 1.f,
-                                R.lLe, R.lpdf, R.lmis);
-    }
-    for (int k = 1; k < K; k++) {
-      Phik[k] = cont_factor<float>(s.bsdfs[bsdfv[k]], xp[k - 1], xp[k], nsv[k], ngv[k], kdv[k], xp[k + 1],
-                                   ngv[k + 1], 1.f, br[k].prev_pdf);
-      // a non-finite weight is what made the forward throughput non-finite:
-      // the scrubbed contributions carry no gradient
-      if (!finite3(Phik[k])) Phik[k] = F3z();
-    }
-    // ---- reverse accumulation of the throughput adjoint ----
-    F3 a[kMaxDepth + 3];
-    a[K + 1] = F3z();
+      r.p = xs.p; r.ns = xs.ns; r.ng = xs.ng; r.bsdf = xs.bsdf;
+      r.kd = bsdf_albedo(s, s.bsdfs[xs.bsdf], xs.tu, xs.tv, r.texel);
+      return r;
+    };
+    VG Gk = load_vg(K), Gn = Gk;
+    F3 a_next = F3z();
+    VAdj acc_next, acc_k, acc_prev;
+    vadj_zero(acc_next); vadj_zero(acc_k); vadj_zero(acc_prev);
     for (int k = K; k >= 1; k--) {
-      F3 ak = g * (Nk[k] + Mk[k]);
-      if (k < K) ak = ak + Phik[k] * a[k + 1];
-      a[k] = ak;
-    }
-    // ---- local vector-Jacobian products ----
-    VAdj va[kMaxDepth + 2];
-    for (int k = 1; k <= K; k++) vadj_zero(va[k]);
-    // primary factor T1 = G / Detach(G) * J
-    {
-      const float gam = a[1].x + a[1].y + a[1].z;
-      if (gam != 0.f && isfinite(gam)) {
-        for (int grp = 0; grp < 3; grp++) {
-          const V3<D3> dx = seed3<3>(xp[1], grp == 0 ? 0 : -1);
-          const V3<D3> dn = seed3<3>(ngv[1], grp == 1 ? 0 : -1);
-          const D3 dJ = seed1<3>(1.f, grp == 2 ? 0 : -1);
-          const D3 r = camera_factor<D3>(cam, dx, dn, dJ);
-          const F3 gg = F3(r.d[0], r.d[1], r.d[2]) * gam;
-          if (grp == 0) va[1].p = va[1].p + gg;
-          else if (grp == 1) va[1].ng = va[1].ng + gg;
-          else va[1].J += gg.x;
-        }
-      }
-    }
-    for (int k = 1; k <= K; k++) {
-      const BsdfDesc b = s.bsdfs[bsdfv[k]];
+      VG Gp;
+      if (k >= 2) Gp = load_vg(k - 1);
+      else { Gp.p = org; Gp.ns = Gp.ng = Gp.kd = F3z(); Gp.texel = -1; Gp.bsdf = 0; }
+      const BsdfDesc b = s.bsdfs[Gk.bsdf];
       const bool need_prev = b.type != kDiffuse;
-      const bool need_kd = P.diff_tex && texel[k] >= 0;
-      F3 gkd = F3z();
-      F3 gprev = F3z();
-      if (k <= D && nee_on[k]) {
+      const bool need_kd = P.diff_tex && Gk.texel >= 0;
+      F3 Nval = F3z(), Phi = F3z(), y = F3z(), nl = F3z();
+      const bool nee = k <= D && nee_on[k];
+      if (nee) {
+        const BounceRec& R = br[k];
+        int j0, j1, j2; tri_vertices(s, R.ltri, j0, j1, j2);
+        y = bary3(R.lu, R.lv, load3(s.pos, j0), load3(s.pos, j1), load3(s.pos, j2));
+        nl = load3(s.fnormal, R.ltri);
+        Nval = nee_factor<float>(b, Gp.p, Gk.p, Gk.ns, Gk.ng, Gk.kd, y, nl, 1.f, R.lLe, R.lpdf, R.lmis);
+      }
+      if (k < K) {
+        Phi = cont_factor<float>(b, Gp.p, Gk.p, Gk.ns, Gk.ng, Gk.kd, Gn.p, Gn.ng, 1.f, br[k].prev_pdf);
+        // a non-finite weight made the forward throughput non-finite: no gradient
+        if (!finite3(Phi)) Phi = F3z();
+      }
+      const F3 a_k = g * (Nval + Mk[k]) + Phi * a_next;
+      F3 gkd = F3z(), gprev = F3z();
+      if (nee) {
         const F3 adj = Tk[k] * g;
         F3 gy = F3z(), gnl = F3z();
         float gJl = 0.f;
-        nee_vjp(b, need_prev, need_kd, xp[k - 1], xp[k], nsv[k], ngv[k], kdv[k], yv[k], nlv[k], br[k].lLe, br[k].lpdf,
-                br[k].lmis, adj, gprev, va[k].p, va[k].ns, gkd, gy, gnl, gJl);
+        nee_vjp(b, need_prev, need_kd, Gp.p, Gk.p, Gk.ns, Gk.ng, Gk.kd, y, nl, br[k].lLe, br[k].lpdf, br[k].lmis, adj,
+                gprev, acc_k.p, acc_k.ns, gkd, gy, gnl, gJl);
         VAdj la; la.p = gy; la.ns = F3z(); la.ng = gnl; la.J = gJl;
         scatter_vertex(P, V, br[k].ltri, br[k].lu, br[k].lv, la, cnt);
       }
-      if (k < K && (Phik[k].x != 0.f || Phik[k].y != 0.f || Phik[k].z != 0.f)) {
-        const F3 adj = Tk[k] * a[k + 1];
+      if (k < K && (Phi.x != 0.f || Phi.y != 0.f || Phi.z != 0.f)) {
+        const F3 adj = Tk[k] * a_next;
         float gJn = 0.f;
-        cont_vjp(b, need_prev, need_kd, xp[k - 1], xp[k], nsv[k], ngv[k], kdv[k], xp[k + 1], ngv[k + 1],
-                 br[k].prev_pdf, adj, gprev, va[k].p, va[k].ns, gkd, va[k + 1].p, va[k + 1].ng, gJn);
-        va[k + 1].J += gJn;
+        cont_vjp(b, need_prev, need_kd, Gp.p, Gk.p, Gk.ns, Gk.ng, Gk.kd, Gn.p, Gn.ng, br[k].prev_pdf, adj, gprev,
+                 acc_k.p, acc_k.ns, gkd, acc_next.p, acc_next.ng, gJn);
+        acc_next.J += gJn;
       }
-      if (k >= 2) va[k - 1].p = va[k - 1].p + gprev;
-      if (need_kd) { cnt.v[kCntTScatter]++; agg_add3(V.gtex, texel[k], gkd); }
+      if (k >= 2) acc_prev.p = acc_prev.p + gprev;
+      if (need_kd) { cnt.v[kCntTScatter]++; agg_add3(V.gtex, Gk.texel, gkd); }
+      // vertex k+1 has received all of its contributions
+      if (k < K) scatter_vertex(P, V, vr[k + 1].tri, vr[k + 1].u, vr[k + 1].v, acc_next, cnt);
+      acc_next = acc_k; acc_k = acc_prev; vadj_zero(acc_prev);
+      a_next = a_k; Gn = Gk; Gk = Gp;
     }
-    for (int k = 1; k <= K; k++) scatter_vertex(P, V, vr[k].tri, vr[k].u, vr[k].v, va[k], cnt);
+    // primary factor T1 = G / Detach(G) * J at vertex 1 (now in Gn / acc_next)
+    {
+      const float gam = a_next.x + a_next.y + a_next.z;
+      if (gam != 0.f && isfinite(gam)) {
+        for (int grp = 0; grp < 3; grp++) {
+          const V3<D3> dx = seed3<3>(Gn.p, grp == 0 ? 0 : -1);
+          const V3<D3> dn = seed3<3>(Gn.ng, grp == 1 ? 0 : -1);
+          const D3 dJ = seed1<3>(1.f, grp == 2 ? 0 : -1);
+          const D3 r = camera_factor<D3>(cam, dx, dn, dJ);
+          const F3 gg = F3(r.d[0], r.d[1], r.d[2]) * gam;
+          if (grp == 0) acc_next.p = acc_next.p + gg;
+          else if (grp == 1) acc_next.ng = acc_next.ng + gg;
+          else acc_next.J += gg.x;
+        }
+      }
+    }
+    scatter_vertex(P, V, vr[1].tri, vr[1].u, vr[1].v, acc_next, cnt);
     });
   flush_cnt(cnt, P.stats);
 }
@@ -952,6 +962,7 @@ __global__ void __launch_bounds__(256) k_direct_adj(Params P) {
 // ---------------------------------------------------------------------------
 // indirect boundary (BoundaryIndirect.cpp:38-192, Edge.cpp:146-199)
 // ---------------------------------------------------------------------------
+template <int MAXD>
 __global__ void __launch_bounds__(256) k_indirect_adj(Params P) {
   const DeviceScene& s = P.s;
   Cnt cnt;
@@ -1021,10 +1032,10 @@ __global__ void __launch_bounds__(256) k_indirect_adj(Params P) {
     },
     [&](EdgeState& st) {
       const ViewDesc& V = *st.V;
-      const int D = min(V.D, kMaxDepth);
+      const int D = min(V.D, MAXD);
       const PathSmp S{&P, V.seed, st.gslot, st.p + V.slot_off};
       // emitter side: cumulative radiance per depth
-      F3 rad[kMaxDepth];
+      F3 rad[MAXD];
       {
         F3 T(1.f, 1.f, 1.f);
         F3 rd = -st.rdir;
@@ -1264,11 +1275,8 @@ struct trn_viewset {
   int uploaded_key = -2;
   long long total = 0;
   // image / dL/dI base buffers of the uploaded table (views without their own)
-  float* cur_image = nullptr;
-  const float* cur_dLdI = nullptr;
   int cur_depth = -1;
-  float* want_image = nullptr;
-  const float* want_dLdI = nullptr;
+  int max_depth = kMaxDepth;
 };
 
 namespace {
@@ -1306,8 +1314,7 @@ int upload_views(trn_viewset* vs, const trn_render_options* o, int integrator, i
   float* s_gvn = vs->scene->g_vnormal;
   float* s_gtex = vs->scene->g_texels;
   const int key = spp_override;  // the layout depends on the per-view spp, buffers and depth
-  if (vs->uploaded_key == key && key != -2 && vs->cur_image == vs->want_image && vs->cur_dLdI == vs->want_dLdI &&
-      vs->cur_depth == o->max_bounces) {
+  if (vs->uploaded_key == key && key != -2 && vs->cur_depth == o->max_bounces) {
     total = vs->total;
     if (integrator == TRN_PIXEL_EDGE)
       for (int v = 0; v < vs->nviews; v++) {
@@ -1319,9 +1326,11 @@ int upload_views(trn_viewset* vs, const trn_render_options* o, int integrator, i
       }
     return 0;
   }
-  vs->cur_image = vs->want_image;
-  vs->cur_dLdI = vs->want_dLdI;
   vs->cur_depth = o->max_bounces;
+  vs->max_depth = 0;
+  for (int v = 0; v < vs->nviews; v++)
+    vs->max_depth = std::max(vs->max_depth, vs->h_views[v].max_bounces > 0 ? vs->h_views[v].max_bounces
+                                                                            : o->max_bounces);
   if (vs->copy_done) cudaEventSynchronize(vs->copy_done);  // previous upload has left the staging buffer
   ViewDesc* d = vs->h_stage;
   long long* begin = vs->h_stage_begin;
@@ -1341,8 +1350,8 @@ int upload_views(trn_viewset* vs, const trn_render_options* o, int integrator, i
     d[v].inv_spp = hv.weight > 0.f ? hv.weight : (spp > 0 ? 1.0f / (float)spp : 0.f);
     d[v].slot_off = hv.slot_offset;
     d[v].D = hv.max_bounces > 0 ? std::min(hv.max_bounces, (int)kMaxDepth) : o->max_bounces;
-    d[v].image = hv.image ? hv.image : (vs->cur_image ? vs->cur_image + 3 * vs->h_pbegin[v] : nullptr);
-    d[v].dLdI = hv.dLdI ? hv.dLdI : (vs->cur_dLdI ? vs->cur_dLdI + 3 * vs->h_pbegin[v] : nullptr);
+    d[v].image = hv.image;
+    d[v].dLdI = hv.dLdI;
     d[v].gpos = hv.grad_positions ? hv.grad_positions : s_gpos;
     d[v].gvn = hv.grad_vertex_normals ? hv.grad_vertex_normals : s_gvn;
     d[v].gtex = hv.grad_texels ? hv.grad_texels : s_gtex;
@@ -1422,10 +1431,10 @@ int render_views(trn_scene* s, trn_viewset* vs, const trn_render_options* o, int
   if (!vs || vs->nviews <= 0) { set_error("empty view set"); return -1; }
   if (validate_launch(ln)) return -1;
   long long total = 0;
-  vs->want_image = forward ? image : nullptr;
-  vs->want_dLdI = forward ? nullptr : dLdI;
   if (upload_views(vs, o, integrator, spp_override, total, st)) return -1;
   Params P = base_params(s, vs, o, integrator, smp, ln, total);
+  P.image = forward ? image : nullptr;
+  P.dLdI = forward ? nullptr : dLdI;
   const long long slots = integrator == TRN_PIXEL_EDGE ? total / 4 : total;
   if (P.table && P.stride < slots) { set_error("sample table too small"); return -1; }
   if (forward) {
@@ -1449,11 +1458,16 @@ int render_views(trn_scene* s, trn_viewset* vs, const trn_render_options* o, int
     return 0;
   }
   TRN_CUDA_TRY(cudaMemsetAsync(vs->work, 0, sizeof(unsigned long long), st));
+  const bool shallow = vs->max_depth <= 8;  // smaller per-thread path records
   switch (integrator) {
-    case TRN_PATH_TRACER: launch(k_path_adj, ln, total, P, st); break;
+    case TRN_PATH_TRACER:
+      if (shallow) launch(k_path_adj<8>, ln, total, P, st); else launch(k_path_adj<kMaxDepth>, ln, total, P, st);
+      break;
     case TRN_PRIMARY_EDGE: launch(k_primary_adj, ln, total, P, st); break;
     case TRN_DIRECT_EDGE: launch(k_direct_adj, ln, total, P, st); break;
-    case TRN_INDIRECT_EDGE: launch(k_indirect_adj, ln, total, P, st); break;
+    case TRN_INDIRECT_EDGE:
+      if (shallow) launch(k_indirect_adj<8>, ln, total, P, st); else launch(k_indirect_adj<kMaxDepth>, ln, total, P, st);
+      break;
     default: launch(k_pixel_adj, ln, total, P, st); break;
   }
   TRN_CUDA_TRY(cudaGetLastError());

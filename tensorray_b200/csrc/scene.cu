@@ -782,8 +782,12 @@ int trn_scene_destroy(trn_scene* s) {
   return 0;
 }
 
-int trn_scene_configure(trn_scene* s, cudaStream_t st) {
-  if (!s) { set_error("trn_scene_configure: null scene"); return -1; }
+}  // extern "C"
+
+namespace {
+// Primitive::Configure + ComputeFaceNormalAndDistrib + ComputeVertexNormal +
+// ConfigureLight + ConstructSecEdgeList (everything but the acceleration structure)
+int configure_geometry(trn_scene* s, cudaStream_t st) {
   const int nv = s->nv, nt = s->nt;
   k_transform<<<nblk(nv), 256, 0, st>>>(nv, s->raw_pos, s->vert_mesh, s->translation, s->pos);
   k_face<<<nblk(nt), 256, 0, st>>>(nt, s->pos, s->idx, s->fnormal, s->area);
@@ -806,6 +810,16 @@ int trn_scene_configure(trn_scene* s, cudaStream_t st) {
     k_cdf<<<1, 1024, 0, st>>>(s->ne, s->sec_func, s->sec_cdf, s->sec_integral_dev);
     count_launch(2);
   }
+  return 0;
+}
+}  // namespace
+
+extern "C" {
+
+int trn_scene_configure(trn_scene* s, cudaStream_t st) {
+  if (!s) { set_error("trn_scene_configure: null scene"); return -1; }
+  const int nt = s->nt;
+  if (configure_geometry(s, st)) return -1;
   // LBVH
   k_bounds_init<<<1, 32, 0, st>>>((unsigned int*)s->bounds);
   k_bounds<<<nblk(nt), 256, 0, st>>>(nt, s->pos, s->idx, (unsigned int*)s->bounds);
@@ -825,7 +839,7 @@ int trn_scene_configure(trn_scene* s, cudaStream_t st) {
   count_launch(1);
   // 8-wide quantised BVH
   s->n_wnodes = 0;
-  if (nt > 1) {
+  if (TRN_WIDE_BVH && nt > 1) {
     int2* qa = reinterpret_cast<int2*>(s->wqueue);
     int2* qb = qa + nt;
     const int init[4] = {1, 0, 0, 0};
@@ -849,6 +863,22 @@ int trn_scene_configure(trn_scene* s, cudaStream_t st) {
   }
   TRN_CUDA_TRY(cudaGetLastError());
   TRN_CUDA_TRY(cudaStreamSynchronize(st));
+  s->configured = true;
+  s->built = true;
+  return 0;
+}
+
+// Scene::UpdateAccelerationStructure (Scene.cpp:368-469): new positions, same
+// BVH topology; leaf boxes and node boxes are recomputed bottom-up.
+int trn_scene_refit(trn_scene* s, cudaStream_t st) {
+  if (!s) { set_error("trn_scene_refit: null scene"); return -1; }
+  if (!s->built) return trn_scene_configure(s, st);
+  const int nt = s->nt;
+  if (configure_geometry(s, st)) return -1;
+  if (nt > 1) TRN_CUDA_TRY(cudaMemsetAsync(s->flags, 0, sizeof(int) * (nt - 1), st));
+  k_refit<<<nblk(nt), 256, 0, st>>>(nt, s->keys_alt, s->pos, s->idx, s->nodes, s->parent, s->flags, s->tri_verts);
+  count_launch(1);
+  TRN_CUDA_TRY(cudaGetLastError());
   s->configured = true;
   return 0;
 }

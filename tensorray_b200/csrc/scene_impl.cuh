@@ -72,6 +72,7 @@ struct trn_scene {
   bool stats_on = false;
   float h_light_integral = 0.f;
   bool configured = false;
+  bool built = false;             // an LBVH topology exists (refit possible)
   bool grads_finalized = true;
 
   trn::DeviceScene view() const {

@@ -60,6 +60,12 @@ static_assert(sizeof(WNode) == 80, "WNode must be 80 bytes");
 
 constexpr int kTopNodes = 73;  // root + 8 + 64 wide nodes staged in shared memory
 
+// Traversal structure: the binary LBVH with child boxes in the parent (default;
+// measured faster on B200 for the scenes here) or the 8-wide quantised BVH.
+#ifndef TRN_WIDE_BVH
+#define TRN_WIDE_BVH 0
+#endif
+
 struct DeviceScene {
   int nv, nt;
   const float* pos;

@@ -121,6 +121,7 @@ TRN_D WNode* top_nodes() {
 
 // every kernel that traces rays calls this once before its work loop
 TRN_D void stage_top(const DeviceScene& s) {
+  if (!TRN_WIDE_BVH) return;
   const int n = min(s.n_wnodes, kTopNodes);
   const uint4* src = reinterpret_cast<const uint4*>(s.wnodes);
   uint4* dst = reinterpret_cast<uint4*>(top_nodes());
@@ -142,7 +143,8 @@ TRN_D void load_wnode(const DeviceScene& s, int idx, WNode& n) {
 }
 
 template <bool ANY>
-TRN_D bool trace_wide(const DeviceScene& s, const RayPre& r, float tmin, float tmax, Hit& hit, int* err) {
+__device__ __noinline__ bool trace_wide(const DeviceScene& s, const RayPre& r, float tmin, float tmax, Hit& hit,
+                                        int* err) {
   float best_t = tmax;
   int best_tri = 0x7fffffff;
   bool found = false;
@@ -155,40 +157,62 @@ TRN_D bool trace_wide(const DeviceScene& s, const RayPre& r, float tmin, float t
     const float sx = __uint_as_float((unsigned)n.ex << 23);
     const float sy = __uint_as_float((unsigned)n.ey << 23);
     const float sz = __uint_as_float((unsigned)n.ez << 23);
-    int next = -1;
-    float next_t = 0.f;
+    // box tests of all children first; hits go to two bit masks
+    unsigned leaf_mask = 0u, node_mask = 0u;
+    float tnear[8];
 #pragma unroll
     for (int i = 0; i < 8; i++) {
       const unsigned m = n.meta[i];
+      tnear[i] = 0.f;
       if (!(m & 0x80u)) continue;
       const float lx = __fmaf_rn((float)n.qlo[0][i], sx, n.ox), hx = __fmaf_rn((float)n.qhi[0][i], sx, n.ox);
       const float ly = __fmaf_rn((float)n.qlo[1][i], sy, n.oy), hy = __fmaf_rn((float)n.qhi[1][i], sy, n.oy);
       const float lz = __fmaf_rn((float)n.qlo[2][i], sz, n.oz), hz = __fmaf_rn((float)n.qhi[2][i], sz, n.oz);
       float tn;
-      if (!slab(r, lx, ly, lz, hx, hy, hz, tmin, best_t, tn)) continue;
-      if (m & 0x40u) {
-        const int slot = n.tri_base + (int)(m & 0x3fu);
-        const float4 a = __ldg(&s.wtri[3 * slot + 0]);
-        const float4 b = __ldg(&s.wtri[3 * slot + 1]);
-        const float4 c = __ldg(&s.wtri[3 * slot + 2]);
-        const int tri = __float_as_int(a.w);
-        float t, u, v;
-        if (intersect_tri(r, F3(a.x, a.y, a.z), F3(b.x, b.y, b.z), F3(c.x, c.y, c.z), tmin, tmax, t, u, v)) {
-          if (ANY) { hit.tri = tri; hit.t = t; hit.u = u; hit.v = v; return true; }
-          if (t < best_t || (t == best_t && tri < best_tri)) {
-            best_t = t; best_tri = tri; hit.u = u; hit.v = v; found = true;
-          }
+      if (slab(r, lx, ly, lz, hx, hy, hz, tmin, best_t, tn)) {
+        tnear[i] = tn;
+        if (m & 0x40u) leaf_mask |= 1u << i; else node_mask |= 1u << i;
+      }
+    }
+    // leaf triangles
+    while (leaf_mask) {
+      const int i = __ffs(leaf_mask) - 1;
+      leaf_mask &= leaf_mask - 1u;
+      const int slot = n.tri_base + (int)(n.meta[i] & 0x3fu);
+      const float4 a = __ldg(&s.wtri[3 * slot + 0]);
+      const float4 b = __ldg(&s.wtri[3 * slot + 1]);
+      const float4 c = __ldg(&s.wtri[3 * slot + 2]);
+      const int tri = __float_as_int(a.w);
+      float t, u, v;
+      if (intersect_tri(r, F3(a.x, a.y, a.z), F3(b.x, b.y, b.z), F3(c.x, c.y, c.z), tmin, tmax, t, u, v)) {
+        if (ANY) { hit.tri = tri; hit.t = t; hit.u = u; hit.v = v; return true; }
+        if (t < best_t || (t == best_t && tri < best_tri)) {
+          best_t = t; best_tri = tri; hit.u = u; hit.v = v; found = true;
         }
-      } else {
-        const int child = n.child_base + (int)(m & 0x3fu);
-        if (next < 0) { next = child; next_t = tn; }
-        else {
-          // keep the nearer child to descend into, push the other
-          int pushc = child; float pusht = tn;
-          if (tn < next_t) { pushc = next; pusht = next_t; next = child; next_t = tn; }
-          if (sp < kStackSize) stack[sp++] = make_int2(pushc, __float_as_int(pusht));
-          else if (err) atomicExch(err, 1);
+      }
+    }
+    // internal children: descend into the nearest, push the rest far-to-near
+    int next = -1;
+    if (node_mask) {
+      float nt = 3.4e38f;
+      int ni = 0;
+      for (unsigned mm = node_mask; mm; mm &= mm - 1u) {
+        const int i = __ffs(mm) - 1;
+        if (tnear[i] < nt) { nt = tnear[i]; ni = i; }
+      }
+      node_mask &= ~(1u << ni);
+      next = n.child_base + (int)(n.meta[ni] & 0x3fu);
+      while (node_mask) {
+        // push the farthest remaining first so nearer ones pop earlier
+        float ft = -1.f;
+        int fi = 0;
+        for (unsigned mm = node_mask; mm; mm &= mm - 1u) {
+          const int i = __ffs(mm) - 1;
+          if (tnear[i] >= ft) { ft = tnear[i]; fi = i; }
         }
+        node_mask &= ~(1u << fi);
+        if (sp < kStackSize) stack[sp++] = make_int2(n.child_base + (int)(n.meta[fi] & 0x3fu), __float_as_int(ft));
+        else if (err) atomicExch(err, 1);
       }
     }
     if (next >= 0) { cur = next; continue; }
@@ -212,7 +236,7 @@ TRN_D bool trace(const DeviceScene& s, const F3& o, const F3& d, float tmin, flo
   hit.tri = -1; hit.u = 0.f; hit.v = 0.f; hit.t = -1.f;
   if (s.nt <= 0) return false;
   const RayPre r = ray_setup(o, d);
-  if (s.n_wnodes > 0) return trace_wide<ANY>(s, r, tmin, tmax, hit, err);
+  if (TRN_WIDE_BVH && s.n_wnodes > 0) return trace_wide<ANY>(s, r, tmin, tmax, hit, err);
   float best_t = tmax;
   int best_tri = 0x7fffffff;
   bool found = false;
