@@ -98,6 +98,20 @@ typedef struct {
   int sppse0;     /* direct edge */
   int sppse1;     /* indirect edge */
   int sppe0;      /* pixel boundary */
+  /* AQ guiding of the direct boundary term (RenderOptions::g_*,
+   * Integrator.h:72-77; AdaptiveQuadratureDistribution, AQ_distrb.h:62-197).
+   * g_direct != 0 builds a depth-0 guiding distribution per direct-boundary
+   * call from g_direct_spp samples per secondary edge and mixes it with
+   * g_eps. Guided samples use one extra sample dimension (3 + 3*max_bounces).
+   * g_direct_depth, g_direct_max_size and g_direct_thold are accepted for
+   * interface parity; like the reference, only depth 0 is built, and the leaf
+   * arrays are sized by the edge count rather than by g_direct_max_size. */
+  int g_direct;
+  int g_direct_depth;
+  int g_direct_max_size;
+  int g_direct_spp;
+  float g_direct_thold;
+  float g_eps;
 } trn_render_options;
 
 /* Sample source for one integrator call. If `samples` is non-NULL it is a

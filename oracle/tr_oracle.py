@@ -947,16 +947,94 @@ def importance_step(scene, cam, surf, rdir, T, b0, b1, b2):
     return contrib, pix, keep, None, None, None
 
 
-def direct_edge(scene, cam, spp, D, smp):
-    """DirectBoundaryIntegrator::Integrate without guiding
-    (BoundaryDirect.cpp:38-143, Edge.cpp:90-144, 201-309)."""
+GUIDE_TERM = 5  # hash-sampler term of the guiding set-up samples
+
+
+def _guide_base_val(scene, x, y, z):
+    """|baseVal| of EvalBoundarySegmentDirect in guiding mode (Edge.cpp:201-259
+    with guiding_mode=true): the sample-stage mask of SampleBoundarySegmentDirect
+    is replaced by the evaluation mask (same point, both rays hit), and the
+    value is |baseVal| without radiance or pdf. Invalid samples give 0."""
+    es = _edge_point(scene, scene.sec_func, scene.sec_cdf, scene.sec_integral, x)
+    ls = scene.light_sample(y, z)
+    p0, p2, nL = es["p0"].detach(), ls["p"].detach(), ls["n"].detach()
+    rdir = normalize(p0 - p2)
+    tri0, _, _, t0 = scene.intersect(p0, -rdir, SHADOW_EPS, RAY_MAX)
+    tri, u, v, _ = scene.intersect(p0, rdir, SHADOW_EPS, RAY_MAX)
+    hp = p0 + t0[:, None] * (-rdir)
+    ok = (length(hp - p2) < SHADOW_EPS) & (tri0 >= 0) & (tri >= 0)
+    out = torch.zeros(x.shape[0])
+    m = torch.nonzero(ok).reshape(-1)
+    if len(m) == 0:
+        return out
+    surf = scene.post_intersect(tri[m], u[m], v[m])
+    xp = surf["p"].detach()
+    dl = length(p2[m] - xp)
+    cos2 = dot(nL[m], rdir[m]).abs()
+    its_t = length(xp - p0[m])
+    bval, _ = _base_val(its_t / dl, es["edge"][m], -rdir[m], nL[m], es["edge2"][m])
+    bval = (bval * cos2).abs()
+    out[m] = torch.where(torch.isfinite(bval), bval, torch.zeros_like(bval))
+    return out
+
+
+def aq_guide(scene, seed, g_spp, eps):
+    """AdaptiveQuadratureDistribution::setup at tree depth 0 (AQ_distrb.h:83-173,
+    NEE.cu:70-89 build_tree): one leaf per secondary edge, box
+    [cdf[i-1], cdf[i]] x [0,1] x [0,1] of the (edge, light) sample cube; the
+    leaf weight is the mean |baseVal| of g_spp uniform samples in the box,
+    normalised to sum 1, mixed with eps, and the leaf distribution is
+    weight x box volume. Leaves of non-secondary edges (zero length in the
+    edge distribution) get weight 0 and zero volume, as if absent.
+    Returns (weight, cdf, integral, sum of weight x volume)."""
+    E = scene.edges.shape[0]
+    cdf = scene.sec_cdf
+    lo = torch.cat([torch.zeros(1), cdf[:-1]])
+    hi = cdf
+    live = scene.sec_func.detach() > 0
+    poly = torch.zeros(E)
+    leaf = torch.arange(E)
+    stream = (seed * 1000003) & 0xFFFFFFFF
+    for k in range(g_spp):
+        slot = (leaf * g_spp + k).numpy().astype(np.uint64)
+        r = [torch.from_numpy(hash_uniform(stream, GUIDE_TERM, d, slot)) for d in range(3)]
+        x = lo + r[0] * (hi - lo)
+        bv = _guide_base_val(scene, x, r[1], r[2])
+        poly = poly + torch.where(live, bv, torch.zeros_like(bv)) / np.float32(g_spp)
+    tot = float(poly.double().sum())
+    if tot > 0:
+        poly = poly / np.float32(tot)
+    poly = np.float32(eps) + np.float32(1.0 - eps) * poly
+    func = poly * (hi - lo)
+    gcdf, gint = cdf_of(func)
+    fsum = torch.tensor(float(func.double().sum()), dtype=F32)
+    return poly, gcdf, gint, fsum
+
+
+def direct_edge(scene, cam, spp, D, smp, guide=None):
+    """DirectBoundaryIntegrator::Integrate (BoundaryDirect.cpp:38-143,
+    Edge.cpp:90-144, 201-309). With guide = aq_guide(...) the (edge, light)
+    sample comes from the leaf distribution (AdaptiveQuadratureDistribution::sample,
+    AQ_distrb.h:176-195): a leaf by the extra uniform of dimension 3+3D, then a
+    point uniform in its box; the sample pdf is multiplied by weight/sum."""
     W, H = cam["width"], cam["height"]
     N = W * H * spp
     img = torch.zeros(W * H, 3)
     if not scene.sec_integral > 0:
         return img
     slots = torch.arange(N)
-    es = _edge_point(scene, scene.sec_func, scene.sec_cdf, scene.sec_integral, smp[0][slots])
+    r0 = smp[0][slots]
+    pdf_b = torch.ones(N)
+    if guide is not None:
+        poly, gcdf, gint, fsum = guide
+        if not gint > 0:
+            return img
+        leaf = torch.searchsorted(gcdf, smp[3 + 3 * D][slots], right=False).clamp(0, gcdf.shape[0] - 1)
+        cdf = scene.sec_cdf
+        lo = torch.where(leaf > 0, cdf[(leaf - 1).clamp(min=0)], torch.zeros_like(r0))
+        r0 = lo + r0 * (cdf[leaf] - lo)
+        pdf_b = poly[leaf] / fsum
+    es = _edge_point(scene, scene.sec_func, scene.sec_cdf, scene.sec_integral, r0)
     ls = scene.light_sample(smp[1][slots], smp[2][slots])
     p0, p2, nL = es["p0"], ls["p"], ls["n"]
     ev = p2.detach() - p0.detach()
@@ -973,7 +1051,7 @@ def direct_edge(scene, cam, spp, D, smp):
     v1 = ((c0 > EDGE_EPS) & (c1 < -EDGE_EPS)) | ((c0 < -EDGE_EPS) & (c1 > EDGE_EPS))
     right = (isb & v0) | (~isb & v1)
     ok = right & (cos_t > EPS) & (dist > SHADOW_EPS)
-    pdf = es["pdf"] * ls["pdf"] * dsq / cos_t
+    pdf = es["pdf"] * ls["pdf"] * dsq / cos_t * pdf_b
     rdir = normalize(p0.detach() - p2.detach())
     tri0, u0, v0_, t0 = scene.intersect(p0.detach(), -rdir, SHADOW_EPS, RAY_MAX)
     tri, u, v, _ = scene.intersect(p0.detach(), rdir, SHADOW_EPS, RAY_MAX)
@@ -1169,17 +1247,21 @@ def pixel_edge(scene, cam, spp, D, smp):
 INTEGRATORS = {0: path_tracer, 1: primary_edge, 2: direct_edge, 3: indirect_edge, 4: pixel_edge}
 
 
-def render(scene, cam, integrator, spp, D, smp):
+def render(scene, cam, integrator, spp, D, smp, guiding=None):
+    """guiding = (seed, g_direct_spp, g_eps) turns on AQ guiding of the direct
+    boundary term."""
+    if integrator == 2 and guiding is not None:
+        return direct_edge(scene, cam, spp, D, smp, guide=aq_guide(scene, *guiding))
     return INTEGRATORS[integrator](scene, cam, spp, D, smp)
 
 
-def grads(scene, cam, integrator, spp, D, smp, dLdI):
+def grads(scene, cam, integrator, spp, D, smp, dLdI, guiding=None):
     """dL/d(parameters) for loss sum(dLdI * image), via autograd."""
     for t in (scene.translation, scene.raw, scene.texels):
         if t.grad is not None:
             t.grad = None
     scene.configure()  # rebuild the differentiable geometry chain
-    img = render(scene, cam, integrator, spp, D, smp)
+    img = render(scene, cam, integrator, spp, D, smp, guiding)
     loss = (img * dLdI.reshape(-1, 3)).sum()
     params = [t for t in (scene.translation, scene.raw, scene.texels) if t.requires_grad]
     if loss.requires_grad:

@@ -55,7 +55,9 @@ class TrnCamera(C.Structure):
 
 class TrnRenderOptions(C.Structure):
     _fields_ = [("seed", C.c_int), ("max_bounces", C.c_int), ("spp", C.c_int), ("sppe", C.c_int),
-                ("sppse0", C.c_int), ("sppse1", C.c_int), ("sppe0", C.c_int)]
+                ("sppse0", C.c_int), ("sppse1", C.c_int), ("sppe0", C.c_int),
+                ("g_direct", C.c_int), ("g_direct_depth", C.c_int), ("g_direct_max_size", C.c_int),
+                ("g_direct_spp", C.c_int), ("g_direct_thold", C.c_float), ("g_eps", C.c_float)]
 
 
 class TrnSamples(C.Structure):

@@ -69,10 +69,19 @@ class RenderOptions:
         self.sppse1_batch, self.sppe0_batch = sppse1, sppe0
         self.export_deriv = False
         self.quiet = True
+        # guiding options (Integrator.h:72-77)
+        self.g_direct = False
+        self.g_direct_depth = 0
+        self.g_direct_max_size = 100000
+        self.g_direct_spp = 16
+        self.g_direct_thold = 0.01
+        self.g_eps = 0.01
 
     def _c(self) -> TrnRenderOptions:
         return TrnRenderOptions(int(self.seed), int(self.max_bounces), int(self.spp), int(self.sppe),
-                                int(self.sppse0), int(self.sppse1), int(self.sppe0))
+                                int(self.sppse0), int(self.sppse1), int(self.sppe0), int(bool(self.g_direct)),
+                                int(self.g_direct_depth), int(self.g_direct_max_size), int(self.g_direct_spp),
+                                float(self.g_direct_thold), float(self.g_eps))
 
 
 class Camera:
@@ -393,11 +402,13 @@ class PixelBoundaryIntegrator(Integrator):
     integrator_id = TRN_PIXEL_EDGE
 
 
-def sample_dims(integrator_id: int, max_bounces: int) -> int:
+def sample_dims(integrator_id: int, max_bounces: int, guided: bool = False) -> int:
     """Uniform dimensions one sample slot consumes (see the sample layout in
-    the library: camera/edge draws first, then per-bounce light and BSDF draws)."""
+    the library: camera/edge draws first, then per-bounce light and BSDF draws).
+    A guided direct-boundary sample takes one more (the guiding leaf)."""
     D = max_bounces
-    return {TRN_PATH_TRACER: 2 + 5 * D, TRN_PRIMARY_EDGE: 2 + 5 * D, TRN_DIRECT_EDGE: 3 + 3 * D,
+    return {TRN_PATH_TRACER: 2 + 5 * D, TRN_PRIMARY_EDGE: 2 + 5 * D,
+            TRN_DIRECT_EDGE: 3 + 3 * D + (1 if guided else 0),
             TRN_INDIRECT_EDGE: 3 + 8 * max(D - 1, 0), TRN_PIXEL_EDGE: 1 + 5 * D}[integrator_id]
 
 

@@ -43,6 +43,10 @@ struct Params {
   int ne;
   int* err;
   unsigned long long* stats;  // optional work counters (see Cnt), nullptr = off
+  // AQ guiding of the direct boundary term (nullptr = unguided)
+  const float* aq_poly;       // [E] leaf weights
+  const float* aq_cdf;        // [E] leaf distribution
+  const float* aq_int;        // [2] integral, sum of weight x volume
 };
 
 constexpr int kMaxDepth = 16;
@@ -882,10 +886,22 @@ __global__ void __launch_bounds__(256) k_direct_adj(Params P) {
       const ViewDesc& V = view_of(P, gslot);
       const long long p = gslot - V.begin;
       const PathSmp S{&P, V.seed, gslot, p + V.slot_off};
-      const float r0 = S(0), r1 = S(1), r2 = S(2);
+      float r0 = S(0);
+      const float r1 = S(1), r2 = S(2);
       float reuse;
       const float integral = __ldg(P.eint);
       if (!(integral > 0.f)) return false;
+      float pdf_b = 1.f;
+      if (P.aq_cdf) {
+        // AdaptiveQuadratureDistribution::sample (AQ_distrb.h:176-195): pick a
+        // leaf with the extra uniform, then place the edge coordinate in its box
+        if (!(__ldg(P.aq_int) > 0.f)) return false;
+        float unused;
+        const int leaf = sample_discrete(P.aq_cdf, P.ne, S(3 + 3 * V.D), unused);
+        const float lo = leaf > 0 ? __ldg(P.ecdf + leaf - 1) : 0.f, hi = __ldg(P.ecdf + leaf);
+        r0 = __fadd_rn(lo, __fmul_rn(r0, __fsub_rn(hi, lo)));
+        pdf_b = __fdiv_rn(__ldg(P.aq_poly + leaf), __ldg(P.aq_int + 1));
+      }
       const int e = sample_discrete(P.ecdf, P.ne, r0, reuse);
       const int v0 = P.edges[5 * e], v1 = P.edges[5 * e + 1], f0 = P.edges[5 * e + 2], f1 = P.edges[5 * e + 3],
                 v2 = P.edges[5 * e + 4];
@@ -914,7 +930,7 @@ __global__ void __launch_bounds__(256) k_direct_adj(Params P) {
       const bool valid1 = (c0 > kEdgeEps && c1 < -kEdgeEps) || (c0 < -kEdgeEps && c1 > kEdgeEps);
       const bool right = (is_b && valid0) || (!is_b && valid1);
       if (!(right && cos_t > kEps && dist > kShadowEps)) return false;
-      const float pdf = pdf_e * ls.pdf * dist_sqr / cos_t;
+      const float pdf = pdf_e * ls.pdf * dist_sqr / cos_t * pdf_b;
       const F3 rdir = normalize(p0 - p2);
       Hit h0, h;
       cnt.v[kCntClosest] += 2;
@@ -960,6 +976,105 @@ __global__ void __launch_bounds__(256) k_direct_adj(Params P) {
 }
 
 // ---------------------------------------------------------------------------
+// AQ guiding of the direct boundary term (AdaptiveQuadratureDistribution::setup,
+// AQ_distrb.h:83-173; leaf boxes of NEE.cu:70-89 build_tree at depth 0)
+// ---------------------------------------------------------------------------
+constexpr uint32_t kGuideTerm = 5;  // hash-sampler term of the set-up samples
+
+// |baseVal| of one (edge, light) sample in guiding mode (Edge.cpp:201-259 with
+// guiding_mode=true): only the evaluation mask (same point, both rays hit)
+// applies, and neither radiance nor pdf enters. Invalid samples give 0.
+TRN_D float guide_base_val(const Params& P, float x, float y, float z) {
+  const DeviceScene& s = P.s;
+  float reuse;
+  const int e = sample_discrete(P.ecdf, P.ne, x, reuse);
+  const int v0 = P.edges[5 * e], v1 = P.edges[5 * e + 1], v2 = P.edges[5 * e + 4];
+  const F3 Pa = load3(s.pos, v0), Pb = load3(s.pos, v1), Pc = load3(s.pos, v2);
+  const F3 e1 = Pb - Pa;
+  const F3 p0 = Pa + e1 * reuse;
+  const F3 edge = normalize(e1), edge2 = normalize(Pc - Pa);
+  LightSample ls;
+  if (!light_sample(s, y, z, ls)) return 0.f;
+  int j0, j1, j2; tri_vertices(s, ls.tri, j0, j1, j2);
+  const F3 p2 = bary3(ls.bu, ls.bv, load3(s.pos, j0), load3(s.pos, j1), load3(s.pos, j2));
+  const F3 nL = load3(s.fnormal, ls.tri);
+  const F3 rdir = normalize(p0 - p2);
+  Hit h0, h;
+  if (!trace<false>(s, p0, -rdir, kShadowEps, kRayMax, h0, P.err)) return 0.f;
+  if (!trace<false>(s, p0, rdir, kShadowEps, kRayMax, h, P.err)) return 0.f;
+  const F3 hp = p0 + (-rdir) * h0.t;
+  if (!(length(hp - p2) < kShadowEps)) return 0.f;
+  const SurfF xs = post_intersect(s, h.tri, h.u, h.v);
+  const float dl = length(p2 - xs.p);
+  const float cos2 = fabsf(dot(nL, rdir));
+  const float its_t = length(xs.p - p0);
+  F3 n;
+  const float bv = fabsf(base_val(its_t / dl, edge, -rdir, nL, edge2, n) * cos2);
+  return isfinite(bv) ? bv : 0.f;
+}
+
+// Leaf weight = mean |baseVal| over gspp uniform samples in the leaf box
+// [cdf[i-1], cdf[i]] x [0,1]^2. Leaves of non-secondary edges (zero length in
+// the edge distribution) do not exist in the reference's compacted edge list
+// and get weight 0 here.
+__global__ void k_aq_poly(Params P, uint32_t stream, int gspp, float* poly) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= P.ne) return;
+  float acc = 0.f;
+  if (P.efunc[i] > 0.f && __ldg(P.eint) > 0.f) {
+    const float lo = i > 0 ? P.ecdf[i - 1] : 0.f, hi = P.ecdf[i];
+    const float fs = (float)gspp;
+    for (int k = 0; k < gspp; k++) {
+      const uint32_t slot = (uint32_t)i * (uint32_t)gspp + (uint32_t)k;
+      const float r0 = hash_uniform(stream, kGuideTerm, 0, slot);
+      const float r1 = hash_uniform(stream, kGuideTerm, 1, slot);
+      const float r2 = hash_uniform(stream, kGuideTerm, 2, slot);
+      const float x = __fadd_rn(lo, __fmul_rn(r0, __fsub_rn(hi, lo)));
+      acc = __fadd_rn(acc, __fdiv_rn(guide_base_val(P, x, r1, r2), fs));
+    }
+  }
+  poly[i] = acc;
+}
+
+// poly /= sum(poly); poly = eps + (1 - eps) poly; func = poly x leaf volume;
+// out[1] = sum(func) (the pdf normaliser of AQ_distrb.h:194). One block of
+// 1024 threads.
+__global__ void k_aq_mix(int n, float* poly, const float* ecdf, float eps, float* func, float* out) {
+  __shared__ double part[1024];
+  const int tid = threadIdx.x, T = blockDim.x;
+  double acc = 0.0;
+  for (int i = tid; i < n; i += T) acc += (double)poly[i];
+  part[tid] = acc;
+  __syncthreads();
+  for (int w = T / 2; w > 0; w >>= 1) {
+    if (tid < w) part[tid] += part[tid + w];
+    __syncthreads();
+  }
+  const double tot = part[0];
+  __syncthreads();
+  const float ftot = (float)tot;
+  const float one_m = (float)(1.0 - (double)eps);
+  acc = 0.0;
+  for (int i = tid; i < n; i += T) {
+    float p = poly[i];
+    if (tot > 0.0) p = __fdiv_rn(p, ftot);
+    p = __fadd_rn(eps, __fmul_rn(one_m, p));
+    const float lo = i > 0 ? ecdf[i - 1] : 0.f;
+    const float f = __fmul_rn(p, __fsub_rn(ecdf[i], lo));
+    poly[i] = p;
+    func[i] = f;
+    acc += (double)f;
+  }
+  part[tid] = acc;
+  __syncthreads();
+  for (int w = T / 2; w > 0; w >>= 1) {
+    if (tid < w) part[tid] += part[tid + w];
+    __syncthreads();
+  }
+  if (tid == 0) out[1] = (float)part[0];
+}
+
+// ---------------------------------------------------------------------------
 // indirect boundary (BoundaryIndirect.cpp:38-192, Edge.cpp:146-199)
 // ---------------------------------------------------------------------------
 template <int MAXD>
@@ -973,10 +1088,22 @@ __global__ void __launch_bounds__(256) k_indirect_adj(Params P) {
       const long long p = gslot - V.begin;
       if (V.D < 2) return false;
       const PathSmp S{&P, V.seed, gslot, p + V.slot_off};
-      const float r0 = S(0), r1 = S(1), r2 = S(2);
+      float r0 = S(0);
+      const float r1 = S(1), r2 = S(2);
       float reuse;
       const float integral = __ldg(P.eint);
       if (!(integral > 0.f)) return false;
+      float pdf_b = 1.f;
+      if (P.aq_cdf) {
+        // AdaptiveQuadratureDistribution::sample (AQ_distrb.h:176-195): pick a
+        // leaf with the extra uniform, then place the edge coordinate in its box
+        if (!(__ldg(P.aq_int) > 0.f)) return false;
+        float unused;
+        const int leaf = sample_discrete(P.aq_cdf, P.ne, S(3 + 3 * V.D), unused);
+        const float lo = leaf > 0 ? __ldg(P.ecdf + leaf - 1) : 0.f, hi = __ldg(P.ecdf + leaf);
+        r0 = __fadd_rn(lo, __fmul_rn(r0, __fsub_rn(hi, lo)));
+        pdf_b = __fdiv_rn(__ldg(P.aq_poly + leaf), __ldg(P.aq_int + 1));
+      }
       const int e = sample_discrete(P.ecdf, P.ne, r0, reuse);
       const int v0 = P.edges[5 * e], v1 = P.edges[5 * e + 1], f0 = P.edges[5 * e + 2], f1 = P.edges[5 * e + 3],
                 v2 = P.edges[5 * e + 4];
@@ -1391,7 +1518,34 @@ Params base_params(trn_scene* s, trn_viewset* vs, const trn_render_options* o, i
   P.edges = s->edges; P.ecdf = s->sec_cdf; P.efunc = s->sec_func; P.eint = s->sec_integral_dev; P.ne = s->ne;
   P.err = s->err;
   P.stats = s->stats_on ? s->stats : nullptr;
+  P.aq_poly = P.aq_cdf = P.aq_int = nullptr;
   return P;
+}
+
+// AdaptiveQuadratureDistribution::setup (AQ_distrb.h:83-173) for one
+// direct-boundary call: leaf weights from g_direct_spp samples per leaf, eps
+// mixing, leaf distribution. The set-up samples come from the counter hash
+// (its own term), also when the call's samples come from a table.
+int guide_setup(trn_scene* s, const trn_render_options* o, Params& P, cudaStream_t st) {
+  if (!o->g_direct || s->ne == 0) return 0;
+  if (o->g_direct_spp <= 0) { set_error("g_direct_spp must be positive when g_direct is set"); return -1; }
+  if (!(o->g_eps >= 0.f && o->g_eps <= 1.f)) { set_error("g_eps must be in [0, 1]"); return -1; }
+  if ((long long)s->ne * o->g_direct_spp > 0xFFFFFFFFLL) {
+    set_error("guiding: edges x g_direct_spp exceeds 2^32 set-up samples");
+    return -1;
+  }
+  Params G = P;
+  G.table = nullptr;
+  G.stats = nullptr;
+  k_aq_poly<<<(s->ne + 255) / 256, 256, 0, st>>>(G, (uint32_t)o->seed * 1000003u, o->g_direct_spp, s->aq_poly);
+  k_aq_mix<<<1, 1024, 0, st>>>(s->ne, s->aq_poly, s->sec_cdf, o->g_eps, s->aq_func, s->aq_int);
+  k_cdf_views<<<1, 1024, 0, st>>>(s->ne, s->aq_func, s->aq_cdf, s->aq_int);
+  count_launch(3);
+  TRN_CUDA_TRY(cudaGetLastError());
+  P.aq_poly = s->aq_poly;
+  P.aq_cdf = s->aq_cdf;
+  P.aq_int = s->aq_int;
+  return 0;
 }
 
 void launch_dims(const trn_launch* ln, long long total, int& grid, int& block) {
@@ -1457,6 +1611,7 @@ int render_views(trn_scene* s, trn_viewset* vs, const trn_render_options* o, int
   } else if ((integrator == TRN_DIRECT_EDGE || integrator == TRN_INDIRECT_EDGE) && s->ne == 0) {
     return 0;
   }
+  if (integrator == TRN_DIRECT_EDGE && guide_setup(s, o, P, st)) return -1;
   TRN_CUDA_TRY(cudaMemsetAsync(vs->work, 0, sizeof(unsigned long long), st));
   const bool shallow = vs->max_depth <= 8;  // smaller per-thread path records
   switch (integrator) {

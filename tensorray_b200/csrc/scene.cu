@@ -733,6 +733,10 @@ int trn_scene_create(const trn_scene_desc* d, trn_scene** out) {
       dev_alloc_copy(&s->sec_func, (const float*)nullptr, std::max<size_t>(1, (size_t)s->ne)) ||
       dev_alloc_copy(&s->sec_cdf, (const float*)nullptr, std::max<size_t>(1, (size_t)s->ne)) ||
       dev_alloc_copy(&s->sec_integral_dev, (const float*)nullptr, 1) ||
+      dev_alloc_copy(&s->aq_poly, (const float*)nullptr, std::max<size_t>(1, (size_t)s->ne)) ||
+      dev_alloc_copy(&s->aq_func, (const float*)nullptr, std::max<size_t>(1, (size_t)s->ne)) ||
+      dev_alloc_copy(&s->aq_cdf, (const float*)nullptr, std::max<size_t>(1, (size_t)s->ne)) ||
+      dev_alloc_copy(&s->aq_int, (const float*)nullptr, 2) ||
       dev_alloc_copy(&s->nodes, (const BvhNode*)nullptr, std::max(1, nt - 1)) ||
       dev_alloc_copy(&s->tri_verts, (const float4*)nullptr, 3 * (size_t)nt) ||
       dev_alloc_copy(&s->parent, (const int*)nullptr, 2 * (size_t)nt) ||
@@ -775,7 +779,8 @@ int trn_scene_destroy(trn_scene* s) {
                   s->light_integral_dev, s->bsdfs, s->texs, s->edges, s->sec_func, s->sec_cdf,
                   s->sec_integral_dev, s->nodes, s->tri_verts, s->parent, s->flags, s->keys, s->keys_alt,
                   s->sort_tmp, s->bounds, s->g_pos, s->g_vnormal, s->g_texels, s->g_translation, s->err,
-                  s->stats, s->wnodes, s->wtri, s->wqueue, s->wcount};
+                  s->stats, s->wnodes, s->wtri, s->wqueue, s->wcount, s->aq_poly, s->aq_func, s->aq_cdf,
+                  s->aq_int};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   delete s;
@@ -872,7 +877,7 @@ int trn_scene_configure(trn_scene* s, cudaStream_t st) {
 // BVH topology; leaf boxes and node boxes are recomputed bottom-up.
 int trn_scene_refit(trn_scene* s, cudaStream_t st) {
   if (!s) { set_error("trn_scene_refit: null scene"); return -1; }
-  if (!s->built) return trn_scene_configure(s, st);
+  if (!s->built || TRN_WIDE_BVH) return trn_scene_configure(s, st);  // the wide BVH is re-collapsed
   const int nt = s->nt;
   if (configure_geometry(s, st)) return -1;
   if (nt > 1) TRN_CUDA_TRY(cudaMemsetAsync(s->flags, 0, sizeof(int) * (nt - 1), st));

@@ -47,6 +47,12 @@ struct trn_scene {
   float* sec_func = nullptr;      // [E] length if the edge is a secondary edge else 0
   float* sec_cdf = nullptr;       // [E]
   float* sec_integral_dev = nullptr;
+  // AQ guiding of the direct boundary term, one leaf per edge
+  // (AdaptiveQuadratureDistribution, AQ_distrb.h:62-197)
+  float* aq_poly = nullptr;       // [E] leaf weight after eps mixing
+  float* aq_func = nullptr;       // [E] weight x leaf volume
+  float* aq_cdf = nullptr;        // [E]
+  float* aq_int = nullptr;        // [2] integral of aq_func/E, sum of aq_func
   // acceleration structure
   trn::BvhNode* nodes = nullptr;  // [T-1]
   float4* tri_verts = nullptr;    // [T][3]

@@ -1,0 +1,77 @@
+"""Multi-view inverse rendering loop on the GPU.
+
+The reference optimises scene parameters from Python: per view it calls
+RenderFunction (forward renderC, backward renderD of every integrator,
+pyTensorRay/renderer_multi_view.py:40-98), reads the gradients through the
+parameter manager (pyTensorRay/parameter_manager.py:36-101) and steps a torch
+optimiser. Here one step is: new vertex positions -> geometry chain + LBVH
+refit (Scene::Update, Scene.cpp:535-546) -> one batched forward launch over
+all views -> per-view loss and dL/dI in one launch -> one batched adjoint
+launch per integrator -> geometry adjoint -> Adam on the device. Nothing
+leaves the GPU inside a step; the loss stays a device tensor until read.
+"""
+from __future__ import annotations
+
+import torch
+
+from . import api
+
+
+class InverseRenderer:
+    """Optimise the raw vertex positions of a scene against target images.
+
+    integrators: ids of the terms whose gradients drive the step (the forward
+    image is always the interior path tracer's). options: one RenderOptions for
+    every term (its seed advances each step so sample noise decorrelates)."""
+
+    def __init__(self, scene: api.Scene, cameras: list, spps: list, targets: torch.Tensor,
+                 options: api.RenderOptions, integrators=(api.TRN_PATH_TRACER, api.TRN_PRIMARY_EDGE,
+                                                          api.TRN_DIRECT_EDGE),
+                 lr: float = 1e-3, refit: bool = True, launch=None):
+        self.scene = scene
+        self.views = api.ViewSet(scene, cameras, spps)
+        if targets.numel() != 3 * self.views.npix:
+            raise RuntimeError("targets must hold npix x 3 values (all views concatenated)")
+        self.targets = targets.reshape(-1, 3).to(scene.device, torch.float32).contiguous()
+        self.options = options
+        self.integrators = tuple(integrators)
+        self.refit = refit
+        self.launch = launch
+        dev = scene.device
+        self.x = scene._raw_positions.detach().clone().requires_grad_(True)
+        self.opt = torch.optim.Adam([self.x], lr=lr)
+        self.image = torch.empty(self.views.npix, 3, device=dev)
+        self.dLdI = torch.empty(self.views.npix, 3, device=dev)
+        self.loss = torch.zeros(len(cameras), device=dev)
+        self.steps = 0
+
+    def samples_per_step(self) -> int:
+        """Grad path-samples of one step: every view's W*H*spp per term."""
+        n = sum(c.width * c.height * s for c, s in zip(self.views.cameras, self.views.spps))
+        return n * len(self.integrators)
+
+    def step(self) -> torch.Tensor:
+        """One optimisation step; returns the per-view losses (device tensor)
+        of the parameters before the update."""
+        sc = self.scene
+        sc.set_vertex_positions(self.x.detach())
+        sc.configure(refit=self.refit and self.steps > 0)
+        self.options.seed = self.steps
+        self.views.render(api.TRN_PATH_TRACER, self.options, launch=self.launch, out=self.image)
+        self.loss = self.views.loss(self.image, self.targets, self.dLdI)
+        sc.clear_grads()
+        for i in self.integrators:
+            self.views.render_grad(i, self.options, self.dLdI, launch=self.launch)
+        g = sc.get_grads()["positions"]
+        self.x.grad = torch.nan_to_num(g, nan=0.0, posinf=0.0, neginf=0.0)
+        self.opt.step()
+        self.steps += 1
+        return self.loss
+
+
+def render_targets(scene: api.Scene, cameras: list, spps: list, options: api.RenderOptions,
+                   launch=None) -> torch.Tensor:
+    """Forward images of all views (concatenated [npix, 3]) for the current
+    scene parameters, e.g. the targets of an inverse-rendering run."""
+    vs = api.ViewSet(scene, cameras, spps)
+    return vs.render(api.TRN_PATH_TRACER, options, launch=launch)

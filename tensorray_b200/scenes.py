@@ -304,3 +304,57 @@ def fibonacci_cameras(n: int, radius: float, resolutions, seed: int = 0):
         res = int(rng.choice(resolutions))
         cams.append(CameraSpec(tuple(float(x) for x in p), (0.0, 0.0, 0.0), up, res, res, 45.0))
     return cams
+
+
+def load_obj(path: str, bsdf: int = 0, smooth: bool = True, light: int = -1,
+             translation=(0.0, 0.0, 0.0)) -> MeshSpec:
+    """Wavefront OBJ -> MeshSpec, following ObjMesh::LoadFromObj
+    (EDXUtil/Graphics/ObjMesh.cpp:39-345) with makeLeftHanded = false, as every
+    reference Primitive loads meshes (Renderer/Primitive.cpp:213-245):
+    `v` positions as given, `vt` texture coordinates with v flipped to 1 - v,
+    faces of 3 or 4 corners in the forms i, i/t, i/t/n, i//n with 1-based or
+    negative (relative) indices, quads split into (0, 1, 2) and (3, 0, 2).
+    Normals (`vn`), smoothing groups and materials are not used by the
+    renderer and are skipped. The reference leaves the texture indices of a
+    quad's second triangle unset; here they follow its position corners."""
+    pos, uv, faces, uvf = [], [], [], []
+    textured = False
+    with open(path, "r") as f:
+        for raw in f:
+            parts = raw.split()
+            if not parts or parts[0].startswith("#"):
+                continue
+            tag = parts[0]
+            if tag == "v":
+                pos.append([float(x) for x in parts[1:4]])
+            elif tag == "vt":
+                uv.append([float(parts[1]), 1.0 - float(parts[2])])
+                textured = True
+            elif tag == "f":
+                corners = parts[1:]
+                if len(corners) not in (3, 4):
+                    raise ValueError(f"{path}: faces must have 3 or 4 corners, got {len(corners)}")
+                pi, ti = [], []
+                for c in corners:
+                    fields = c.split("/")
+                    p = int(fields[0])
+                    pi.append(p - 1 if p > 0 else len(pos) + p)
+                    if len(fields) > 1 and fields[1]:
+                        t = int(fields[1])
+                        ti.append(t - 1 if t > 0 else len(uv) + t)
+                    else:
+                        ti.append(0)
+                faces.append([pi[0], pi[1], pi[2]])
+                uvf.append([ti[0], ti[1], ti[2]])
+                if len(corners) == 4:
+                    faces.append([pi[3], pi[0], pi[2]])
+                    uvf.append([ti[3], ti[0], ti[2]])
+    P = np.asarray(pos, np.float32).reshape(-1, 3)
+    F = np.asarray(faces, np.int32).reshape(-1, 3)
+    if F.size and (F.min() < 0 or F.max() >= len(P)):
+        raise ValueError(f"{path}: face index out of range")
+    m = MeshSpec(P, F, bsdf=bsdf, light=light, smooth=smooth, translation=tuple(translation))
+    if textured:
+        m.uvs = np.asarray(uv, np.float32).reshape(-1, 2)
+        m.uv_faces = np.asarray(uvf, np.int32).reshape(-1, 3)
+    return m

@@ -129,3 +129,26 @@ def test_grad_parity(cfg1, integrator):
     assert float(p_o.abs().sum()) > 0
     assert rel_l2(p_g, p_o) < 2e-3, f"vertex grads rel L2 {rel_l2(p_g, p_o):.2e}"
     assert rel_l2(t_g, t_o) < 2e-3, f"translation grads {t_g.tolist()} vs {t_o.tolist()}"
+
+
+@pytest.mark.parametrize("eps", [0.01, 0.5])
+def test_guided_direct_grad_parity(cfg1, eps):
+    """AQ-guided direct boundary term (AdaptiveQuadratureDistribution,
+    AQ_distrb.h:83-195): same leaf weights, same guided samples, same grads."""
+    spec, scene, osc, cam = cfg1
+    spp, gspp = 4, 4
+    dims = api.sample_dims(api.TRN_DIRECT_EDGE, D, guided=True)
+    smp = O.uniform_table(77, dims, api.sample_slots(api.TRN_DIRECT_EDGE, W, H, spp))
+    g = torch.Generator().manual_seed(13)
+    dLdI = torch.rand(W * H, 3, generator=g) - 0.3
+    opts = api.RenderOptions(5, D, spp, spp, spp, spp, spp)
+    opts.g_direct, opts.g_direct_spp, opts.g_eps = True, gspp, eps
+    scene.clear_grads()
+    api.DirectEdgeIntegrator().renderD(scene, opts, dLdI.reshape(H, W, 3).to(scene.device),
+                                       samples=smp.to(scene.device))
+    gg = scene.get_grads()
+    go, _ = O.grads(osc, cam, api.TRN_DIRECT_EDGE, spp, D, smp, dLdI, guiding=(5, gspp, eps))
+    p_g, p_o = gg["positions"].cpu(), go["positions"].detach()
+    assert float(p_o.abs().sum()) > 0
+    assert rel_l2(p_g, p_o) < 2e-3, f"vertex grads rel L2 {rel_l2(p_g, p_o):.2e}"
+    assert rel_l2(gg["translation"].cpu(), go["translation"].detach()) < 2e-3
