@@ -217,6 +217,25 @@ int trn_render_fwd(trn_scene* scene, const trn_camera* camera, const trn_render_
 int trn_render_grad(trn_scene* scene, const trn_camera* camera, const trn_render_options* options,
                     int integrator, const trn_samples* samples, const float* dLdI, cudaStream_t stream);
 
+/* trn_render_grad without any device allocation. No counterpart in the
+ * reference: it is for callers that may not call cudaMalloc or cudaFree while
+ * rendering (a host application that owns all device memory through its own
+ * allocator, or a loop that cannot take the device-wide synchronisation of
+ * cudaFree). Same arguments and results as trn_render_grad, but all scratch
+ * (view table, work counter, silhouette-edge distribution) lives in one fixed
+ * array compiled into the library (about 8 MiB, held on every GPU that loads
+ * the library until the process exits), and the call does not synchronise
+ * the stream.
+ * - Limit: for TRN_PRIMARY_EDGE the scene may have at most 1048576 edges;
+ *   larger scenes are rejected with an error.
+ * - The first call on each device looks up the array's device address
+ *   (cudaGetSymbolAddress); make that first call before any stream capture.
+ * - Calls that overlap on the GPU (other streams or host threads, same
+ *   device) share the array and race; the array keeps the last call's
+ *   contents, and each call rewrites what it reads. */
+int trn_render_grad_noalloc(trn_scene* scene, const trn_camera* camera, const trn_render_options* options,
+                            int integrator, const trn_samples* samples, const float* dLdI, cudaStream_t stream);
+
 /* Batched multi-view rendering: all views of a view set in one persistent
  * launch per integrator, images concatenated [npix*3]. The per-view spp of
  * trn_view applies to the integrator being rendered; options supplies

@@ -98,6 +98,8 @@ _SIGNATURES = {
                                  C.POINTER(TrnSamples), C.c_void_p, C.c_void_p]),
     "trn_render_grad": (C.c_int, [C.c_void_p, C.POINTER(TrnCamera), C.POINTER(TrnRenderOptions), C.c_int,
                                   C.POINTER(TrnSamples), C.c_void_p, C.c_void_p]),
+    "trn_render_grad_noalloc": (C.c_int, [C.c_void_p, C.POINTER(TrnCamera), C.POINTER(TrnRenderOptions), C.c_int,
+                                          C.POINTER(TrnSamples), C.c_void_p, C.c_void_p]),
     "trn_scene_get_grads": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
     "trn_scene_clear_grads": (C.c_int, [C.c_void_p, C.c_void_p]),
     "trn_viewset_create": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(TrnView), C.POINTER(C.c_void_p)]),

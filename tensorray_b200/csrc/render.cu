@@ -7,6 +7,7 @@
 // state in registers and simply stops; the per-slot sample layout replaces
 // the reference's per-call RandomFloat tensors (see SampleSource).
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -1793,6 +1794,166 @@ int trn_render_grad(trn_scene* s, const trn_camera* cam, const trn_render_option
   cudaStreamSynchronize(st);
   trn_viewset_destroy(vs);
   return rc;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free single-view gradient.
+//
+// trn_render_grad builds a temporary view set, which allocates device memory
+// for the view table, the work counter and the per-view silhouette-edge
+// distribution. Callers that may not allocate (a host that forbids cudaMalloc
+// between set-up and teardown, a caching allocator that must not be bypassed,
+// a real-time loop that cannot afford the implicit synchronisation of
+// cudaFree) use trn_render_grad_noalloc instead: all of its scratch lives in
+// the fixed-size array below, which is part of the loaded module.
+//
+// Scratch layout (each part 256-byte aligned): the view table (one ViewDesc),
+// the first-sample index of that view, the work counter, the silhouette
+// integral, then the silhouette function and its CDF (kNoAllocMaxEdges floats
+// each). Every call rewrites all of it that it reads, so it keeps the last
+// call's contents but never needs clearing from the outside. Two calls that
+// overlap in time on one device share this one array and race; such callers
+// must serialise them.
+constexpr int kNoAllocMaxEdges = 1 << 20;
+constexpr size_t kNoAllocHeader = 4096;  // ViewDesc, vbegin, work counter, integral
+constexpr size_t kNoAllocScratchBytes = kNoAllocHeader + 2 * sizeof(float) * (size_t)kNoAllocMaxEdges;
+static_assert(sizeof(ViewDesc) + 3 * 256 <= kNoAllocHeader, "view table does not fit the scratch header");
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+namespace {
+
+constexpr int kNoAllocMaxDevices = 64;
+std::atomic<unsigned char*> g_noalloc_base[kNoAllocMaxDevices];
+
+// Device address of the scratch array for the current device. In host code
+// the array's name only stands in for it, so the address comes from
+// cudaGetSymbolAddress, once per device (this may load the module on that
+// device, which is why the first call must not run inside stream capture).
+unsigned char* noalloc_scratch() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) {
+    set_error("trn_render_grad_noalloc: no usable current device");
+    return nullptr;
+  }
+  unsigned char* p = g_noalloc_base[dev].load(std::memory_order_acquire);
+  if (p) return p;
+  void* addr = nullptr;
+  const cudaError_t rc = cudaGetSymbolAddress(&addr, g_noalloc_scratch);
+  if (rc != cudaSuccess || !addr) {
+    set_error(std::string("trn_render_grad_noalloc: cudaGetSymbolAddress failed: ") + cudaGetErrorString(rc));
+    return nullptr;
+  }
+  g_noalloc_base[dev].store((unsigned char*)addr, std::memory_order_release);
+  return (unsigned char*)addr;
+}
+
+// Write the one-view table, its first-sample index (0) and a zero work
+// counter into the scratch header; the view is passed by value, so no host
+// staging buffer is involved.
+__global__ void k_noalloc_setup(ViewDesc v, ViewDesc* table, long long* vbegin, unsigned long long* work) {
+  if (threadIdx.x == 0) {
+    *table = v;
+    *vbegin = 0;
+    *work = 0ull;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int trn_render_grad_noalloc(trn_scene* s, const trn_camera* cam, const trn_render_options* o, int integrator,
+                            const trn_samples* smp, const float* dLdI, cudaStream_t st) {
+  if (check_common(s, o, integrator)) return -1;
+  if (!cam || !dLdI) { set_error("trn_render_grad_noalloc: null camera or dLdI"); return -1; }
+  if (cam->width <= 0 || cam->height <= 0) { set_error("trn_render_grad_noalloc: invalid resolution"); return -1; }
+  if (integrator == TRN_PRIMARY_EDGE && s->ne > kNoAllocMaxEdges) {
+    set_error("trn_render_grad_noalloc: the scene has " + std::to_string(s->ne) +
+              " edges; the static scratch holds the silhouette distribution of at most " +
+              std::to_string(kNoAllocMaxEdges));
+    return -1;
+  }
+  const int spp = spp_of(o, integrator);
+  if (spp < 0) { set_error("trn_render_grad_noalloc: negative spp"); return -1; }
+  const long long total = (long long)cam->width * cam->height * spp;
+  if (integrator == TRN_PIXEL_EDGE && total % 4 != 0) {
+    set_error("pixel boundary needs W*H*spp divisible by 4");
+    return -1;
+  }
+  unsigned char* base = noalloc_scratch();
+  if (!base) return -1;
+  ViewDesc* table = (ViewDesc*)base;
+  long long* vbegin = (long long*)(base + kNoAllocHeader - 3 * 256);
+  unsigned long long* work = (unsigned long long*)(base + kNoAllocHeader - 2 * 256);
+  float* pint = (float*)(base + kNoAllocHeader - 256);
+  float* pfunc = (float*)(base + kNoAllocHeader);
+  float* pcdf = pfunc + kNoAllocMaxEdges;
+
+  ViewDesc v;
+  std::memset(&v, 0, sizeof(v));
+  std::memcpy(&v.cam, cam, sizeof(CameraDesc));
+  v.begin = 0;
+  v.n = total;
+  v.pix_off = 0;
+  v.slot_off = 0;
+  v.inv_spp = spp > 0 ? 1.0f / (float)spp : 0.f;
+  v.seed = 0;
+  v.spp = spp;
+  v.D = o->max_bounces;
+  v.gpos = s->g_pos;
+  v.gvn = s->g_vnormal;
+  v.gtex = s->g_texels;
+  v.pfunc = pfunc;
+  v.pcdf = pcdf;
+  v.pint = pint;
+
+  // host-side view of the scratch (no device memory of its own)
+  trn_viewset vs;
+  vs.scene = s;
+  vs.nviews = 1;
+  vs.ne = s->ne;
+  vs.views = table;
+  vs.vbegin = vbegin;
+  vs.work = work;
+  Params P = base_params(s, &vs, o, integrator, smp, nullptr, total);
+  P.image = nullptr;
+  P.dLdI = dLdI;
+  const long long slots = integrator == TRN_PIXEL_EDGE ? total / 4 : total;
+  if (P.table && P.stride < slots) { set_error("sample table too small"); return -1; }
+  if (total == 0) return 0;
+  if ((integrator == TRN_PRIMARY_EDGE || integrator == TRN_DIRECT_EDGE || integrator == TRN_INDIRECT_EDGE) &&
+      s->ne == 0)
+    return 0;
+
+  k_noalloc_setup<<<1, 32, 0, st>>>(v, table, vbegin, work);
+  count_launch(1);
+  s->grads_finalized = false;
+  if (integrator == TRN_PRIMARY_EDGE) {
+    dim3 g((s->ne + 255) / 256, 1);
+    k_prim_edges_views<<<g, 256, 0, st>>>(s->ne, s->edges, s->pos, s->fnormal, table, pfunc);
+    k_cdf_views<<<1, 1024, 0, st>>>(s->ne, pfunc, pcdf, pint);
+    count_launch(2);
+  }
+  // the guiding distribution lives in buffers the scene allocated at creation
+  if (integrator == TRN_DIRECT_EDGE && guide_setup(s, o, P, st)) return -1;
+  const bool shallow = o->max_bounces <= 8;
+  switch (integrator) {
+    case TRN_PATH_TRACER:
+      if (shallow) launch(k_path_adj<8>, nullptr, total, P, st); else launch(k_path_adj<kMaxDepth>, nullptr, total, P, st);
+      break;
+    case TRN_PRIMARY_EDGE: launch(k_primary_adj, nullptr, total, P, st); break;
+    case TRN_DIRECT_EDGE: launch(k_direct_adj, nullptr, total, P, st); break;
+    case TRN_INDIRECT_EDGE:
+      if (shallow) launch(k_indirect_adj<8>, nullptr, total, P, st);
+      else launch(k_indirect_adj<kMaxDepth>, nullptr, total, P, st);
+      break;
+    default: launch(k_pixel_adj, nullptr, total, P, st); break;
+  }
+  TRN_CUDA_TRY(cudaGetLastError());
+  return 0;
 }
 
 int trn_intersect(trn_scene* s, int n, const float* org, const float* dir, const float* tmin, const float* tmax,
