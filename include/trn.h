@@ -204,7 +204,13 @@ int trn_intersect(trn_scene* scene, int n, const float* org, const float* dir, c
 int trn_occluded(trn_scene* scene, int n, const float* org, const float* dir, const float* tmin,
                  const float* tmax, int* out_visible, cudaStream_t stream);
 
-/* Forward render of one integrator (Integrator::RenderC, Integrator.h:96-104,
+/* Single-view calls (trn_render_fwd / trn_render_grad) reuse one view table
+ * held by the scene: the first such call allocates it, later calls neither
+ * allocate nor synchronise the stream. Calls on one scene must therefore be
+ * ordered on one stream (as the reference's single default stream orders
+ * them); use view sets for concurrent rendering.
+ *
+ * Forward render of one integrator (Integrator::RenderC, Integrator.h:96-104,
  * PathTracer.h:60-68). image_out [W*H*3] is overwritten. Only
  * TRN_PATH_TRACER produces radiance; edge integrators produce their
  * (zero-valued in the reference) primal and return 0. */

@@ -52,6 +52,20 @@ struct Params {
 
 constexpr int kMaxDepth = 16;
 
+// Minimum resident 256-thread blocks per SM the integrator kernels are
+// compiled for (caps registers per thread at 65536 / (256 * minimum)). The
+// interior adjoint keeps its path records in registers and runs best uncapped;
+// the other integrators run best capped at 128 registers.
+#ifndef TRN_MINB
+#define TRN_MINB 2
+#endif
+#ifndef TRN_MINB_PATHADJ
+#define TRN_MINB_PATHADJ 1
+#endif
+#ifndef TRN_MINB_INDIRECT
+#define TRN_MINB_INDIRECT 2
+#endif
+
 // Per-thread work counters behind the roofline's algorithmic-byte model:
 // ray queries, shading vertices, light samples, gradient scatters, pixels.
 enum { kCntClosest = 0, kCntShadow, kCntShade, kCntSmooth, kCntTex, kCntLight, kCntVScatter, kCntNScatter,
@@ -295,6 +309,7 @@ struct BounceRec {
 
 // Returns the contribution of this bounce (already NaN-scrubbed). On return
 // x/rdir/T hold the next vertex; the return flag says whether it exists.
+template <bool NI = false>
 TRN_D bool radiance_step(const DeviceScene& s, SurfF& x, F3& rdir, F3& T, float l0, float l1, float b0, float b1,
                          float b2, F3& contrib, BounceRec* rec, Cnt& cnt) {
   const BsdfDesc b = s.bsdfs[x.bsdf];
@@ -319,7 +334,7 @@ TRN_D bool radiance_step(const DeviceScene& s, SurfF& x, F3& rdir, F3& T, float 
     const bool stable = d > kShadowEps && fabsf(dotSh) > kEdgeEps;
     const bool noleak = dotSh * dotGeo > 0.f;
     if (stable && noleak) cnt.v[kCntShadow]++;
-    if (stable && noleak && !occluded(s, x.p, wi, kShadowEps, d - kShadowEps)) {
+    if (stable && noleak && !occluded_k<NI>(s, x.p, wi, kShadowEps, d - kShadowEps)) {
       const F3 Le = dot(-wi, nl) > 0.f ? light_radiance(s, ls.light) : F3z();
       const float G = fabsf(dot(nl, -wi)) / d2;
       const float bpdf = bsdf_pdf_local(b, fr.to_local(wo), fr.to_local(wi)) * G;
@@ -339,7 +354,7 @@ TRN_D bool radiance_step(const DeviceScene& s, SurfF& x, F3& rdir, F3& T, float 
   bsdf_sample_only(b, fr, wo, b0, b1, b2, wi, pdf);
   Hit h;
   bool ok = pdf > 0.f && out_dir_valid(b, x.ns, x.ng, wi);
-  if (ok) { cnt.v[kCntClosest]++; ok = trace<false>(s, x.p, wi, kShadowEps, kRayMax, h); }
+  if (ok) { cnt.v[kCntClosest]++; ok = trace_k<NI, false>(s, x.p, wi, kShadowEps, kRayMax, h); }
   if (!ok) {
     contrib = scrub(val);
     if (rec) rec->scrubbed = !finite3(val);
@@ -427,7 +442,7 @@ struct FwdState {
   F3 T, rdir, L;
 };
 
-__global__ void __launch_bounds__(256) k_path_fwd(Params P) {
+__global__ void __launch_bounds__(256, TRN_MINB) k_path_fwd(Params P) {
   Cnt cnt;
   stage_top(P.s);
   for_each_valid<FwdState>(P,
@@ -478,6 +493,7 @@ __global__ void __launch_bounds__(256) k_path_fwd(Params P) {
 TRN_D void nee_vjp(const BsdfDesc& b, bool need_prev, bool need_kd, const F3& xprev, const F3& x, const F3& ns,
                    const F3& ng, const F3& kd, const F3& y, const F3& nl, const F3& Le, float lpdf, float mis,
                    const F3& adj, F3& g_prev, F3& g_x, F3& g_ns, F3& g_kd, F3& g_y, F3& g_nl, float& g_Jl) {
+  #pragma unroll 1  // one copy of the dual-number factor code (instruction cache)
   for (int grp = 0; grp < 7; grp++) {
     if (grp == 0 && !need_prev) continue;
     if (grp == 3 && !need_kd) continue;
@@ -506,6 +522,7 @@ TRN_D void nee_vjp(const BsdfDesc& b, bool need_prev, bool need_kd, const F3& xp
 TRN_D void cont_vjp(const BsdfDesc& b, bool need_prev, bool need_kd, const F3& xprev, const F3& x, const F3& ns,
                     const F3& ng, const F3& kd, const F3& xn, const F3& ngn, float prev_pdf, const F3& adj,
                     F3& g_prev, F3& g_x, F3& g_ns, F3& g_kd, F3& g_xn, F3& g_ngn, float& g_Jn) {
+  #pragma unroll 1  // one copy of the dual-number factor code (instruction cache)
   for (int grp = 0; grp < 7; grp++) {
     if (grp == 0 && !need_prev) continue;
     if (grp == 3 && !need_kd) continue;
@@ -541,7 +558,7 @@ struct AdjState {
 };
 
 template <int MAXD>
-__global__ void __launch_bounds__(256) k_path_adj(Params P) {
+__global__ void __launch_bounds__(256, TRN_MINB_PATHADJ) k_path_adj(Params P) {
   const DeviceScene& s = P.s;
   Cnt cnt;
   stage_top(P.s);
@@ -664,6 +681,7 @@ __global__ void __launch_bounds__(256) k_path_adj(Params P) {
     {
       const float gam = a_next.x + a_next.y + a_next.z;
       if (gam != 0.f && isfinite(gam)) {
+        #pragma unroll 1  // one copy of the dual-number factor code (instruction cache)
         for (int grp = 0; grp < 3; grp++) {
           const V3<D3> dx = seed3<3>(Gn.p, grp == 0 ? 0 : -1);
           const V3<D3> dn = seed3<3>(Gn.ng, grp == 1 ? 0 : -1);
@@ -684,6 +702,7 @@ __global__ void __launch_bounds__(256) k_path_adj(Params P) {
 // ---------------------------------------------------------------------------
 // EvalImportance for one ray (Integrator.cpp:75-176)
 // ---------------------------------------------------------------------------
+template <bool NI = false>
 TRN_D bool importance_step(const DeviceScene& s, const CameraDesc& cam, SurfF& x, F3& rdir, F3& T, float b0,
                            float b1, float b2, F3& contrib, int& pix, Cnt& cnt) {
   contrib = F3z();
@@ -700,7 +719,7 @@ TRN_D bool importance_step(const DeviceScene& s, const CameraDesc& cam, SurfF& x
     const F3 dirc = sensor_ray_dir(cam, sds.qx, sds.qy);
     const float dist2cam = length(x.p - cpos);
     cnt.v[kCntShadow]++;
-    if (!occluded(s, cpos, dirc, kShadowEps, dist2cam - kShadowEps)) {
+    if (!occluded_k<NI>(s, cpos, dirc, kShadowEps, dist2cam - kShadowEps)) {
       F3 val = F3z();
       if (out_dir_valid(b, x.ns, x.ng, wo)) {
         const F3 wi = normalize(cpos - x.p);
@@ -719,7 +738,7 @@ TRN_D bool importance_step(const DeviceScene& s, const CameraDesc& cam, SurfF& x
   if (!(pdf > 0.f) || !out_dir_valid(b, x.ns, x.ng, wi)) return false;
   Hit h;
   cnt.v[kCntClosest]++;
-  if (!trace<false>(s, x.p, wi, kShadowEps, kRayMax, h)) return false;
+  if (!trace_k<NI, false>(s, x.p, wi, kShadowEps, kRayMax, h)) return false;
   x = post_intersect(s, h.tri, h.u, h.v);
   rdir = wi;
   T = Tn;
@@ -737,6 +756,7 @@ TRN_D void xdotn_vjp(const Params& P, const ViewDesc& V, float W, const F3& org,
   const F3 Pa = edge_attached ? load3(s.pos, va_) : F3z();
   const F3 Pb = edge_attached ? load3(s.pos, vb_) : F3z();
   F3 gPa = F3z(), gPb = F3z(), gorg = F3z(), g0 = F3z(), g1 = F3z(), g2 = F3z();
+  #pragma unroll 1  // one copy of the dual-number factor code (instruction cache)
   for (int grp = 0; grp < 6; grp++) {
     if ((grp == 0 || grp == 1) && !edge_attached) continue;
     if (grp == 2 && !org_attached) continue;
@@ -802,7 +822,7 @@ struct EdgeState {
   F3 g;
 };
 
-__global__ void __launch_bounds__(256) k_primary_adj(Params P) {
+__global__ void __launch_bounds__(256, TRN_MINB) k_primary_adj(Params P) {
   const DeviceScene& s = P.s;
   Cnt cnt;
   stage_top(P.s);
@@ -878,7 +898,7 @@ __global__ void __launch_bounds__(256) k_primary_adj(Params P) {
 // ---------------------------------------------------------------------------
 // direct boundary (BoundaryDirect.cpp:38-143, Edge.cpp:90-144, 201-309)
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_direct_adj(Params P) {
+__global__ void __launch_bounds__(256, TRN_MINB) k_direct_adj(Params P) {
   const DeviceScene& s = P.s;
   Cnt cnt;
   stage_top(P.s);
@@ -1079,7 +1099,7 @@ __global__ void k_aq_mix(int n, float* poly, const float* ecdf, float eps, float
 // indirect boundary (BoundaryIndirect.cpp:38-192, Edge.cpp:146-199)
 // ---------------------------------------------------------------------------
 template <int MAXD>
-__global__ void __launch_bounds__(256) k_indirect_adj(Params P) {
+__global__ void __launch_bounds__(256, TRN_MINB_INDIRECT) k_indirect_adj(Params P) {
   const DeviceScene& s = P.s;
   Cnt cnt;
   stage_top(P.s);
@@ -1144,8 +1164,8 @@ __global__ void __launch_bounds__(256) k_indirect_adj(Params P) {
       const float pdf = pdf_e * pdf_d;
       Hit he, hs;
       cnt.v[kCntClosest] += 2;
-      if (!trace<false>(s, p0, -dir, kShadowEps, kRayMax, he, P.err)) return false;
-      if (!trace<false>(s, p0, dir, kShadowEps, kRayMax, hs, P.err)) return false;
+      if (!trace_k<true, false>(s, p0, -dir, kShadowEps, kRayMax, he, P.err)) return false;
+      if (!trace_k<true, false>(s, p0, dir, kShadowEps, kRayMax, hs, P.err)) return false;
       const SurfF xe = post_intersect(s, he.tri, he.u, he.v);
       const SurfF xs = post_intersect(s, hs.tri, hs.u, hs.v);
       const float dl = length(xe.p - xs.p);
@@ -1174,7 +1194,8 @@ __global__ void __launch_bounds__(256) k_indirect_adj(Params P) {
           if (alive) {
             const int o = 3 + 5 * b;
             F3 c;
-            alive = radiance_step(s, xx, rd, T, S(o), S(o + 1), S(o + 2), S(o + 3), S(o + 4), c, nullptr, cnt);
+            alive = radiance_step<true>(s, xx, rd, T, S(o), S(o + 1), S(o + 2), S(o + 3), S(o + 4), c, nullptr,
+                                        cnt);
             cur = cur + c;
             if (T.x == 0.f && T.y == 0.f && T.z == 0.f) alive = false;
           }
@@ -1190,7 +1211,7 @@ __global__ void __launch_bounds__(256) k_indirect_adj(Params P) {
         for (int b = 0; b < D - 1; b++) {
           const int o = 3 + 5 * (D - 1) + 3 * b;
           F3 c; int pix;
-          const bool more = importance_step(s, V.cam, xx, rd, T, S(o), S(o + 1), S(o + 2), c, pix, cnt);
+          const bool more = importance_step<true>(s, V.cam, xx, rd, T, S(o), S(o + 1), S(o + 2), c, pix, cnt);
           if (pix >= 0) W += dot(g_at(P, V, pix), rad[D - b - 2] * c) * st.w0;
           if (!more) break;
         }
@@ -1205,7 +1226,7 @@ __global__ void __launch_bounds__(256) k_indirect_adj(Params P) {
 // ---------------------------------------------------------------------------
 // pixel boundary (BoundaryPixel.cpp:36-159, Edge.cpp:377-409, Camera.cpp:433-467)
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_pixel_adj(Params P) {
+__global__ void __launch_bounds__(256, TRN_MINB) k_pixel_adj(Params P) {
   const DeviceScene& s = P.s;
   Cnt cnt;
   stage_top(P.s);
@@ -1690,12 +1711,22 @@ int upload_pbegin(trn_viewset* vs, cudaStream_t st) {
   return 0;
 }
 
+// The scene's cached one-view set, re-pointed at `cam`: the first call
+// allocates it, later calls only restage the view table (pinned staging,
+// guarded by the set's copy event), so single-view calls neither allocate nor
+// synchronise the stream.
 int single_view(trn_scene* s, const trn_camera* cam, trn_viewset** out) {
   if (!cam) { set_error("null camera"); return -1; }
   trn_view v;
   std::memset(&v, 0, sizeof(v));
   std::memcpy(&v.camera, cam, sizeof(trn_camera));
-  return trn_viewset_create(s, 1, &v, out);
+  if (s->single) {
+    if (set_views(s->single, 1, &v)) return -1;
+  } else if (trn_viewset_create(s, 1, &v, &s->single)) {
+    return -1;
+  }
+  *out = s->single;
+  return 0;
 }
 
 }  // namespace
@@ -1778,10 +1809,7 @@ int trn_render_fwd(trn_scene* s, const trn_camera* cam, const trn_render_options
   if (!image) { set_error("trn_render_fwd: null image"); return -1; }
   trn_viewset* vs = nullptr;
   if (single_view(s, cam, &vs)) return -1;
-  const int rc = render_views(s, vs, o, integrator, smp, nullptr, spp_of(o, integrator), true, image, nullptr, st);
-  cudaStreamSynchronize(st);
-  trn_viewset_destroy(vs);
-  return rc;
+  return render_views(s, vs, o, integrator, smp, nullptr, spp_of(o, integrator), true, image, nullptr, st);
 }
 
 int trn_render_grad(trn_scene* s, const trn_camera* cam, const trn_render_options* o, int integrator,
@@ -1790,10 +1818,7 @@ int trn_render_grad(trn_scene* s, const trn_camera* cam, const trn_render_option
   if (!dLdI) { set_error("trn_render_grad: null dLdI"); return -1; }
   trn_viewset* vs = nullptr;
   if (single_view(s, cam, &vs)) return -1;
-  const int rc = render_views(s, vs, o, integrator, smp, nullptr, spp_of(o, integrator), false, nullptr, dLdI, st);
-  cudaStreamSynchronize(st);
-  trn_viewset_destroy(vs);
-  return rc;
+  return render_views(s, vs, o, integrator, smp, nullptr, spp_of(o, integrator), false, nullptr, dLdI, st);
 }
 
 }  // extern "C"
@@ -1801,9 +1826,9 @@ int trn_render_grad(trn_scene* s, const trn_camera* cam, const trn_render_option
 // ---------------------------------------------------------------------------
 // Allocation-free single-view gradient.
 //
-// trn_render_grad builds a temporary view set, which allocates device memory
-// for the view table, the work counter and the per-view silhouette-edge
-// distribution. Callers that may not allocate (a host that forbids cudaMalloc
+// trn_render_grad allocates device memory (the scene's one-view table, work
+// counter and silhouette-edge distribution) on a scene's first single-view
+// call. Callers that may not allocate (a host that forbids cudaMalloc
 // between set-up and teardown, a caching allocator that must not be bypassed,
 // a real-time loop that cannot afford the implicit synchronisation of
 // cudaFree) use trn_render_grad_noalloc instead: all of its scratch lives in

@@ -773,6 +773,8 @@ int trn_scene_create(const trn_scene_desc* d, trn_scene** out) {
 
 int trn_scene_destroy(trn_scene* s) {
   if (!s) return 0;
+  if (s->single) trn_viewset_destroy(s->single);
+  s->single = nullptr;
   void* ptrs[] = {s->raw_pos, s->translation, s->texels, s->pos, s->idx, s->fnormal, s->area, s->vnormal,
                   s->smooth, s->uv, s->uvidx, s->bsdf_id, s->emitter_id, s->vert_mesh, s->vf_off, s->vf_list,
                   s->emit_tris, s->tri_to_emit, s->light_func, s->light_cdf, s->light_radiance,

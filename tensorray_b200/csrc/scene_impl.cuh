@@ -5,7 +5,12 @@
 #include <vector>
 #include "scene_types.cuh"
 
+struct trn_viewset;
+
 struct trn_scene {
+  // one-view set reused by trn_render_fwd / trn_render_grad (no per-call
+  // allocation); created on the first single-view call
+  trn_viewset* single = nullptr;
   // ---- sizes -----------------------------------------------------------------
   int nv = 0, nt = 0, nuv = 0, nmesh = 0, nlight = 0, nbsdf = 0, ntex = 0, ne = 0;
   long long ntexel = 0;

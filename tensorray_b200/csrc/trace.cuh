@@ -294,4 +294,28 @@ TRN_D bool occluded(const DeviceScene& s, const F3& o, const F3& d, float tmin, 
   return trace<true>(s, o, d, tmin, tmax, h);
 }
 
+// One shared, non-inlined copy of the traversal. Kernels with many ray-query
+// sites (the indirect boundary term traces on both sides of the edge, with
+// NEE and importance rays on each) call this one (NI = true): inlined copies
+// would inflate them past the instruction cache. Kernels with few sites keep
+// the inlined form (NI = false), which avoids the call's register traffic.
+template <bool ANY>
+__device__ __noinline__ bool trace_shared(const DeviceScene& s, const F3& o, const F3& d, float tmin, float tmax,
+                                          Hit& hit, int* err) {
+  return trace<ANY>(s, o, d, tmin, tmax, hit, err);
+}
+
+template <bool NI, bool ANY>
+TRN_D bool trace_k(const DeviceScene& s, const F3& o, const F3& d, float tmin, float tmax, Hit& hit,
+                   int* err = nullptr) {
+  if constexpr (NI) return trace_shared<ANY>(s, o, d, tmin, tmax, hit, err);
+  else return trace<ANY>(s, o, d, tmin, tmax, hit, err);
+}
+
+template <bool NI>
+TRN_D bool occluded_k(const DeviceScene& s, const F3& o, const F3& d, float tmin, float tmax) {
+  Hit h;
+  return trace_k<NI, true>(s, o, d, tmin, tmax, h);
+}
+
 }  // namespace trn
