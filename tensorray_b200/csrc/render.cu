@@ -91,7 +91,7 @@ TRN_D void count_shade(Cnt& c, const DeviceScene& s, const SurfF& x) {
   if (s.bsdfs[x.bsdf].tex >= 0) c.v[kCntTex]++;
 }
 
-TRN_D F3 F3z() { return F3(0.f, 0.f, 0.f); }
+TRN_HD F3 F3z() { return F3(0.f, 0.f, 0.f); }
 TRN_D F3 scrub(const F3& a) { return finite3(a) ? a : F3z(); }
 TRN_D void atomic_add3(float* a, const F3& g) {
   if (g.x != 0.f) atomicAdd(a, g.x);
@@ -238,7 +238,7 @@ TRN_HD S xdotn(const V3<S>& org, const V3<S>& target, const V3<S>& P0, const V3<
 }
 
 using D3 = Dual<3>;
-TRN_D F3 contract(const V3<D3>& r, const F3& adj) {
+TRN_HD F3 contract(const V3<D3>& r, const F3& adj) {
   F3 g;
   for (int i = 0; i < 3; i++) g[i] = adj.x * r.x.d[i] + adj.y * r.y.d[i] + adj.z * r.z.d[i];
   return g;
@@ -490,61 +490,181 @@ __global__ void __launch_bounds__(256, TRN_MINB) k_path_fwd(Params P) {
 // interior term: replaying adjoint
 // ---------------------------------------------------------------------------
 // Gradient of NEE factor w.r.t. (xprev, x, ns, kd, y, nl, Jl).
-TRN_D void nee_vjp(const BsdfDesc& b, bool need_prev, bool need_kd, const F3& xprev, const F3& x, const F3& ns,
-                   const F3& ng, const F3& kd, const F3& y, const F3& nl, const F3& Le, float lpdf, float mis,
-                   const F3& adj, F3& g_prev, F3& g_x, F3& g_ns, F3& g_kd, F3& g_y, F3& g_nl, float& g_Jl) {
-  #pragma unroll 1  // one copy of the dual-number factor code (instruction cache)
-  for (int grp = 0; grp < 7; grp++) {
-    if (grp == 0 && !need_prev) continue;
-    if (grp == 3 && !need_kd) continue;
-    const V3<D3> a_prev = seed3<3>(xprev, grp == 0 ? 0 : -1);
-    const V3<D3> a_x = seed3<3>(x, grp == 1 ? 0 : -1);
-    const V3<D3> a_ns = seed3<3>(ns, grp == 2 ? 0 : -1);
-    const V3<D3> a_kd = seed3<3>(kd, grp == 3 ? 0 : -1);
-    const V3<D3> a_y = seed3<3>(y, grp == 4 ? 0 : -1);
-    const V3<D3> a_nl = seed3<3>(nl, grp == 5 ? 0 : -1);
-    const D3 a_J = seed1<3>(1.f, grp == 6 ? 0 : -1);
-    const V3<D3> r = nee_factor<D3>(b, a_prev, a_x, a_ns, lift<D3>(ng), a_kd, a_y, a_nl, a_J, Le, lpdf, mis);
-    const F3 g = contract(r, adj);
-    switch (grp) {
-      case 0: g_prev = g_prev + g; break;
-      case 1: g_x = g_x + g; break;
-      case 2: g_ns = g_ns + g; break;
-      case 3: g_kd = g_kd + g; break;
-      case 4: g_y = g_y + g; break;
-      case 5: g_nl = g_nl + g; break;
-      default: g_Jl += g.x; break;
+// ---------------------------------------------------------------------------
+// Hand-written reverse mode of the two path factors. Both have the form
+//   F_c = B_c(kd, to_local(wo), to_local(wi)) |ns.wi| |nz.wi| / d^2 J K_c
+// with wo = -normalize(x - xprev), wi = (z - x) / d, d^2 = |z - x|^2, the
+// frame of the (unnormalised, as in the reference) shading normal ns built by
+// coordinate_system, and K_c constant (NEE: Le_c mis / lpdf, z = light point,
+// nz = light normal; continuation: 1 / prev_pdf, z = next vertex, nz = its
+// geometric normal). The derivative conventions are the reference AD's
+// (d|x|/dx = +1 for x > 0, else -1, AbsOp::Backward). One backward sweep
+// replaces seven forward-mode evaluations per factor.
+// ---------------------------------------------------------------------------
+
+// eval_inner in the local frame: returns B and accumulates dB.gB into g_lo,
+// g_li (local directions) and g_kd.
+TRN_HD F3 eval_inner_vjp(const BsdfDesc& b, const F3& kd, const F3& lo, const F3& li, const F3& gB, F3& g_lo,
+                        F3& g_li, F3& g_kd) {
+  if (b.type == kDiffuse) {
+    const bool reflect = lo.z > 0.f && lo.z * li.z > 0.f;
+    if (!reflect) return F3z();
+    const float inv_pi = kInvPi;
+    g_kd = g_kd + gB * inv_pi;
+    return kd * inv_pi;
+  }
+  const float cv = lo.z, cl = li.z;
+  if (!(cv > 0.f && cl > 0.f)) return F3z();
+  const F3 hs = lo + li;
+  const float Lh = length(hs);
+  const F3 wh = hs / Lh;
+  const float nh = wh.z, vh = dot(lo, wh);
+  const float r = b.roughness;
+  const float alpha = r * r;
+  const float k = (r + 1.f) * (r + 1.f) * 0.125f;
+  const float am1 = alpha * alpha - 1.f;
+  const float qd = nh * nh * am1 + 1.f;
+  const float tmp = alpha / qd;
+  const float ggx = tmp * tmp * kInvPi;
+  const float coeff = vh * (vh * -5.55473f - 6.8316f);
+  const float e = expf(logf(2.f) * coeff);
+  const float q1 = cv * (1.f - k) + k, q2 = cl * (1.f - k) + k;
+  const float G1 = cv / q1, G2 = cl / q2;
+  const float G = G1 * G2;
+  const float den = 4.f * fabsf(cv) * fabsf(cl) + 1e-6f;
+  F3 B;
+  float g_ggx = 0.f, g_G = 0.f, g_e = 0.f, g_den = 0.f;
+  for (int c = 0; c < 3; c++) {
+    const float F0 = b.spec[c];
+    const float fres = F0 + (1.f - F0) * e;
+    const float spec = ggx * G * fres / den;
+    B[c] = kd[c] * kInvPi + spec;
+    g_ggx += gB[c] * G * fres / den;
+    g_G += gB[c] * ggx * fres / den;
+    g_e += gB[c] * ggx * G * (1.f - F0) / den;
+    g_den -= gB[c] * spec / den;
+  }
+  g_kd = g_kd + gB * (float)kInvPi;
+  const float g_tmp = g_ggx * 2.f * tmp * kInvPi;
+  const float g_qd = -g_tmp * tmp / qd;
+  const float g_nh = g_qd * 2.f * nh * am1;
+  const float g_coeff = g_e * e * logf(2.f);
+  const float g_vh = g_coeff * (vh * (2.f * -5.55473f) - 6.8316f);
+  float g_cv = g_G * G2 * k / (q1 * q1) + g_den * 4.f * fabsf(cl) * (cv > 0.f ? 1.f : -1.f);
+  float g_cl = g_G * G1 * k / (q2 * q2) + g_den * 4.f * fabsf(cv) * (cl > 0.f ? 1.f : -1.f);
+  const F3 g_wh = F3(0.f, 0.f, g_nh) + lo * g_vh;
+  const F3 g_hs = (g_wh - wh * dot(g_wh, wh)) / Lh;
+  g_lo = g_lo + g_hs + wh * g_vh;
+  g_li = g_li + g_hs;
+  g_lo.z += g_cv;
+  g_li.z += g_cl;
+  return B;
+}
+
+// coordinate_system (Utils.cpp:118-140): t = f(n) on the branch the value took;
+// accumulates dt.g_t into g_n.
+TRN_HD void tangent_vjp(const F3& n, const F3& g_t, F3& g_n) {
+  if (fabsf(n.x) > fabsf(n.y)) {
+    const float q = n.x * n.x + n.z * n.z;
+    const float inv = 1.f / sqrtf(fmaxf(q, 1e-3f));
+    // t = (-n.z inv, 0, n.x inv)
+    g_n.z -= g_t.x * inv;
+    g_n.x += g_t.z * inv;
+    if (q > 1e-3f) {
+      const float g_inv = -g_t.x * n.z + g_t.z * n.x;
+      const float g_q = -0.5f * g_inv * inv * inv * inv;
+      g_n.x += 2.f * g_q * n.x;
+      g_n.z += 2.f * g_q * n.z;
+    }
+  } else {
+    const float q = n.y * n.y + n.z * n.z;
+    const float inv = 1.f / sqrtf(fmaxf(q, 1e-3f));
+    // t = (0, n.z inv, -n.y inv)
+    g_n.z += g_t.y * inv;
+    g_n.y -= g_t.z * inv;
+    if (q > 1e-3f) {
+      const float g_inv = g_t.y * n.z - g_t.z * n.y;
+      const float g_q = -0.5f * g_inv * inv * inv * inv;
+      g_n.y += 2.f * g_q * n.y;
+      g_n.z += 2.f * g_q * n.z;
     }
   }
 }
 
+// Reverse mode of F above for the output adjoint `adj`; accumulates into the
+// gradient outputs (g_prev only if need_prev, g_kd only if need_kd).
+TRN_HD void factor_vjp(const BsdfDesc& b, bool need_prev, bool need_kd, const F3& xprev, const F3& x, const F3& ns,
+                      const F3& kd, const F3& z, const F3& nz, float J, const F3& K, const F3& adj, F3& g_prev,
+                      F3& g_x, F3& g_ns, F3& g_kd, F3& g_z, F3& g_nz, float& g_J) {
+  const F3 v0 = x - xprev;
+  const float L0 = length(v0);
+  const F3 n0 = v0 / L0;
+  const F3 wo = -n0;
+  const F3 vi = z - x;
+  const float d2 = dot(vi, vi);
+  const float d = sqrtf(d2);
+  const F3 wi = vi / d;
+  const Frame<float> fr = make_frame(ns);
+  const F3 lo = fr.to_local(wo), li = fr.to_local(wi);
+  const float cs = dot(ns, wi);
+  const float u = dot(nz, -wi);
+  const float Q = fabsf(cs) * fabsf(u) / d2 * J;
+  const F3 A = adj * K;
+  // B(kd, lo, li) with its adjoint gB = A Q
+  F3 g_lo = F3z(), g_li = F3z(), gkd = F3z();
+  const F3 B = eval_inner_vjp(b, kd, lo, li, A * Q, g_lo, g_li, gkd);
+  if (need_kd) g_kd = g_kd + gkd;
+  const float gQ = dot(A, B);
+  if (gQ == 0.f && g_lo.x == 0.f && g_lo.y == 0.f && g_lo.z == 0.f && g_li.x == 0.f && g_li.y == 0.f &&
+      g_li.z == 0.f)
+    return;
+  // Q = |cs| |u| / d2 J
+  const float g_cs = gQ * (cs > 0.f ? 1.f : -1.f) * fabsf(u) / d2 * J;
+  const float g_u = gQ * fabsf(cs) * (u > 0.f ? 1.f : -1.f) / d2 * J;
+  const float g_d2 = -gQ * Q / d2;
+  g_J += gQ * fabsf(cs) * fabsf(u) / d2;
+  F3 g_n = wi * g_cs;                    // cs = ns . wi
+  F3 g_wi = ns * g_cs - nz * g_u;        // u = -nz . wi
+  g_nz = g_nz - wi * g_u;
+  // local coordinates (v.t, v.b, v.n)
+  const F3 g_wo = fr.t * g_lo.x + fr.b * g_lo.y + fr.n * g_lo.z;
+  g_wi = g_wi + fr.t * g_li.x + fr.b * g_li.y + fr.n * g_li.z;
+  F3 g_t = wo * g_lo.x + wi * g_li.x;
+  const F3 g_b = wo * g_lo.y + wi * g_li.y;
+  g_n = g_n + wo * g_lo.z + wi * g_li.z;
+  // b = n x t
+  g_n = g_n + cross(fr.t, g_b);
+  g_t = g_t + cross(g_b, fr.n);
+  tangent_vjp(fr.n, g_t, g_n);
+  g_ns = g_ns + g_n;
+  // wi = vi / |vi|, d2 = vi . vi
+  const F3 g_vi = (g_wi - wi * dot(g_wi, wi)) / d + vi * (2.f * g_d2);
+  g_z = g_z + g_vi;
+  g_x = g_x - g_vi;
+  // wo = -v0 / |v0|
+  const F3 g_n0 = -g_wo;
+  const F3 g_v0 = (g_n0 - n0 * dot(g_n0, n0)) / L0;
+  g_x = g_x + g_v0;
+  if (need_prev) g_prev = g_prev - g_v0;
+}
+
+// Gradient of the NEE factor w.r.t. (xprev, x, ns, kd, y, nl, Jl).
+TRN_HD void nee_vjp(const BsdfDesc& b, bool need_prev, bool need_kd, const F3& xprev, const F3& x, const F3& ns,
+                   const F3& ng, const F3& kd, const F3& y, const F3& nl, const F3& Le, float lpdf, float mis,
+                   const F3& adj, F3& g_prev, F3& g_x, F3& g_ns, F3& g_kd, F3& g_y, F3& g_nl, float& g_Jl) {
+  (void)ng;  // the factor evaluates the BSDF without the shading-normal correction
+  const F3 K(Le.x / lpdf * mis, Le.y / lpdf * mis, Le.z / lpdf * mis);
+  factor_vjp(b, need_prev, need_kd, xprev, x, ns, kd, y, nl, 1.f, K, adj, g_prev, g_x, g_ns, g_kd, g_y, g_nl, g_Jl);
+}
+
 // Gradient of the continuation factor w.r.t. (xprev, x, ns, kd, xn, ngn, Jn).
-TRN_D void cont_vjp(const BsdfDesc& b, bool need_prev, bool need_kd, const F3& xprev, const F3& x, const F3& ns,
+TRN_HD void cont_vjp(const BsdfDesc& b, bool need_prev, bool need_kd, const F3& xprev, const F3& x, const F3& ns,
                     const F3& ng, const F3& kd, const F3& xn, const F3& ngn, float prev_pdf, const F3& adj,
                     F3& g_prev, F3& g_x, F3& g_ns, F3& g_kd, F3& g_xn, F3& g_ngn, float& g_Jn) {
-  #pragma unroll 1  // one copy of the dual-number factor code (instruction cache)
-  for (int grp = 0; grp < 7; grp++) {
-    if (grp == 0 && !need_prev) continue;
-    if (grp == 3 && !need_kd) continue;
-    const V3<D3> a_prev = seed3<3>(xprev, grp == 0 ? 0 : -1);
-    const V3<D3> a_x = seed3<3>(x, grp == 1 ? 0 : -1);
-    const V3<D3> a_ns = seed3<3>(ns, grp == 2 ? 0 : -1);
-    const V3<D3> a_kd = seed3<3>(kd, grp == 3 ? 0 : -1);
-    const V3<D3> a_xn = seed3<3>(xn, grp == 4 ? 0 : -1);
-    const V3<D3> a_ngn = seed3<3>(ngn, grp == 5 ? 0 : -1);
-    const D3 a_J = seed1<3>(1.f, grp == 6 ? 0 : -1);
-    const V3<D3> r = cont_factor<D3>(b, a_prev, a_x, a_ns, lift<D3>(ng), a_kd, a_xn, a_ngn, a_J, prev_pdf);
-    const F3 g = contract(r, adj);
-    switch (grp) {
-      case 0: g_prev = g_prev + g; break;
-      case 1: g_x = g_x + g; break;
-      case 2: g_ns = g_ns + g; break;
-      case 3: g_kd = g_kd + g; break;
-      case 4: g_xn = g_xn + g; break;
-      case 5: g_ngn = g_ngn + g; break;
-      default: g_Jn += g.x; break;
-    }
-  }
+  (void)ng;
+  const float ip = 1.f / prev_pdf;
+  factor_vjp(b, need_prev, need_kd, xprev, x, ns, kd, xn, ngn, 1.f, F3(ip, ip, ip), adj, g_prev, g_x, g_ns, g_kd,
+             g_xn, g_ngn, g_Jn);
 }
 
 struct VRec { int tri; float u, v; };
