@@ -387,6 +387,34 @@ TRN_D bool radiance_step(const DeviceScene& s, SurfF& x, F3& rdir, F3& T, float 
   return true;
 }
 
+// One shared (non-inlined) copy of each per-bounce step, with the traversal
+// inlined inside it. Kernels that run both kinds of steps in one body (the
+// indirect boundary term) or many of them call these: inlining every step at
+// every call site inflates those kernels past the instruction cache. The
+// other kernels choose per kernel (measured) between this and the inlined step.
+#ifndef TRN_SHARED_STEPS_PRIMARY
+#define TRN_SHARED_STEPS_PRIMARY 0
+#endif
+#ifndef TRN_SHARED_STEPS_PIXEL
+#define TRN_SHARED_STEPS_PIXEL 0
+#endif
+#ifndef TRN_SHARED_STEPS_FWD
+#define TRN_SHARED_STEPS_FWD 0
+#endif
+#ifndef TRN_SHARED_STEPS_DIRECT
+#define TRN_SHARED_STEPS_DIRECT 0
+#endif
+__device__ __noinline__ bool radiance_step_shared(const DeviceScene& s, SurfF& x, F3& rdir, F3& T, float l0, float l1,
+                                                  float b0, float b1, float b2, F3& contrib, BounceRec* rec, Cnt& cnt) {
+  return radiance_step<false>(s, x, rdir, T, l0, l1, b0, b1, b2, contrib, rec, cnt);
+}
+template <bool SHARED>
+TRN_D bool radiance_step_k(const DeviceScene& s, SurfF& x, F3& rdir, F3& T, float l0, float l1, float b0, float b1,
+                           float b2, F3& contrib, BounceRec* rec, Cnt& cnt) {
+  if constexpr (SHARED) return radiance_step_shared(s, x, rdir, T, l0, l1, b0, b1, b2, contrib, rec, cnt);
+  else return radiance_step<false>(s, x, rdir, T, l0, l1, b0, b1, b2, contrib, rec, cnt);
+}
+
 
 // Per-warp compaction of the work queue: lanes keep pulling sample slots (one
 // warp-aggregated atomic per round) until each holds a slot that survives the
@@ -474,7 +502,7 @@ __global__ void __launch_bounds__(256, TRN_MINB) k_path_fwd(Params P) {
       for (int b = 0; b < V.D; b++) {
         const int o = 2 + 5 * b;
         F3 c;
-        const bool more = radiance_step(P.s, x, rdir, T, S(o), S(o + 1), S(o + 2), S(o + 3), S(o + 4), c, nullptr,
+        const bool more = radiance_step_k<TRN_SHARED_STEPS_FWD>(P.s, x, rdir, T, S(o), S(o + 1), S(o + 2), S(o + 3), S(o + 4), c, nullptr,
                                         cnt);
         L = L + c;
         if (!more || (T.x == 0.f && T.y == 0.f && T.z == 0.f)) break;
@@ -865,6 +893,61 @@ TRN_D bool importance_step(const DeviceScene& s, const CameraDesc& cam, SurfF& x
   return true;
 }
 
+__device__ __noinline__ bool importance_step_shared(const DeviceScene& s, const CameraDesc& cam, SurfF& x, F3& rdir,
+                                                    F3& T, float b0, float b1, float b2, F3& contrib, int& pix,
+                                                    Cnt& cnt) {
+  return importance_step<false>(s, cam, x, rdir, T, b0, b1, b2, contrib, pix, cnt);
+}
+template <bool SHARED>
+TRN_D bool importance_step_k(const DeviceScene& s, const CameraDesc& cam, SurfF& x, F3& rdir, F3& T, float b0,
+                             float b1, float b2, F3& contrib, int& pix, Cnt& cnt) {
+  if constexpr (SHARED) return importance_step_shared(s, cam, x, rdir, T, b0, b1, b2, contrib, pix, cnt);
+  else return importance_step<false>(s, cam, x, rdir, T, b0, b1, b2, contrib, pix, cnt);
+}
+
+// scatter W * d xDotN / d(edge vertices, receiver point, far triangle)
+// Reverse mode of xdotn (RayIntersectAD + n . (w P0 + u P1 + v P2) with
+// detached vertices) for the upstream scalar W; returns the gradients w.r.t.
+// org, target and the attached triangle vertices P0, P1, P2.
+TRN_HD void xdotn_grad(const F3& org, const F3& target, const F3& P0, const F3& P1, const F3& P2, const F3& n,
+                       float W, F3& g_org, F3& g_target, F3& g0, F3& g1, F3& g2) {
+  const F3 vd = target - org;
+  const float Ld = length(vd);
+  const F3 dir = vd / Ld;
+  const F3 e1 = P1 - P0, e2 = P2 - P0;
+  const F3 h = cross(dir, e2);
+  const float f = 1.f / dot(e1, h);
+  const F3 sv = org - P0;
+  const F3 q = cross(sv, e1);
+  const float g_u = W * dot(n, P1 - P0);
+  const float g_v = W * dot(n, P2 - P0);
+  // v = f (dir . q), u = f (sv . h)
+  const float g_f = g_v * dot(dir, q) + g_u * dot(sv, h);
+  F3 g_dir = q * (g_v * f);
+  const F3 g_q = dir * (g_v * f);
+  F3 g_sv = h * (g_u * f);
+  F3 g_h = sv * (g_u * f);
+  // q = sv x e1
+  g_sv = g_sv + cross(e1, g_q);
+  F3 g_e1 = cross(g_q, sv);
+  // f = 1 / (e1 . h)
+  const float g_a = -g_f * f * f;
+  g_e1 = g_e1 + h * g_a;
+  g_h = g_h + e1 * g_a;
+  // h = dir x e2
+  g_dir = g_dir + cross(e2, g_h);
+  const F3 g_e2 = cross(g_h, dir);
+  // sv = org - P0, e1 = P1 - P0, e2 = P2 - P0
+  g_org = g_sv;
+  g0 = -(g_sv + g_e1 + g_e2);
+  g1 = g_e1;
+  g2 = g_e2;
+  // dir = vd / |vd|
+  const F3 g_vd = (g_dir - dir * dot(g_dir, dir)) / Ld;
+  g_target = g_vd;
+  g_org = g_org - g_vd;
+}
+
 // scatter W * d xDotN / d(edge vertices, receiver point, far triangle)
 TRN_D void xdotn_vjp(const Params& P, const ViewDesc& V, float W, const F3& org, bool org_attached, int recv_tri, float ru, float rv,
                      int va_, int vb_, float sedge, const F3& target_const, int far_tri, const F3& n, Cnt& cnt) {
@@ -873,37 +956,20 @@ TRN_D void xdotn_vjp(const Params& P, const ViewDesc& V, float W, const F3& org,
   int i0, i1, i2; tri_vertices(s, far_tri, i0, i1, i2);
   const F3 P0 = load3(s.pos, i0), P1 = load3(s.pos, i1), P2 = load3(s.pos, i2);
   const bool edge_attached = va_ >= 0;
-  const F3 Pa = edge_attached ? load3(s.pos, va_) : F3z();
-  const F3 Pb = edge_attached ? load3(s.pos, vb_) : F3z();
-  F3 gPa = F3z(), gPb = F3z(), gorg = F3z(), g0 = F3z(), g1 = F3z(), g2 = F3z();
-  #pragma unroll 1  // one copy of the dual-number factor code (instruction cache)
-  for (int grp = 0; grp < 6; grp++) {
-    if ((grp == 0 || grp == 1) && !edge_attached) continue;
-    if (grp == 2 && !org_attached) continue;
-    const V3<D3> a = seed3<3>(Pa, grp == 0 ? 0 : -1), bb = seed3<3>(Pb, grp == 1 ? 0 : -1);
-    const V3<D3> o = seed3<3>(org, grp == 2 ? 0 : -1);
-    const V3<D3> q0 = seed3<3>(P0, grp == 3 ? 0 : -1), q1 = seed3<3>(P1, grp == 4 ? 0 : -1),
-                 q2 = seed3<3>(P2, grp == 5 ? 0 : -1);
-    V3<D3> target;
-    if (edge_attached) target = a + (bb - a) * D3(sedge);
-    else target = lift<D3>(target_const);
-    const D3 r = xdotn<D3>(o, target, q0, q1, q2, n);
-    const F3 gg = F3(r.d[0], r.d[1], r.d[2]) * W;
-    switch (grp) {
-      case 0: gPa = gg; break;
-      case 1: gPb = gg; break;
-      case 2: gorg = gg; break;
-      case 3: g0 = gg; break;
-      case 4: g1 = gg; break;
-      default: g2 = gg; break;
-    }
+  F3 target = target_const, Pa = F3z(), Pb = F3z();
+  if (edge_attached) {
+    Pa = load3(s.pos, va_);
+    Pb = load3(s.pos, vb_);
+    target = Pa + (Pb - Pa) * sedge;
   }
+  F3 gorg, gt, g0, g1, g2;
+  xdotn_grad(org, target, P0, P1, P2, n, W, gorg, gt, g0, g1, g2);
   agg_add3(V.gpos, i0, g0);
   agg_add3(V.gpos, i1, g1);
   agg_add3(V.gpos, i2, g2);
   if (edge_attached) {
-    agg_add3(V.gpos, va_, gPa);
-    agg_add3(V.gpos, vb_, gPb);
+    agg_add3(V.gpos, va_, gt * (1.f - sedge));
+    agg_add3(V.gpos, vb_, gt * sedge);
   }
   if (org_attached) scatter_point(P, V, recv_tri, ru, rv, gorg, cnt);
 }
@@ -1003,7 +1069,7 @@ __global__ void __launch_bounds__(256, TRN_MINB) k_primary_adj(Params P) {
       for (int b = 0; b < V.D; b++) {
         const int o = 2 + 5 * b;
         F3 c;
-        const bool more = radiance_step(s, x, rdir, T, S(o), S(o + 1), S(o + 2), S(o + 3), S(o + 4), c, nullptr,
+        const bool more = radiance_step_k<TRN_SHARED_STEPS_PRIMARY>(s, x, rdir, T, S(o), S(o + 1), S(o + 2), S(o + 3), S(o + 4), c, nullptr,
                                         cnt);
         L = L + c;
         if (!more || (T.x == 0.f && T.y == 0.f && T.z == 0.f)) break;
@@ -1105,7 +1171,7 @@ __global__ void __launch_bounds__(256, TRN_MINB) k_direct_adj(Params P) {
       for (int b = 0; b < V.D; b++) {
         const int o = 3 + 3 * b;
         F3 c; int pix;
-        const bool more = importance_step(s, V.cam, xs, dirs, T, S(o), S(o + 1), S(o + 2), c, pix, cnt);
+        const bool more = importance_step_k<TRN_SHARED_STEPS_DIRECT>(s, V.cam, xs, dirs, T, S(o), S(o + 1), S(o + 2), c, pix, cnt);
         if (pix >= 0) W += dot(g_at(P, V, pix), ev0 * c);
         if (!more) break;
       }
@@ -1229,22 +1295,10 @@ __global__ void __launch_bounds__(256, TRN_MINB_INDIRECT) k_indirect_adj(Params 
       const long long p = gslot - V.begin;
       if (V.D < 2) return false;
       const PathSmp S{&P, V.seed, gslot, p + V.slot_off};
-      float r0 = S(0);
-      const float r1 = S(1), r2 = S(2);
+      const float r0 = S(0), r1 = S(1), r2 = S(2);
       float reuse;
       const float integral = __ldg(P.eint);
       if (!(integral > 0.f)) return false;
-      float pdf_b = 1.f;
-      if (P.aq_cdf) {
-        // AdaptiveQuadratureDistribution::sample (AQ_distrb.h:176-195): pick a
-        // leaf with the extra uniform, then place the edge coordinate in its box
-        if (!(__ldg(P.aq_int) > 0.f)) return false;
-        float unused;
-        const int leaf = sample_discrete(P.aq_cdf, P.ne, S(3 + 3 * V.D), unused);
-        const float lo = leaf > 0 ? __ldg(P.ecdf + leaf - 1) : 0.f, hi = __ldg(P.ecdf + leaf);
-        r0 = __fadd_rn(lo, __fmul_rn(r0, __fsub_rn(hi, lo)));
-        pdf_b = __fdiv_rn(__ldg(P.aq_poly + leaf), __ldg(P.aq_int + 1));
-      }
       const int e = sample_discrete(P.ecdf, P.ne, r0, reuse);
       const int v0 = P.edges[5 * e], v1 = P.edges[5 * e + 1], f0 = P.edges[5 * e + 2], f1 = P.edges[5 * e + 3],
                 v2 = P.edges[5 * e + 4];
@@ -1314,8 +1368,8 @@ __global__ void __launch_bounds__(256, TRN_MINB_INDIRECT) k_indirect_adj(Params 
           if (alive) {
             const int o = 3 + 5 * b;
             F3 c;
-            alive = radiance_step<true>(s, xx, rd, T, S(o), S(o + 1), S(o + 2), S(o + 3), S(o + 4), c, nullptr,
-                                        cnt);
+            alive = radiance_step_shared(s, xx, rd, T, S(o), S(o + 1), S(o + 2), S(o + 3), S(o + 4), c, nullptr,
+                                         cnt);
             cur = cur + c;
             if (T.x == 0.f && T.y == 0.f && T.z == 0.f) alive = false;
           }
@@ -1331,7 +1385,7 @@ __global__ void __launch_bounds__(256, TRN_MINB_INDIRECT) k_indirect_adj(Params 
         for (int b = 0; b < D - 1; b++) {
           const int o = 3 + 5 * (D - 1) + 3 * b;
           F3 c; int pix;
-          const bool more = importance_step<true>(s, V.cam, xx, rd, T, S(o), S(o + 1), S(o + 2), c, pix, cnt);
+          const bool more = importance_step_shared(s, V.cam, xx, rd, T, S(o), S(o + 1), S(o + 2), c, pix, cnt);
           if (pix >= 0) W += dot(g_at(P, V, pix), rad[D - b - 2] * c) * st.w0;
           if (!more) break;
         }
@@ -1414,7 +1468,7 @@ __global__ void __launch_bounds__(256, TRN_MINB) k_pixel_adj(Params P) {
       for (int b = 0; b < V.D; b++) {
         const int o = 1 + 5 * b;
         F3 c;
-        const bool more = radiance_step(s, x, rdir, T, S(o), S(o + 1), S(o + 2), S(o + 3), S(o + 4), c, nullptr,
+        const bool more = radiance_step_k<TRN_SHARED_STEPS_PIXEL>(s, x, rdir, T, S(o), S(o + 1), S(o + 2), S(o + 3), S(o + 4), c, nullptr,
                                         cnt);
         L = L + c;
         if (!more || (T.x == 0.f && T.y == 0.f && T.z == 0.f)) break;
