@@ -53,14 +53,13 @@ struct Params {
 constexpr int kMaxDepth = 16;
 
 // Minimum resident 256-thread blocks per SM the integrator kernels are
-// compiled for (caps registers per thread at 65536 / (256 * minimum)). The
-// interior adjoint keeps its path records in registers and runs best uncapped;
-// the other integrators run best capped at 128 registers.
+// compiled for (caps registers per thread at 65536 / (256 * minimum)); all
+// integrators run best capped at 128 registers (measured).
 #ifndef TRN_MINB
 #define TRN_MINB 2
 #endif
 #ifndef TRN_MINB_PATHADJ
-#define TRN_MINB_PATHADJ 1
+#define TRN_MINB_PATHADJ 2
 #endif
 #ifndef TRN_MINB_INDIRECT
 #define TRN_MINB_INDIRECT 2
@@ -253,7 +252,16 @@ TRN_D void vadj_zero(VAdj& a) { a.p = F3z(); a.ns = F3z(); a.ng = F3z(); a.J = 0
 // position = w P0 + u P1 + v P2 (detached u, v), face normal c/|c| and
 // J = A / Detach(A) with c = cross(P1 - P0, P2 - P0), shading normal
 // w n0 + u n1 + v n2 (Scene.cpp:668-730, Primitive.cpp:299-340).
-TRN_D void scatter_vertex(const Params& P, const ViewDesc& V, int tri, float u, float v, const VAdj& a, Cnt& cnt) {
+#ifndef TRN_SHARED_SCATTER
+#define TRN_SHARED_SCATTER 1
+#endif
+#if TRN_SHARED_SCATTER
+#define TRN_SCATTER_FN __device__ __noinline__
+#else
+#define TRN_SCATTER_FN TRN_D
+#endif
+TRN_SCATTER_FN void scatter_vertex(const Params& P, const ViewDesc& V, int tri, float u, float v, const VAdj& a,
+                                   Cnt& cnt) {
   const DeviceScene& s = P.s;
   cnt.v[kCntVScatter] += 3;
   int i0, i1, i2; tri_vertices(s, tri, i0, i1, i2);
@@ -403,6 +411,9 @@ TRN_D bool radiance_step(const DeviceScene& s, SurfF& x, F3& rdir, F3& T, float 
 #endif
 #ifndef TRN_SHARED_STEPS_DIRECT
 #define TRN_SHARED_STEPS_DIRECT 0
+#endif
+#ifndef TRN_SHARED_STEPS_PATHADJ
+#define TRN_SHARED_STEPS_PATHADJ 1
 #endif
 __device__ __noinline__ bool radiance_step_shared(const DeviceScene& s, SurfF& x, F3& rdir, F3& T, float l0, float l1,
                                                   float b0, float b1, float b2, F3& contrib, BounceRec* rec, Cnt& cnt) {
@@ -621,7 +632,15 @@ TRN_HD void tangent_vjp(const F3& n, const F3& g_t, F3& g_n) {
 
 // Reverse mode of F above for the output adjoint `adj`; accumulates into the
 // gradient outputs (g_prev only if need_prev, g_kd only if need_kd).
-TRN_HD void factor_vjp(const BsdfDesc& b, bool need_prev, bool need_kd, const F3& xprev, const F3& x, const F3& ns,
+#ifndef TRN_SHARED_FACTOR_VJP
+#define TRN_SHARED_FACTOR_VJP 1
+#endif
+#if TRN_SHARED_FACTOR_VJP
+#define TRN_FACTOR_FN __host__ __device__ __noinline__
+#else
+#define TRN_FACTOR_FN TRN_HD
+#endif
+TRN_FACTOR_FN void factor_vjp(const BsdfDesc& b, bool need_prev, bool need_kd, const F3& xprev, const F3& x, const F3& ns,
                       const F3& kd, const F3& z, const F3& nz, float J, const F3& K, const F3& adj, F3& g_prev,
                       F3& g_x, F3& g_ns, F3& g_kd, F3& g_z, F3& g_nz, float& g_J) {
   const F3 v0 = x - xprev;
@@ -755,7 +774,7 @@ __global__ void __launch_bounds__(256, TRN_MINB_PATHADJ) k_path_adj(Params P) {
       const int o = 2 + 5 * b;
       F3 c;
       BounceRec& R = br[k];
-      const bool more = radiance_step(s, x, rdir, T, S(o), S(o + 1), S(o + 2),
+      const bool more = radiance_step_k<TRN_SHARED_STEPS_PATHADJ>(s, x, rdir, T, S(o), S(o + 1), S(o + 2),
                                       S(o + 3), S(o + 4), c, &R, cnt);
       // a scrubbed (non-finite) bounce contributes nothing and carries no gradient
       nee_on[k] = R.nee_ok && !R.scrubbed;
