@@ -1375,38 +1375,50 @@ __global__ void __launch_bounds__(256, TRN_MINB_INDIRECT) k_indirect_adj(Params 
       const ViewDesc& V = *st.V;
       const int D = min(V.D, MAXD);
       const PathSmp S{&P, V.seed, st.gslot, st.p + V.slot_off};
-      // emitter side: cumulative radiance per depth
-      F3 rad[MAXD];
+      // Sensor side first (BoundaryIndirect.cpp:158-175 pairs sensor depth b
+      // with the emitter radiance accumulated over D-1-b bounces): record the
+      // importance contributions, weighted by dL/dI of their pixels. The
+      // emitter side then only runs as deep as the shallowest sensor depth
+      // that reached the image needs, and not at all when none did.
+      F3 sc[MAXD];
+      int bmin = D;
+      {
+        F3 T(1.f, 1.f, 1.f);
+        F3 rd = st.rdir;
+        SurfF xx = st.x;
+        for (int b = 0; b < D - 1; b++) sc[b] = F3z();
+        for (int b = 0; b < D - 1; b++) {
+          const int o = 3 + 5 * (D - 1) + 3 * b;
+          F3 c; int pix;
+          const bool more = importance_step_shared(s, V.cam, xx, rd, T, S(o), S(o + 1), S(o + 2), c, pix, cnt);
+          if (pix >= 0) {
+            sc[b] = g_at(P, V, pix) * c;
+            if (sc[b].x != 0.f || sc[b].y != 0.f || sc[b].z != 0.f) bmin = min(bmin, b);
+          }
+          if (!more) break;
+        }
+      }
+      if (bmin >= D - 1) return;
+      // emitter side: the radiance accumulated over j+1 bounces pairs with
+      // sensor depth D-2-j
+      float W = 0.f;
       {
         F3 T(1.f, 1.f, 1.f);
         F3 rd = -st.rdir;
         SurfF xx = st.xe;
         F3 cur = F3z();
+        const int jmax = D - 2 - bmin;
         bool alive = true;
-        for (int b = 0; b < D - 1; b++) {
+        for (int j = 0; j <= jmax; j++) {
           if (alive) {
-            const int o = 3 + 5 * b;
+            const int o = 3 + 5 * j;
             F3 c;
             alive = radiance_step_shared(s, xx, rd, T, S(o), S(o + 1), S(o + 2), S(o + 3), S(o + 4), c, nullptr,
                                          cnt);
             cur = cur + c;
             if (T.x == 0.f && T.y == 0.f && T.z == 0.f) alive = false;
           }
-          rad[b] = cur;
-        }
-      }
-      // sensor side, paired by depth (BoundaryIndirect.cpp:158-175)
-      float W = 0.f;
-      {
-        F3 T(1.f, 1.f, 1.f);
-        F3 rd = st.rdir;
-        SurfF xx = st.x;
-        for (int b = 0; b < D - 1; b++) {
-          const int o = 3 + 5 * (D - 1) + 3 * b;
-          F3 c; int pix;
-          const bool more = importance_step_shared(s, V.cam, xx, rd, T, S(o), S(o + 1), S(o + 2), c, pix, cnt);
-          if (pix >= 0) W += dot(g_at(P, V, pix), rad[D - b - 2] * c) * st.w0;
-          if (!more) break;
+          W += dot(sc[D - 2 - j], cur) * st.w0;
         }
       }
       if (W == 0.f || !isfinite(W)) return;
