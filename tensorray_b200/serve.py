@@ -3,12 +3,15 @@
 Requests (scene, camera, spp, depth, target image) arrive over time. The
 server keeps every scene's BVH, geometry and textures resident, admits a
 request when its device buffers fit in the HBM budget, and advances all
-admitted requests together. Each iteration issues, per scene, one batched
+admitted requests in batches. Each iteration issues, per scene, one batched
 launch for the next forward chunk of every request still rendering and one
 batched launch per gradient term for every request in its gradient phase:
 iteration-level continuous batching, so a request that arrives while others
 are on the GPU joins at the next iteration instead of waiting for them to
-finish. Every scene has its own CUDA stream, so launches of different scenes
+finish. An iteration carries at most `iter_samples` path samples, filled
+shortest-remaining-work first (SRPT), so small requests are not held behind
+large ones while the GPU stays saturated. Every scene has its own CUDA stream,
+so launches of different scenes
 overlap on the device. A request's samples depend only on its own seed and
 chunk offsets, never on the batch it shares, so its result is the same alone
 and in the mix (up to float atomic ordering).
@@ -72,10 +75,11 @@ class ServerStats:
 
 class Server:
     def __init__(self, scenes: dict, hbm_budget_bytes: float = 120e9, chunk_spp: int = 8, max_active: int = 256,
-                 clock=time.perf_counter):
+                 clock=time.perf_counter, iter_samples: int = 1 << 25):
         self.scenes = scenes
         self.budget = int(hbm_budget_bytes)
         self.chunk_spp = chunk_spp
+        self.iter_samples = int(iter_samples)
         self.max_active = max_active
         self.clock = clock
         self.streams = {k: torch.cuda.Stream() for k in scenes}
@@ -110,11 +114,44 @@ class Server:
     def idle(self) -> bool:
         return not self.pending and not self.active
 
+    def _remaining(self, r: RenderRequest) -> int:
+        """Path samples a request still needs (forward chunks + gradient chunks)."""
+        npix = r.camera.width * r.camera.height
+        per_chunk = npix * self.chunk_spp
+        n = self._nchunks(r)
+        if r.phase == PHASE_FWD:
+            return per_chunk * ((n - r.chunk) + n * len(r.terms))
+        if r.phase == PHASE_GRAD:
+            return per_chunk * (n - r.chunk) * len(r.terms)
+        return 0
+
+    def _chunk_samples(self, r: RenderRequest) -> int:
+        npix = r.camera.width * r.camera.height
+        k0 = r.chunk * self.chunk_spp
+        spp = min(self.chunk_spp, r.spp - k0)
+        return npix * spp * (1 if r.phase == PHASE_FWD else len(r.terms))
+
+    def _select(self) -> list:
+        """Requests that advance this iteration: shortest remaining work first,
+        until the iteration's sample budget is used (at least one request)."""
+        runnable = [r for r in self.active if r.phase in (PHASE_FWD, PHASE_GRAD)]
+        runnable.sort(key=lambda r: (self._remaining(r), r.arrival, r.rid))
+        chosen, used = [], 0
+        for r in runnable:
+            cs = self._chunk_samples(r)
+            if chosen and used + cs > self.iter_samples:
+                continue
+            chosen.append(r)
+            used += cs
+        return chosen
+
     def step(self) -> None:
-        """One scheduling iteration: admit, launch one chunk per request, retire."""
+        """One scheduling iteration: admit, launch one chunk for each selected
+        request, retire."""
         self._admit()
+        chosen = set(id(r) for r in self._select())
         for name, sc in self.scenes.items():
-            reqs = [r for r in self.active if r.scene == name]
+            reqs = [r for r in self.active if r.scene == name and id(r) in chosen]
             if not reqs:
                 continue
             with torch.cuda.stream(self.streams[name]):
