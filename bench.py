@@ -429,11 +429,14 @@ def run_views(a):
     scene.shapes[0].translation = torch.zeros(3)
     scene.configure()
     units = sum(c.width * c.height * s for c, s in zip(cams, spps)) * len(terms)
-    # autotuned launch shapes
-    ln_f = autotune.tune_forward(vs, opts)
-    ln_g = {t: autotune.tune(vs, t, opts) for t in terms}
+    # launch shapes: the library defaults and the per-integrator autotuned
+    # ones; the whole captured step is timed with both and the faster is kept
+    shapes = {"default": (None, {t: None for t in terms}),
+              "autotuned": (autotune.tune_forward(vs, opts, reps=2),
+                            {t: autotune.tune(vs, t, opts, reps=2) for t in terms})}
     img = torch.empty(vs.npix, 3, device=scene.device)
     dLdI = torch.empty(vs.npix, 3, device=scene.device)
+    ln_f, ln_g = shapes["default"]
 
     def batched_step():
         vs.render(api.TRN_PATH_TRACER, opts, launch=ln_f, out=img)
@@ -462,16 +465,20 @@ def run_views(a):
         batched_step()
         plain_step()
     torch.cuda.synchronize()
-    graph = torch.cuda.CUDAGraph()
-    s = torch.cuda.Stream()
-    s.wait_stream(torch.cuda.current_stream())
-    with torch.cuda.stream(s):
-        batched_step()
-    torch.cuda.current_stream().wait_stream(s)
-    torch.cuda.synchronize()
-    with torch.cuda.graph(graph):
-        out_loss, out_grad = batched_step()
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=scene.device)
+    graphs = {}
+    for name, (lf, lg) in shapes.items():
+        ln_f, ln_g = lf, lg
+        graph = torch.cuda.CUDAGraph()
+        s = torch.cuda.Stream()
+        s.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(s):
+            batched_step()
+        torch.cuda.current_stream().wait_stream(s)
+        torch.cuda.synchronize()
+        with torch.cuda.graph(graph):
+            out_loss, out_grad = batched_step()
+        graphs[name] = (graph, out_loss, out_grad)
 
     def timed(fn):
         tot = 0.0
@@ -486,9 +493,15 @@ def run_views(a):
             tot += e0.elapsed_time(e1)
         return tot / a.steps
 
-    for _ in range(a.warmup):
-        graph.replay()
-    ms_batched = timed(graph.replay)
+    shape_ms = {}
+    for name, (graph, _, _) in graphs.items():
+        for _ in range(a.warmup):
+            graph.replay()
+        shape_ms[name] = timed(graph.replay)
+    best = min(shape_ms, key=shape_ms.get)
+    graph, out_loss, out_grad = graphs[best]
+    ln_f, ln_g = shapes[best]
+    ms_batched = shape_ms[best]
     ms_plain = timed(plain_step)
     # the graph-captured step computes what the eager batched step computes
     graph.replay()
@@ -506,8 +519,10 @@ def run_views(a):
             "plain_per_view": {"value": units / (ms_plain / 1e3), "ms_per_step": ms_plain},
             "batched_over_plain": ms_plain / ms_batched,
             "graph_vs_eager_grad_rel_l2": rel,
-            "launch": {"fwd": [ln_f.block, ln_f.blocks_per_sm, ln_f.chunk],
-                       **{str(t): [ln_g[t].block, ln_g[t].blocks_per_sm, ln_g[t].chunk] for t in terms}}}
+            "launch": {"shape": best, "ms_by_shape": shape_ms,
+                       "fwd": [ln_f.block, ln_f.blocks_per_sm, ln_f.chunk] if ln_f else "default",
+                       **{str(t): ([ln_g[t].block, ln_g[t].blocks_per_sm, ln_g[t].chunk] if ln_g[t] else "default")
+                          for t in terms}}}
     print(json.dumps(line), flush=True)
 
 
@@ -541,6 +556,32 @@ def run_inverse(a):
     losses = []
     for _ in range(a.warmup):
         losses.append(float(inv.step().sum()))
+    # one probe step per BVH policy (refit of the first topology vs rebuild),
+    # timed per phase; the timed steps use the refit the workload names
+    probe = {}
+    for policy in ("refit", "rebuild"):
+        inv.refit = policy == "refit"
+        ph = {}
+        losses.append(float(inv.step(phases=ph).sum()))
+        probe[policy] = {k: round(v, 2) for k, v in inverse.phase_ms(ph).items()}
+    inv.refit = True
+    # work counters of one step per integrator (ray queries, shading vertices)
+    import ctypes as C
+    lib = scene._lib
+    buf = (C.c_ulonglong * 16)()
+    lib.trn_stats_enable(scene.handle, 1)
+    st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    lib.trn_stats_read(scene.handle, buf, 1, st)
+    work = {}
+    inv.views.render(api.TRN_PATH_TRACER, inv.options, out=inv.image)
+    lib.trn_stats_read(scene.handle, buf, 1, st)
+    work["forward"] = dict(zip(CNT_NAMES, list(buf)[:10]))
+    for i in inv.integrators:
+        inv.views.render_grad(i, inv.options, inv.dLdI)
+        lib.trn_stats_read(scene.handle, buf, 1, st)
+        work[f"grad_{i}"] = dict(zip(CNT_NAMES, list(buf)[:10]))
+    lib.trn_stats_enable(scene.handle, 0)
+    scene.clear_grads()
     torch.cuda.synchronize()
     clk = Clocks(torch.cuda.current_device())
     clk.start()
@@ -565,7 +606,7 @@ def run_inverse(a):
                                    "LBVH refit per step; inputs larger than L2",
                        "samples_per_step": units},
             "loss": {"first": losses[0], "last": losses[-1], "per_step": losses},
-            "clocks": clocks}
+            "phases_ms": probe, "work": work, "clocks": clocks}
     print(json.dumps(line), flush=True)
 
 

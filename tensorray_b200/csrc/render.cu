@@ -435,6 +435,10 @@ TRN_D bool radiance_step_k(const DeviceScene& s, SurfF& x, F3& rdir, F3& T, floa
 #ifndef TRN_COMPACT
 #define TRN_COMPACT 1
 #endif
+// lanes that must hold a valid sample before the warp runs the body
+#ifndef TRN_COMPACT_MIN
+#define TRN_COMPACT_MIN 28
+#endif
 
 template <class State, class Setup, class Body>
 TRN_D void for_each_valid(const Params& P, Setup&& setup, Body&& body) {
@@ -454,6 +458,9 @@ TRN_D void for_each_valid(const Params& P, Setup&& setup, Body&& body) {
     for (;;) {
       const unsigned need = __ballot_sync(0xffffffffu, !have && !done);
       if (!need) break;
+      // enough lanes are ready: run the body now rather than spend more
+      // nearly-empty set-up rounds on the last rejections
+      if (__popc(__ballot_sync(0xffffffffu, have)) >= TRN_COMPACT_MIN) break;
       const int leader = __ffs(need) - 1;
       unsigned long long base = 0;
       if (lane == leader) base = atomicAdd(P.work, (unsigned long long)__popc(need));

@@ -50,23 +50,42 @@ class InverseRenderer:
         n = sum(c.width * c.height * s for c, s in zip(self.views.cameras, self.views.spps))
         return n * len(self.integrators)
 
-    def step(self) -> torch.Tensor:
+    def step(self, phases: dict | None = None) -> torch.Tensor:
         """One optimisation step; returns the per-view losses (device tensor)
-        of the parameters before the update."""
+        of the parameters before the update. With `phases` (a dict), CUDA
+        events around each phase are stored there under its name."""
+        def mark(name):
+            if phases is not None:
+                ev = torch.cuda.Event(enable_timing=True)
+                ev.record()
+                phases.setdefault("_order", []).append((name, ev))
+
         sc = self.scene
+        mark("start")
         sc.set_vertex_positions(self.x.detach())
         sc.configure(refit=self.refit and self.steps > 0)
+        mark("configure")
         self.options.seed = self.steps
         self.views.render(api.TRN_PATH_TRACER, self.options, launch=self.launch, out=self.image)
+        mark("forward")
         self.loss = self.views.loss(self.image, self.targets, self.dLdI)
         sc.clear_grads()
         for i in self.integrators:
             self.views.render_grad(i, self.options, self.dLdI, launch=self.launch)
+            mark(f"grad_{i}")
         g = sc.get_grads()["positions"]
         self.x.grad = torch.nan_to_num(g, nan=0.0, posinf=0.0, neginf=0.0)
         self.opt.step()
+        mark("update")
         self.steps += 1
         return self.loss
+
+
+def phase_ms(phases: dict) -> dict:
+    """Milliseconds between consecutive marks recorded by step(phases=...)."""
+    torch.cuda.synchronize()
+    order = phases.get("_order", [])
+    return {name: order[i - 1][1].elapsed_time(ev) for i, (name, ev) in enumerate(order) if i > 0}
 
 
 def render_targets(scene: api.Scene, cameras: list, spps: list, options: api.RenderOptions,
