@@ -393,7 +393,7 @@ def main():
                        "res": a.res, "spp_per_term": a.spp, "depth": D, "triangles": scene.num_triangles,
                        "l2": "flushed between timed steps (256 MB write)", "parallelism": f"seeds x{world}"},
             "e2e": e2e, "gpu_launches": int(launches), "clocks": clk, "roofline": roofline,
-            "kernels": {k: {"ms": v["ms"], "GB/s": v["gbs"]} for k, v in per_kernel_roof.items()},
+            "kernels": {k: {"ms": v["ms"], "GB/s": v["gbs"], "counts": v["counts"]} for k, v in per_kernel_roof.items()},
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
@@ -509,6 +509,29 @@ def run_views(a):
     g_graph = out_grad.clone()
     _, g_eager = batched_step()
     rel = float((g_graph - g_eager).norm() / g_eager.norm().clamp_min(1e-30))
+    # per-integrator split of one eager batched step and one plain step
+    def split(fn_list):
+        out = {}
+        for name, fn in fn_list:
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            out[name] = round(e0.elapsed_time(e1), 2)
+        return out
+    scene.clear_grads()
+    split_b = split([("fwd", lambda: vs.render(api.TRN_PATH_TRACER, opts, launch=ln_f, out=img))] +
+                    [(str(t), (lambda t=t: vs.render_grad(t, opts, dLdI, launch=ln_g[t]))) for t in terms])
+    pimgs = [sv.render(api.TRN_PATH_TRACER, opts) for sv in singles]
+    pd = [torch.empty_like(im) for im in pimgs]
+    for i, sv in enumerate(singles):
+        sv.loss(pimgs[i], tgt_v[i], pd[i])
+    split_p = split([("fwd", lambda: [sv.render(api.TRN_PATH_TRACER, opts) for sv in singles])] +
+                    [(str(t), (lambda t=t: [sv.render_grad(t, opts, pd[i]) for i, sv in enumerate(singles)]))
+                     for t in terms])
+    scene.clear_grads()
     line = {"metric": "grad path-samples/sec", "value": units / (ms_batched / 1e3), "unit": "grad path-samples/s",
             "n_gpus": 1, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_batched, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
@@ -519,6 +542,7 @@ def run_views(a):
             "plain_per_view": {"value": units / (ms_plain / 1e3), "ms_per_step": ms_plain},
             "batched_over_plain": ms_plain / ms_batched,
             "graph_vs_eager_grad_rel_l2": rel,
+            "split_ms": {"batched": split_b, "plain": split_p},
             "launch": {"shape": best, "ms_by_shape": shape_ms,
                        "fwd": [ln_f.block, ln_f.blocks_per_sm, ln_f.chunk] if ln_f else "default",
                        **{str(t): ([ln_g[t].block, ln_g[t].blocks_per_sm, ln_g[t].chunk] if ln_g[t] else "default")
