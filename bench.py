@@ -524,6 +524,8 @@ def run_views(a):
     scene.clear_grads()
     split_b = split([("fwd", lambda: vs.render(api.TRN_PATH_TRACER, opts, launch=ln_f, out=img))] +
                     [(str(t), (lambda t=t: vs.render_grad(t, opts, dLdI, launch=ln_g[t]))) for t in terms])
+    split_bd = split([("fwd", lambda: vs.render(api.TRN_PATH_TRACER, opts, out=img))] +
+                     [(str(t), (lambda t=t: vs.render_grad(t, opts, dLdI))) for t in terms])
     pimgs = [sv.render(api.TRN_PATH_TRACER, opts) for sv in singles]
     pd = [torch.empty_like(im) for im in pimgs]
     for i, sv in enumerate(singles):
@@ -542,7 +544,7 @@ def run_views(a):
             "plain_per_view": {"value": units / (ms_plain / 1e3), "ms_per_step": ms_plain},
             "batched_over_plain": ms_plain / ms_batched,
             "graph_vs_eager_grad_rel_l2": rel,
-            "split_ms": {"batched": split_b, "plain": split_p},
+            "split_ms": {"batched": split_b, "batched_default_shape": split_bd, "plain": split_p},
             "launch": {"shape": best, "ms_by_shape": shape_ms,
                        "fwd": [ln_f.block, ln_f.blocks_per_sm, ln_f.chunk] if ln_f else "default",
                        **{str(t): ([ln_g[t].block, ln_g[t].blocks_per_sm, ln_g[t].chunk] if ln_g[t] else "default")
