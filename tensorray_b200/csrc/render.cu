@@ -131,12 +131,18 @@ TRN_D F3 g_at(const Params& P, const ViewDesc& V, int pix) {
 }
 
 // the view owning global slot g (last view whose first slot is <= g)
-TRN_D const ViewDesc& view_of(const Params& P, long long g) {
+// View of a launch-global slot. `hint` is the lane's previous view: a lane's
+// consecutive slots nearly always fall in the same view, so the range check
+// usually replaces the binary search over the view table.
+TRN_D const ViewDesc& view_of(const Params& P, long long g, int& hint) {
+  const int h = hint;
+  if (__ldg(P.vbegin + h) <= g && (h + 1 >= P.nviews || g < __ldg(P.vbegin + h + 1))) return P.views[h];
   int lo = 0, hi = P.nviews - 1;
   while (lo < hi) {
     const int mid = (lo + hi + 1) >> 1;
     if (__ldg(P.vbegin + mid) <= g) lo = mid; else hi = mid - 1;
   }
+  hint = lo;
   return P.views[lo];
 }
 
@@ -491,9 +497,10 @@ struct FwdState {
 __global__ void __launch_bounds__(256, TRN_MINB) k_path_fwd(Params P) {
   Cnt cnt;
   stage_top(P.s);
+  int vhint = 0;
   for_each_valid<FwdState>(P,
     [&](long long gslot, FwdState& st) -> bool {
-      const ViewDesc& V = view_of(P, gslot);
+      const ViewDesc& V = view_of(P, gslot, vhint);
       const long long p = gslot - V.begin;
       const CameraDesc& cam = V.cam;
       const PathSmp S{&P, V.seed, gslot, p + V.slot_off};
@@ -736,9 +743,10 @@ __global__ void __launch_bounds__(256, TRN_MINB_PATHADJ) k_path_adj(Params P) {
   const DeviceScene& s = P.s;
   Cnt cnt;
   stage_top(P.s);
+  int vhint = 0;
   for_each_valid<AdjState>(P,
     [&](long long gslot, AdjState& st) -> bool {
-      const ViewDesc& V = view_of(P, gslot);
+      const ViewDesc& V = view_of(P, gslot, vhint);
       const long long p = gslot - V.begin;
       const CameraDesc& cam = V.cam;
       const PathSmp S{&P, V.seed, gslot, p + V.slot_off};
@@ -1038,9 +1046,10 @@ __global__ void __launch_bounds__(256, TRN_MINB) k_primary_adj(Params P) {
   const DeviceScene& s = P.s;
   Cnt cnt;
   stage_top(P.s);
+  int vhint = 0;
   for_each_valid<EdgeState>(P,
     [&](long long gslot, EdgeState& st) -> bool {
-      const ViewDesc& V = view_of(P, gslot);
+      const ViewDesc& V = view_of(P, gslot, vhint);
       const long long p = gslot - V.begin;
       const CameraDesc& cam = V.cam;
       const PathSmp S{&P, V.seed, gslot, p + V.slot_off};
@@ -1114,9 +1123,10 @@ __global__ void __launch_bounds__(256, TRN_MINB) k_direct_adj(Params P) {
   const DeviceScene& s = P.s;
   Cnt cnt;
   stage_top(P.s);
+  int vhint = 0;
   for_each_valid<EdgeState>(P,
     [&](long long gslot, EdgeState& st) -> bool {
-      const ViewDesc& V = view_of(P, gslot);
+      const ViewDesc& V = view_of(P, gslot, vhint);
       const long long p = gslot - V.begin;
       const PathSmp S{&P, V.seed, gslot, p + V.slot_off};
       float r0 = S(0);
@@ -1315,9 +1325,10 @@ __global__ void __launch_bounds__(256, TRN_MINB_INDIRECT) k_indirect_adj(Params 
   const DeviceScene& s = P.s;
   Cnt cnt;
   stage_top(P.s);
+  int vhint = 0;
   for_each_valid<EdgeState>(P,
     [&](long long gslot, EdgeState& st) -> bool {
-      const ViewDesc& V = view_of(P, gslot);
+      const ViewDesc& V = view_of(P, gslot, vhint);
       const long long p = gslot - V.begin;
       if (V.D < 2) return false;
       const PathSmp S{&P, V.seed, gslot, p + V.slot_off};
@@ -1442,9 +1453,10 @@ __global__ void __launch_bounds__(256, TRN_MINB) k_pixel_adj(Params P) {
   const DeviceScene& s = P.s;
   Cnt cnt;
   stage_top(P.s);
+  int vhint = 0;
   for_each_valid<EdgeState>(P,
     [&](long long gslot, EdgeState& st) -> bool {
-      const ViewDesc& V = view_of(P, gslot);
+      const ViewDesc& V = view_of(P, gslot, vhint);
       const long long p = gslot - V.begin;
       const CameraDesc& cam = V.cam;
       const int W_ = cam.w, WH = cam.w * cam.h;

@@ -172,6 +172,9 @@ __device__ __forceinline__ unsigned int expand_bits(unsigned int v) {
   return v;
 }
 
+#ifndef TRN_LARGE_SPLIT
+#define TRN_LARGE_SPLIT 1
+#endif
 __global__ void k_morton(int nt, const float* pos, const int* idx, const unsigned int* b,
                          unsigned long long* keys) {
   int f = blockIdx.x * blockDim.x + threadIdx.x;
@@ -187,7 +190,19 @@ __global__ void k_morton(int nt, const float* pos, const int* idx, const unsigne
     x = fminf(fmaxf(x * 1024.f, 0.f), 1023.f);
     m[k] = expand_bits((unsigned int)x);
   }
-  const unsigned int code = (m[0] << 2) | (m[1] << 1) | m[2];
+  unsigned int code = (m[0] << 2) | (m[1] << 1) | m[2];
+  // Oversized triangles (box diagonal above 1/16 of the scene's, e.g. a ground
+  // plane) get a code above the 30-bit Morton range: they sort last and the
+  // root split puts them in their own subtree instead of inflating the boxes
+  // of every ancestor among the small triangles near their centroids.
+  float sd2 = 0.f, td2 = 0.f;
+  for (int k = 0; k < 3; k++) {
+    const float e = unordered(b[3 + k]) - unordered(b[k]);
+    const float t = fmaxf(fmaxf(p0[k], p1[k]), p2[k]) - fminf(fminf(p0[k], p1[k]), p2[k]);
+    sd2 += e * e;
+    td2 += t * t;
+  }
+  if (TRN_LARGE_SPLIT && td2 * 256.f > sd2) code = 1u << 30;
   keys[f] = ((unsigned long long)code << 32) | (unsigned int)f;
 }
 
