@@ -243,6 +243,104 @@ __global__ void k_karras(int n, const unsigned long long* keys, BvhNode* nodes, 
   if (i == 0) parent[0] = -1;
 }
 
+// ---------------------------------------------------------------------------
+// PLOC build (Meister and Bittner 2018, "Parallel Locally-Ordered Clustering
+// for Bounding Volume Construction"): clusters start as the Morton-ordered
+// leaves; each round every cluster finds, within +-kPlocR positions, the
+// neighbour whose union box has the smallest surface area, mutual nearest
+// neighbours merge into a new internal node, and the survivors are compacted
+// in order. The output has the LBVH's layout (internal nodes [0, T-1) with the
+// root at 0, parent links for k_refit), so traversal and refit are unchanged.
+// ---------------------------------------------------------------------------
+#ifndef TRN_PLOC
+#define TRN_PLOC 1
+#endif
+constexpr int kPlocR = 16;
+constexpr int kPlocBlock = 256;
+
+__global__ void k_ploc_init(int n, const unsigned long long* keys, const float* pos, const int* idx, int* cnode,
+                            float* cbox) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int f = (int)(keys[i] & 0xffffffffull);
+  const F3 p0 = make_f3(pos + 3 * idx[3 * f]), p1 = make_f3(pos + 3 * idx[3 * f + 1]),
+           p2 = make_f3(pos + 3 * idx[3 * f + 2]);
+  for (int k = 0; k < 3; k++) {
+    cbox[6 * i + k] = fminf(fminf(p0[k], p1[k]), p2[k]);
+    cbox[6 * i + 3 + k] = fmaxf(fmaxf(p0[k], p1[k]), p2[k]);
+  }
+  cnode[i] = ~i;
+}
+
+__device__ __forceinline__ float union_area(const float* a, const float* b) {
+  const float dx = fmaxf(a[3], b[3]) - fminf(a[0], b[0]);
+  const float dy = fmaxf(a[4], b[4]) - fminf(a[1], b[1]);
+  const float dz = fmaxf(a[5], b[5]) - fminf(a[2], b[2]);
+  return dx * dy + dy * dz + dz * dx;
+}
+
+// Nearest neighbour in the window; ties go to the smaller index, which keeps
+// at least one mutual pair (the smallest index among the closest pairs).
+__global__ void k_ploc_nn(int n, const float* cbox, int* nn) {
+  __shared__ float sb[(kPlocBlock + 2 * kPlocR) * 6];
+  const int start = blockIdx.x * kPlocBlock - kPlocR;
+  for (int t = threadIdx.x; t < (kPlocBlock + 2 * kPlocR) * 6; t += blockDim.x) {
+    const int c = start + t / 6;
+    sb[t] = (c >= 0 && c < n) ? cbox[(size_t)6 * c + t % 6] : 0.f;
+  }
+  __syncthreads();
+  const int i = blockIdx.x * kPlocBlock + threadIdx.x;
+  if (i >= n) return;
+  const float* bi = sb + 6 * (threadIdx.x + kPlocR);
+  float best = 3.402823466e+38f;
+  int bj = -1;
+  const int j0 = max(0, i - kPlocR), j1 = min(n - 1, i + kPlocR);
+  for (int j = j0; j <= j1; j++) {
+    if (j == i) continue;
+    const float a = union_area(bi, sb + 6 * (j - start));
+    if (a < best) { best = a; bj = j; }
+  }
+  nn[i] = bj;
+}
+
+__global__ void k_ploc_merge(int nleaf, int n, const int* nn, const int* cnode, const float* cbox, int* onode,
+                             float* obox, int* flag, BvhNode* nodes, int* parent, int* counter) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int j = nn[i];
+  const float* bi = cbox + (size_t)6 * i;
+  if (j >= 0 && nn[j] == i) {
+    if (i > j) { flag[i] = 0; return; }
+    const int id = nleaf - 2 - atomicAdd(counter, 1);
+    const int a = cnode[i], b = cnode[j];
+    nodes[id].d = make_int4(a, b, 0, 0);
+    parent[a < 0 ? nleaf - 1 + ~a : a] = id;
+    parent[b < 0 ? nleaf - 1 + ~b : b] = id;
+    const float* bj = cbox + (size_t)6 * j;
+    for (int k = 0; k < 3; k++) {
+      obox[6 * i + k] = fminf(bi[k], bj[k]);
+      obox[6 * i + 3 + k] = fmaxf(bi[3 + k], bj[3 + k]);
+    }
+    onode[i] = id;
+  } else {
+    for (int k = 0; k < 6; k++) obox[6 * i + k] = bi[k];
+    onode[i] = cnode[i];
+  }
+  flag[i] = 1;
+}
+
+__global__ void k_ploc_compact(int n, const int* flag, const int* pos, const int* onode, const float* obox,
+                               int* cnode, float* cbox, int* count) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (flag[i]) {
+    const int d = pos[i];
+    cnode[d] = onode[i];
+    for (int k = 0; k < 6; k++) cbox[6 * d + k] = obox[6 * i + k];
+  }
+  if (i == n - 1) count[1] = pos[i] + flag[i];
+}
+
 __device__ __forceinline__ void write_child_box(BvhNode* nd, int side, const float lo[3], const float hi[3]) {
   float* a = reinterpret_cast<float*>(nd);
   if (side == 0) {
@@ -782,6 +880,21 @@ int trn_scene_create(const trn_scene_desc* d, trn_scene** out) {
   cub::DeviceRadixSort::SortKeys(nullptr, bytes, s->keys, s->keys_alt, nt);
   s->sort_tmp_bytes = bytes;
   if (cudaMalloc(&s->sort_tmp, bytes) != cudaSuccess) { set_error("trn_scene_create: out of memory"); return fail(); }
+  if (TRN_PLOC) {
+    size_t sb = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, sb, s->ploc_flag, s->ploc_pos, nt);
+    s->scan_tmp_bytes = sb;
+    if (dev_alloc_copy(&s->ploc_node, (const int*)nullptr, 2 * (size_t)nt) ||
+        dev_alloc_copy(&s->ploc_box, (const float*)nullptr, 12 * (size_t)nt) ||
+        dev_alloc_copy(&s->ploc_nn, (const int*)nullptr, (size_t)nt) ||
+        dev_alloc_copy(&s->ploc_flag, (const int*)nullptr, (size_t)nt) ||
+        dev_alloc_copy(&s->ploc_pos, (const int*)nullptr, (size_t)nt) ||
+        dev_alloc_copy(&s->ploc_count, (const int*)nullptr, 2) ||
+        cudaMalloc(&s->scan_tmp, std::max<size_t>(sb, 16)) != cudaSuccess) {
+      set_error("trn_scene_create: out of memory");
+      return fail();
+    }
+  }
   *out = s;
   return 0;
 }
@@ -797,7 +910,8 @@ int trn_scene_destroy(trn_scene* s) {
                   s->sec_integral_dev, s->nodes, s->tri_verts, s->parent, s->flags, s->keys, s->keys_alt,
                   s->sort_tmp, s->bounds, s->g_pos, s->g_vnormal, s->g_texels, s->g_translation, s->err,
                   s->stats, s->wnodes, s->wtri, s->wqueue, s->wcount, s->aq_poly, s->aq_func, s->aq_cdf,
-                  s->aq_int};
+                  s->aq_int, s->ploc_node, s->ploc_box, s->ploc_nn, s->ploc_flag, s->ploc_pos, s->ploc_count,
+                  s->scan_tmp};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   delete s;
@@ -834,6 +948,43 @@ int configure_geometry(trn_scene* s, cudaStream_t st) {
   }
   return 0;
 }
+// PLOC rounds until one cluster is left; the cluster count is read back once
+// per round (about log-many rounds).
+int ploc_build(trn_scene* s, cudaStream_t st) {
+  const int nt = s->nt;
+  int* cur_node = s->ploc_node;
+  int* tmp_node = s->ploc_node + nt;
+  float* cur_box = s->ploc_box;
+  float* tmp_box = s->ploc_box + 6 * (size_t)nt;
+  TRN_CUDA_TRY(cudaMemsetAsync(s->ploc_count, 0, 2 * sizeof(int), st));
+  k_ploc_init<<<nblk(nt), 256, 0, st>>>(nt, s->keys_alt, s->pos, s->idx, cur_node, cur_box);
+  count_launch(1);
+  int n = nt;
+  for (int round = 0; n > 1; round++) {
+    if (round > 4 * nt) { set_error("trn_scene_configure: PLOC did not converge"); return -1; }
+    k_ploc_nn<<<(n + kPlocBlock - 1) / kPlocBlock, kPlocBlock, 0, st>>>(n, cur_box, s->ploc_nn);
+    k_ploc_merge<<<nblk(n), 256, 0, st>>>(nt, n, s->ploc_nn, cur_node, cur_box, tmp_node, tmp_box, s->ploc_flag,
+                                          s->nodes, s->parent, s->ploc_count);
+    size_t sb = s->scan_tmp_bytes;
+    if (cub::DeviceScan::ExclusiveSum(s->scan_tmp, sb, s->ploc_flag, s->ploc_pos, n, st) != cudaSuccess) {
+      set_error("trn_scene_configure: scan failed");
+      return -1;
+    }
+    k_ploc_compact<<<nblk(n), 256, 0, st>>>(n, s->ploc_flag, s->ploc_pos, tmp_node, tmp_box, cur_node, cur_box,
+                                            s->ploc_count);
+    count_launch(4);
+    int counts[2];
+    TRN_CUDA_TRY(cudaMemcpyAsync(counts, s->ploc_count, sizeof(counts), cudaMemcpyDeviceToHost, st));
+    TRN_CUDA_TRY(cudaStreamSynchronize(st));
+    if (counts[1] >= n) { set_error("trn_scene_configure: PLOC round merged nothing"); return -1; }
+    n = counts[1];
+  }
+  const int root_parent = -1;
+  TRN_CUDA_TRY(cudaMemcpyAsync(s->parent, &root_parent, sizeof(int), cudaMemcpyHostToDevice, st));
+  TRN_CUDA_TRY(cudaStreamSynchronize(st));
+  return 0;
+}
+
 }  // namespace
 
 extern "C" {
@@ -854,8 +1005,12 @@ int trn_scene_configure(trn_scene* s, cudaStream_t st) {
   }
   if (nt > 1) {
     TRN_CUDA_TRY(cudaMemsetAsync(s->flags, 0, sizeof(int) * (nt - 1), st));
-    k_karras<<<nblk(nt - 1), 256, 0, st>>>(nt, s->keys_alt, s->nodes, s->parent);
-    count_launch(1);
+    if (TRN_PLOC) {
+      if (ploc_build(s, st)) return -1;
+    } else {
+      k_karras<<<nblk(nt - 1), 256, 0, st>>>(nt, s->keys_alt, s->nodes, s->parent);
+      count_launch(1);
+    }
   }
   k_refit<<<nblk(nt), 256, 0, st>>>(nt, s->keys_alt, s->pos, s->idx, s->nodes, s->parent, s->flags, s->tri_verts);
   count_launch(1);

@@ -67,6 +67,15 @@ struct trn_scene {
   unsigned long long* keys_alt = nullptr; // [T]
   void* sort_tmp = nullptr;
   size_t sort_tmp_bytes = 0;
+  // PLOC build scratch (cluster node ids and boxes, current + merged copies)
+  int* ploc_node = nullptr;       // [2][T]
+  float* ploc_box = nullptr;      // [2][T][6]
+  int* ploc_nn = nullptr;         // [T]
+  int* ploc_flag = nullptr;       // [T]
+  int* ploc_pos = nullptr;        // [T]
+  int* ploc_count = nullptr;      // [2] merge counter, cluster count
+  void* scan_tmp = nullptr;
+  size_t scan_tmp_bytes = 0;
   float* bounds = nullptr;        // [6]
   trn::WNode* wnodes = nullptr;   // [<= T] 8-wide nodes
   float4* wtri = nullptr;         // [T][3]
