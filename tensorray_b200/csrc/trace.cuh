@@ -230,6 +230,10 @@ __device__ __noinline__ bool trace_wide(const DeviceScene& s, const RayPre& r, f
 }
 
 // Closest hit (ANY == false) or occlusion (ANY == true). Returns true on hit.
+#ifndef TRN_ONE_LEAF_SITE
+#define TRN_ONE_LEAF_SITE 1
+#endif
+
 template <bool ANY>
 TRN_D bool trace(const DeviceScene& s, const F3& o, const F3& d, float tmin, float tmax, Hit& hit,
                  int* err = nullptr) {
@@ -254,6 +258,40 @@ TRN_D bool trace(const DeviceScene& s, const F3& o, const F3& d, float tmin, flo
   };
   if (s.root_is_leaf) {
     if (test_leaf(0)) return true;
+  } else if (TRN_ONE_LEAF_SITE) {
+    // leaves are visited through the loop like inner nodes, so the triangle
+    // test is instantiated once per traversal (smaller code)
+    int stack[kStackSize];
+    int sp = 0;
+    int cur = 0;
+    for (;;) {
+      if (cur < 0) {
+        if (test_leaf(~cur)) return true;
+        if (sp == 0) break;
+        cur = stack[--sp];
+        continue;
+      }
+      const BvhNode* n = &s.nodes[cur];
+      const float4 a = __ldg(&n->a), b = __ldg(&n->b), c = __ldg(&n->c);
+      const int4 dd = __ldg(&n->d);
+      float tn0, tn1;
+      const bool h0 = slab(r, a.x, a.y, a.z, a.w, b.x, b.y, tmin, best_t, tn0);
+      const bool h1 = slab(r, b.z, b.w, c.x, c.y, c.z, c.w, tmin, best_t, tn1);
+      if (h0 && h1) {
+        int nearc = dd.x, farc = dd.y;
+        if (tn1 < tn0) { nearc = dd.y; farc = dd.x; }
+        if (sp < kStackSize) stack[sp++] = farc;
+        else if (err) atomicExch(err, 1);
+        cur = nearc;
+      } else if (h0) {
+        cur = dd.x;
+      } else if (h1) {
+        cur = dd.y;
+      } else {
+        if (sp == 0) break;
+        cur = stack[--sp];
+      }
+    }
   } else {
     int stack[kStackSize];
     int sp = 0;
