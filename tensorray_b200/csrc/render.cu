@@ -654,7 +654,7 @@ TRN_HD void tangent_vjp(const F3& n, const F3& g_t, F3& g_n) {
 #else
 #define TRN_FACTOR_FN TRN_HD
 #endif
-TRN_FACTOR_FN void factor_vjp(const BsdfDesc& b, bool need_prev, bool need_kd, const F3& xprev, const F3& x, const F3& ns,
+TRN_FACTOR_FN F3 factor_vjp(const BsdfDesc& b, bool need_prev, bool need_kd, const F3& xprev, const F3& x, const F3& ns,
                       const F3& kd, const F3& z, const F3& nz, float J, const F3& K, const F3& adj, F3& g_prev,
                       F3& g_x, F3& g_ns, F3& g_kd, F3& g_z, F3& g_nz, float& g_J) {
   const F3 v0 = x - xprev;
@@ -674,11 +674,12 @@ TRN_FACTOR_FN void factor_vjp(const BsdfDesc& b, bool need_prev, bool need_kd, c
   // B(kd, lo, li) with its adjoint gB = A Q
   F3 g_lo = F3z(), g_li = F3z(), gkd = F3z();
   const F3 B = eval_inner_vjp(b, kd, lo, li, A * Q, g_lo, g_li, gkd);
+  const F3 F(B.x * Q * K.x, B.y * Q * K.y, B.z * Q * K.z);
   if (need_kd) g_kd = g_kd + gkd;
   const float gQ = dot(A, B);
   if (gQ == 0.f && g_lo.x == 0.f && g_lo.y == 0.f && g_lo.z == 0.f && g_li.x == 0.f && g_li.y == 0.f &&
       g_li.z == 0.f)
-    return;
+    return F;
   // Q = |cs| |u| / d2 J
   const float g_cs = gQ * (cs > 0.f ? 1.f : -1.f) * fabsf(u) / d2 * J;
   const float g_u = gQ * fabsf(cs) * (u > 0.f ? 1.f : -1.f) / d2 * J;
@@ -707,25 +708,29 @@ TRN_FACTOR_FN void factor_vjp(const BsdfDesc& b, bool need_prev, bool need_kd, c
   const F3 g_v0 = (g_n0 - n0 * dot(g_n0, n0)) / L0;
   g_x = g_x + g_v0;
   if (need_prev) g_prev = g_prev - g_v0;
+  return F;
 }
 
 // Gradient of the NEE factor w.r.t. (xprev, x, ns, kd, y, nl, Jl).
-TRN_HD void nee_vjp(const BsdfDesc& b, bool need_prev, bool need_kd, const F3& xprev, const F3& x, const F3& ns,
-                   const F3& ng, const F3& kd, const F3& y, const F3& nl, const F3& Le, float lpdf, float mis,
-                   const F3& adj, F3& g_prev, F3& g_x, F3& g_ns, F3& g_kd, F3& g_y, F3& g_nl, float& g_Jl) {
+// Returns the factor's value.
+TRN_HD F3 nee_vjp(const BsdfDesc& b, bool need_prev, bool need_kd, const F3& xprev, const F3& x, const F3& ns,
+                  const F3& ng, const F3& kd, const F3& y, const F3& nl, const F3& Le, float lpdf, float mis,
+                  const F3& adj, F3& g_prev, F3& g_x, F3& g_ns, F3& g_kd, F3& g_y, F3& g_nl, float& g_Jl) {
   (void)ng;  // the factor evaluates the BSDF without the shading-normal correction
   const F3 K(Le.x / lpdf * mis, Le.y / lpdf * mis, Le.z / lpdf * mis);
-  factor_vjp(b, need_prev, need_kd, xprev, x, ns, kd, y, nl, 1.f, K, adj, g_prev, g_x, g_ns, g_kd, g_y, g_nl, g_Jl);
+  return factor_vjp(b, need_prev, need_kd, xprev, x, ns, kd, y, nl, 1.f, K, adj, g_prev, g_x, g_ns, g_kd, g_y, g_nl,
+                    g_Jl);
 }
 
 // Gradient of the continuation factor w.r.t. (xprev, x, ns, kd, xn, ngn, Jn).
-TRN_HD void cont_vjp(const BsdfDesc& b, bool need_prev, bool need_kd, const F3& xprev, const F3& x, const F3& ns,
-                    const F3& ng, const F3& kd, const F3& xn, const F3& ngn, float prev_pdf, const F3& adj,
-                    F3& g_prev, F3& g_x, F3& g_ns, F3& g_kd, F3& g_xn, F3& g_ngn, float& g_Jn) {
+// Returns the factor's value.
+TRN_HD F3 cont_vjp(const BsdfDesc& b, bool need_prev, bool need_kd, const F3& xprev, const F3& x, const F3& ns,
+                   const F3& ng, const F3& kd, const F3& xn, const F3& ngn, float prev_pdf, const F3& adj,
+                   F3& g_prev, F3& g_x, F3& g_ns, F3& g_kd, F3& g_xn, F3& g_ngn, float& g_Jn) {
   (void)ng;
   const float ip = 1.f / prev_pdf;
-  factor_vjp(b, need_prev, need_kd, xprev, x, ns, kd, xn, ngn, 1.f, F3(ip, ip, ip), adj, g_prev, g_x, g_ns, g_kd,
-             g_xn, g_ngn, g_Jn);
+  return factor_vjp(b, need_prev, need_kd, xprev, x, ns, kd, xn, ngn, 1.f, F3(ip, ip, ip), adj, g_prev, g_x, g_ns,
+                    g_kd, g_xn, g_ngn, g_Jn);
 }
 
 struct VRec { int tri; float u, v; };
@@ -820,38 +825,36 @@ __global__ void __launch_bounds__(256, TRN_MINB_PATHADJ) k_path_adj(Params P) {
       const BsdfDesc b = s.bsdfs[Gk.bsdf];
       const bool need_prev = b.type != kDiffuse;
       const bool need_kd = P.diff_tex && Gk.texel >= 0;
-      F3 Nval = F3z(), Phi = F3z(), y = F3z(), nl = F3z();
-      const bool nee = k <= D && nee_on[k];
-      if (nee) {
+      F3 Nval = F3z(), Phi = F3z();
+      F3 gkd = F3z(), gprev = F3z();
+      if (k <= D && nee_on[k]) {
+        // NEE factor value and its reverse mode in one sweep
         const BounceRec& R = br[k];
         int j0, j1, j2; tri_vertices(s, R.ltri, j0, j1, j2);
-        y = bary3(R.lu, R.lv, load3(s.pos, j0), load3(s.pos, j1), load3(s.pos, j2));
-        nl = load3(s.fnormal, R.ltri);
-        Nval = nee_factor<float>(b, Gp.p, Gk.p, Gk.ns, Gk.ng, Gk.kd, y, nl, 1.f, R.lLe, R.lpdf, R.lmis);
-      }
-      if (k < K) {
-        Phi = cont_factor<float>(b, Gp.p, Gk.p, Gk.ns, Gk.ng, Gk.kd, Gn.p, Gn.ng, 1.f, br[k].prev_pdf);
-        // a non-finite weight made the forward throughput non-finite: no gradient
-        if (!finite3(Phi)) Phi = F3z();
-      }
-      const F3 a_k = g * (Nval + Mk[k]) + Phi * a_next;
-      F3 gkd = F3z(), gprev = F3z();
-      if (nee) {
-        const F3 adj = Tk[k] * g;
+        const F3 y = bary3(R.lu, R.lv, load3(s.pos, j0), load3(s.pos, j1), load3(s.pos, j2));
+        const F3 nl = load3(s.fnormal, R.ltri);
         F3 gy = F3z(), gnl = F3z();
         float gJl = 0.f;
-        nee_vjp(b, need_prev, need_kd, Gp.p, Gk.p, Gk.ns, Gk.ng, Gk.kd, y, nl, br[k].lLe, br[k].lpdf, br[k].lmis, adj,
-                gprev, acc_k.p, acc_k.ns, gkd, gy, gnl, gJl);
+        Nval = nee_vjp(b, need_prev, need_kd, Gp.p, Gk.p, Gk.ns, Gk.ng, Gk.kd, y, nl, R.lLe, R.lpdf, R.lmis,
+                       Tk[k] * g, gprev, acc_k.p, acc_k.ns, gkd, gy, gnl, gJl);
         VAdj la; la.p = gy; la.ns = F3z(); la.ng = gnl; la.J = gJl;
-        scatter_vertex(P, V, br[k].ltri, br[k].lu, br[k].lv, la, cnt);
+        scatter_vertex(P, V, R.ltri, R.lu, R.lv, la, cnt);
       }
-      if (k < K && (Phi.x != 0.f || Phi.y != 0.f || Phi.z != 0.f)) {
-        const F3 adj = Tk[k] * a_next;
+      if (k < K) {
+        // continuation factor value and its reverse mode; a non-finite weight
+        // made the forward throughput non-finite: no value, no gradient
+        F3 cprev = F3z(), cx = F3z(), cns = F3z(), ckd = F3z(), cxn = F3z(), cngn = F3z();
         float gJn = 0.f;
-        cont_vjp(b, need_prev, need_kd, Gp.p, Gk.p, Gk.ns, Gk.ng, Gk.kd, Gn.p, Gn.ng, br[k].prev_pdf, adj, gprev,
-                 acc_k.p, acc_k.ns, gkd, acc_next.p, acc_next.ng, gJn);
-        acc_next.J += gJn;
+        Phi = cont_vjp(b, need_prev, need_kd, Gp.p, Gk.p, Gk.ns, Gk.ng, Gk.kd, Gn.p, Gn.ng, br[k].prev_pdf,
+                       Tk[k] * a_next, cprev, cx, cns, ckd, cxn, cngn, gJn);
+        if (finite3(Phi)) {
+          gprev = gprev + cprev; acc_k.p = acc_k.p + cx; acc_k.ns = acc_k.ns + cns; gkd = gkd + ckd;
+          acc_next.p = acc_next.p + cxn; acc_next.ng = acc_next.ng + cngn; acc_next.J += gJn;
+        } else {
+          Phi = F3z();
+        }
       }
+      const F3 a_k = g * (Nval + Mk[k]) + Phi * a_next;
       if (k >= 2) acc_prev.p = acc_prev.p + gprev;
       if (need_kd) { cnt.v[kCntTScatter]++; agg_add3(V.gtex, Gk.texel, gkd); }
       // vertex k+1 has received all of its contributions
