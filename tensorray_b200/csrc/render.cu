@@ -64,6 +64,10 @@ constexpr int kMaxDepth = 16;
 #ifndef TRN_MINB_INDIRECT
 #define TRN_MINB_INDIRECT 2
 #endif
+// the indirect kernel's two set-up rays use the shared traversal
+#ifndef TRN_INDIRECT_SETUP_SHARED
+#define TRN_INDIRECT_SETUP_SHARED 1
+#endif
 
 // Per-thread work counters behind the roofline's algorithmic-byte model:
 // ray queries, shading vertices, light samples, gradient scatters, pixels.
@@ -1378,8 +1382,8 @@ __global__ void __launch_bounds__(256, TRN_MINB_INDIRECT) k_indirect_adj(Params 
       const float pdf = pdf_e * pdf_d;
       Hit he, hs;
       cnt.v[kCntClosest] += 2;
-      if (!trace_k<true, false>(s, p0, -dir, kShadowEps, kRayMax, he, P.err)) return false;
-      if (!trace_k<true, false>(s, p0, dir, kShadowEps, kRayMax, hs, P.err)) return false;
+      if (!trace_k<TRN_INDIRECT_SETUP_SHARED, false>(s, p0, -dir, kShadowEps, kRayMax, he, P.err)) return false;
+      if (!trace_k<TRN_INDIRECT_SETUP_SHARED, false>(s, p0, dir, kShadowEps, kRayMax, hs, P.err)) return false;
       const SurfF xe = post_intersect(s, he.tri, he.u, he.v);
       const SurfF xs = post_intersect(s, hs.tri, hs.u, hs.v);
       const float dl = length(xe.p - xs.p);
