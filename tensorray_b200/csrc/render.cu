@@ -68,6 +68,22 @@ constexpr int kMaxDepth = 16;
 #ifndef TRN_INDIRECT_SETUP_SHARED
 #define TRN_INDIRECT_SETUP_SHARED 1
 #endif
+// set-up rays of the other kernels: shared or inlined traversal (measured)
+#ifndef TRN_SETUP_SHARED_FWD
+#define TRN_SETUP_SHARED_FWD 0
+#endif
+#ifndef TRN_SETUP_SHARED_PATHADJ
+#define TRN_SETUP_SHARED_PATHADJ 0
+#endif
+#ifndef TRN_SETUP_SHARED_PRIMARY
+#define TRN_SETUP_SHARED_PRIMARY 0
+#endif
+#ifndef TRN_SETUP_SHARED_DIRECT
+#define TRN_SETUP_SHARED_DIRECT 0
+#endif
+#ifndef TRN_SETUP_SHARED_PIXEL
+#define TRN_SETUP_SHARED_PIXEL 1
+#endif
 
 // Per-thread work counters behind the roofline's algorithmic-byte model:
 // ray queries, shading vertices, light samples, gradient scatters, pixels.
@@ -514,7 +530,7 @@ __global__ void __launch_bounds__(256, TRN_MINB) k_path_fwd(Params P) {
       const F3 dir = camera_ray_dir(cam, pix % W, pix / W, S(0), S(1));
       Hit h;
       cnt.v[kCntClosest]++;
-      if (!trace<false>(P.s, org, dir, kShadowEps, kRayMax, h, P.err)) return false;
+      if (!trace_k<TRN_SETUP_SHARED_FWD, false>(P.s, org, dir, kShadowEps, kRayMax, h, P.err)) return false;
       st.V = &V; st.gslot = gslot; st.p = p; st.pix = pix;
       st.x = post_intersect(P.s, h.tri, h.u, h.v);
       const float t1 = camera_factor<float>(cam, st.x.p, st.x.ng, 1.f);
@@ -716,6 +732,23 @@ TRN_FACTOR_FN F3 factor_vjp(const BsdfDesc& b, bool need_prev, bool need_kd, con
 }
 
 // Gradient of the NEE factor w.r.t. (xprev, x, ns, kd, y, nl, Jl).
+// Reverse mode of camera_factor (Camera::EvalFilter, Camera.cpp:279-303) at
+// J = 1: the value G / Detach(G) is 1, so the gradient is W grad(log G) with
+// log G = log|cos_x| - 3 log cos_y - 2 log dist, plus W for J.
+TRN_HD void camera_factor_grad(const CameraDesc& c, const F3& p, const F3& ng, float W, F3& g_p, F3& g_ng,
+                               float& g_J) {
+  const F3 v = p - F3(c.pos[0], c.pos[1], c.pos[2]);
+  const float dist = length(v);
+  const F3 dir = v / dist;
+  const F3 cdir(c.dir[0], c.dir[1], c.dir[2]);
+  const float cosy = dot(dir, cdir);
+  const float cosx = dot(-dir, ng);
+  const F3 g_dir = (-ng) * (W / cosx) - cdir * (3.f * W / cosy);
+  g_p = (g_dir - dir * dot(g_dir, dir)) / dist - dir * (2.f * W / dist);
+  g_ng = (-dir) * (W / cosx);
+  g_J = W;
+}
+
 // Returns the factor's value.
 TRN_HD F3 nee_vjp(const BsdfDesc& b, bool need_prev, bool need_kd, const F3& xprev, const F3& x, const F3& ns,
                   const F3& ng, const F3& kd, const F3& y, const F3& nl, const F3& Le, float lpdf, float mis,
@@ -766,7 +799,7 @@ __global__ void __launch_bounds__(256, TRN_MINB_PATHADJ) k_path_adj(Params P) {
       if (g.x == 0.f && g.y == 0.f && g.z == 0.f) return false;
       const F3 dir = camera_ray_dir(cam, pix % W, pix / W, S(0), S(1));
       cnt.v[kCntClosest]++;
-      if (!trace<false>(s, cam_pos(cam), dir, kShadowEps, kRayMax, st.h, P.err)) return false;
+      if (!trace_k<TRN_SETUP_SHARED_PATHADJ, false>(s, cam_pos(cam), dir, kShadowEps, kRayMax, st.h, P.err)) return false;
       st.V = &V; st.gslot = gslot; st.p = p; st.pix = pix; st.g = g;
       return true;
     },
@@ -870,17 +903,12 @@ __global__ void __launch_bounds__(256, TRN_MINB_PATHADJ) k_path_adj(Params P) {
     {
       const float gam = a_next.x + a_next.y + a_next.z;
       if (gam != 0.f && isfinite(gam)) {
-        #pragma unroll 1  // one copy of the dual-number factor code (instruction cache)
-        for (int grp = 0; grp < 3; grp++) {
-          const V3<D3> dx = seed3<3>(Gn.p, grp == 0 ? 0 : -1);
-          const V3<D3> dn = seed3<3>(Gn.ng, grp == 1 ? 0 : -1);
-          const D3 dJ = seed1<3>(1.f, grp == 2 ? 0 : -1);
-          const D3 r = camera_factor<D3>(cam, dx, dn, dJ);
-          const F3 gg = F3(r.d[0], r.d[1], r.d[2]) * gam;
-          if (grp == 0) acc_next.p = acc_next.p + gg;
-          else if (grp == 1) acc_next.ng = acc_next.ng + gg;
-          else acc_next.J += gg.x;
-        }
+        F3 gp, gn;
+        float gJ;
+        camera_factor_grad(cam, Gn.p, Gn.ng, gam, gp, gn, gJ);
+        acc_next.p = acc_next.p + gp;
+        acc_next.ng = acc_next.ng + gn;
+        acc_next.J += gJ;
       }
     }
     scatter_vertex(P, V, vr[1].tri, vr[1].u, vr[1].v, acc_next, cnt);
@@ -1078,14 +1106,14 @@ __global__ void __launch_bounds__(256, TRN_MINB) k_primary_adj(Params P) {
       const F3 dir = normalize(p0 - cpos);
       Hit h;
       cnt.v[kCntClosest]++;
-      if (!trace<false>(s, p0, dir, kShadowEps, kRayMax, h, P.err)) return false;
+      if (!trace_k<TRN_SETUP_SHARED_PRIMARY, false>(s, p0, dir, kShadowEps, kRayMax, h, P.err)) return false;
       const F3 hitP = p0 + dir * h.t;
       const SensorSample sds = sample_direct(cam, hitP);
       if (!sds.valid) return false;
       const F3 dirc = sensor_ray_dir(cam, sds.qx, sds.qy);
       const float dist2cam = length(p0 - cpos);
       cnt.v[kCntShadow]++;
-      if (occluded(s, cpos, dirc, kShadowEps, dist2cam - kShadowEps)) return false;
+      if (occluded_k<TRN_SETUP_SHARED_PRIMARY>(s, cpos, dirc, kShadowEps, dist2cam - kShadowEps)) return false;
       const SurfF x = post_intersect(s, h.tri, h.u, h.v);
       const float dist = length(x.p - cpos);
       const float dist1 = length(p0 - cpos);
@@ -1185,8 +1213,8 @@ __global__ void __launch_bounds__(256, TRN_MINB) k_direct_adj(Params P) {
       Hit h0, h;
       cnt.v[kCntClosest] += 2;
       cnt.v[kCntLight]++;
-      if (!trace<false>(s, p0, -rdir, kShadowEps, kRayMax, h0, P.err)) return false;
-      if (!trace<false>(s, p0, rdir, kShadowEps, kRayMax, h, P.err)) return false;
+      if (!trace_k<TRN_SETUP_SHARED_DIRECT, false>(s, p0, -rdir, kShadowEps, kRayMax, h0, P.err)) return false;
+      if (!trace_k<TRN_SETUP_SHARED_DIRECT, false>(s, p0, rdir, kShadowEps, kRayMax, h, P.err)) return false;
       const F3 hp = p0 + (-rdir) * h0.t;
       if (!(length(hp - p2) < kShadowEps)) return false;
       const SurfF xl = post_intersect(s, h0.tri, h0.u, h0.v);
@@ -1498,7 +1526,7 @@ __global__ void __launch_bounds__(256, TRN_MINB) k_pixel_adj(Params P) {
       const F3 dir = normalize(p0 - cpos);
       Hit h;
       cnt.v[kCntClosest]++;
-      if (!trace<false>(s, p0, dir, kShadowEps, kRayMax, h, P.err)) return false;
+      if (!trace_k<TRN_SETUP_SHARED_PIXEL, false>(s, p0, dir, kShadowEps, kRayMax, h, P.err)) return false;
       const F3 hitP = p0 + dir * h.t;
       const SensorSample sds = sample_direct(cam, hitP);
       const F3 dirc = sensor_ray_dir(cam, sds.qx, sds.qy);
