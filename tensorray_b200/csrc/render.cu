@@ -48,6 +48,10 @@ struct Params {
   const float* aq_poly;       // [E] leaf weights
   const float* aq_cdf;        // [E] leaf distribution
   const float* aq_int;        // [2] integral, sum of weight x volume
+  // queue of the split indirect boundary term (nullptr = fused kernel)
+  void* queue;
+  unsigned long long* q_count;
+  long long q_cap;
 };
 
 constexpr int kMaxDepth = 16;
@@ -812,7 +816,10 @@ __global__ void __launch_bounds__(256, TRN_MINB_PATHADJ) k_path_adj(Params P) {
     const Hit h = st.h;
     // ---- forward replay, recording vertices and factor values ----
     VRec vr[MAXD + 2];
-    BounceRec br[MAXD + 1];
+    // per bounce: the NEE light sample and the continuation pdf (the light's
+    // radiance is recomputed in the reverse pass from the same values)
+    struct LRec { int ltri; float lu, lv, lpdf, lmis, ppdf; };
+    LRec br[MAXD + 1];
     bool nee_on[MAXD + 2];
     F3 Tk[MAXD + 2], Mk[MAXD + 2];
     SurfF x = post_intersect(s, h.tri, h.u, h.v);
@@ -830,11 +837,12 @@ __global__ void __launch_bounds__(256, TRN_MINB_PATHADJ) k_path_adj(Params P) {
       const int k = b + 1;
       const int o = 2 + 5 * b;
       F3 c;
-      BounceRec& R = br[k];
+      BounceRec R;
       const bool more = radiance_step_k<TRN_SHARED_STEPS_PATHADJ>(s, x, rdir, T, S(o), S(o + 1), S(o + 2),
                                       S(o + 3), S(o + 4), c, &R, cnt);
       // a scrubbed (non-finite) bounce contributes nothing and carries no gradient
       nee_on[k] = R.nee_ok && !R.scrubbed;
+      br[k] = {R.ltri, R.lu, R.lv, R.lpdf, R.lmis, R.prev_pdf};
       if (!more) break;
       vr[k + 1] = {x.tri, x.u, x.v};
       Tk[k + 1] = T;
@@ -866,13 +874,17 @@ __global__ void __launch_bounds__(256, TRN_MINB_PATHADJ) k_path_adj(Params P) {
       F3 gkd = F3z(), gprev = F3z();
       if (k <= D && nee_on[k]) {
         // NEE factor value and its reverse mode in one sweep
-        const BounceRec& R = br[k];
+        const LRec& R = br[k];
         int j0, j1, j2; tri_vertices(s, R.ltri, j0, j1, j2);
         const F3 y = bary3(R.lu, R.lv, load3(s.pos, j0), load3(s.pos, j1), load3(s.pos, j2));
         const F3 nl = load3(s.fnormal, R.ltri);
+        // the forward step's emitter radiance (one-sided, AreaLight::Eval), same arithmetic
+        F3 wl = y - Gk.p;
+        wl = wl / sqrtf(dot(wl, wl));
+        const F3 Le = dot(-wl, nl) > 0.f ? light_radiance(s, s.emitter_id[R.ltri]) : F3z();
         F3 gy = F3z(), gnl = F3z();
         float gJl = 0.f;
-        Nval = nee_vjp(b, need_prev, need_kd, Gp.p, Gk.p, Gk.ns, Gk.ng, Gk.kd, y, nl, R.lLe, R.lpdf, R.lmis,
+        Nval = nee_vjp(b, need_prev, need_kd, Gp.p, Gk.p, Gk.ns, Gk.ng, Gk.kd, y, nl, Le, R.lpdf, R.lmis,
                        Tk[k] * g, gprev, acc_k.p, acc_k.ns, gkd, gy, gnl, gJl);
         VAdj la; la.p = gy; la.ns = F3z(); la.ng = gnl; la.J = gJl;
         scatter_vertex(P, V, R.ltri, R.lu, R.lv, la, cnt);
@@ -882,7 +894,7 @@ __global__ void __launch_bounds__(256, TRN_MINB_PATHADJ) k_path_adj(Params P) {
         // made the forward throughput non-finite: no value, no gradient
         F3 cprev = F3z(), cx = F3z(), cns = F3z(), ckd = F3z(), cxn = F3z(), cngn = F3z();
         float gJn = 0.f;
-        Phi = cont_vjp(b, need_prev, need_kd, Gp.p, Gk.p, Gk.ns, Gk.ng, Gk.kd, Gn.p, Gn.ng, br[k].prev_pdf,
+        Phi = cont_vjp(b, need_prev, need_kd, Gp.p, Gk.p, Gk.ns, Gk.ng, Gk.kd, Gn.p, Gn.ng, br[k].ppdf,
                        Tk[k] * a_next, cprev, cx, cns, ckd, cxn, cngn, gJn);
         if (finite3(Phi)) {
           gprev = gprev + cprev; acc_k.p = acc_k.p + cx; acc_k.ns = acc_k.ns + cns; gkd = gkd + ckd;
@@ -1355,131 +1367,222 @@ __global__ void k_aq_mix(int n, float* poly, const float* ecdf, float eps, float
 // ---------------------------------------------------------------------------
 // indirect boundary (BoundaryIndirect.cpp:38-192, Edge.cpp:146-199)
 // ---------------------------------------------------------------------------
+// Indirect boundary set-up (SampleBoundarySegmentIndirect, Edge.cpp:146-199,
+// BoundaryIndirect.cpp:58-130): edge point, direction in the edge wedge, both
+// rays, boundary geometry. Returns false for a rejected sample.
+TRN_D bool indirect_setup(const Params& P, long long gslot, EdgeState& st, int& vhint, Cnt& cnt) {
+  const DeviceScene& s = P.s;
+  const ViewDesc& V = view_of(P, gslot, vhint);
+  const long long p = gslot - V.begin;
+  if (V.D < 2) return false;
+  const PathSmp S{&P, V.seed, gslot, p + V.slot_off};
+  const float r0 = S(0), r1 = S(1), r2 = S(2);
+  float reuse;
+  const float integral = __ldg(P.eint);
+  if (!(integral > 0.f)) return false;
+  const int e = sample_discrete(P.ecdf, P.ne, r0, reuse);
+  const int v0 = P.edges[5 * e], v1 = P.edges[5 * e + 1], f0 = P.edges[5 * e + 2], f1 = P.edges[5 * e + 3],
+            v2 = P.edges[5 * e + 4];
+  const float len_e = P.efunc[e];
+  if (!(len_e > 0.f)) return false;
+  const float pdf_e = (len_e / (integral * (float)P.ne)) / len_e;
+  const F3 Pa = load3(s.pos, v0), Pb = load3(s.pos, v1), Pc = load3(s.pos, v2);
+  const F3 e1 = Pb - Pa;
+  const F3 p0 = Pa + e1 * reuse;
+  const F3 edge = normalize(e1), edge2 = normalize(Pc - Pa);
+  const F3 n0 = load3(s.fnormal, f0);
+  F3 dir;
+  float pdf_d;
+  if (f1 < 0) {
+    const F3 nrm = cross(n0, edge);
+    F3 tg, bt; coordinate_system(nrm, tg, bt);
+    const float z = fminf(1.f - 2.f * r1, 1.f - kEdgeEps);
+    const float r = sqrtf(fmaxf(0.f, 1.f - z * z));
+    const float phi = 2.f * kPi * r2;
+    dir = tg * (r * cosf(phi)) + bt * (r * sinf(phi)) + nrm * z;
+    pdf_d = 0.25f / kPi;
+  } else {
+    const F3 n1 = load3(s.fnormal, f1);
+    const float phi0 = acosf(dot(n0, n1));
+    pdf_d = 0.25f / phi0;
+    const F3 zz = normalize(n0 + n1);
+    const F3 yy = normalize(cross(n0, zz));
+    const F3 xx = cross(yy, zz);
+    float phi = (r1 - 0.5f) * phi0;
+    phi = fminf(fmaxf(phi, -0.5f * phi0 + kEdgeEps), 0.5f * phi0 - kEdgeEps);
+    const F3 x1 = xx * cosf(phi) + zz * sinf(phi);
+    const bool m0 = r2 > 0.5f;
+    const float bq = 4.f * r2 - (m0 ? 3.f : 1.f);
+    const float aq = sqrtf(1.f - bq * bq) * (1.f - (m0 ? 1.f : 0.f) * 2.f);
+    dir = x1 * aq + yy * bq;
+  }
+  const float pdf = pdf_e * pdf_d;
+  Hit he, hs;
+  cnt.v[kCntClosest] += 2;
+  if (!trace_k<TRN_INDIRECT_SETUP_SHARED, false>(s, p0, -dir, kShadowEps, kRayMax, he, P.err)) return false;
+  if (!trace_k<TRN_INDIRECT_SETUP_SHARED, false>(s, p0, dir, kShadowEps, kRayMax, hs, P.err)) return false;
+  const SurfF xe = post_intersect(s, he.tri, he.u, he.v);
+  const SurfF xs = post_intersect(s, hs.tri, hs.u, hs.v);
+  const float dl = length(xe.p - xs.p);
+  const float cos2 = fabsf(dot(xe.ng, dir));
+  const float its_t = length(xs.p - p0);
+  F3 n;
+  const float bval = base_val(its_t / dl, edge, -dir, xe.ng, edge2, n) * cos2;
+  if (bval == 0.f) return false;
+  st.V = &V; st.gslot = gslot; st.p = p; st.x = xs; st.xe = xe; st.rdir = dir; st.p0 = p0; st.n = n;
+  st.w0 = bval / pdf; st.sedge = reuse; st.v0 = v0; st.v1 = v1; st.far_tri = he.tri;
+  return true;
+}
+
+// Indirect boundary sensor side (BoundaryIndirect.cpp:158-175 pairs sensor
+// depth b with the emitter radiance accumulated over D-1-b bounces): the
+// importance contributions of every depth, weighted by dL/dI of their pixels.
+// Returns the shallowest depth that reached the image with a nonzero weight
+// (D when none did).
+template <int MAXD>
+TRN_D int indirect_sensor(const Params& P, const EdgeState& st, int D, F3* sc, Cnt& cnt) {
+  const DeviceScene& s = P.s;
+  const ViewDesc& V = *st.V;
+  const PathSmp S{&P, V.seed, st.gslot, st.p + V.slot_off};
+  int bmin = D;
+  F3 T(1.f, 1.f, 1.f);
+  F3 rd = st.rdir;
+  SurfF xx = st.x;
+  for (int b = 0; b < D - 1; b++) sc[b] = F3z();
+  for (int b = 0; b < D - 1; b++) {
+    const int o = 3 + 5 * (D - 1) + 3 * b;
+    F3 c; int pix;
+    const bool more = importance_step_shared(s, V.cam, xx, rd, T, S(o), S(o + 1), S(o + 2), c, pix, cnt);
+    if (pix >= 0) {
+      sc[b] = g_at(P, V, pix) * c;
+      if (sc[b].x != 0.f || sc[b].y != 0.f || sc[b].z != 0.f) bmin = min(bmin, b);
+    }
+    if (!more) break;
+  }
+  return bmin;
+}
+
+// Indirect boundary emitter side: the radiance accumulated over j+1 bounces
+// from the emitter-side surface pairs with sensor depth D-2-j; returns the
+// weight W of the xDotN scatter.
+template <int MAXD>
+TRN_D float indirect_emitter(const Params& P, const ViewDesc& V, long long gslot, long long p, const SurfF& xe,
+                             const F3& rdir, float w0, int D, int jmax, const F3* sc, Cnt& cnt) {
+  const DeviceScene& s = P.s;
+  const PathSmp S{&P, V.seed, gslot, p + V.slot_off};
+  float W = 0.f;
+  F3 T(1.f, 1.f, 1.f);
+  F3 rd = -rdir;
+  SurfF xx = xe;
+  F3 cur = F3z();
+  bool alive = true;
+  for (int j = 0; j <= jmax; j++) {
+    if (alive) {
+      const int o = 3 + 5 * j;
+      F3 c;
+      alive = radiance_step_shared(s, xx, rd, T, S(o), S(o + 1), S(o + 2), S(o + 3), S(o + 4), c, nullptr, cnt);
+      cur = cur + c;
+      if (T.x == 0.f && T.y == 0.f && T.z == 0.f) alive = false;
+    }
+    W += dot(sc[D - 2 - j], cur) * w0;
+  }
+  return W;
+}
+
 template <int MAXD>
 __global__ void __launch_bounds__(256, TRN_MINB_INDIRECT) k_indirect_adj(Params P) {
-  const DeviceScene& s = P.s;
   Cnt cnt;
   stage_top(P.s);
   int vhint = 0;
   for_each_valid<EdgeState>(P,
-    [&](long long gslot, EdgeState& st) -> bool {
-      const ViewDesc& V = view_of(P, gslot, vhint);
-      const long long p = gslot - V.begin;
-      if (V.D < 2) return false;
-      const PathSmp S{&P, V.seed, gslot, p + V.slot_off};
-      const float r0 = S(0), r1 = S(1), r2 = S(2);
-      float reuse;
-      const float integral = __ldg(P.eint);
-      if (!(integral > 0.f)) return false;
-      const int e = sample_discrete(P.ecdf, P.ne, r0, reuse);
-      const int v0 = P.edges[5 * e], v1 = P.edges[5 * e + 1], f0 = P.edges[5 * e + 2], f1 = P.edges[5 * e + 3],
-                v2 = P.edges[5 * e + 4];
-      const float len_e = P.efunc[e];
-      if (!(len_e > 0.f)) return false;
-      const float pdf_e = (len_e / (integral * (float)P.ne)) / len_e;
-      const F3 Pa = load3(s.pos, v0), Pb = load3(s.pos, v1), Pc = load3(s.pos, v2);
-      const F3 e1 = Pb - Pa;
-      const F3 p0 = Pa + e1 * reuse;
-      const F3 edge = normalize(e1), edge2 = normalize(Pc - Pa);
-      const F3 n0 = load3(s.fnormal, f0);
-      F3 dir;
-      float pdf_d;
-      if (f1 < 0) {
-        const F3 nrm = cross(n0, edge);
-        F3 tg, bt; coordinate_system(nrm, tg, bt);
-        const float z = fminf(1.f - 2.f * r1, 1.f - kEdgeEps);
-        const float r = sqrtf(fmaxf(0.f, 1.f - z * z));
-        const float phi = 2.f * kPi * r2;
-        dir = tg * (r * cosf(phi)) + bt * (r * sinf(phi)) + nrm * z;
-        pdf_d = 0.25f / kPi;
-      } else {
-        const F3 n1 = load3(s.fnormal, f1);
-        const float phi0 = acosf(dot(n0, n1));
-        pdf_d = 0.25f / phi0;
-        const F3 zz = normalize(n0 + n1);
-        const F3 yy = normalize(cross(n0, zz));
-        const F3 xx = cross(yy, zz);
-        float phi = (r1 - 0.5f) * phi0;
-        phi = fminf(fmaxf(phi, -0.5f * phi0 + kEdgeEps), 0.5f * phi0 - kEdgeEps);
-        const F3 x1 = xx * cosf(phi) + zz * sinf(phi);
-        const bool m0 = r2 > 0.5f;
-        const float bq = 4.f * r2 - (m0 ? 3.f : 1.f);
-        const float aq = sqrtf(1.f - bq * bq) * (1.f - (m0 ? 1.f : 0.f) * 2.f);
-        dir = x1 * aq + yy * bq;
-      }
-      const float pdf = pdf_e * pdf_d;
-      Hit he, hs;
-      cnt.v[kCntClosest] += 2;
-      if (!trace_k<TRN_INDIRECT_SETUP_SHARED, false>(s, p0, -dir, kShadowEps, kRayMax, he, P.err)) return false;
-      if (!trace_k<TRN_INDIRECT_SETUP_SHARED, false>(s, p0, dir, kShadowEps, kRayMax, hs, P.err)) return false;
-      const SurfF xe = post_intersect(s, he.tri, he.u, he.v);
-      const SurfF xs = post_intersect(s, hs.tri, hs.u, hs.v);
-      const float dl = length(xe.p - xs.p);
-      const float cos2 = fabsf(dot(xe.ng, dir));
-      const float its_t = length(xs.p - p0);
-      F3 n;
-      const float bval = base_val(its_t / dl, edge, -dir, xe.ng, edge2, n) * cos2;
-      if (bval == 0.f) return false;
-      st.V = &V; st.gslot = gslot; st.p = p; st.x = xs; st.xe = xe; st.rdir = dir; st.p0 = p0; st.n = n;
-      st.w0 = bval / pdf; st.sedge = reuse; st.v0 = v0; st.v1 = v1; st.far_tri = he.tri;
-      return true;
-    },
+    [&](long long gslot, EdgeState& st) -> bool { return indirect_setup(P, gslot, st, vhint, cnt); },
     [&](EdgeState& st) {
       const ViewDesc& V = *st.V;
       const int D = min(V.D, MAXD);
-      const PathSmp S{&P, V.seed, st.gslot, st.p + V.slot_off};
-      // Sensor side first (BoundaryIndirect.cpp:158-175 pairs sensor depth b
-      // with the emitter radiance accumulated over D-1-b bounces): record the
-      // importance contributions, weighted by dL/dI of their pixels. The
-      // emitter side then only runs as deep as the shallowest sensor depth
-      // that reached the image needs, and not at all when none did.
+      // sensor side first; the emitter side then only runs as deep as the
+      // shallowest sensor depth that reached the image needs, and not at all
+      // when none did
       F3 sc[MAXD];
-      int bmin = D;
-      {
-        F3 T(1.f, 1.f, 1.f);
-        F3 rd = st.rdir;
-        SurfF xx = st.x;
-        for (int b = 0; b < D - 1; b++) sc[b] = F3z();
-        for (int b = 0; b < D - 1; b++) {
-          const int o = 3 + 5 * (D - 1) + 3 * b;
-          F3 c; int pix;
-          const bool more = importance_step_shared(s, V.cam, xx, rd, T, S(o), S(o + 1), S(o + 2), c, pix, cnt);
-          if (pix >= 0) {
-            sc[b] = g_at(P, V, pix) * c;
-            if (sc[b].x != 0.f || sc[b].y != 0.f || sc[b].z != 0.f) bmin = min(bmin, b);
-          }
-          if (!more) break;
-        }
-      }
+      const int bmin = indirect_sensor<MAXD>(P, st, D, sc, cnt);
       if (bmin >= D - 1) return;
-      // emitter side: the radiance accumulated over j+1 bounces pairs with
-      // sensor depth D-2-j
-      float W = 0.f;
-      {
-        F3 T(1.f, 1.f, 1.f);
-        F3 rd = -st.rdir;
-        SurfF xx = st.xe;
-        F3 cur = F3z();
-        const int jmax = D - 2 - bmin;
-        bool alive = true;
-        for (int j = 0; j <= jmax; j++) {
-          if (alive) {
-            const int o = 3 + 5 * j;
-            F3 c;
-            alive = radiance_step_shared(s, xx, rd, T, S(o), S(o + 1), S(o + 2), S(o + 3), S(o + 4), c, nullptr,
-                                         cnt);
-            cur = cur + c;
-            if (T.x == 0.f && T.y == 0.f && T.z == 0.f) alive = false;
-          }
-          W += dot(sc[D - 2 - j], cur) * st.w0;
-        }
-      }
+      const float W = indirect_emitter<MAXD>(P, V, st.gslot, st.p, st.xe, st.rdir, st.w0, D, D - 2 - bmin, sc, cnt);
       if (W == 0.f || !isfinite(W)) return;
       xdotn_vjp(P, V, W, st.x.p, true, st.x.tri, st.x.u, st.x.v, st.v0, st.v1, st.sedge, st.p0, st.far_tri, st.n,
                 cnt);
     });
   flush_cnt(cnt, P.stats);
 }
+
+// Split form of the same term: k_indirect_sensor runs the set-up and the
+// sensor side and queues the samples whose sensor side reached the image;
+// k_indirect_emitter runs the emitter side and the scatter for the queue.
+// Each kernel carries half of the fused kernel's code (the fused kernel is
+// instruction-fetch bound), and the emitter pass runs on survivors only.
+template <int MAXD>
+struct IndirectItem {
+  long long gslot, p;
+  int view, jmax, D;
+  int xe_tri, xs_tri;
+  float xe_u, xe_v, xs_u, xs_v;
+  F3 rdir, p0, n;
+  float w0, sedge;
+  int v0, v1, far_tri;
+  F3 sc[MAXD];
+};
+
+template <int MAXD>
+__global__ void __launch_bounds__(256, TRN_MINB_INDIRECT) k_indirect_sensor(Params P) {
+  Cnt cnt;
+  stage_top(P.s);
+  int vhint = 0;
+  IndirectItem<MAXD>* q = reinterpret_cast<IndirectItem<MAXD>*>(P.queue);
+  for_each_valid<EdgeState>(P,
+    [&](long long gslot, EdgeState& st) -> bool { return indirect_setup(P, gslot, st, vhint, cnt); },
+    [&](EdgeState& st) {
+      const int D = min(st.V->D, MAXD);
+      F3 sc[MAXD];
+      const int bmin = indirect_sensor<MAXD>(P, st, D, sc, cnt);
+      if (bmin >= D - 1) return;
+      const unsigned long long k = atomicAdd(P.q_count, 1ull);
+      if (k >= (unsigned long long)P.q_cap) { atomicExch(P.err, 2); return; }
+      IndirectItem<MAXD>& it = q[k];
+      it.gslot = st.gslot; it.p = st.p;
+      it.view = (int)(st.V - P.views); it.jmax = D - 2 - bmin; it.D = D;
+      it.xe_tri = st.xe.tri; it.xe_u = st.xe.u; it.xe_v = st.xe.v;
+      it.xs_tri = st.x.tri; it.xs_u = st.x.u; it.xs_v = st.x.v;
+      it.rdir = st.rdir; it.p0 = st.p0; it.n = st.n; it.w0 = st.w0; it.sedge = st.sedge;
+      it.v0 = st.v0; it.v1 = st.v1; it.far_tri = st.far_tri;
+      for (int b = 0; b < D - 1; b++) it.sc[b] = sc[b];
+    });
+  flush_cnt(cnt, P.stats);
+}
+
+template <int MAXD>
+__global__ void __launch_bounds__(256, TRN_MINB_INDIRECT) k_indirect_emitter(Params P) {
+  Cnt cnt;
+  stage_top(P.s);
+  const IndirectItem<MAXD>* q = reinterpret_cast<const IndirectItem<MAXD>*>(P.queue);
+  const unsigned long long n = min(*P.q_count, (unsigned long long)P.q_cap);
+  for (unsigned long long k = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; k < n;
+       k += (unsigned long long)gridDim.x * blockDim.x) {
+    const IndirectItem<MAXD>& it = q[k];
+    const ViewDesc& V = P.views[it.view];
+    const SurfF xe = post_intersect(P.s, it.xe_tri, it.xe_u, it.xe_v);
+    const float W = indirect_emitter<MAXD>(P, V, it.gslot, it.p, xe, it.rdir, it.w0, it.D, it.jmax, it.sc, cnt);
+    if (W == 0.f || !isfinite(W)) continue;
+    const SurfF xs = post_intersect(P.s, it.xs_tri, it.xs_u, it.xs_v);
+    xdotn_vjp(P, V, W, xs.p, true, it.xs_tri, it.xs_u, it.xs_v, it.v0, it.v1, it.sedge, it.p0, it.far_tri, it.n,
+              cnt);
+  }
+  flush_cnt(cnt, P.stats);
+}
+
+// Slot range of one split round: the work counter starts at `first`, the
+// queue is empty.
+__global__ void k_indirect_round(unsigned long long* work, unsigned long long first, unsigned long long* q_count) {
+  if (threadIdx.x == 0) { *work = first; *q_count = 0ull; }
+}
+
 
 // ---------------------------------------------------------------------------
 // pixel boundary (BoundaryPixel.cpp:36-159, Edge.cpp:377-409, Camera.cpp:433-467)
@@ -1678,6 +1781,11 @@ struct trn_viewset {
   float* pcdf = nullptr;          // device [nviews][E]
   float* pint = nullptr;          // device [nviews]
   unsigned long long* work = nullptr;
+  // queue of the split indirect boundary term: one round of at most
+  // kIndirectRound slots at a time
+  void* iq = nullptr;
+  size_t iq_bytes = 0;
+  unsigned long long* iq_count = nullptr;
   int ne = 0;
   // slot layout currently uploaded: spp multiplier and per-view spp
   int uploaded_key = -2;
@@ -1800,6 +1908,9 @@ Params base_params(trn_scene* s, trn_viewset* vs, const trn_render_options* o, i
   P.err = s->err;
   P.stats = s->stats_on ? s->stats : nullptr;
   P.aq_poly = P.aq_cdf = P.aq_int = nullptr;
+  P.queue = nullptr;
+  P.q_count = nullptr;
+  P.q_cap = 0;
   return P;
 }
 
@@ -1859,6 +1970,57 @@ void launch(K kernel, const trn_launch* ln, long long total, const Params& P, cu
   count_launch(1);
 }
 
+#ifndef TRN_INDIRECT_SPLIT
+#define TRN_INDIRECT_SPLIT 1
+#endif
+constexpr long long kIndirectRound = 1LL << 22;  // slots per split round (queue of 4M items)
+
+// The split indirect term in rounds of at most kIndirectRound slots. The
+// queue is the view set's and grows on first use (not inside stream capture:
+// run the integrator once before capturing it).
+int indirect_split(trn_viewset* vs, Params P, const trn_launch* ln, long long total, bool shallow, cudaStream_t st) {
+  const long long cap = std::min(total, kIndirectRound);
+  const size_t item = shallow ? sizeof(IndirectItem<8>) : sizeof(IndirectItem<kMaxDepth>);
+  const size_t need = item * (size_t)cap;
+  if (vs->iq_bytes < need || !vs->iq_count) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    TRN_CUDA_TRY(cudaStreamIsCapturing(st, &cs));
+    if (cs != cudaStreamCaptureStatusNone) {
+      set_error("indirect boundary: its queue must be allocated before stream capture (run it once first)");
+      return -1;
+    }
+    TRN_CUDA_TRY(cudaStreamSynchronize(st));
+    if (vs->iq) cudaFree(vs->iq);
+    vs->iq = nullptr;
+    vs->iq_bytes = 0;
+    if (cudaMalloc(&vs->iq, need) != cudaSuccess) { set_error("indirect boundary: out of memory for its queue"); return -1; }
+    vs->iq_bytes = need;
+    if (!vs->iq_count && cudaMalloc(&vs->iq_count, sizeof(unsigned long long)) != cudaSuccess) {
+      set_error("indirect boundary: out of memory");
+      return -1;
+    }
+  }
+  P.queue = vs->iq;
+  P.q_count = vs->iq_count;
+  P.q_cap = cap;
+  int grid, block;
+  launch_dims(ln, cap, grid, block);
+  for (long long first = 0; first < total; first += cap) {
+    P.total = std::min(total, first + cap);
+    k_indirect_round<<<1, 32, 0, st>>>(P.work, (unsigned long long)first, P.q_count);
+    if (shallow) {
+      k_indirect_sensor<8><<<grid, block, 0, st>>>(P);
+      k_indirect_emitter<8><<<grid, block, 0, st>>>(P);
+    } else {
+      k_indirect_sensor<kMaxDepth><<<grid, block, 0, st>>>(P);
+      k_indirect_emitter<kMaxDepth><<<grid, block, 0, st>>>(P);
+    }
+    count_launch(3);
+  }
+  TRN_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
 int render_views(trn_scene* s, trn_viewset* vs, const trn_render_options* o, int integrator,
                  const trn_samples* smp, const trn_launch* ln, int spp_override, bool forward, float* image,
                  const float* dLdI, cudaStream_t st) {
@@ -1902,6 +2064,7 @@ int render_views(trn_scene* s, trn_viewset* vs, const trn_render_options* o, int
     case TRN_PRIMARY_EDGE: launch(k_primary_adj, ln, total, P, st); break;
     case TRN_DIRECT_EDGE: launch(k_direct_adj, ln, total, P, st); break;
     case TRN_INDIRECT_EDGE:
+      if (TRN_INDIRECT_SPLIT) return indirect_split(vs, P, ln, total, shallow, st);
       if (shallow) launch(k_indirect_adj<8>, ln, total, P, st); else launch(k_indirect_adj<kMaxDepth>, ln, total, P, st);
       break;
     default: launch(k_pixel_adj, ln, total, P, st); break;
@@ -2017,7 +2180,7 @@ int trn_viewset_update(trn_viewset* vs, int nviews, const trn_view* views) {
 int trn_viewset_destroy(trn_viewset* vs) {
   if (!vs) return 0;
   if (vs->copy_done) cudaEventSynchronize(vs->copy_done);
-  void* ptrs[] = {vs->views, vs->vbegin, vs->pbegin, vs->pfunc, vs->pcdf, vs->pint, vs->work};
+  void* ptrs[] = {vs->views, vs->vbegin, vs->pbegin, vs->pfunc, vs->pcdf, vs->pint, vs->work, vs->iq, vs->iq_count};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (vs->h_stage) cudaFreeHost(vs->h_stage);
