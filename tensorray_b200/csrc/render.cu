@@ -136,7 +136,10 @@ TRN_D float* warp_scratch() {
 TRN_D void agg_add3(float* base, long long idx, const F3& g) {
   const unsigned active = __activemask();
   const int lane = threadIdx.x & 31;
-  const unsigned peers = __match_any_sync(active, idx);
+  // peers share the target address, not just the index: lanes of one warp can
+  // scatter into different views' gradient buffers
+  float* const target = base + 3 * idx;
+  const unsigned peers = __match_any_sync(active, reinterpret_cast<unsigned long long>(target));
   const int leader = __ffs(peers) - 1;
   float* w = warp_scratch();
   if (lane == leader) { w[3 * lane] = g.x; w[3 * lane + 1] = g.y; w[3 * lane + 2] = g.z; }
@@ -145,7 +148,7 @@ TRN_D void agg_add3(float* base, long long idx, const F3& g) {
     atomicAdd(w + 3 * leader, g.x); atomicAdd(w + 3 * leader + 1, g.y); atomicAdd(w + 3 * leader + 2, g.z);
   }
   __syncwarp(active);
-  if (lane == leader) atomic_add3(base + 3 * idx, F3(w[3 * lane], w[3 * lane + 1], w[3 * lane + 2]));
+  if (lane == leader) atomic_add3(target, F3(w[3 * lane], w[3 * lane + 1], w[3 * lane + 2]));
   __syncwarp(active);
 }
 TRN_D F3 g_at(const Params& P, const ViewDesc& V, int pix) {
@@ -1089,77 +1092,149 @@ struct EdgeState {
   F3 g;
 };
 
-__global__ void __launch_bounds__(256, TRN_MINB) k_primary_adj(Params P) {
+// Primary boundary set-up (SampleFromPrimEdges, Edge.cpp:350-367;
+// BoundaryPrimary.cpp:60-130): silhouette edge point, camera ray through it,
+// visibility, boundary geometry. Returns false for a rejected sample.
+TRN_D bool primary_setup(const Params& P, long long gslot, EdgeState& st, int& vhint, Cnt& cnt) {
   const DeviceScene& s = P.s;
+  const ViewDesc& V = view_of(P, gslot, vhint);
+  const long long p = gslot - V.begin;
+  const CameraDesc& cam = V.cam;
+  const PathSmp S{&P, V.seed, gslot, p + V.slot_off};
+  const F3 cpos = cam_pos(cam);
+  const float r0 = S(0), r1 = S(1);
+  float reuse;
+  const float integral = __ldg(V.pint);
+  if (!(integral > 0.f)) return false;
+  const int e = sample_discrete(V.pcdf, P.ne, r0, reuse);
+  const int v0 = P.edges[5 * e], v1 = P.edges[5 * e + 1], v2 = P.edges[5 * e + 4];
+  const float len_e = V.pfunc[e];
+  if (!(len_e > 0.f)) return false;
+  const float pmf = len_e / (integral * (float)P.ne);
+  const float pdf = pmf / len_e;
+  const F3 Pa = load3(s.pos, v0), Pb = load3(s.pos, v1), Pc = load3(s.pos, v2);
+  const F3 e1 = Pb - Pa;
+  const F3 p0 = Pa + e1 * r1;
+  const F3 edge = normalize(e1), edge2 = normalize(Pc - Pa);
+  const F3 dir = normalize(p0 - cpos);
+  Hit h;
+  cnt.v[kCntClosest]++;
+  if (!trace_k<TRN_SETUP_SHARED_PRIMARY, false>(s, p0, dir, kShadowEps, kRayMax, h, P.err)) return false;
+  const F3 hitP = p0 + dir * h.t;
+  const SensorSample sds = sample_direct(cam, hitP);
+  if (!sds.valid) return false;
+  const F3 dirc = sensor_ray_dir(cam, sds.qx, sds.qy);
+  const float dist2cam = length(p0 - cpos);
+  cnt.v[kCntShadow]++;
+  if (occluded_k<TRN_SETUP_SHARED_PRIMARY>(s, cpos, dirc, kShadowEps, dist2cam - kShadowEps)) return false;
+  const SurfF x = post_intersect(s, h.tri, h.u, h.v);
+  const float dist = length(x.p - cpos);
+  const float dist1 = length(p0 - cpos);
+  const float cos2 = fabsf(dot(x.ng, -dirc));
+  F3 n;
+  const float bval = base_val((dist / dist1), edge, dirc, x.ng, edge2, n) * cos2;
+  const int pix = image_pixel(cam, sds.qx, sds.qy);
+  const F3 g = g_at(P, V, pix);
+  if (bval == 0.f || (g.x == 0.f && g.y == 0.f && g.z == 0.f)) return false;
+  st.V = &V; st.gslot = gslot; st.p = p; st.x = x; st.rdir = dirc;
+  st.T0 = F3(sds.sensor_val, sds.sensor_val, sds.sensor_val);
+  st.p0 = p0; st.n = n; st.w0 = bval / pdf; st.sedge = r1; st.v0 = v0; st.v1 = v1; st.far_tri = h.tri;
+  st.pix = pix; st.g = g;
+  return true;
+}
+
+// Primary boundary body: detached radiance along the camera ray through the
+// sensor point (BoundaryPrimary.cpp:150-175), then the xDotN scatter.
+TRN_D void primary_body(const Params& P, const ViewDesc& V, long long gslot, long long p, SurfF x, F3 rdir, F3 T,
+                        float w0, const F3& g, int v0, int v1, float sedge, const F3& p0, int far_tri, const F3& n,
+                        Cnt& cnt) {
+  const DeviceScene& s = P.s;
+  const PathSmp S{&P, V.seed, gslot, p + V.slot_off};
+  F3 L = scrub(T * emitted(s, x, -rdir));
+  for (int b = 0; b < V.D; b++) {
+    const int o = 2 + 5 * b;
+    F3 c;
+    const bool more = radiance_step_k<TRN_SHARED_STEPS_PRIMARY>(s, x, rdir, T, S(o), S(o + 1), S(o + 2), S(o + 3),
+                                                                S(o + 4), c, nullptr, cnt);
+    L = L + c;
+    if (!more || (T.x == 0.f && T.y == 0.f && T.z == 0.f)) break;
+  }
+  const float W = dot(g, L * w0);
+  if (W == 0.f || !isfinite(W)) return;
+  xdotn_vjp(P, V, W, cam_pos(V.cam), false, -1, 0.f, 0.f, v0, v1, sedge, p0, far_tri, n, cnt);
+}
+
+__global__ void __launch_bounds__(256, TRN_MINB) k_primary_adj(Params P) {
   Cnt cnt;
   stage_top(P.s);
   int vhint = 0;
   for_each_valid<EdgeState>(P,
-    [&](long long gslot, EdgeState& st) -> bool {
-      const ViewDesc& V = view_of(P, gslot, vhint);
-      const long long p = gslot - V.begin;
-      const CameraDesc& cam = V.cam;
-      const PathSmp S{&P, V.seed, gslot, p + V.slot_off};
-      const F3 cpos = cam_pos(cam);
-      const float r0 = S(0), r1 = S(1);
-      float reuse;
-      const float integral = __ldg(V.pint);
-      if (!(integral > 0.f)) return false;
-      const int e = sample_discrete(V.pcdf, P.ne, r0, reuse);
-      const int v0 = P.edges[5 * e], v1 = P.edges[5 * e + 1], v2 = P.edges[5 * e + 4];
-      const float len_e = V.pfunc[e];
-      if (!(len_e > 0.f)) return false;
-      const float pmf = len_e / (integral * (float)P.ne);
-      const float pdf = pmf / len_e;
-      const F3 Pa = load3(s.pos, v0), Pb = load3(s.pos, v1), Pc = load3(s.pos, v2);
-      const F3 e1 = Pb - Pa;
-      const F3 p0 = Pa + e1 * r1;
-      const F3 edge = normalize(e1), edge2 = normalize(Pc - Pa);
-      const F3 dir = normalize(p0 - cpos);
-      Hit h;
-      cnt.v[kCntClosest]++;
-      if (!trace_k<TRN_SETUP_SHARED_PRIMARY, false>(s, p0, dir, kShadowEps, kRayMax, h, P.err)) return false;
-      const F3 hitP = p0 + dir * h.t;
-      const SensorSample sds = sample_direct(cam, hitP);
-      if (!sds.valid) return false;
-      const F3 dirc = sensor_ray_dir(cam, sds.qx, sds.qy);
-      const float dist2cam = length(p0 - cpos);
-      cnt.v[kCntShadow]++;
-      if (occluded_k<TRN_SETUP_SHARED_PRIMARY>(s, cpos, dirc, kShadowEps, dist2cam - kShadowEps)) return false;
-      const SurfF x = post_intersect(s, h.tri, h.u, h.v);
-      const float dist = length(x.p - cpos);
-      const float dist1 = length(p0 - cpos);
-      const float cos2 = fabsf(dot(x.ng, -dirc));
-      F3 n;
-      const float bval = base_val((dist / dist1), edge, dirc, x.ng, edge2, n) * cos2;
-      const int pix = image_pixel(cam, sds.qx, sds.qy);
-      const F3 g = g_at(P, V, pix);
-      if (bval == 0.f || (g.x == 0.f && g.y == 0.f && g.z == 0.f)) return false;
-      st.V = &V; st.gslot = gslot; st.p = p; st.x = x; st.rdir = dirc;
-      st.T0 = F3(sds.sensor_val, sds.sensor_val, sds.sensor_val);
-      st.p0 = p0; st.n = n; st.w0 = bval / pdf; st.sedge = r1; st.v0 = v0; st.v1 = v1; st.far_tri = h.tri;
-      st.pix = pix; st.g = g;
-      return true;
-    },
+    [&](long long gslot, EdgeState& st) -> bool { return primary_setup(P, gslot, st, vhint, cnt); },
     [&](EdgeState& st) {
-      const ViewDesc& V = *st.V;
-      const PathSmp S{&P, V.seed, st.gslot, st.p + V.slot_off};
-      // detached radiance along the camera ray through the sensor point
-      SurfF x = st.x;
-      F3 T = st.T0, rdir = st.rdir;
-      F3 L = scrub(T * emitted(s, x, -rdir));
-      for (int b = 0; b < V.D; b++) {
-        const int o = 2 + 5 * b;
-        F3 c;
-        const bool more = radiance_step_k<TRN_SHARED_STEPS_PRIMARY>(s, x, rdir, T, S(o), S(o + 1), S(o + 2), S(o + 3), S(o + 4), c, nullptr,
-                                        cnt);
-        L = L + c;
-        if (!more || (T.x == 0.f && T.y == 0.f && T.z == 0.f)) break;
-      }
-      const float W = dot(st.g, L * st.w0);
-      if (W == 0.f || !isfinite(W)) return;
-      xdotn_vjp(P, V, W, cam_pos(V.cam), false, -1, 0.f, 0.f, st.v0, st.v1, st.sedge, st.p0, st.far_tri, st.n, cnt);
+      primary_body(P, *st.V, st.gslot, st.p, st.x, st.rdir, st.T0, st.w0, st.g, st.v0, st.v1, st.sedge, st.p0,
+                   st.far_tri, st.n, cnt);
     });
+  flush_cnt(cnt, P.stats);
+}
+
+// Split form: k_primary_setup tests every slot once (no lane waits for the
+// others to find an accepted sample, which matters at the ~4 % acceptance of
+// silhouette samples) and queues the accepted ones; k_primary_body runs the
+// radiance path and the scatter for the queue.
+struct PrimaryItem {
+  long long gslot, p;
+  int view, x_tri;
+  float x_u, x_v, T0, w0, sedge;
+  int v0, v1, far_tri;
+  F3 rdir, p0, n, g;
+};
+
+__global__ void __launch_bounds__(256, TRN_MINB) k_primary_setup(Params P) {
+  Cnt cnt;
+  stage_top(P.s);
+  int vhint = 0;
+  PrimaryItem* q = reinterpret_cast<PrimaryItem*>(P.queue);
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;
+  for (;;) {
+    unsigned long long start = 0;
+    if (lane == 0) start = atomicAdd(P.work, 32ull);
+    start = __shfl_sync(0xffffffffu, start, 0);
+    if ((long long)start >= P.total) break;
+    const long long g = (long long)start + lane;
+    EdgeState st;
+    const bool ok = g < P.total && primary_setup(P, g, st, vhint, cnt);
+    const unsigned m = __ballot_sync(0xffffffffu, ok);
+    if (!m) continue;
+    const int leader = __ffs(m) - 1;
+    unsigned long long base = 0;
+    if (lane == leader) base = atomicAdd(P.q_count, (unsigned long long)__popc(m));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    const unsigned long long k = base + __popc(m & lt);
+    if (ok && k >= (unsigned long long)P.q_cap) atomicExch(P.err, 2);
+    if (ok && k < (unsigned long long)P.q_cap) {
+      PrimaryItem& it = q[k];
+      it.gslot = st.gslot; it.p = st.p; it.view = (int)(st.V - P.views);
+      it.x_tri = st.x.tri; it.x_u = st.x.u; it.x_v = st.x.v; it.T0 = st.T0.x; it.w0 = st.w0; it.sedge = st.sedge;
+      it.v0 = st.v0; it.v1 = st.v1; it.far_tri = st.far_tri;
+      it.rdir = st.rdir; it.p0 = st.p0; it.n = st.n; it.g = st.g;
+    }
+  }
+  flush_cnt(cnt, P.stats);
+}
+
+__global__ void __launch_bounds__(256, TRN_MINB) k_primary_body(Params P) {
+  Cnt cnt;
+  stage_top(P.s);
+  const PrimaryItem* q = reinterpret_cast<const PrimaryItem*>(P.queue);
+  const unsigned long long n = min(*P.q_count, (unsigned long long)P.q_cap);
+  for (unsigned long long k = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; k < n;
+       k += (unsigned long long)gridDim.x * blockDim.x) {
+    const PrimaryItem& it = q[k];
+    const SurfF x = post_intersect(P.s, it.x_tri, it.x_u, it.x_v);
+    primary_body(P, P.views[it.view], it.gslot, it.p, x, it.rdir, F3(it.T0, it.T0, it.T0), it.w0, it.g, it.v0, it.v1,
+                 it.sedge, it.p0, it.far_tri, it.n, cnt);
+  }
   flush_cnt(cnt, P.stats);
 }
 
@@ -1975,31 +2050,61 @@ void launch(K kernel, const trn_launch* ln, long long total, const Params& P, cu
 #endif
 constexpr long long kIndirectRound = 1LL << 22;  // slots per split round (queue of 4M items)
 
-// The split indirect term in rounds of at most kIndirectRound slots. The
-// queue is the view set's and grows on first use (not inside stream capture:
-// run the integrator once before capturing it).
-int indirect_split(trn_viewset* vs, Params P, const trn_launch* ln, long long total, bool shallow, cudaStream_t st) {
-  const long long cap = std::min(total, kIndirectRound);
-  const size_t item = shallow ? sizeof(IndirectItem<8>) : sizeof(IndirectItem<kMaxDepth>);
-  const size_t need = item * (size_t)cap;
-  if (vs->iq_bytes < need || !vs->iq_count) {
-    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-    TRN_CUDA_TRY(cudaStreamIsCapturing(st, &cs));
-    if (cs != cudaStreamCaptureStatusNone) {
-      set_error("indirect boundary: its queue must be allocated before stream capture (run it once first)");
-      return -1;
-    }
-    TRN_CUDA_TRY(cudaStreamSynchronize(st));
+#ifndef TRN_PRIMARY_SPLIT
+#define TRN_PRIMARY_SPLIT 1
+#endif
+
+// The view set's queue of the split boundary terms, grown on first use to
+// `need` bytes (not inside stream capture: run the integrator once before
+// capturing it).
+int ensure_queue(trn_viewset* vs, size_t need, cudaStream_t st) {
+  if (vs->iq_bytes >= need && vs->iq_count) return 0;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  TRN_CUDA_TRY(cudaStreamIsCapturing(st, &cs));
+  if (cs != cudaStreamCaptureStatusNone) {
+    set_error("boundary term: its queue must be allocated before stream capture (run it once first)");
+    return -1;
+  }
+  TRN_CUDA_TRY(cudaStreamSynchronize(st));
+  if (vs->iq_bytes < need) {
     if (vs->iq) cudaFree(vs->iq);
     vs->iq = nullptr;
     vs->iq_bytes = 0;
-    if (cudaMalloc(&vs->iq, need) != cudaSuccess) { set_error("indirect boundary: out of memory for its queue"); return -1; }
+    if (cudaMalloc(&vs->iq, need) != cudaSuccess) { set_error("boundary term: out of memory for its queue"); return -1; }
     vs->iq_bytes = need;
-    if (!vs->iq_count && cudaMalloc(&vs->iq_count, sizeof(unsigned long long)) != cudaSuccess) {
-      set_error("indirect boundary: out of memory");
-      return -1;
-    }
   }
+  if (!vs->iq_count && cudaMalloc(&vs->iq_count, sizeof(unsigned long long)) != cudaSuccess) {
+    set_error("boundary term: out of memory");
+    return -1;
+  }
+  return 0;
+}
+
+// The split primary term in rounds of at most kIndirectRound slots.
+int primary_split(trn_viewset* vs, Params P, const trn_launch* ln, long long total, cudaStream_t st) {
+  const long long cap = std::min(total, kIndirectRound);
+  if (ensure_queue(vs, sizeof(PrimaryItem) * (size_t)cap, st)) return -1;
+  P.queue = vs->iq;
+  P.q_count = vs->iq_count;
+  P.q_cap = cap;
+  int grid, block;
+  launch_dims(ln, cap, grid, block);
+  for (long long first = 0; first < total; first += cap) {
+    P.total = std::min(total, first + cap);
+    k_indirect_round<<<1, 32, 0, st>>>(P.work, (unsigned long long)first, P.q_count);
+    k_primary_setup<<<grid, block, 0, st>>>(P);
+    k_primary_body<<<grid, block, 0, st>>>(P);
+    count_launch(3);
+  }
+  TRN_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+// The split indirect term in rounds of at most kIndirectRound slots.
+int indirect_split(trn_viewset* vs, Params P, const trn_launch* ln, long long total, bool shallow, cudaStream_t st) {
+  const long long cap = std::min(total, kIndirectRound);
+  const size_t item = shallow ? sizeof(IndirectItem<8>) : sizeof(IndirectItem<kMaxDepth>);
+  if (ensure_queue(vs, item * (size_t)cap, st)) return -1;
   P.queue = vs->iq;
   P.q_count = vs->iq_count;
   P.q_cap = cap;
@@ -2061,7 +2166,10 @@ int render_views(trn_scene* s, trn_viewset* vs, const trn_render_options* o, int
     case TRN_PATH_TRACER:
       if (shallow) launch(k_path_adj<8>, ln, total, P, st); else launch(k_path_adj<kMaxDepth>, ln, total, P, st);
       break;
-    case TRN_PRIMARY_EDGE: launch(k_primary_adj, ln, total, P, st); break;
+    case TRN_PRIMARY_EDGE:
+      if (TRN_PRIMARY_SPLIT) return primary_split(vs, P, ln, total, st);
+      launch(k_primary_adj, ln, total, P, st);
+      break;
     case TRN_DIRECT_EDGE: launch(k_direct_adj, ln, total, P, st); break;
     case TRN_INDIRECT_EDGE:
       if (TRN_INDIRECT_SPLIT) return indirect_split(vs, P, ln, total, shallow, st);
