@@ -264,6 +264,7 @@ def main():
     clocks.start()
     launches0 = lib.trn_kernel_launches()
     total_ms = 0.0
+    step_ms = []
     for s in range(a.steps):
         if world > 1:
             dist.barrier()
@@ -276,6 +277,7 @@ def main():
         e1.record(stream)
         torch.cuda.synchronize()
         total_ms += e0.elapsed_time(e1)
+        step_ms.append(round(e0.elapsed_time(e1), 2))
         for k in ev_keys:
             per_kernel[k].append(ev[k][0].elapsed_time(ev[k][1]))
     launches = lib.trn_kernel_launches() - launches0
@@ -392,7 +394,7 @@ def main():
             "config": {"workload": workload_name(a), "global_batch_samples": units_per_step * world,
                        "res": a.res, "spp_per_term": a.spp, "depth": D, "triangles": scene.num_triangles,
                        "l2": "flushed between timed steps (256 MB write)", "parallelism": f"seeds x{world}"},
-            "e2e": e2e, "gpu_launches": int(launches), "clocks": clk, "roofline": roofline,
+            "e2e": e2e, "gpu_launches": int(launches), "clocks": clk, "roofline": roofline, "step_ms": step_ms,
             "kernels": {k: {"ms": v["ms"], "GB/s": v["gbs"], "counts": v["counts"]} for k, v in per_kernel_roof.items()},
             "cpu_baseline": cpu,
         }

@@ -787,147 +787,222 @@ struct AdjState {
   Hit h;
 };
 
+// Interior adjoint set-up: the camera ray of the slot (paths whose pixel has a
+// zero dL/dI carry no gradient and are skipped).
+TRN_D bool path_adj_setup(const Params& P, long long gslot, AdjState& st, int& vhint, Cnt& cnt) {
+  const DeviceScene& s = P.s;
+  const ViewDesc& V = view_of(P, gslot, vhint);
+  const long long p = gslot - V.begin;
+  const CameraDesc& cam = V.cam;
+  const PathSmp S{&P, V.seed, gslot, p + V.slot_off};
+  const int W = cam.w, WH = cam.w * cam.h;
+  const int pix = (int)(p % WH);
+  cnt.v[kCntPixel]++;
+  const F3 g = g_at(P, V, pix);
+  if (g.x == 0.f && g.y == 0.f && g.z == 0.f) return false;
+  const F3 dir = camera_ray_dir(cam, pix % W, pix / W, S(0), S(1));
+  cnt.v[kCntClosest]++;
+  if (!trace_k<TRN_SETUP_SHARED_PATHADJ, false>(s, cam_pos(cam), dir, kShadowEps, kRayMax, st.h, P.err)) return false;
+  st.V = &V; st.gslot = gslot; st.p = p; st.pix = pix; st.g = g;
+  return true;
+}
+
+struct LRec { int ltri; float lu, lv, lpdf, lmis, ppdf; };
+
+// Everything the reverse sweep of one interior path needs from its forward
+// replay: vertices (hit records), per-bounce NEE light samples and
+// continuation pdfs, throughputs T_k and emission terms M_k.
+template <int MAXD>
+struct PathRec {
+  long long gslot, p;
+  int view, K, D;
+  unsigned nee_mask;        // bit k: bounce k's NEE contributes
+  F3 g;                     // dL/dI of the path's pixel (times 1/spp)
+  VRec vr[MAXD + 2];
+  LRec br[MAXD + 1];
+  F3 Tk[MAXD + 2], Mk[MAXD + 2];
+};
+
+// Forward replay of one interior path from its primary hit, recording into r.
+template <int MAXD, class Rec>
+TRN_D void path_replay(const Params& P, const AdjState& st, Rec& r, Cnt& cnt) {
+  const DeviceScene& s = P.s;
+  const ViewDesc& V = *st.V;
+  const CameraDesc& cam = V.cam;
+  const PathSmp S{&P, V.seed, st.gslot, st.p + V.slot_off};
+  const F3 org = cam_pos(cam);
+  const Hit h = st.h;
+  r.gslot = st.gslot; r.p = st.p; r.view = (int)(st.V - P.views); r.g = st.g;
+  SurfF x = post_intersect(s, h.tri, h.u, h.v);
+  r.vr[1] = {h.tri, h.u, h.v};
+  const float t1 = camera_factor<float>(cam, x.p, x.ng, 1.f);
+  F3 T(t1, t1, t1);
+  F3 rdir = normalize(x.p - org);
+  r.Tk[1] = T;
+  F3 m1 = emitted(s, x, -rdir);
+  if (!finite3(T * m1)) m1 = F3z();
+  r.Mk[1] = m1;
+  int K = 1;  // vertices reached
+  const int D = min(V.D, MAXD);
+  unsigned mask = 0u;
+  for (int b = 0; b < D; b++) {
+    const int k = b + 1;
+    const int o = 2 + 5 * b;
+    F3 c;
+    BounceRec R;
+    const bool more = radiance_step_k<TRN_SHARED_STEPS_PATHADJ>(s, x, rdir, T, S(o), S(o + 1), S(o + 2),
+                                    S(o + 3), S(o + 4), c, &R, cnt);
+    // a scrubbed (non-finite) bounce contributes nothing and carries no gradient
+    if (R.nee_ok && !R.scrubbed) mask |= 1u << k;
+    r.br[k] = {R.ltri, R.lu, R.lv, R.lpdf, R.lmis, R.prev_pdf};
+    if (!more) break;
+    r.vr[k + 1] = {x.tri, x.u, x.v};
+    r.Tk[k + 1] = T;
+    r.Mk[k + 1] = (R.scrubbed || R.emis == 0.f) ? F3z() : R.eLe * R.emis;
+    K = k + 1;
+    if (T.x == 0.f && T.y == 0.f && T.z == 0.f) break;
+  }
+  r.K = K;
+  r.D = D;
+  r.nee_mask = mask;
+}
+
+// Reverse sweep of one recorded interior path:
+// a_k = g*(N_k + M_k) + phi_k * a_{k+1}, one vertex window at a time, then
+// the camera factor at vertex 1.
+template <int MAXD, class Rec>
+TRN_D void path_reverse(const Params& P, const Rec& r, Cnt& cnt) {
+  const DeviceScene& s = P.s;
+  const ViewDesc& V = P.views[r.view];
+  const CameraDesc& cam = V.cam;
+  const F3 org = cam_pos(cam);
+  const F3 g = r.g;
+  const int K = r.K, D = r.D;
+  struct VG { F3 p, ns, ng, kd; long long texel; int bsdf; };
+  auto load_vg = [&](int k) {
+    VG o;
+    const SurfF xs = post_intersect(s, r.vr[k].tri, r.vr[k].u, r.vr[k].v);
+    o.p = xs.p; o.ns = xs.ns; o.ng = xs.ng; o.bsdf = xs.bsdf;
+    o.kd = bsdf_albedo(s, s.bsdfs[xs.bsdf], xs.tu, xs.tv, o.texel);
+    return o;
+  };
+  VG Gk = load_vg(K), Gn = Gk;
+  F3 a_next = F3z();
+  VAdj acc_next, acc_k, acc_prev;
+  vadj_zero(acc_next); vadj_zero(acc_k); vadj_zero(acc_prev);
+  for (int k = K; k >= 1; k--) {
+    VG Gp;
+    if (k >= 2) Gp = load_vg(k - 1);
+    else { Gp.p = org; Gp.ns = Gp.ng = Gp.kd = F3z(); Gp.texel = -1; Gp.bsdf = 0; }
+    const BsdfDesc b = s.bsdfs[Gk.bsdf];
+    const bool need_prev = b.type != kDiffuse;
+    const bool need_kd = P.diff_tex && Gk.texel >= 0;
+    F3 Nval = F3z(), Phi = F3z();
+    F3 gkd = F3z(), gprev = F3z();
+    if (k <= D && ((r.nee_mask >> k) & 1u)) {
+      // NEE factor value and its reverse mode in one sweep
+      const LRec& R = r.br[k];
+      int j0, j1, j2; tri_vertices(s, R.ltri, j0, j1, j2);
+      const F3 y = bary3(R.lu, R.lv, load3(s.pos, j0), load3(s.pos, j1), load3(s.pos, j2));
+      const F3 nl = load3(s.fnormal, R.ltri);
+      // the forward step's emitter radiance (one-sided, AreaLight::Eval), same arithmetic
+      F3 wl = y - Gk.p;
+      wl = wl / sqrtf(dot(wl, wl));
+      const F3 Le = dot(-wl, nl) > 0.f ? light_radiance(s, s.emitter_id[R.ltri]) : F3z();
+      F3 gy = F3z(), gnl = F3z();
+      float gJl = 0.f;
+      Nval = nee_vjp(b, need_prev, need_kd, Gp.p, Gk.p, Gk.ns, Gk.ng, Gk.kd, y, nl, Le, R.lpdf, R.lmis,
+                     r.Tk[k] * g, gprev, acc_k.p, acc_k.ns, gkd, gy, gnl, gJl);
+      VAdj la; la.p = gy; la.ns = F3z(); la.ng = gnl; la.J = gJl;
+      scatter_vertex(P, V, R.ltri, R.lu, R.lv, la, cnt);
+    }
+    if (k < K) {
+      // continuation factor value and its reverse mode; a non-finite weight
+      // made the forward throughput non-finite: no value, no gradient
+      F3 cprev = F3z(), cx = F3z(), cns = F3z(), ckd = F3z(), cxn = F3z(), cngn = F3z();
+      float gJn = 0.f;
+      Phi = cont_vjp(b, need_prev, need_kd, Gp.p, Gk.p, Gk.ns, Gk.ng, Gk.kd, Gn.p, Gn.ng, r.br[k].ppdf,
+                     r.Tk[k] * a_next, cprev, cx, cns, ckd, cxn, cngn, gJn);
+      if (finite3(Phi)) {
+        gprev = gprev + cprev; acc_k.p = acc_k.p + cx; acc_k.ns = acc_k.ns + cns; gkd = gkd + ckd;
+        acc_next.p = acc_next.p + cxn; acc_next.ng = acc_next.ng + cngn; acc_next.J += gJn;
+      } else {
+        Phi = F3z();
+      }
+    }
+    const F3 a_k = g * (Nval + r.Mk[k]) + Phi * a_next;
+    if (k >= 2) acc_prev.p = acc_prev.p + gprev;
+    if (need_kd) { cnt.v[kCntTScatter]++; agg_add3(V.gtex, Gk.texel, gkd); }
+    // vertex k+1 has received all of its contributions
+    if (k < K) scatter_vertex(P, V, r.vr[k + 1].tri, r.vr[k + 1].u, r.vr[k + 1].v, acc_next, cnt);
+    acc_next = acc_k; acc_k = acc_prev; vadj_zero(acc_prev);
+    a_next = a_k; Gn = Gk; Gk = Gp;
+  }
+  // primary factor T1 = G / Detach(G) * J at vertex 1 (now in Gn / acc_next)
+  {
+    const float gam = a_next.x + a_next.y + a_next.z;
+    if (gam != 0.f && isfinite(gam)) {
+      F3 gp, gn;
+      float gJ;
+      camera_factor_grad(cam, Gn.p, Gn.ng, gam, gp, gn, gJ);
+      acc_next.p = acc_next.p + gp;
+      acc_next.ng = acc_next.ng + gn;
+      acc_next.J += gJ;
+    }
+  }
+  scatter_vertex(P, V, r.vr[1].tri, r.vr[1].u, r.vr[1].v, acc_next, cnt);
+}
+
 template <int MAXD>
 __global__ void __launch_bounds__(256, TRN_MINB_PATHADJ) k_path_adj(Params P) {
-  const DeviceScene& s = P.s;
   Cnt cnt;
   stage_top(P.s);
   int vhint = 0;
   for_each_valid<AdjState>(P,
-    [&](long long gslot, AdjState& st) -> bool {
-      const ViewDesc& V = view_of(P, gslot, vhint);
-      const long long p = gslot - V.begin;
-      const CameraDesc& cam = V.cam;
-      const PathSmp S{&P, V.seed, gslot, p + V.slot_off};
-      const int W = cam.w, WH = cam.w * cam.h;
-      const int pix = (int)(p % WH);
-      cnt.v[kCntPixel]++;
-      const F3 g = g_at(P, V, pix);
-      if (g.x == 0.f && g.y == 0.f && g.z == 0.f) return false;
-      const F3 dir = camera_ray_dir(cam, pix % W, pix / W, S(0), S(1));
-      cnt.v[kCntClosest]++;
-      if (!trace_k<TRN_SETUP_SHARED_PATHADJ, false>(s, cam_pos(cam), dir, kShadowEps, kRayMax, st.h, P.err)) return false;
-      st.V = &V; st.gslot = gslot; st.p = p; st.pix = pix; st.g = g;
-      return true;
-    },
+    [&](long long gslot, AdjState& st) -> bool { return path_adj_setup(P, gslot, st, vhint, cnt); },
     [&](AdjState& st) {
-    const ViewDesc& V = *st.V;
-    const CameraDesc& cam = V.cam;
-    const PathSmp S{&P, V.seed, st.gslot, st.p + V.slot_off};
-    const F3 org = cam_pos(cam);
-    const F3 g = st.g;
-    const Hit h = st.h;
-    // ---- forward replay, recording vertices and factor values ----
-    VRec vr[MAXD + 2];
-    // per bounce: the NEE light sample and the continuation pdf (the light's
-    // radiance is recomputed in the reverse pass from the same values)
-    struct LRec { int ltri; float lu, lv, lpdf, lmis, ppdf; };
-    LRec br[MAXD + 1];
-    bool nee_on[MAXD + 2];
-    F3 Tk[MAXD + 2], Mk[MAXD + 2];
-    SurfF x = post_intersect(s, h.tri, h.u, h.v);
-    vr[1] = {h.tri, h.u, h.v};
-    const float t1 = camera_factor<float>(cam, x.p, x.ng, 1.f);
-    F3 T(t1, t1, t1);
-    F3 rdir = normalize(x.p - org);
-    Tk[1] = T;
-    Mk[1] = emitted(s, x, -rdir);
-    if (!finite3(T * Mk[1])) Mk[1] = F3z();
-    int K = 1;  // vertices reached
-    const int D = min(V.D, MAXD);
-    for (int k = 0; k <= D + 1; k++) nee_on[k] = false;
-    for (int b = 0; b < D; b++) {
-      const int k = b + 1;
-      const int o = 2 + 5 * b;
-      F3 c;
-      BounceRec R;
-      const bool more = radiance_step_k<TRN_SHARED_STEPS_PATHADJ>(s, x, rdir, T, S(o), S(o + 1), S(o + 2),
-                                      S(o + 3), S(o + 4), c, &R, cnt);
-      // a scrubbed (non-finite) bounce contributes nothing and carries no gradient
-      nee_on[k] = R.nee_ok && !R.scrubbed;
-      br[k] = {R.ltri, R.lu, R.lv, R.lpdf, R.lmis, R.prev_pdf};
-      if (!more) break;
-      vr[k + 1] = {x.tri, x.u, x.v};
-      Tk[k + 1] = T;
-      Mk[k + 1] = (R.scrubbed || R.emis == 0.f) ? F3z() : R.eLe * R.emis;
-      K = k + 1;
-      if (T.x == 0.f && T.y == 0.f && T.z == 0.f) break;
-    }
-    // ---- reverse pass: a_k = g*(N_k + M_k) + phi_k * a_{k+1}, one vertex window at a time ----
-    struct VG { F3 p, ns, ng, kd; long long texel; int bsdf; };
-    auto load_vg = [&](int k) {
-      VG r;
-      const SurfF xs = post_intersect(s, vr[k].tri, vr[k].u, vr[k].v);
-      r.p = xs.p; r.ns = xs.ns; r.ng = xs.ng; r.bsdf = xs.bsdf;
-      r.kd = bsdf_albedo(s, s.bsdfs[xs.bsdf], xs.tu, xs.tv, r.texel);
-      return r;
-    };
-    VG Gk = load_vg(K), Gn = Gk;
-    F3 a_next = F3z();
-    VAdj acc_next, acc_k, acc_prev;
-    vadj_zero(acc_next); vadj_zero(acc_k); vadj_zero(acc_prev);
-    for (int k = K; k >= 1; k--) {
-      VG Gp;
-      if (k >= 2) Gp = load_vg(k - 1);
-      else { Gp.p = org; Gp.ns = Gp.ng = Gp.kd = F3z(); Gp.texel = -1; Gp.bsdf = 0; }
-      const BsdfDesc b = s.bsdfs[Gk.bsdf];
-      const bool need_prev = b.type != kDiffuse;
-      const bool need_kd = P.diff_tex && Gk.texel >= 0;
-      F3 Nval = F3z(), Phi = F3z();
-      F3 gkd = F3z(), gprev = F3z();
-      if (k <= D && nee_on[k]) {
-        // NEE factor value and its reverse mode in one sweep
-        const LRec& R = br[k];
-        int j0, j1, j2; tri_vertices(s, R.ltri, j0, j1, j2);
-        const F3 y = bary3(R.lu, R.lv, load3(s.pos, j0), load3(s.pos, j1), load3(s.pos, j2));
-        const F3 nl = load3(s.fnormal, R.ltri);
-        // the forward step's emitter radiance (one-sided, AreaLight::Eval), same arithmetic
-        F3 wl = y - Gk.p;
-        wl = wl / sqrtf(dot(wl, wl));
-        const F3 Le = dot(-wl, nl) > 0.f ? light_radiance(s, s.emitter_id[R.ltri]) : F3z();
-        F3 gy = F3z(), gnl = F3z();
-        float gJl = 0.f;
-        Nval = nee_vjp(b, need_prev, need_kd, Gp.p, Gk.p, Gk.ns, Gk.ng, Gk.kd, y, nl, Le, R.lpdf, R.lmis,
-                       Tk[k] * g, gprev, acc_k.p, acc_k.ns, gkd, gy, gnl, gJl);
-        VAdj la; la.p = gy; la.ns = F3z(); la.ng = gnl; la.J = gJl;
-        scatter_vertex(P, V, R.ltri, R.lu, R.lv, la, cnt);
-      }
-      if (k < K) {
-        // continuation factor value and its reverse mode; a non-finite weight
-        // made the forward throughput non-finite: no value, no gradient
-        F3 cprev = F3z(), cx = F3z(), cns = F3z(), ckd = F3z(), cxn = F3z(), cngn = F3z();
-        float gJn = 0.f;
-        Phi = cont_vjp(b, need_prev, need_kd, Gp.p, Gk.p, Gk.ns, Gk.ng, Gk.kd, Gn.p, Gn.ng, br[k].ppdf,
-                       Tk[k] * a_next, cprev, cx, cns, ckd, cxn, cngn, gJn);
-        if (finite3(Phi)) {
-          gprev = gprev + cprev; acc_k.p = acc_k.p + cx; acc_k.ns = acc_k.ns + cns; gkd = gkd + ckd;
-          acc_next.p = acc_next.p + cxn; acc_next.ng = acc_next.ng + cngn; acc_next.J += gJn;
-        } else {
-          Phi = F3z();
-        }
-      }
-      const F3 a_k = g * (Nval + Mk[k]) + Phi * a_next;
-      if (k >= 2) acc_prev.p = acc_prev.p + gprev;
-      if (need_kd) { cnt.v[kCntTScatter]++; agg_add3(V.gtex, Gk.texel, gkd); }
-      // vertex k+1 has received all of its contributions
-      if (k < K) scatter_vertex(P, V, vr[k + 1].tri, vr[k + 1].u, vr[k + 1].v, acc_next, cnt);
-      acc_next = acc_k; acc_k = acc_prev; vadj_zero(acc_prev);
-      a_next = a_k; Gn = Gk; Gk = Gp;
-    }
-    // primary factor T1 = G / Detach(G) * J at vertex 1 (now in Gn / acc_next)
-    {
-      const float gam = a_next.x + a_next.y + a_next.z;
-      if (gam != 0.f && isfinite(gam)) {
-        F3 gp, gn;
-        float gJ;
-        camera_factor_grad(cam, Gn.p, Gn.ng, gam, gp, gn, gJ);
-        acc_next.p = acc_next.p + gp;
-        acc_next.ng = acc_next.ng + gn;
-        acc_next.J += gJ;
-      }
-    }
-    scatter_vertex(P, V, vr[1].tri, vr[1].u, vr[1].v, acc_next, cnt);
+      PathRec<MAXD> r;
+      path_replay<MAXD>(P, st, r, cnt);
+      path_reverse<MAXD>(P, r, cnt);
     });
+  flush_cnt(cnt, P.stats);
+}
+
+// Split form: k_path_replay traces and records every path into the queue;
+// k_path_reverse runs the reverse sweep over the queue. Each kernel carries
+// half of the fused kernel's code (the fused kernel is instruction-fetch
+// bound).
+template <int MAXD>
+__global__ void __launch_bounds__(256, TRN_MINB_PATHADJ) k_path_replay(Params P) {
+  Cnt cnt;
+  stage_top(P.s);
+  int vhint = 0;
+  PathRec<MAXD>* q = reinterpret_cast<PathRec<MAXD>*>(P.queue);
+  for_each_valid<AdjState>(P,
+    [&](long long gslot, AdjState& st) -> bool { return path_adj_setup(P, gslot, st, vhint, cnt); },
+    [&](AdjState& st) {
+      const unsigned act = __activemask();
+      const int lane = threadIdx.x & 31;
+      const int leader = __ffs(act) - 1;
+      unsigned long long base = 0;
+      if (lane == leader) base = atomicAdd(P.q_count, (unsigned long long)__popc(act));
+      base = __shfl_sync(act, base, leader);
+      const unsigned long long k = base + __popc(act & ((1u << lane) - 1u));
+      if (k >= (unsigned long long)P.q_cap) { atomicExch(P.err, 2); return; }
+      path_replay<MAXD>(P, st, q[k], cnt);
+    });
+  flush_cnt(cnt, P.stats);
+}
+
+template <int MAXD>
+__global__ void __launch_bounds__(256, TRN_MINB_PATHADJ) k_path_reverse(Params P) {
+  Cnt cnt;
+  stage_top(P.s);
+  const PathRec<MAXD>* q = reinterpret_cast<const PathRec<MAXD>*>(P.queue);
+  const unsigned long long n = min(*P.q_count, (unsigned long long)P.q_cap);
+  for (unsigned long long k = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; k < n;
+       k += (unsigned long long)gridDim.x * blockDim.x)
+    path_reverse<MAXD>(P, q[k], cnt);
   flush_cnt(cnt, P.stats);
 }
 
@@ -2080,6 +2155,38 @@ int ensure_queue(trn_viewset* vs, size_t need, cudaStream_t st) {
   return 0;
 }
 
+#ifndef TRN_PATHADJ_SPLIT
+#define TRN_PATHADJ_SPLIT 1
+#endif
+constexpr long long kPathRound = 1LL << 21;  // paths per split round of the interior adjoint
+
+// The split interior adjoint in rounds of at most kPathRound paths (a queue
+// of about 1.3 GB at depth <= 8).
+int path_adj_split(trn_viewset* vs, Params P, const trn_launch* ln, long long total, bool shallow, cudaStream_t st) {
+  const long long cap = std::min(total, kPathRound);
+  const size_t item = shallow ? sizeof(PathRec<8>) : sizeof(PathRec<kMaxDepth>);
+  if (ensure_queue(vs, item * (size_t)cap, st)) return -1;
+  P.queue = vs->iq;
+  P.q_count = vs->iq_count;
+  P.q_cap = cap;
+  int grid, block;
+  launch_dims(ln, cap, grid, block);
+  for (long long first = 0; first < total; first += cap) {
+    P.total = std::min(total, first + cap);
+    k_indirect_round<<<1, 32, 0, st>>>(P.work, (unsigned long long)first, P.q_count);
+    if (shallow) {
+      k_path_replay<8><<<grid, block, 0, st>>>(P);
+      k_path_reverse<8><<<grid, block, 0, st>>>(P);
+    } else {
+      k_path_replay<kMaxDepth><<<grid, block, 0, st>>>(P);
+      k_path_reverse<kMaxDepth><<<grid, block, 0, st>>>(P);
+    }
+    count_launch(3);
+  }
+  TRN_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
 // The split primary term in rounds of at most kIndirectRound slots.
 int primary_split(trn_viewset* vs, Params P, const trn_launch* ln, long long total, cudaStream_t st) {
   const long long cap = std::min(total, kIndirectRound);
@@ -2164,6 +2271,7 @@ int render_views(trn_scene* s, trn_viewset* vs, const trn_render_options* o, int
   const bool shallow = vs->max_depth <= 8;  // smaller per-thread path records
   switch (integrator) {
     case TRN_PATH_TRACER:
+      if (TRN_PATHADJ_SPLIT) return path_adj_split(vs, P, ln, total, shallow, st);
       if (shallow) launch(k_path_adj<8>, ln, total, P, st); else launch(k_path_adj<kMaxDepth>, ln, total, P, st);
       break;
     case TRN_PRIMARY_EDGE:

@@ -281,8 +281,10 @@ __device__ __forceinline__ float union_area(const float* a, const float* b) {
 
 // Nearest neighbour in the window; ties go to the smaller index, which keeps
 // at least one mutual pair (the smallest index among the closest pairs).
-__global__ void k_ploc_nn(int n, const float* cbox, int* nn) {
+__global__ void k_ploc_nn(const int* count, const float* cbox, int* nn) {
   __shared__ float sb[(kPlocBlock + 2 * kPlocR) * 6];
+  const int n = count[1];  // clusters of this round (the launch covers an upper bound)
+  if ((int)(blockIdx.x * kPlocBlock) >= n) return;
   const int start = blockIdx.x * kPlocBlock - kPlocR;
   for (int t = threadIdx.x; t < (kPlocBlock + 2 * kPlocR) * 6; t += blockDim.x) {
     const int c = start + t / 6;
@@ -303,10 +305,12 @@ __global__ void k_ploc_nn(int n, const float* cbox, int* nn) {
   nn[i] = bj;
 }
 
-__global__ void k_ploc_merge(int nleaf, int n, const int* nn, const int* cnode, const float* cbox, int* onode,
+__global__ void k_ploc_merge(int nleaf, int nmax, const int* nn, const int* cnode, const float* cbox, int* onode,
                              float* obox, int* flag, BvhNode* nodes, int* parent, int* counter) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+  if (i >= nmax) return;
+  const int n = counter[1];
+  if (i >= n) { flag[i] = 0; return; }
   const int j = nn[i];
   const float* bi = cbox + (size_t)6 * i;
   if (j >= 0 && nn[j] == i) {
@@ -329,16 +333,16 @@ __global__ void k_ploc_merge(int nleaf, int n, const int* nn, const int* cnode, 
   flag[i] = 1;
 }
 
-__global__ void k_ploc_compact(int n, const int* flag, const int* pos, const int* onode, const float* obox,
+__global__ void k_ploc_compact(int nmax, const int* flag, const int* pos, const int* onode, const float* obox,
                                int* cnode, float* cbox, int* count) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+  if (i >= nmax) return;
   if (flag[i]) {
     const int d = pos[i];
     cnode[d] = onode[i];
     for (int k = 0; k < 6; k++) cbox[6 * d + k] = obox[6 * i + k];
   }
-  if (i == n - 1) count[1] = pos[i] + flag[i];
+  if (i == nmax - 1) count[1] = pos[i] + flag[i];
 }
 
 __device__ __forceinline__ void write_child_box(BvhNode* nd, int side, const float lo[3], const float hi[3]) {
@@ -948,35 +952,41 @@ int configure_geometry(trn_scene* s, cudaStream_t st) {
   }
   return 0;
 }
-// PLOC rounds until one cluster is left; the cluster count is read back once
-// per round (about log-many rounds).
+// PLOC rounds until one cluster is left. The kernels read the round's cluster
+// count from the device (count[1]); the host launches for an upper bound and
+// reads the count back only every kPlocBatch rounds, so the GPU does not wait
+// on the host between rounds (rounds after convergence are no-ops).
+constexpr int kPlocBatch = 8;
 int ploc_build(trn_scene* s, cudaStream_t st) {
   const int nt = s->nt;
   int* cur_node = s->ploc_node;
   int* tmp_node = s->ploc_node + nt;
   float* cur_box = s->ploc_box;
   float* tmp_box = s->ploc_box + 6 * (size_t)nt;
-  TRN_CUDA_TRY(cudaMemsetAsync(s->ploc_count, 0, 2 * sizeof(int), st));
+  const int init[2] = {0, nt};
+  TRN_CUDA_TRY(cudaMemcpyAsync(s->ploc_count, init, sizeof(init), cudaMemcpyHostToDevice, st));
   k_ploc_init<<<nblk(nt), 256, 0, st>>>(nt, s->keys_alt, s->pos, s->idx, cur_node, cur_box);
   count_launch(1);
-  int n = nt;
-  for (int round = 0; n > 1; round++) {
-    if (round > 4 * nt) { set_error("trn_scene_configure: PLOC did not converge"); return -1; }
-    k_ploc_nn<<<(n + kPlocBlock - 1) / kPlocBlock, kPlocBlock, 0, st>>>(n, cur_box, s->ploc_nn);
-    k_ploc_merge<<<nblk(n), 256, 0, st>>>(nt, n, s->ploc_nn, cur_node, cur_box, tmp_node, tmp_box, s->ploc_flag,
-                                          s->nodes, s->parent, s->ploc_count);
-    size_t sb = s->scan_tmp_bytes;
-    if (cub::DeviceScan::ExclusiveSum(s->scan_tmp, sb, s->ploc_flag, s->ploc_pos, n, st) != cudaSuccess) {
-      set_error("trn_scene_configure: scan failed");
-      return -1;
+  int n = nt;  // upper bound of the device-side count
+  for (int batch = 0; n > 1; batch++) {
+    if (batch * kPlocBatch > 4 * nt + 64) { set_error("trn_scene_configure: PLOC did not converge"); return -1; }
+    for (int r = 0; r < kPlocBatch; r++) {
+      k_ploc_nn<<<(n + kPlocBlock - 1) / kPlocBlock, kPlocBlock, 0, st>>>(s->ploc_count, cur_box, s->ploc_nn);
+      k_ploc_merge<<<nblk(n), 256, 0, st>>>(nt, n, s->ploc_nn, cur_node, cur_box, tmp_node, tmp_box, s->ploc_flag,
+                                            s->nodes, s->parent, s->ploc_count);
+      size_t sb = s->scan_tmp_bytes;
+      if (cub::DeviceScan::ExclusiveSum(s->scan_tmp, sb, s->ploc_flag, s->ploc_pos, n, st) != cudaSuccess) {
+        set_error("trn_scene_configure: scan failed");
+        return -1;
+      }
+      k_ploc_compact<<<nblk(n), 256, 0, st>>>(n, s->ploc_flag, s->ploc_pos, tmp_node, tmp_box, cur_node, cur_box,
+                                              s->ploc_count);
+      count_launch(4);
     }
-    k_ploc_compact<<<nblk(n), 256, 0, st>>>(n, s->ploc_flag, s->ploc_pos, tmp_node, tmp_box, cur_node, cur_box,
-                                            s->ploc_count);
-    count_launch(4);
     int counts[2];
     TRN_CUDA_TRY(cudaMemcpyAsync(counts, s->ploc_count, sizeof(counts), cudaMemcpyDeviceToHost, st));
     TRN_CUDA_TRY(cudaStreamSynchronize(st));
-    if (counts[1] >= n) { set_error("trn_scene_configure: PLOC round merged nothing"); return -1; }
+    if (counts[1] >= n && n > 1) { set_error("trn_scene_configure: PLOC rounds merged nothing"); return -1; }
     n = counts[1];
   }
   const int root_parent = -1;
