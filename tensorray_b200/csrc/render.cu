@@ -48,8 +48,10 @@ struct Params {
   const float* aq_poly;       // [E] leaf weights
   const float* aq_cdf;        // [E] leaf distribution
   const float* aq_int;        // [2] integral, sum of weight x volume
-  // queue of the split indirect boundary term (nullptr = fused kernel)
+  // queues of the split kernels (nullptr = fused kernel): q_count[0] counts
+  // `queue`, q_count[1] counts `queue2` (the indirect term's second stage)
   void* queue;
+  void* queue2;
   unsigned long long* q_count;
   long long q_cap;
 };
@@ -1711,8 +1713,9 @@ template <int MAXD>
 __global__ void __launch_bounds__(256, TRN_MINB_INDIRECT) k_indirect_emitter(Params P) {
   Cnt cnt;
   stage_top(P.s);
-  const IndirectItem<MAXD>* q = reinterpret_cast<const IndirectItem<MAXD>*>(P.queue);
-  const unsigned long long n = min(*P.q_count, (unsigned long long)P.q_cap);
+  // two-stage form: the queue and its count; three-stage form: the second queue
+  const IndirectItem<MAXD>* q = reinterpret_cast<const IndirectItem<MAXD>*>(P.queue2 ? P.queue2 : P.queue);
+  const unsigned long long n = min(P.q_count[P.queue2 ? 1 : 0], (unsigned long long)P.q_cap);
   for (unsigned long long k = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; k < n;
        k += (unsigned long long)gridDim.x * blockDim.x) {
     const IndirectItem<MAXD>& it = q[k];
@@ -1727,10 +1730,102 @@ __global__ void __launch_bounds__(256, TRN_MINB_INDIRECT) k_indirect_emitter(Par
   flush_cnt(cnt, P.stats);
 }
 
+// Three-stage form of the indirect term: k_indirect_setup tests every slot
+// once (the two set-up rays are most of the term's rays) and queues the
+// accepted samples; k_indirect_sensor_q runs the sensor side over that queue
+// and queues survivors for k_indirect_emitter.
+struct IndirectSetupItem {
+  long long gslot, p;
+  int view, xe_tri, xs_tri, v0, v1, far_tri;
+  float xe_u, xe_v, xs_u, xs_v, w0, sedge;
+  F3 rdir, p0, n;
+};
+
+__global__ void __launch_bounds__(256, TRN_MINB_INDIRECT) k_indirect_setup(Params P) {
+  Cnt cnt;
+  stage_top(P.s);
+  int vhint = 0;
+  IndirectSetupItem* q = reinterpret_cast<IndirectSetupItem*>(P.queue);
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;
+  for (;;) {
+    unsigned long long start = 0;
+    if (lane == 0) start = atomicAdd(P.work, 32ull);
+    start = __shfl_sync(0xffffffffu, start, 0);
+    if ((long long)start >= P.total) break;
+    const long long g = (long long)start + lane;
+    EdgeState st;
+    const bool ok = g < P.total && indirect_setup(P, g, st, vhint, cnt);
+    const unsigned m = __ballot_sync(0xffffffffu, ok);
+    if (!m) continue;
+    const int leader = __ffs(m) - 1;
+    unsigned long long base = 0;
+    if (lane == leader) base = atomicAdd(P.q_count, (unsigned long long)__popc(m));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    const unsigned long long k = base + __popc(m & lt);
+    if (ok && k >= (unsigned long long)P.q_cap) atomicExch(P.err, 2);
+    if (ok && k < (unsigned long long)P.q_cap) {
+      IndirectSetupItem& it = q[k];
+      it.gslot = st.gslot; it.p = st.p; it.view = (int)(st.V - P.views);
+      it.xe_tri = st.xe.tri; it.xe_u = st.xe.u; it.xe_v = st.xe.v;
+      it.xs_tri = st.x.tri; it.xs_u = st.x.u; it.xs_v = st.x.v;
+      it.v0 = st.v0; it.v1 = st.v1; it.far_tri = st.far_tri; it.w0 = st.w0; it.sedge = st.sedge;
+      it.rdir = st.rdir; it.p0 = st.p0; it.n = st.n;
+    }
+  }
+  flush_cnt(cnt, P.stats);
+}
+
+template <int MAXD>
+__global__ void __launch_bounds__(256, TRN_MINB_INDIRECT) k_indirect_sensor_q(Params P) {
+  Cnt cnt;
+  stage_top(P.s);
+  const IndirectSetupItem* qa = reinterpret_cast<const IndirectSetupItem*>(P.queue);
+  IndirectItem<MAXD>* qb = reinterpret_cast<IndirectItem<MAXD>*>(P.queue2);
+  const unsigned long long n = min(P.q_count[0], (unsigned long long)P.q_cap);
+  const int lane = threadIdx.x & 31;
+  for (unsigned long long k0 = (blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x) & ~31ull; k0 < n;
+       k0 += (unsigned long long)gridDim.x * blockDim.x) {
+    const unsigned long long k = k0 + lane;
+    bool push = false;
+    EdgeState st;
+    F3 sc[MAXD];
+    int D = 0, bmin = 0;
+    if (k < n) {
+      const IndirectSetupItem& a = qa[k];
+      st.V = P.views + a.view; st.gslot = a.gslot; st.p = a.p;
+      st.x = post_intersect(P.s, a.xs_tri, a.xs_u, a.xs_v);
+      st.rdir = a.rdir;
+      D = min(st.V->D, MAXD);
+      bmin = indirect_sensor<MAXD>(P, st, D, sc, cnt);
+      push = bmin < D - 1;
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, push);
+    if (!m) continue;
+    const int leader = __ffs(m) - 1;
+    unsigned long long base = 0;
+    if (lane == leader) base = atomicAdd(P.q_count + 1, (unsigned long long)__popc(m));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    const unsigned long long j = base + __popc(m & ((1u << lane) - 1u));
+    if (push && j >= (unsigned long long)P.q_cap) atomicExch(P.err, 2);
+    if (push && j < (unsigned long long)P.q_cap) {
+      const IndirectSetupItem& a = qa[k];
+      IndirectItem<MAXD>& it = qb[j];
+      it.gslot = a.gslot; it.p = a.p; it.view = a.view; it.jmax = D - 2 - bmin; it.D = D;
+      it.xe_tri = a.xe_tri; it.xe_u = a.xe_u; it.xe_v = a.xe_v;
+      it.xs_tri = a.xs_tri; it.xs_u = a.xs_u; it.xs_v = a.xs_v;
+      it.rdir = a.rdir; it.p0 = a.p0; it.n = a.n; it.w0 = a.w0; it.sedge = a.sedge;
+      it.v0 = a.v0; it.v1 = a.v1; it.far_tri = a.far_tri;
+      for (int b = 0; b < D - 1; b++) it.sc[b] = sc[b];
+    }
+  }
+  flush_cnt(cnt, P.stats);
+}
+
 // Slot range of one split round: the work counter starts at `first`, the
 // queue is empty.
 __global__ void k_indirect_round(unsigned long long* work, unsigned long long first, unsigned long long* q_count) {
-  if (threadIdx.x == 0) { *work = first; *q_count = 0ull; }
+  if (threadIdx.x == 0) { *work = first; q_count[0] = 0ull; q_count[1] = 0ull; }
 }
 
 
@@ -2059,6 +2154,7 @@ Params base_params(trn_scene* s, trn_viewset* vs, const trn_render_options* o, i
   P.stats = s->stats_on ? s->stats : nullptr;
   P.aq_poly = P.aq_cdf = P.aq_int = nullptr;
   P.queue = nullptr;
+  P.queue2 = nullptr;
   P.q_count = nullptr;
   P.q_cap = 0;
   return P;
@@ -2148,7 +2244,7 @@ int ensure_queue(trn_viewset* vs, size_t need, cudaStream_t st) {
     if (cudaMalloc(&vs->iq, need) != cudaSuccess) { set_error("boundary term: out of memory for its queue"); return -1; }
     vs->iq_bytes = need;
   }
-  if (!vs->iq_count && cudaMalloc(&vs->iq_count, sizeof(unsigned long long)) != cudaSuccess) {
+  if (!vs->iq_count && cudaMalloc(&vs->iq_count, 2 * sizeof(unsigned long long)) != cudaSuccess) {
     set_error("boundary term: out of memory");
     return -1;
   }
@@ -2207,12 +2303,21 @@ int primary_split(trn_viewset* vs, Params P, const trn_launch* ln, long long tot
   return 0;
 }
 
-// The split indirect term in rounds of at most kIndirectRound slots.
+#ifndef TRN_INDIRECT_STAGES
+#define TRN_INDIRECT_STAGES 3
+#endif
+
+// The split indirect term in rounds of at most kIndirectRound slots: two
+// stages (set-up + sensor side, emitter side) or three (set-up, sensor side,
+// emitter side; the default).
 int indirect_split(trn_viewset* vs, Params P, const trn_launch* ln, long long total, bool shallow, cudaStream_t st) {
   const long long cap = std::min(total, kIndirectRound);
   const size_t item = shallow ? sizeof(IndirectItem<8>) : sizeof(IndirectItem<kMaxDepth>);
-  if (ensure_queue(vs, item * (size_t)cap, st)) return -1;
+  const size_t item_a = TRN_INDIRECT_STAGES == 3 ? sizeof(IndirectSetupItem) : 0;
+  const size_t bytes_a = (item_a * (size_t)cap + 255) / 256 * 256;
+  if (ensure_queue(vs, bytes_a + item * (size_t)cap, st)) return -1;
   P.queue = vs->iq;
+  P.queue2 = TRN_INDIRECT_STAGES == 3 ? static_cast<char*>(vs->iq) + bytes_a : nullptr;
   P.q_count = vs->iq_count;
   P.q_cap = cap;
   int grid, block;
@@ -2220,14 +2325,26 @@ int indirect_split(trn_viewset* vs, Params P, const trn_launch* ln, long long to
   for (long long first = 0; first < total; first += cap) {
     P.total = std::min(total, first + cap);
     k_indirect_round<<<1, 32, 0, st>>>(P.work, (unsigned long long)first, P.q_count);
-    if (shallow) {
-      k_indirect_sensor<8><<<grid, block, 0, st>>>(P);
-      k_indirect_emitter<8><<<grid, block, 0, st>>>(P);
+    if (TRN_INDIRECT_STAGES == 3) {
+      k_indirect_setup<<<grid, block, 0, st>>>(P);
+      if (shallow) {
+        k_indirect_sensor_q<8><<<grid, block, 0, st>>>(P);
+        k_indirect_emitter<8><<<grid, block, 0, st>>>(P);
+      } else {
+        k_indirect_sensor_q<kMaxDepth><<<grid, block, 0, st>>>(P);
+        k_indirect_emitter<kMaxDepth><<<grid, block, 0, st>>>(P);
+      }
+      count_launch(4);
     } else {
-      k_indirect_sensor<kMaxDepth><<<grid, block, 0, st>>>(P);
-      k_indirect_emitter<kMaxDepth><<<grid, block, 0, st>>>(P);
+      if (shallow) {
+        k_indirect_sensor<8><<<grid, block, 0, st>>>(P);
+        k_indirect_emitter<8><<<grid, block, 0, st>>>(P);
+      } else {
+        k_indirect_sensor<kMaxDepth><<<grid, block, 0, st>>>(P);
+        k_indirect_emitter<kMaxDepth><<<grid, block, 0, st>>>(P);
+      }
+      count_launch(3);
     }
-    count_launch(3);
   }
   TRN_CUDA_TRY(cudaGetLastError());
   return 0;
