@@ -1222,14 +1222,16 @@ TRN_D bool primary_setup(const Params& P, long long gslot, EdgeState& st, int& v
 
 // Primary boundary body: detached radiance along the camera ray through the
 // sensor point (BoundaryPrimary.cpp:150-175), then the xDotN scatter.
+// (also the pixel boundary's body: its samples start at dimension 1 and its
+// edge point is not a scene parameter, v0 = v1 = -1)
 TRN_D void primary_body(const Params& P, const ViewDesc& V, long long gslot, long long p, SurfF x, F3 rdir, F3 T,
                         float w0, const F3& g, int v0, int v1, float sedge, const F3& p0, int far_tri, const F3& n,
-                        Cnt& cnt) {
+                        Cnt& cnt, int dim0 = 2) {
   const DeviceScene& s = P.s;
   const PathSmp S{&P, V.seed, gslot, p + V.slot_off};
   F3 L = scrub(T * emitted(s, x, -rdir));
   for (int b = 0; b < V.D; b++) {
-    const int o = 2 + 5 * b;
+    const int o = dim0 + 5 * b;
     F3 c;
     const bool more = radiance_step_k<TRN_SHARED_STEPS_PRIMARY>(s, x, rdir, T, S(o), S(o + 1), S(o + 2), S(o + 3),
                                                                 S(o + 4), c, nullptr, cnt);
@@ -1260,7 +1262,7 @@ __global__ void __launch_bounds__(256, TRN_MINB) k_primary_adj(Params P) {
 // radiance path and the scatter for the queue.
 struct PrimaryItem {
   long long gslot, p;
-  int view, x_tri;
+  int view, x_tri, dim0, pad_;
   float x_u, x_v, T0, w0, sedge;
   int v0, v1, far_tri;
   F3 rdir, p0, n, g;
@@ -1291,7 +1293,7 @@ __global__ void __launch_bounds__(256, TRN_MINB) k_primary_setup(Params P) {
     if (ok && k >= (unsigned long long)P.q_cap) atomicExch(P.err, 2);
     if (ok && k < (unsigned long long)P.q_cap) {
       PrimaryItem& it = q[k];
-      it.gslot = st.gslot; it.p = st.p; it.view = (int)(st.V - P.views);
+      it.gslot = st.gslot; it.p = st.p; it.view = (int)(st.V - P.views); it.dim0 = 2;
       it.x_tri = st.x.tri; it.x_u = st.x.u; it.x_v = st.x.v; it.T0 = st.T0.x; it.w0 = st.w0; it.sedge = st.sedge;
       it.v0 = st.v0; it.v1 = st.v1; it.far_tri = st.far_tri;
       it.rdir = st.rdir; it.p0 = st.p0; it.n = st.n; it.g = st.g;
@@ -1310,7 +1312,7 @@ __global__ void __launch_bounds__(256, TRN_MINB) k_primary_body(Params P) {
     const PrimaryItem& it = q[k];
     const SurfF x = post_intersect(P.s, it.x_tri, it.x_u, it.x_v);
     primary_body(P, P.views[it.view], it.gslot, it.p, x, it.rdir, F3(it.T0, it.T0, it.T0), it.w0, it.g, it.v0, it.v1,
-                 it.sedge, it.p0, it.far_tri, it.n, cnt);
+                 it.sedge, it.p0, it.far_tri, it.n, cnt, it.dim0);
   }
   flush_cnt(cnt, P.stats);
 }
@@ -1832,85 +1834,113 @@ __global__ void k_indirect_round(unsigned long long* work, unsigned long long fi
 // ---------------------------------------------------------------------------
 // pixel boundary (BoundaryPixel.cpp:36-159, Edge.cpp:377-409, Camera.cpp:433-467)
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256, TRN_MINB) k_pixel_adj(Params P) {
+// Pixel boundary set-up (SampleBoundarySegmentPixel, Edge.cpp:377-409;
+// GeneratePixelBoundarySamples, Camera.cpp:433-467): a point on the pixel's
+// boundary from the antithetic copy's sample, the camera ray through it, the
+// boundary geometry. Returns false for a rejected sample.
+TRN_D bool pixel_setup(const Params& P, long long gslot, EdgeState& st, int& vhint, Cnt& cnt) {
   const DeviceScene& s = P.s;
+  const ViewDesc& V = view_of(P, gslot, vhint);
+  const long long p = gslot - V.begin;
+  const CameraDesc& cam = V.cam;
+  const int W_ = cam.w, WH = cam.w * cam.h;
+  const F3 cpos = cam_pos(cam);
+  const long long nanti = V.n / 4;
+  const long long slot = p % nanti;
+  const int anti = (int)(p / nanti);
+  // the 4 antithetic copies of a slot share its samples (BoundaryPixel.cpp:135-138)
+  const PathSmp S{&P, V.seed, V.begin / 4 + slot, slot + V.slot_off};
+  const float r = S(0);
+  float rr;
+  if (anti == 0) rr = r;
+  else if (anti == 1) rr = r < 0.5f ? r + 0.5f : r - 0.5f;
+  else if (anti == 2) rr = r < 0.75f ? 0.75f - r : 1.75f - r;
+  else rr = r < 0.25f ? 0.25f - r : 1.25f - r;
+  const float r4 = rr * 4.f;
+  const int bi = (int)floorf(r4);
+  float ox, oy;
+  if (bi == 0) { ox = 0.f; oy = r4; }
+  else if (bi == 1) { ox = r4 - 1.f; oy = 1.f; }
+  else if (bi == 2) { ox = 1.f; oy = 3.f - r4; }
+  else { ox = 4.f - r4; oy = 0.f; }
+  const int bsel = bi < 0 ? 0 : (bi > 3 ? 3 : bi);
+  const float pdf = (bsel & 1) ? 0.25f / (cam.plane_len_x * (float)cam.h) : 0.25f / (cam.plane_len_y * (float)cam.w);
+  const F3 dedge = (bsel & 1) ? F3(1.f, 0.f, 0.f) : F3(0.f, 1.f, 0.f);
+  const F3 dvis = bsel == 0 ? F3(1.f, 0.f, 0.f) : (bsel == 1 ? F3(0.f, -1.f, 0.f)
+                                                : (bsel == 2 ? F3(-1.f, 0.f, 0.f) : F3(0.f, 1.f, 0.f)));
+  const F3 edge = normalize(xform_vector(cam.raster_to_world, dedge));
+  const F3 edge2 = normalize(xform_vector(cam.raster_to_world, dvis));
+  const int pixel = (int)(p % WH);
+  const F3 p0 = xform_point(cam.raster_to_world, F3((float)(pixel % W_) + ox, (float)(pixel / W_) + oy, 0.f));
+  const F3 dir = normalize(p0 - cpos);
+  Hit h;
+  cnt.v[kCntClosest]++;
+  if (!trace_k<TRN_SETUP_SHARED_PIXEL, false>(s, p0, dir, kShadowEps, kRayMax, h, P.err)) return false;
+  const F3 hitP = p0 + dir * h.t;
+  const SensorSample sds = sample_direct(cam, hitP);
+  const F3 dirc = sensor_ray_dir(cam, sds.qx, sds.qy);
+  const SurfF x = post_intersect(s, h.tri, h.u, h.v);
+  const float dist = length(x.p - cpos);
+  const float dist1 = length(p0 - cpos);
+  const float cos2 = fabsf(dot(x.ng, -dirc));
+  F3 n;
+  // BoundaryPixel.cpp:92 reverses the sign convention
+  const float bval = -base_val(dist / dist1, edge, dirc, x.ng, edge2, n) * cos2;
+  const F3 g = g_at(P, V, pixel);
+  if (bval == 0.f || (g.x == 0.f && g.y == 0.f && g.z == 0.f)) return false;
+  st.V = &V; st.gslot = V.begin / 4 + slot; st.p = slot; st.x = x; st.rdir = dirc;
+  st.T0 = F3(sds.sensor_val, sds.sensor_val, sds.sensor_val);
+  st.p0 = p0; st.n = n; st.w0 = bval / pdf; st.far_tri = h.tri; st.g = g;
+  return true;
+}
+
+__global__ void __launch_bounds__(256, TRN_MINB) k_pixel_adj(Params P) {
   Cnt cnt;
   stage_top(P.s);
   int vhint = 0;
   for_each_valid<EdgeState>(P,
-    [&](long long gslot, EdgeState& st) -> bool {
-      const ViewDesc& V = view_of(P, gslot, vhint);
-      const long long p = gslot - V.begin;
-      const CameraDesc& cam = V.cam;
-      const int W_ = cam.w, WH = cam.w * cam.h;
-      const F3 cpos = cam_pos(cam);
-      const long long nanti = V.n / 4;
-      const long long slot = p % nanti;
-      const int anti = (int)(p / nanti);
-      // the 4 antithetic copies of a slot share its samples (BoundaryPixel.cpp:135-138)
-      const PathSmp S{&P, V.seed, V.begin / 4 + slot, slot + V.slot_off};
-      const float r = S(0);
-      float rr;
-      if (anti == 0) rr = r;
-      else if (anti == 1) rr = r < 0.5f ? r + 0.5f : r - 0.5f;
-      else if (anti == 2) rr = r < 0.75f ? 0.75f - r : 1.75f - r;
-      else rr = r < 0.25f ? 0.25f - r : 1.25f - r;
-      const float r4 = rr * 4.f;
-      const int bi = (int)floorf(r4);
-      float ox, oy;
-      if (bi == 0) { ox = 0.f; oy = r4; }
-      else if (bi == 1) { ox = r4 - 1.f; oy = 1.f; }
-      else if (bi == 2) { ox = 1.f; oy = 3.f - r4; }
-      else { ox = 4.f - r4; oy = 0.f; }
-      const int bsel = bi < 0 ? 0 : (bi > 3 ? 3 : bi);
-      const float pdf = (bsel & 1) ? 0.25f / (cam.plane_len_x * (float)cam.h) : 0.25f / (cam.plane_len_y * (float)cam.w);
-      const F3 dedge = (bsel & 1) ? F3(1.f, 0.f, 0.f) : F3(0.f, 1.f, 0.f);
-      const F3 dvis = bsel == 0 ? F3(1.f, 0.f, 0.f) : (bsel == 1 ? F3(0.f, -1.f, 0.f)
-                                                    : (bsel == 2 ? F3(-1.f, 0.f, 0.f) : F3(0.f, 1.f, 0.f)));
-      const F3 edge = normalize(xform_vector(cam.raster_to_world, dedge));
-      const F3 edge2 = normalize(xform_vector(cam.raster_to_world, dvis));
-      const int pixel = (int)(p % WH);
-      const F3 p0 = xform_point(cam.raster_to_world, F3((float)(pixel % W_) + ox, (float)(pixel / W_) + oy, 0.f));
-      const F3 dir = normalize(p0 - cpos);
-      Hit h;
-      cnt.v[kCntClosest]++;
-      if (!trace_k<TRN_SETUP_SHARED_PIXEL, false>(s, p0, dir, kShadowEps, kRayMax, h, P.err)) return false;
-      const F3 hitP = p0 + dir * h.t;
-      const SensorSample sds = sample_direct(cam, hitP);
-      const F3 dirc = sensor_ray_dir(cam, sds.qx, sds.qy);
-      const SurfF x = post_intersect(s, h.tri, h.u, h.v);
-      const float dist = length(x.p - cpos);
-      const float dist1 = length(p0 - cpos);
-      const float cos2 = fabsf(dot(x.ng, -dirc));
-      F3 n;
-      // BoundaryPixel.cpp:92 reverses the sign convention
-      const float bval = -base_val(dist / dist1, edge, dirc, x.ng, edge2, n) * cos2;
-      const F3 g = g_at(P, V, pixel);
-      if (bval == 0.f || (g.x == 0.f && g.y == 0.f && g.z == 0.f)) return false;
-      st.V = &V; st.gslot = V.begin / 4 + slot; st.p = slot; st.x = x; st.rdir = dirc;
-      st.T0 = F3(sds.sensor_val, sds.sensor_val, sds.sensor_val);
-      st.p0 = p0; st.n = n; st.w0 = bval / pdf; st.far_tri = h.tri; st.g = g;
-      return true;
-    },
+    [&](long long gslot, EdgeState& st) -> bool { return pixel_setup(P, gslot, st, vhint, cnt); },
     [&](EdgeState& st) {
-      const ViewDesc& V = *st.V;
-      const PathSmp S{&P, V.seed, st.gslot, st.p + V.slot_off};
-      SurfF x = st.x;
-      F3 T = st.T0, rdir = st.rdir;
-      F3 L = scrub(T * emitted(s, x, -rdir));
-      for (int b = 0; b < V.D; b++) {
-        const int o = 1 + 5 * b;
-        F3 c;
-        const bool more = radiance_step_k<TRN_SHARED_STEPS_PIXEL>(s, x, rdir, T, S(o), S(o + 1), S(o + 2), S(o + 3), S(o + 4), c, nullptr,
-                                        cnt);
-        L = L + c;
-        if (!more || (T.x == 0.f && T.y == 0.f && T.z == 0.f)) break;
-      }
-      const float Wt = dot(st.g, L * st.w0);
-      if (Wt == 0.f || !isfinite(Wt)) return;
       // the pixel-edge point is not a scene parameter: only the hit triangle moves
-      xdotn_vjp(P, V, Wt, cam_pos(V.cam), false, -1, 0.f, 0.f, -1, -1, 0.f, st.p0, st.far_tri, st.n, cnt);
+      primary_body(P, *st.V, st.gslot, st.p, st.x, st.rdir, st.T0, st.w0, st.g, -1, -1, 0.f, st.p0, st.far_tri,
+                   st.n, cnt, 1);
     });
+  flush_cnt(cnt, P.stats);
+}
+
+// Split form: k_pixel_setup queues the accepted samples as PrimaryItem
+// (dimension 1 onwards, no edge vertices); k_primary_body runs them.
+__global__ void __launch_bounds__(256, TRN_MINB) k_pixel_setup(Params P) {
+  Cnt cnt;
+  stage_top(P.s);
+  int vhint = 0;
+  PrimaryItem* q = reinterpret_cast<PrimaryItem*>(P.queue);
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;
+  for (;;) {
+    unsigned long long start = 0;
+    if (lane == 0) start = atomicAdd(P.work, 32ull);
+    start = __shfl_sync(0xffffffffu, start, 0);
+    if ((long long)start >= P.total) break;
+    const long long g = (long long)start + lane;
+    EdgeState st;
+    const bool ok = g < P.total && pixel_setup(P, g, st, vhint, cnt);
+    const unsigned m = __ballot_sync(0xffffffffu, ok);
+    if (!m) continue;
+    const int leader = __ffs(m) - 1;
+    unsigned long long base = 0;
+    if (lane == leader) base = atomicAdd(P.q_count, (unsigned long long)__popc(m));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    const unsigned long long k = base + __popc(m & lt);
+    if (ok && k >= (unsigned long long)P.q_cap) atomicExch(P.err, 2);
+    if (ok && k < (unsigned long long)P.q_cap) {
+      PrimaryItem& it = q[k];
+      it.gslot = st.gslot; it.p = st.p; it.view = (int)(st.V - P.views); it.dim0 = 1;
+      it.x_tri = st.x.tri; it.x_u = st.x.u; it.x_v = st.x.v; it.T0 = st.T0.x; it.w0 = st.w0; it.sedge = 0.f;
+      it.v0 = -1; it.v1 = -1; it.far_tri = st.far_tri;
+      it.rdir = st.rdir; it.p0 = st.p0; it.n = st.n; it.g = st.g;
+    }
+  }
   flush_cnt(cnt, P.stats);
 }
 
@@ -2283,6 +2313,30 @@ int path_adj_split(trn_viewset* vs, Params P, const trn_launch* ln, long long to
   return 0;
 }
 
+#ifndef TRN_PIXEL_SPLIT
+#define TRN_PIXEL_SPLIT 1
+#endif
+
+// The split pixel boundary term in rounds of at most kIndirectRound samples.
+int pixel_split(trn_viewset* vs, Params P, const trn_launch* ln, long long total, cudaStream_t st) {
+  const long long cap = std::min(total, kIndirectRound);
+  if (ensure_queue(vs, sizeof(PrimaryItem) * (size_t)cap, st)) return -1;
+  P.queue = vs->iq;
+  P.q_count = vs->iq_count;
+  P.q_cap = cap;
+  int grid, block;
+  launch_dims(ln, cap, grid, block);
+  for (long long first = 0; first < total; first += cap) {
+    P.total = std::min(total, first + cap);
+    k_indirect_round<<<1, 32, 0, st>>>(P.work, (unsigned long long)first, P.q_count);
+    k_pixel_setup<<<grid, block, 0, st>>>(P);
+    k_primary_body<<<grid, block, 0, st>>>(P);
+    count_launch(3);
+  }
+  TRN_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
 // The split primary term in rounds of at most kIndirectRound slots.
 int primary_split(trn_viewset* vs, Params P, const trn_launch* ln, long long total, cudaStream_t st) {
   const long long cap = std::min(total, kIndirectRound);
@@ -2400,7 +2454,10 @@ int render_views(trn_scene* s, trn_viewset* vs, const trn_render_options* o, int
       if (TRN_INDIRECT_SPLIT) return indirect_split(vs, P, ln, total, shallow, st);
       if (shallow) launch(k_indirect_adj<8>, ln, total, P, st); else launch(k_indirect_adj<kMaxDepth>, ln, total, P, st);
       break;
-    default: launch(k_pixel_adj, ln, total, P, st); break;
+    default:
+      if (TRN_PIXEL_SPLIT) return pixel_split(vs, P, ln, total, st);
+      launch(k_pixel_adj, ln, total, P, st);
+      break;
   }
   TRN_CUDA_TRY(cudaGetLastError());
   return 0;
