@@ -970,6 +970,58 @@ __global__ void __launch_bounds__(256, TRN_MINB_PATHADJ) k_path_adj(Params P) {
   flush_cnt(cnt, P.stats);
 }
 
+// Path records of the split interior adjoint in structure-of-arrays layout:
+// field k of path i lives at k * cap + i, so the lanes of a warp (consecutive
+// queue slots) read and write consecutive addresses. PathRecSoA gives the same
+// member syntax as PathRec over that layout.
+template <class T>
+struct Strided {
+  T* b;
+  long long s;
+  TRN_D T& operator[](int k) const { return b[(long long)k * s]; }
+};
+
+template <int MAXD>
+struct PathRecSoA {
+  long long& gslot;
+  long long& p;
+  int& view;
+  int& K;
+  int& D;
+  unsigned& nee_mask;
+  F3& g;
+  Strided<VRec> vr;
+  Strided<LRec> br;
+  Strided<F3> Tk, Mk;
+};
+
+template <int MAXD>
+TRN_HD size_t path_soa_bytes(long long cap) {
+  return (size_t)cap * (2 * sizeof(long long) + 3 * sizeof(int) + sizeof(unsigned) + sizeof(F3) +
+                        (MAXD + 2) * sizeof(VRec) + (MAXD + 1) * sizeof(LRec) + 2 * (MAXD + 2) * sizeof(F3)) +
+         16 * 256;
+}
+
+template <int MAXD>
+TRN_D PathRecSoA<MAXD> path_soa(void* base, long long cap, long long i) {
+  char* c = static_cast<char*>(base);
+  auto take = [&](size_t bytes) { char* r = c; c += (bytes + 255) / 256 * 256; return r; };
+  long long* gslot = reinterpret_cast<long long*>(take(sizeof(long long) * cap));
+  long long* pp = reinterpret_cast<long long*>(take(sizeof(long long) * cap));
+  int* view = reinterpret_cast<int*>(take(sizeof(int) * cap));
+  int* K = reinterpret_cast<int*>(take(sizeof(int) * cap));
+  int* D = reinterpret_cast<int*>(take(sizeof(int) * cap));
+  unsigned* nee = reinterpret_cast<unsigned*>(take(sizeof(unsigned) * cap));
+  F3* g = reinterpret_cast<F3*>(take(sizeof(F3) * cap));
+  VRec* vr = reinterpret_cast<VRec*>(take(sizeof(VRec) * (MAXD + 2) * cap));
+  LRec* br = reinterpret_cast<LRec*>(take(sizeof(LRec) * (MAXD + 1) * cap));
+  F3* Tk = reinterpret_cast<F3*>(take(sizeof(F3) * (MAXD + 2) * cap));
+  F3* Mk = reinterpret_cast<F3*>(take(sizeof(F3) * (MAXD + 2) * cap));
+  return PathRecSoA<MAXD>{gslot[i], pp[i], view[i], K[i], D[i], nee[i], g[i],
+                          Strided<VRec>{vr + i, cap}, Strided<LRec>{br + i, cap},
+                          Strided<F3>{Tk + i, cap}, Strided<F3>{Mk + i, cap}};
+}
+
 // Split form: k_path_replay traces and records every path into the queue;
 // k_path_reverse runs the reverse sweep over the queue. Each kernel carries
 // half of the fused kernel's code (the fused kernel is instruction-fetch
@@ -979,7 +1031,6 @@ __global__ void __launch_bounds__(256, TRN_MINB_PATHADJ) k_path_replay(Params P)
   Cnt cnt;
   stage_top(P.s);
   int vhint = 0;
-  PathRec<MAXD>* q = reinterpret_cast<PathRec<MAXD>*>(P.queue);
   for_each_valid<AdjState>(P,
     [&](long long gslot, AdjState& st) -> bool { return path_adj_setup(P, gslot, st, vhint, cnt); },
     [&](AdjState& st) {
@@ -991,7 +1042,8 @@ __global__ void __launch_bounds__(256, TRN_MINB_PATHADJ) k_path_replay(Params P)
       base = __shfl_sync(act, base, leader);
       const unsigned long long k = base + __popc(act & ((1u << lane) - 1u));
       if (k >= (unsigned long long)P.q_cap) { atomicExch(P.err, 2); return; }
-      path_replay<MAXD>(P, st, q[k], cnt);
+      PathRecSoA<MAXD> r = path_soa<MAXD>(P.queue, P.q_cap, (long long)k);
+      path_replay<MAXD>(P, st, r, cnt);
     });
   flush_cnt(cnt, P.stats);
 }
@@ -1000,11 +1052,12 @@ template <int MAXD>
 __global__ void __launch_bounds__(256, TRN_MINB_PATHADJ) k_path_reverse(Params P) {
   Cnt cnt;
   stage_top(P.s);
-  const PathRec<MAXD>* q = reinterpret_cast<const PathRec<MAXD>*>(P.queue);
   const unsigned long long n = min(*P.q_count, (unsigned long long)P.q_cap);
   for (unsigned long long k = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; k < n;
-       k += (unsigned long long)gridDim.x * blockDim.x)
-    path_reverse<MAXD>(P, q[k], cnt);
+       k += (unsigned long long)gridDim.x * blockDim.x) {
+    const PathRecSoA<MAXD> r = path_soa<MAXD>(P.queue, P.q_cap, (long long)k);
+    path_reverse<MAXD>(P, r, cnt);
+  }
   flush_cnt(cnt, P.stats);
 }
 
@@ -1320,102 +1373,170 @@ __global__ void __launch_bounds__(256, TRN_MINB) k_primary_body(Params P) {
 // ---------------------------------------------------------------------------
 // direct boundary (BoundaryDirect.cpp:38-143, Edge.cpp:90-144, 201-309)
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256, TRN_MINB) k_direct_adj(Params P) {
+// Direct boundary set-up (SampleBoundarySegmentDirect, Edge.cpp:108-144, with
+// AQ guiding when enabled; EvalBoundarySegmentDirect's geometry,
+// Edge.cpp:201-291). Returns false for a rejected sample.
+TRN_D bool direct_setup(const Params& P, long long gslot, EdgeState& st, int& vhint, Cnt& cnt) {
   const DeviceScene& s = P.s;
+  const ViewDesc& V = view_of(P, gslot, vhint);
+  const long long p = gslot - V.begin;
+  const PathSmp S{&P, V.seed, gslot, p + V.slot_off};
+  float r0 = S(0);
+  const float r1 = S(1), r2 = S(2);
+  float reuse;
+  const float integral = __ldg(P.eint);
+  if (!(integral > 0.f)) return false;
+  float pdf_b = 1.f;
+  if (P.aq_cdf) {
+    // AdaptiveQuadratureDistribution::sample (AQ_distrb.h:176-195): pick a
+    // leaf with the extra uniform, then place the edge coordinate in its box
+    if (!(__ldg(P.aq_int) > 0.f)) return false;
+    float unused;
+    const int leaf = sample_discrete(P.aq_cdf, P.ne, S(3 + 3 * V.D), unused);
+    const float lo = leaf > 0 ? __ldg(P.ecdf + leaf - 1) : 0.f, hi = __ldg(P.ecdf + leaf);
+    r0 = __fadd_rn(lo, __fmul_rn(r0, __fsub_rn(hi, lo)));
+    pdf_b = __fdiv_rn(__ldg(P.aq_poly + leaf), __ldg(P.aq_int + 1));
+  }
+  const int e = sample_discrete(P.ecdf, P.ne, r0, reuse);
+  const int v0 = P.edges[5 * e], v1 = P.edges[5 * e + 1], f0 = P.edges[5 * e + 2], f1 = P.edges[5 * e + 3],
+            v2 = P.edges[5 * e + 4];
+  const float len_e = P.efunc[e];
+  if (!(len_e > 0.f)) return false;
+  const float pdf_e = (len_e / (integral * (float)P.ne)) / len_e;
+  const F3 Pa = load3(s.pos, v0), Pb = load3(s.pos, v1), Pc = load3(s.pos, v2);
+  const F3 e1 = Pb - Pa;
+  const F3 p0 = Pa + e1 * reuse;
+  const F3 edge = normalize(e1), edge2 = normalize(Pc - Pa);
+  LightSample ls;
+  if (!light_sample(s, r1, r2, ls)) return false;
+  int j0, j1, j2; tri_vertices(s, ls.tri, j0, j1, j2);
+  const F3 p2 = bary3(ls.bu, ls.bv, load3(s.pos, j0), load3(s.pos, j1), load3(s.pos, j2));
+  const F3 nL = load3(s.fnormal, ls.tri);
+  const F3 ev = p2 - p0;
+  const float dist_sqr = dot(ev, ev);
+  const float dist = sqrtf(dist_sqr);
+  const F3 en = ev / dist;
+  const float cos_t = dot(nL, -en);
+  const F3 n0 = load3(s.fnormal, f0);
+  const F3 n1 = f1 >= 0 ? load3(s.fnormal, f1) : F3z();
+  const bool is_b = f1 < 0;
+  const float c0 = dot(en, n0), c1 = dot(en, n1);
+  const bool valid0 = fabsf(c0) > kEdgeEps;
+  const bool valid1 = (c0 > kEdgeEps && c1 < -kEdgeEps) || (c0 < -kEdgeEps && c1 > kEdgeEps);
+  const bool right = (is_b && valid0) || (!is_b && valid1);
+  if (!(right && cos_t > kEps && dist > kShadowEps)) return false;
+  const float pdf = pdf_e * ls.pdf * dist_sqr / cos_t * pdf_b;
+  const F3 rdir = normalize(p0 - p2);
+  Hit h0, h;
+  cnt.v[kCntClosest] += 2;
+  cnt.v[kCntLight]++;
+  if (!trace_k<TRN_SETUP_SHARED_DIRECT, false>(s, p0, -rdir, kShadowEps, kRayMax, h0, P.err)) return false;
+  if (!trace_k<TRN_SETUP_SHARED_DIRECT, false>(s, p0, rdir, kShadowEps, kRayMax, h, P.err)) return false;
+  const F3 hp = p0 + (-rdir) * h0.t;
+  if (!(length(hp - p2) < kShadowEps)) return false;
+  const SurfF xl = post_intersect(s, h0.tri, h0.u, h0.v);
+  const F3 E = emitted(s, xl, rdir);
+  const SurfF x = post_intersect(s, h.tri, h.u, h.v);
+  const float dl = length(p2 - x.p);
+  const float cos2 = fabsf(dot(nL, rdir));
+  const float its_t = length(x.p - p0);
+  F3 n;
+  const float bval = base_val(its_t / dl, edge, -rdir, nL, edge2, n) * cos2;
+  if (bval == 0.f || (E.x == 0.f && E.y == 0.f && E.z == 0.f)) return false;
+  st.V = &V; st.gslot = gslot; st.p = p; st.x = x; st.rdir = rdir; st.T0 = E; st.p0 = p0; st.n = n;
+  st.w0 = bval / pdf; st.sedge = reuse; st.v0 = v0; st.v1 = v1; st.far_tri = h0.tri;
+  return true;
+}
+
+// Direct boundary body: trace towards the sensor (EvalImportance per bounce,
+// Integrator.cpp:75-176), then the xDotN scatter.
+TRN_D void direct_body(const Params& P, const ViewDesc& V, long long gslot, long long p, const SurfF& x0, const F3& rdir,
+                       const F3& ev0, int v0, int v1, float sedge, const F3& p0, int far_tri, const F3& n, Cnt& cnt) {
+  const DeviceScene& s = P.s;
+  const PathSmp S{&P, V.seed, gslot, p + V.slot_off};
+  F3 T(1.f, 1.f, 1.f);
+  F3 dirs = rdir;
+  float W = 0.f;
+  SurfF xs = x0;
+  for (int b = 0; b < V.D; b++) {
+    const int o = 3 + 3 * b;
+    F3 c; int pix;
+    const bool more = importance_step_k<TRN_SHARED_STEPS_DIRECT>(s, V.cam, xs, dirs, T, S(o), S(o + 1), S(o + 2), c,
+                                                                 pix, cnt);
+    if (pix >= 0) W += dot(g_at(P, V, pix), ev0 * c);
+    if (!more) break;
+  }
+  if (W == 0.f || !isfinite(W)) return;
+  xdotn_vjp(P, V, W, x0.p, true, x0.tri, x0.u, x0.v, v0, v1, sedge, p0, far_tri, n, cnt);
+}
+
+__global__ void __launch_bounds__(256, TRN_MINB) k_direct_adj(Params P) {
   Cnt cnt;
   stage_top(P.s);
   int vhint = 0;
   for_each_valid<EdgeState>(P,
-    [&](long long gslot, EdgeState& st) -> bool {
-      const ViewDesc& V = view_of(P, gslot, vhint);
-      const long long p = gslot - V.begin;
-      const PathSmp S{&P, V.seed, gslot, p + V.slot_off};
-      float r0 = S(0);
-      const float r1 = S(1), r2 = S(2);
-      float reuse;
-      const float integral = __ldg(P.eint);
-      if (!(integral > 0.f)) return false;
-      float pdf_b = 1.f;
-      if (P.aq_cdf) {
-        // AdaptiveQuadratureDistribution::sample (AQ_distrb.h:176-195): pick a
-        // leaf with the extra uniform, then place the edge coordinate in its box
-        if (!(__ldg(P.aq_int) > 0.f)) return false;
-        float unused;
-        const int leaf = sample_discrete(P.aq_cdf, P.ne, S(3 + 3 * V.D), unused);
-        const float lo = leaf > 0 ? __ldg(P.ecdf + leaf - 1) : 0.f, hi = __ldg(P.ecdf + leaf);
-        r0 = __fadd_rn(lo, __fmul_rn(r0, __fsub_rn(hi, lo)));
-        pdf_b = __fdiv_rn(__ldg(P.aq_poly + leaf), __ldg(P.aq_int + 1));
-      }
-      const int e = sample_discrete(P.ecdf, P.ne, r0, reuse);
-      const int v0 = P.edges[5 * e], v1 = P.edges[5 * e + 1], f0 = P.edges[5 * e + 2], f1 = P.edges[5 * e + 3],
-                v2 = P.edges[5 * e + 4];
-      const float len_e = P.efunc[e];
-      if (!(len_e > 0.f)) return false;
-      const float pdf_e = (len_e / (integral * (float)P.ne)) / len_e;
-      const F3 Pa = load3(s.pos, v0), Pb = load3(s.pos, v1), Pc = load3(s.pos, v2);
-      const F3 e1 = Pb - Pa;
-      const F3 p0 = Pa + e1 * reuse;
-      const F3 edge = normalize(e1), edge2 = normalize(Pc - Pa);
-      LightSample ls;
-      if (!light_sample(s, r1, r2, ls)) return false;
-      int j0, j1, j2; tri_vertices(s, ls.tri, j0, j1, j2);
-      const F3 p2 = bary3(ls.bu, ls.bv, load3(s.pos, j0), load3(s.pos, j1), load3(s.pos, j2));
-      const F3 nL = load3(s.fnormal, ls.tri);
-      const F3 ev = p2 - p0;
-      const float dist_sqr = dot(ev, ev);
-      const float dist = sqrtf(dist_sqr);
-      const F3 en = ev / dist;
-      const float cos_t = dot(nL, -en);
-      const F3 n0 = load3(s.fnormal, f0);
-      const F3 n1 = f1 >= 0 ? load3(s.fnormal, f1) : F3z();
-      const bool is_b = f1 < 0;
-      const float c0 = dot(en, n0), c1 = dot(en, n1);
-      const bool valid0 = fabsf(c0) > kEdgeEps;
-      const bool valid1 = (c0 > kEdgeEps && c1 < -kEdgeEps) || (c0 < -kEdgeEps && c1 > kEdgeEps);
-      const bool right = (is_b && valid0) || (!is_b && valid1);
-      if (!(right && cos_t > kEps && dist > kShadowEps)) return false;
-      const float pdf = pdf_e * ls.pdf * dist_sqr / cos_t * pdf_b;
-      const F3 rdir = normalize(p0 - p2);
-      Hit h0, h;
-      cnt.v[kCntClosest] += 2;
-      cnt.v[kCntLight]++;
-      if (!trace_k<TRN_SETUP_SHARED_DIRECT, false>(s, p0, -rdir, kShadowEps, kRayMax, h0, P.err)) return false;
-      if (!trace_k<TRN_SETUP_SHARED_DIRECT, false>(s, p0, rdir, kShadowEps, kRayMax, h, P.err)) return false;
-      const F3 hp = p0 + (-rdir) * h0.t;
-      if (!(length(hp - p2) < kShadowEps)) return false;
-      const SurfF xl = post_intersect(s, h0.tri, h0.u, h0.v);
-      const F3 E = emitted(s, xl, rdir);
-      const SurfF x = post_intersect(s, h.tri, h.u, h.v);
-      const float dl = length(p2 - x.p);
-      const float cos2 = fabsf(dot(nL, rdir));
-      const float its_t = length(x.p - p0);
-      F3 n;
-      const float bval = base_val(its_t / dl, edge, -rdir, nL, edge2, n) * cos2;
-      if (bval == 0.f || (E.x == 0.f && E.y == 0.f && E.z == 0.f)) return false;
-      st.V = &V; st.gslot = gslot; st.p = p; st.x = x; st.rdir = rdir; st.T0 = E; st.p0 = p0; st.n = n;
-      st.w0 = bval / pdf; st.sedge = reuse; st.v0 = v0; st.v1 = v1; st.far_tri = h0.tri;
-      return true;
-    },
+    [&](long long gslot, EdgeState& st) -> bool { return direct_setup(P, gslot, st, vhint, cnt); },
     [&](EdgeState& st) {
-      const ViewDesc& V = *st.V;
-      const PathSmp S{&P, V.seed, st.gslot, st.p + V.slot_off};
-      const F3 ev0 = st.T0 * st.w0;
-      // trace towards the sensor (EvalImportance per bounce)
-      F3 T(1.f, 1.f, 1.f);
-      F3 dirs = st.rdir;
-      float W = 0.f;
-      SurfF xs = st.x;
-      for (int b = 0; b < V.D; b++) {
-        const int o = 3 + 3 * b;
-        F3 c; int pix;
-        const bool more = importance_step_k<TRN_SHARED_STEPS_DIRECT>(s, V.cam, xs, dirs, T, S(o), S(o + 1), S(o + 2), c, pix, cnt);
-        if (pix >= 0) W += dot(g_at(P, V, pix), ev0 * c);
-        if (!more) break;
-      }
-      if (W == 0.f || !isfinite(W)) return;
-      xdotn_vjp(P, V, W, st.x.p, true, st.x.tri, st.x.u, st.x.v, st.v0, st.v1, st.sedge, st.p0, st.far_tri, st.n,
-                cnt);
+      direct_body(P, *st.V, st.gslot, st.p, st.x, st.rdir, st.T0 * st.w0, st.v0, st.v1, st.sedge, st.p0, st.far_tri,
+                  st.n, cnt);
     });
+  flush_cnt(cnt, P.stats);
+}
+
+// Split form: k_direct_setup tests every slot once and queues the accepted
+// samples; k_direct_body runs their importance paths and scatters.
+struct DirectItem {
+  long long gslot, p;
+  int view, x_tri, v0, v1, far_tri, pad_;
+  float x_u, x_v, sedge, pad2_;
+  F3 rdir, ev0, p0, n;
+};
+
+__global__ void __launch_bounds__(256, TRN_MINB) k_direct_setup(Params P) {
+  Cnt cnt;
+  stage_top(P.s);
+  int vhint = 0;
+  DirectItem* q = reinterpret_cast<DirectItem*>(P.queue);
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;
+  for (;;) {
+    unsigned long long start = 0;
+    if (lane == 0) start = atomicAdd(P.work, 32ull);
+    start = __shfl_sync(0xffffffffu, start, 0);
+    if ((long long)start >= P.total) break;
+    const long long g = (long long)start + lane;
+    EdgeState st;
+    const bool ok = g < P.total && direct_setup(P, g, st, vhint, cnt);
+    const unsigned m = __ballot_sync(0xffffffffu, ok);
+    if (!m) continue;
+    const int leader = __ffs(m) - 1;
+    unsigned long long base = 0;
+    if (lane == leader) base = atomicAdd(P.q_count, (unsigned long long)__popc(m));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    const unsigned long long k = base + __popc(m & lt);
+    if (ok && k >= (unsigned long long)P.q_cap) atomicExch(P.err, 2);
+    if (ok && k < (unsigned long long)P.q_cap) {
+      DirectItem& it = q[k];
+      it.gslot = st.gslot; it.p = st.p; it.view = (int)(st.V - P.views);
+      it.x_tri = st.x.tri; it.x_u = st.x.u; it.x_v = st.x.v; it.v0 = st.v0; it.v1 = st.v1; it.far_tri = st.far_tri;
+      it.sedge = st.sedge; it.rdir = st.rdir; it.ev0 = st.T0 * st.w0; it.p0 = st.p0; it.n = st.n;
+    }
+  }
+  flush_cnt(cnt, P.stats);
+}
+
+__global__ void __launch_bounds__(256, TRN_MINB) k_direct_body(Params P) {
+  Cnt cnt;
+  stage_top(P.s);
+  const DirectItem* q = reinterpret_cast<const DirectItem*>(P.queue);
+  const unsigned long long n = min(*P.q_count, (unsigned long long)P.q_cap);
+  for (unsigned long long k = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; k < n;
+       k += (unsigned long long)gridDim.x * blockDim.x) {
+    const DirectItem& it = q[k];
+    const SurfF x = post_intersect(P.s, it.x_tri, it.x_u, it.x_v);
+    direct_body(P, P.views[it.view], it.gslot, it.p, x, it.rdir, it.ev0, it.v0, it.v1, it.sedge, it.p0, it.far_tri,
+                it.n, cnt);
+  }
   flush_cnt(cnt, P.stats);
 }
 
@@ -2290,8 +2411,7 @@ constexpr long long kPathRound = 1LL << 21;  // paths per split round of the int
 // of about 1.3 GB at depth <= 8).
 int path_adj_split(trn_viewset* vs, Params P, const trn_launch* ln, long long total, bool shallow, cudaStream_t st) {
   const long long cap = std::min(total, kPathRound);
-  const size_t item = shallow ? sizeof(PathRec<8>) : sizeof(PathRec<kMaxDepth>);
-  if (ensure_queue(vs, item * (size_t)cap, st)) return -1;
+  if (ensure_queue(vs, shallow ? path_soa_bytes<8>(cap) : path_soa_bytes<kMaxDepth>(cap), st)) return -1;
   P.queue = vs->iq;
   P.q_count = vs->iq_count;
   P.q_cap = cap;
@@ -2331,6 +2451,30 @@ int pixel_split(trn_viewset* vs, Params P, const trn_launch* ln, long long total
     k_indirect_round<<<1, 32, 0, st>>>(P.work, (unsigned long long)first, P.q_count);
     k_pixel_setup<<<grid, block, 0, st>>>(P);
     k_primary_body<<<grid, block, 0, st>>>(P);
+    count_launch(3);
+  }
+  TRN_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+#ifndef TRN_DIRECT_SPLIT
+#define TRN_DIRECT_SPLIT 1
+#endif
+
+// The split direct term in rounds of at most kIndirectRound slots.
+int direct_split(trn_viewset* vs, Params P, const trn_launch* ln, long long total, cudaStream_t st) {
+  const long long cap = std::min(total, kIndirectRound);
+  if (ensure_queue(vs, sizeof(DirectItem) * (size_t)cap, st)) return -1;
+  P.queue = vs->iq;
+  P.q_count = vs->iq_count;
+  P.q_cap = cap;
+  int grid, block;
+  launch_dims(ln, cap, grid, block);
+  for (long long first = 0; first < total; first += cap) {
+    P.total = std::min(total, first + cap);
+    k_indirect_round<<<1, 32, 0, st>>>(P.work, (unsigned long long)first, P.q_count);
+    k_direct_setup<<<grid, block, 0, st>>>(P);
+    k_direct_body<<<grid, block, 0, st>>>(P);
     count_launch(3);
   }
   TRN_CUDA_TRY(cudaGetLastError());
@@ -2449,7 +2593,10 @@ int render_views(trn_scene* s, trn_viewset* vs, const trn_render_options* o, int
       if (TRN_PRIMARY_SPLIT) return primary_split(vs, P, ln, total, st);
       launch(k_primary_adj, ln, total, P, st);
       break;
-    case TRN_DIRECT_EDGE: launch(k_direct_adj, ln, total, P, st); break;
+    case TRN_DIRECT_EDGE:
+      if (TRN_DIRECT_SPLIT) return direct_split(vs, P, ln, total, st);
+      launch(k_direct_adj, ln, total, P, st);
+      break;
     case TRN_INDIRECT_EDGE:
       if (TRN_INDIRECT_SPLIT) return indirect_split(vs, P, ln, total, shallow, st);
       if (shallow) launch(k_indirect_adj<8>, ln, total, P, st); else launch(k_indirect_adj<kMaxDepth>, ln, total, P, st);

@@ -956,15 +956,22 @@ int configure_geometry(trn_scene* s, cudaStream_t st) {
 // count from the device (count[1]); the host launches for an upper bound and
 // reads the count back only every kPlocBatch rounds, so the GPU does not wait
 // on the host between rounds (rounds after convergence are no-ops).
-constexpr int kPlocBatch = 8;
+constexpr int kPlocBatch = 32;
+
+__global__ void k_ploc_count_init(int* count, int n) {
+  if (threadIdx.x == 0) { count[0] = 0; count[1] = n; }
+}
+
+__global__ void k_set_root_parent(int* parent) {
+  if (threadIdx.x == 0) parent[0] = -1;
+}
 int ploc_build(trn_scene* s, cudaStream_t st) {
   const int nt = s->nt;
   int* cur_node = s->ploc_node;
   int* tmp_node = s->ploc_node + nt;
   float* cur_box = s->ploc_box;
   float* tmp_box = s->ploc_box + 6 * (size_t)nt;
-  const int init[2] = {0, nt};
-  TRN_CUDA_TRY(cudaMemcpyAsync(s->ploc_count, init, sizeof(init), cudaMemcpyHostToDevice, st));
+  k_ploc_count_init<<<1, 32, 0, st>>>(s->ploc_count, nt);
   k_ploc_init<<<nblk(nt), 256, 0, st>>>(nt, s->keys_alt, s->pos, s->idx, cur_node, cur_box);
   count_launch(1);
   int n = nt;  // upper bound of the device-side count
@@ -989,9 +996,9 @@ int ploc_build(trn_scene* s, cudaStream_t st) {
     if (counts[1] >= n && n > 1) { set_error("trn_scene_configure: PLOC rounds merged nothing"); return -1; }
     n = counts[1];
   }
-  const int root_parent = -1;
-  TRN_CUDA_TRY(cudaMemcpyAsync(s->parent, &root_parent, sizeof(int), cudaMemcpyHostToDevice, st));
-  TRN_CUDA_TRY(cudaStreamSynchronize(st));
+  k_set_root_parent<<<1, 32, 0, st>>>(s->parent);
+  count_launch(1);
+  TRN_CUDA_TRY(cudaGetLastError());
   return 0;
 }
 
@@ -1049,7 +1056,7 @@ int trn_scene_configure(trn_scene* s, cudaStream_t st) {
     }
   }
   TRN_CUDA_TRY(cudaGetLastError());
-  TRN_CUDA_TRY(cudaStreamSynchronize(st));
+  TRN_CUDA_TRY(cudaGetLastError());
   s->configured = true;
   s->built = true;
   return 0;
