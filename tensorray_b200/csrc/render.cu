@@ -70,6 +70,14 @@ constexpr int kMaxDepth = 16;
 #ifndef TRN_MINB_INDIRECT
 #define TRN_MINB_INDIRECT 2
 #endif
+// the split forms' set-up kernels are latency-bound with little state: four
+// blocks per SM (64 registers) hide more of it (measured)
+#ifndef TRN_MINB_SETUP
+#define TRN_MINB_SETUP 4
+#endif
+#ifndef TRN_MINB_BODY
+#define TRN_MINB_BODY 2
+#endif
 // the indirect kernel's two set-up rays use the shared traversal
 #ifndef TRN_INDIRECT_SETUP_SHARED
 #define TRN_INDIRECT_SETUP_SHARED 1
@@ -1321,7 +1329,7 @@ struct PrimaryItem {
   F3 rdir, p0, n, g;
 };
 
-__global__ void __launch_bounds__(256, TRN_MINB) k_primary_setup(Params P) {
+__global__ void __launch_bounds__(256, TRN_MINB_SETUP) k_primary_setup(Params P) {
   Cnt cnt;
   stage_top(P.s);
   int vhint = 0;
@@ -1355,7 +1363,7 @@ __global__ void __launch_bounds__(256, TRN_MINB) k_primary_setup(Params P) {
   flush_cnt(cnt, P.stats);
 }
 
-__global__ void __launch_bounds__(256, TRN_MINB) k_primary_body(Params P) {
+__global__ void __launch_bounds__(256, TRN_MINB_BODY) k_primary_body(Params P) {
   Cnt cnt;
   stage_top(P.s);
   const PrimaryItem* q = reinterpret_cast<const PrimaryItem*>(P.queue);
@@ -1492,7 +1500,7 @@ struct DirectItem {
   F3 rdir, ev0, p0, n;
 };
 
-__global__ void __launch_bounds__(256, TRN_MINB) k_direct_setup(Params P) {
+__global__ void __launch_bounds__(256, TRN_MINB_SETUP) k_direct_setup(Params P) {
   Cnt cnt;
   stage_top(P.s);
   int vhint = 0;
@@ -1525,7 +1533,7 @@ __global__ void __launch_bounds__(256, TRN_MINB) k_direct_setup(Params P) {
   flush_cnt(cnt, P.stats);
 }
 
-__global__ void __launch_bounds__(256, TRN_MINB) k_direct_body(Params P) {
+__global__ void __launch_bounds__(256, TRN_MINB_BODY) k_direct_body(Params P) {
   Cnt cnt;
   stage_top(P.s);
   const DirectItem* q = reinterpret_cast<const DirectItem*>(P.queue);
@@ -1864,7 +1872,7 @@ struct IndirectSetupItem {
   F3 rdir, p0, n;
 };
 
-__global__ void __launch_bounds__(256, TRN_MINB_INDIRECT) k_indirect_setup(Params P) {
+__global__ void __launch_bounds__(256, TRN_MINB_SETUP) k_indirect_setup(Params P) {
   Cnt cnt;
   stage_top(P.s);
   int vhint = 0;
@@ -2031,7 +2039,7 @@ __global__ void __launch_bounds__(256, TRN_MINB) k_pixel_adj(Params P) {
 
 // Split form: k_pixel_setup queues the accepted samples as PrimaryItem
 // (dimension 1 onwards, no edge vertices); k_primary_body runs them.
-__global__ void __launch_bounds__(256, TRN_MINB) k_pixel_setup(Params P) {
+__global__ void __launch_bounds__(256, TRN_MINB_SETUP) k_pixel_setup(Params P) {
   Cnt cnt;
   stage_top(P.s);
   int vhint = 0;
