@@ -59,16 +59,16 @@ struct Params {
 constexpr int kMaxDepth = 16;
 
 // Minimum resident 256-thread blocks per SM the integrator kernels are
-// compiled for (caps registers per thread at 65536 / (256 * minimum)); all
-// integrators run best capped at 128 registers (measured).
+// compiled for (caps registers per thread at 65536 / (256 * minimum)); the
+// values below are the measured best per kernel family.
 #ifndef TRN_MINB
-#define TRN_MINB 2
+#define TRN_MINB 3
 #endif
 #ifndef TRN_MINB_PATHADJ
 #define TRN_MINB_PATHADJ 2
 #endif
 #ifndef TRN_MINB_INDIRECT
-#define TRN_MINB_INDIRECT 2
+#define TRN_MINB_INDIRECT 3
 #endif
 // the split forms' set-up kernels are latency-bound with little state: four
 // blocks per SM (64 registers) hide more of it (measured)
