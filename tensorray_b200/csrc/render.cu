@@ -279,12 +279,6 @@ TRN_HD S xdotn(const V3<S>& org, const V3<S>& target, const V3<S>& P0, const V3<
   return dot(lift<S>(n), u2);
 }
 
-using D3 = Dual<3>;
-TRN_HD F3 contract(const V3<D3>& r, const F3& adj) {
-  F3 g;
-  for (int i = 0; i < 3; i++) g[i] = adj.x * r.x.d[i] + adj.y * r.y.d[i] + adj.z * r.z.d[i];
-  return g;
-}
 
 // ---------------------------------------------------------------------------
 // vertex records -> triangle vertices (the reparameterised PostIntersect)
