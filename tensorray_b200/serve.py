@@ -33,6 +33,11 @@ from ._abi import TRN_DIRECT_EDGE, TRN_PATH_TRACER, TRN_PRIMARY_EDGE, TrnView
 
 PHASE_FWD, PHASE_GRAD, PHASE_FINISH, PHASE_DONE = 0, 1, 2, 3
 
+# Device bytes a view set may hold for the queues of the split integrator
+# kernels (allocated by the library on first use; at most 2M path records of
+# about 620 bytes at depth <= 8, or 4M boundary samples).
+VIEWSET_QUEUE_BYTES = 1_400_000_000
+
 
 @dataclass
 class RenderRequest:
@@ -77,7 +82,9 @@ class Server:
     def __init__(self, scenes: dict, hbm_budget_bytes: float = 120e9, chunk_spp: int = 8, max_active: int = 256,
                  clock=time.perf_counter, iter_samples: int = 1 << 25):
         self.scenes = scenes
-        self.budget = int(hbm_budget_bytes)
+        # the forward and gradient view sets of every scene hold one queue each
+        self.reserve = 2 * len(scenes) * VIEWSET_QUEUE_BYTES
+        self.budget = int(hbm_budget_bytes) - self.reserve
         self.chunk_spp = chunk_spp
         self.iter_samples = int(iter_samples)
         self.max_active = max_active
