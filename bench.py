@@ -64,6 +64,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--quick", action="store_true", help="small smoke-sized run")
+    ap.add_argument("--no-path-cache", action="store_true",
+                    help="gradient calls re-trace the interior paths instead of reusing the forward's records")
     ap.add_argument("--requests", type=int, default=48, help="serve workload: number of requests")
     ap.add_argument("--workload", default="single", choices=["single", "views", "serve", "inverse"],
                     help="single: the 100K-triangle single-view config; views: 32 batched views "
@@ -579,7 +581,10 @@ def run_inverse(a):
     scene.configure()
     opts = api.RenderOptions(0, D, spp, spp, spp, 0, 0)
     opts.g_direct, opts.g_direct_spp, opts.g_eps = True, 16, 0.01
-    inv = inverse.InverseRenderer(scene, cams, [spp] * nviews, targets, opts, lr=1e-3)
+    # the forward render keeps its interior path records for the interior
+    # gradient of the same step (about 42 GB at 16 x 1024^2 x 4 spp, depth 8)
+    inv = inverse.InverseRenderer(scene, cams, [spp] * nviews, targets, opts, lr=1e-3,
+                                  path_cache_bytes=0 if a.no_path_cache else 64 << 30)
     units = inv.samples_per_step()
     losses = []
     for _ in range(a.warmup):
@@ -674,17 +679,11 @@ def run_serve(a):
 
     reqs = [make(i) for i in range(nreq)]
     budget = 120e9
-    # warm up every scene's kernels
-    warm = serve.Server(world, hbm_budget_bytes=budget)
-    for name in names:
-        cam = api.Camera((0.0, 0.0, 4.0), (0.0, 0.0, 0.0), (0.0, 1.0, 0.0), 64, 64, 45.0)
-        warm.submit(serve.RenderRequest(name, cam, 8, 3, torch.zeros(64 * 64, 3, device="cuda"), seed=999))
-    while not warm.idle():
-        warm.step()
-    torch.cuda.synchronize()
+    # the server's own view sets and every kernel warmed up before timing
+    srv = serve.Server(world, hbm_budget_bytes=budget, chunk_spp=8)
+    srv.warmup()
     clocks = Clocks(torch.cuda.current_device())
     clocks.start()
-    srv = serve.Server(world, hbm_budget_bytes=budget, chunk_spp=8)
     t0 = time.perf_counter()
     stats = srv.run(reqs, list(arrivals))
     torch.cuda.synchronize()

@@ -252,6 +252,32 @@ int trn_viewset_destroy(trn_viewset* views);
  * re-uses one set per scene and phase). */
 int trn_viewset_update(trn_viewset* views, int nviews, const trn_view* view_array);
 int trn_viewset_num_pixels(const trn_viewset* views, long long* npix);
+/* Allocate the set's round buffers now: the queue of the split integrator
+ * kernels (one full round of any term at up to max_bounces) and the buffers
+ * of the edge-sorted run order of the boundary set-up. Without it the first
+ * gradient call of each term allocates them, and a larger batch later grows
+ * them (each growth synchronises the stream and frees the old buffer). For a
+ * serving loop, or before capturing render calls into a CUDA graph. No
+ * counterpart in the reference (its tensor library allocates per call).
+ * About 1.5 GB for max_bounces <= 8. */
+int trn_viewset_reserve(trn_viewset* views, int max_bounces, cudaStream_t stream);
+/* Path cache. A forward render of TRN_PATH_TRACER can keep the record of
+ * every path it traced (hit points, light samples, throughputs: about 620
+ * bytes per path at max_bounces <= 8). The next trn_render_views_grad of
+ * TRN_PATH_TRACER over the same paths then runs only the reverse sweep
+ * instead of tracing them again. The reference re-traces them: its RenderD
+ * rebuilds the forward tensor program (Integrator.h:106-121). The gradients
+ * are the same either way. Records are reused only when nothing the paths
+ * depend on has changed since the forward call: the scene (any set_* call,
+ * configure or refit), the views' cameras, spp, seeds, slot offsets and
+ * depths, and the options' seed and max_bounces. Calls with a sample table
+ * and calls under stream capture neither write nor read records.
+ * max_bytes bounds the records' memory (0 = off, the default for view sets);
+ * a forward render whose records would exceed it renders without them. */
+int trn_viewset_path_cache(trn_viewset* views, long long max_bytes);
+/* The same bound for the single-view calls trn_render_fwd / trn_render_grad
+ * (default 16 GiB). */
+int trn_scene_path_cache(trn_scene* scene, long long max_bytes);
 int trn_render_views_fwd(trn_scene* scene, trn_viewset* views, const trn_render_options* options, int integrator,
                          const trn_samples* samples, const trn_launch* launch, float* images, cudaStream_t stream);
 int trn_render_views_grad(trn_scene* scene, trn_viewset* views, const trn_render_options* options, int integrator,

@@ -106,6 +106,9 @@ _SIGNATURES = {
     "trn_viewset_destroy": (C.c_int, [C.c_void_p]),
     "trn_viewset_update": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(TrnView)]),
     "trn_viewset_num_pixels": (C.c_int, [C.c_void_p, C.POINTER(C.c_longlong)]),
+    "trn_viewset_reserve": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "trn_viewset_path_cache": (C.c_int, [C.c_void_p, C.c_longlong]),
+    "trn_scene_path_cache": (C.c_int, [C.c_void_p, C.c_longlong]),
     "trn_render_views_fwd": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(TrnRenderOptions), C.c_int,
                                        C.POINTER(TrnSamples), C.POINTER(TrnLaunch), C.c_void_p, C.c_void_p]),
     "trn_render_views_grad": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(TrnRenderOptions), C.c_int,

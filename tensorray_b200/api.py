@@ -297,6 +297,12 @@ class Scene:
               "trn_scene_get_grads")
         return {"translation": gt, "positions": gp, "texels": gx[: self.num_texels]}
 
+    def set_path_cache(self, max_bytes: int) -> None:
+        """Bound (bytes; 0 = off; default 16 GiB) on the path records that the
+        single-view renderC of the interior term keeps for its renderD."""
+        self._ensure()
+        check(self._lib.trn_scene_path_cache(self.handle, int(max_bytes)), "trn_scene_path_cache")
+
     def clear_grads(self) -> None:
         check(self._lib.trn_scene_clear_grads(self._h, C.c_void_p(_stream())), "trn_scene_clear_grads")
 
@@ -467,6 +473,18 @@ class ViewSet:
         self.npix = npix.value
         self.cameras = list(cameras)
         self.spps = [int(x) for x in spps]
+
+    def reserve(self, max_bounces: int = 8) -> None:
+        """Allocate the split kernels' round buffers now (about 1.5 GB at
+        max_bounces <= 8), so that no later render call of this set allocates
+        device memory or synchronises to grow them."""
+        check(self.scene._lib.trn_viewset_reserve(self._h, int(max_bounces), C.c_void_p(_stream())),
+              "trn_viewset_reserve")
+
+    def set_path_cache(self, max_bytes: int) -> None:
+        """Let forward renders of the interior term keep their path records
+        (up to max_bytes; 0 = off) for the gradient call of the same paths."""
+        check(self.scene._lib.trn_viewset_path_cache(self._h, int(max_bytes)), "trn_viewset_path_cache")
 
     def slots(self, integrator_id: int) -> int:
         n = sum(c.width * c.height * s for c, s in zip(self.cameras, self.spps))

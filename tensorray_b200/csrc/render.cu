@@ -11,6 +11,7 @@
 #include <cstring>
 #include <string>
 #include <vector>
+#include <cub/cub.cuh>
 #include "../../include/trn.h"
 #include "scene_impl.cuh"
 #include "shading.cuh"
@@ -54,7 +55,17 @@ struct Params {
   void* queue2;
   unsigned long long* q_count;
   long long q_cap;
+  // run order of a split set-up round (nullptr = slot order): the i-th slot
+  // of the round [order_first, total) is order_first + order[i - order_first]
+  const unsigned* order;
+  long long order_first;
 };
+
+// Slot that runs at position i of the current round.
+TRN_D long long slot_at(const Params& P, long long i) {
+  if (!P.order || i >= P.total) return i;
+  return P.order_first + (long long)__ldg(P.order + (i - P.order_first));
+}
 
 constexpr int kMaxDepth = 16;
 
@@ -792,8 +803,9 @@ struct AdjState {
 };
 
 // Interior adjoint set-up: the camera ray of the slot (paths whose pixel has a
-// zero dL/dI carry no gradient and are skipped).
-TRN_D bool path_adj_setup(const Params& P, long long gslot, AdjState& st, int& vhint, Cnt& cnt) {
+// zero dL/dI carry no gradient and are skipped; with need_g false, as in the
+// recording forward render, no path is skipped and st.g is zero).
+TRN_D bool path_adj_setup(const Params& P, long long gslot, AdjState& st, int& vhint, Cnt& cnt, bool need_g = true) {
   const DeviceScene& s = P.s;
   const ViewDesc& V = view_of(P, gslot, vhint);
   const long long p = gslot - V.begin;
@@ -801,9 +813,9 @@ TRN_D bool path_adj_setup(const Params& P, long long gslot, AdjState& st, int& v
   const PathSmp S{&P, V.seed, gslot, p + V.slot_off};
   const int W = cam.w, WH = cam.w * cam.h;
   const int pix = (int)(p % WH);
-  cnt.v[kCntPixel]++;
-  const F3 g = g_at(P, V, pix);
-  if (g.x == 0.f && g.y == 0.f && g.z == 0.f) return false;
+  if (need_g) cnt.v[kCntPixel]++;
+  const F3 g = need_g ? g_at(P, V, pix) : F3z();
+  if (need_g && g.x == 0.f && g.y == 0.f && g.z == 0.f) return false;
   const F3 dir = camera_ray_dir(cam, pix % W, pix / W, S(0), S(1));
   cnt.v[kCntClosest]++;
   if (!trace_k<TRN_SETUP_SHARED_PATHADJ, false>(s, cam_pos(cam), dir, kShadowEps, kRayMax, st.h, P.err)) return false;
@@ -827,9 +839,11 @@ struct PathRec {
   F3 Tk[MAXD + 2], Mk[MAXD + 2];
 };
 
-// Forward replay of one interior path from its primary hit, recording into r.
+// Forward replay of one interior path from its primary hit, recording into r;
+// returns the path's radiance (what k_path_fwd adds to its pixel before the
+// 1/spp weight).
 template <int MAXD, class Rec>
-TRN_D void path_replay(const Params& P, const AdjState& st, Rec& r, Cnt& cnt) {
+TRN_D F3 path_replay(const Params& P, const AdjState& st, Rec& r, Cnt& cnt) {
   const DeviceScene& s = P.s;
   const ViewDesc& V = *st.V;
   const CameraDesc& cam = V.cam;
@@ -846,6 +860,7 @@ TRN_D void path_replay(const Params& P, const AdjState& st, Rec& r, Cnt& cnt) {
   F3 m1 = emitted(s, x, -rdir);
   if (!finite3(T * m1)) m1 = F3z();
   r.Mk[1] = m1;
+  F3 L = T * m1;
   int K = 1;  // vertices reached
   const int D = min(V.D, MAXD);
   unsigned mask = 0u;
@@ -858,6 +873,7 @@ TRN_D void path_replay(const Params& P, const AdjState& st, Rec& r, Cnt& cnt) {
                                     S(o + 3), S(o + 4), c, &R, cnt);
     // a scrubbed (non-finite) bounce contributes nothing and carries no gradient
     if (R.nee_ok && !R.scrubbed) mask |= 1u << k;
+    L = L + c;
     r.br[k] = {R.ltri, R.lu, R.lv, R.lpdf, R.lmis, R.prev_pdf};
     if (!more) break;
     r.vr[k + 1] = {x.tri, x.u, x.v};
@@ -869,6 +885,7 @@ TRN_D void path_replay(const Params& P, const AdjState& st, Rec& r, Cnt& cnt) {
   r.K = K;
   r.D = D;
   r.nee_mask = mask;
+  return L;
 }
 
 // Reverse sweep of one recorded interior path:
@@ -1050,7 +1067,10 @@ __global__ void __launch_bounds__(256, TRN_MINB_PATHADJ) k_path_replay(Params P)
   flush_cnt(cnt, P.stats);
 }
 
-template <int MAXD>
+// CACHED: the records come from the recording forward render (k_path_fwd_rec)
+// and carry no dL/dI yet; each path reads its pixel's now and is skipped when
+// that is zero, as path_adj_setup skips it in the replaying form.
+template <int MAXD, bool CACHED = false>
 __global__ void __launch_bounds__(256, TRN_MINB_PATHADJ) k_path_reverse(Params P) {
   Cnt cnt;
   stage_top(P.s);
@@ -1058,8 +1078,43 @@ __global__ void __launch_bounds__(256, TRN_MINB_PATHADJ) k_path_reverse(Params P
   for (unsigned long long k = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; k < n;
        k += (unsigned long long)gridDim.x * blockDim.x) {
     const PathRecSoA<MAXD> r = path_soa<MAXD>(P.queue, P.q_cap, (long long)k);
+    if (CACHED) {
+      const ViewDesc& V = P.views[r.view];
+      const F3 g = g_at(P, V, (int)(r.p % ((long long)V.cam.w * V.cam.h)));
+      if (g.x == 0.f && g.y == 0.f && g.z == 0.f) continue;
+      r.g = g;
+    }
     path_reverse<MAXD>(P, r, cnt);
   }
+  flush_cnt(cnt, P.stats);
+}
+
+// Forward interior render that also keeps every path with a primary hit as a
+// record (the records k_path_replay writes for the gradient call). A gradient
+// call of the same paths then runs k_path_reverse<MAXD, true> over them
+// instead of tracing them again. Same image as k_path_fwd.
+template <int MAXD>
+__global__ void __launch_bounds__(256, TRN_MINB_PATHADJ) k_path_fwd_rec(Params P) {
+  Cnt cnt;
+  stage_top(P.s);
+  int vhint = 0;
+  for_each_valid<AdjState>(P,
+    [&](long long gslot, AdjState& st) -> bool { return path_adj_setup(P, gslot, st, vhint, cnt, false); },
+    [&](AdjState& st) {
+      const unsigned act = __activemask();
+      const int lane = threadIdx.x & 31;
+      const int leader = __ffs(act) - 1;
+      unsigned long long base = 0;
+      if (lane == leader) base = atomicAdd(P.q_count, (unsigned long long)__popc(act));
+      base = __shfl_sync(act, base, leader);
+      const unsigned long long k = base + __popc(act & ((1u << lane) - 1u));
+      if (k >= (unsigned long long)P.q_cap) { atomicExch(P.err, 2); return; }
+      PathRecSoA<MAXD> r = path_soa<MAXD>(P.queue, P.q_cap, (long long)k);
+      const ViewDesc& V = *st.V;
+      const F3 L = path_replay<MAXD>(P, st, r, cnt) * V.inv_spp;
+      cnt.v[kCntPixel]++;
+      atomic_add3((V.image ? V.image : P.image + 3 * V.pix_off) + 3 * st.pix, L);
+    });
   flush_cnt(cnt, P.stats);
 }
 
@@ -1335,7 +1390,7 @@ __global__ void __launch_bounds__(256, TRN_MINB_SETUP) k_primary_setup(Params P)
     if (lane == 0) start = atomicAdd(P.work, 32ull);
     start = __shfl_sync(0xffffffffu, start, 0);
     if ((long long)start >= P.total) break;
-    const long long g = (long long)start + lane;
+    const long long g = slot_at(P, (long long)start + lane);
     EdgeState st;
     const bool ok = g < P.total && primary_setup(P, g, st, vhint, cnt);
     const unsigned m = __ballot_sync(0xffffffffu, ok);
@@ -1506,7 +1561,7 @@ __global__ void __launch_bounds__(256, TRN_MINB_SETUP) k_direct_setup(Params P) 
     if (lane == 0) start = atomicAdd(P.work, 32ull);
     start = __shfl_sync(0xffffffffu, start, 0);
     if ((long long)start >= P.total) break;
-    const long long g = (long long)start + lane;
+    const long long g = slot_at(P, (long long)start + lane);
     EdgeState st;
     const bool ok = g < P.total && direct_setup(P, g, st, vhint, cnt);
     const unsigned m = __ballot_sync(0xffffffffu, ok);
@@ -1878,7 +1933,7 @@ __global__ void __launch_bounds__(256, TRN_MINB_SETUP) k_indirect_setup(Params P
     if (lane == 0) start = atomicAdd(P.work, 32ull);
     start = __shfl_sync(0xffffffffu, start, 0);
     if ((long long)start >= P.total) break;
-    const long long g = (long long)start + lane;
+    const long long g = slot_at(P, (long long)start + lane);
     EdgeState st;
     const bool ok = g < P.total && indirect_setup(P, g, st, vhint, cnt);
     const unsigned m = __ballot_sync(0xffffffffu, ok);
@@ -1951,6 +2006,36 @@ __global__ void __launch_bounds__(256, TRN_MINB_INDIRECT) k_indirect_sensor_q(Pa
 // queue is empty.
 __global__ void k_indirect_round(unsigned long long* work, unsigned long long first, unsigned long long* q_count) {
   if (threadIdx.x == 0) { *work = first; q_count[0] = 0ull; q_count[1] = 0ull; }
+}
+
+// Sort keys of one round of a split boundary set-up: view x (E + 1) + the
+// edge that the slot's edge sample picks (E when it picks none), value = the
+// slot's offset in the round. Run in key order, a warp's rays leave one edge
+// (or a few neighbours) instead of 32 random ones; each slot's own result is
+// unchanged, only the order of the gradient atomics moves.
+// The edge pick restates the set-up functions' first step: primary_setup
+// (view silhouette table), direct_setup (scene table, or the AQ leaf when
+// guided), indirect_setup (scene table).
+__global__ void k_edge_keys(Params P, int term, unsigned* keys, unsigned* vals) {
+  const long long first = P.order_first, n = P.total - first;
+  int vhint = 0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const long long g = first + i;
+    const ViewDesc& V = view_of(P, g, vhint);
+    const PathSmp S{&P, V.seed, g, g - V.begin + V.slot_off};
+    int e = P.ne;
+    float reuse;
+    if (term == TRN_PRIMARY_EDGE) {
+      if (__ldg(V.pint) > 0.f) e = sample_discrete(V.pcdf, P.ne, S(0), reuse);
+    } else if (__ldg(P.eint) > 0.f && (term != TRN_INDIRECT_EDGE || V.D >= 2)) {
+      if (term == TRN_DIRECT_EDGE && P.aq_cdf)
+        e = sample_discrete(P.aq_cdf, P.ne, S(3 + 3 * V.D), reuse);
+      else
+        e = sample_discrete(P.ecdf, P.ne, S(0), reuse);
+    }
+    keys[i] = (unsigned)(&V - P.views) * (unsigned)(P.ne + 1) + (unsigned)e;
+    vals[i] = (unsigned)i;
+  }
 }
 
 
@@ -2184,6 +2269,20 @@ struct trn_viewset {
   void* iq = nullptr;
   size_t iq_bytes = 0;
   unsigned long long* iq_count = nullptr;
+  // run order of the split set-up rounds: keys and values double-buffered for
+  // one round, then the radix sort's temporary storage
+  void* sq = nullptr;
+  long long sq_cap = 0;  // slots per round the order buffers hold
+  size_t sq_tmp = 0;     // bytes of the sort's temporary storage
+  // path cache: interior path records of the last forward render, reused by
+  // the gradient call of the same paths (same scene version, views, seed and
+  // depth; hash samples only)
+  void* pc = nullptr;
+  size_t pc_bytes = 0;
+  unsigned long long* pc_count = nullptr;
+  long long pc_limit = 0;  // bytes the records may take (0 = off)
+  bool pc_valid = false;
+  std::vector<char> pc_key;
   int ne = 0;
   // slot layout currently uploaded: spp multiplier and per-view spp
   int uploaded_key = -2;
@@ -2310,6 +2409,8 @@ Params base_params(trn_scene* s, trn_viewset* vs, const trn_render_options* o, i
   P.queue2 = nullptr;
   P.q_count = nullptr;
   P.q_cap = 0;
+  P.order = nullptr;
+  P.order_first = 0;
   return P;
 }
 
@@ -2373,14 +2474,27 @@ void launch(K kernel, const trn_launch* ln, long long total, const Params& P, cu
 #define TRN_INDIRECT_SPLIT 1
 #endif
 constexpr long long kIndirectRound = 1LL << 22;  // slots per split round (queue of 4M items)
+constexpr long long kPathRound = 1LL << 21;  // paths per split round of the interior adjoint
+
+// Largest queue that any split term needs for one full round (depth <= 8
+// when shallow, else up to kMaxDepth).
+size_t full_queue_bytes(bool shallow) {
+  const size_t c = (size_t)kIndirectRound;
+  const size_t ind = (sizeof(IndirectSetupItem) * c + 255) / 256 * 256 +
+                     (shallow ? sizeof(IndirectItem<8>) : sizeof(IndirectItem<kMaxDepth>)) * c;
+  const size_t path = shallow ? path_soa_bytes<8>(kPathRound) : path_soa_bytes<kMaxDepth>(kPathRound);
+  return std::max(std::max(ind, path), std::max(sizeof(PrimaryItem) * c, sizeof(DirectItem) * c));
+}
 
 #ifndef TRN_PRIMARY_SPLIT
 #define TRN_PRIMARY_SPLIT 1
 #endif
 
-// The view set's queue of the split boundary terms, grown on first use to
+// The view set's queue of the split terms, grown on first use to at least
 // `need` bytes (not inside stream capture: run the integrator once before
-// capturing it).
+// capturing it, or reserve with trn_viewset_reserve). A growth at least
+// doubles the queue, up to one full round, so that a set whose batches grow
+// (a serving loop) reallocates a few times at most.
 int ensure_queue(trn_viewset* vs, size_t need, cudaStream_t st) {
   if (vs->iq_bytes >= need && vs->iq_count) return 0;
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
@@ -2391,11 +2505,12 @@ int ensure_queue(trn_viewset* vs, size_t need, cudaStream_t st) {
   }
   TRN_CUDA_TRY(cudaStreamSynchronize(st));
   if (vs->iq_bytes < need) {
+    const size_t bytes = std::max(need, std::min(2 * vs->iq_bytes, full_queue_bytes(vs->max_depth <= 8)));
     if (vs->iq) cudaFree(vs->iq);
     vs->iq = nullptr;
     vs->iq_bytes = 0;
-    if (cudaMalloc(&vs->iq, need) != cudaSuccess) { set_error("boundary term: out of memory for its queue"); return -1; }
-    vs->iq_bytes = need;
+    if (cudaMalloc(&vs->iq, bytes) != cudaSuccess) { set_error("boundary term: out of memory for its queue"); return -1; }
+    vs->iq_bytes = bytes;
   }
   if (!vs->iq_count && cudaMalloc(&vs->iq_count, 2 * sizeof(unsigned long long)) != cudaSuccess) {
     set_error("boundary term: out of memory");
@@ -2407,7 +2522,6 @@ int ensure_queue(trn_viewset* vs, size_t need, cudaStream_t st) {
 #ifndef TRN_PATHADJ_SPLIT
 #define TRN_PATHADJ_SPLIT 1
 #endif
-constexpr long long kPathRound = 1LL << 21;  // paths per split round of the interior adjoint
 
 // The split interior adjoint in rounds of at most kPathRound paths (a queue
 // of about 1.3 GB at depth <= 8).
@@ -2463,6 +2577,66 @@ int pixel_split(trn_viewset* vs, Params P, const trn_launch* ln, long long total
 #define TRN_DIRECT_SPLIT 1
 #endif
 
+#ifndef TRN_EDGE_ORDER
+#define TRN_EDGE_ORDER 1
+#endif
+
+// Buffers of the edge-sorted run order for rounds of up to `cap` slots: keys
+// and values double-buffered (16 bytes per slot) plus the radix sort's
+// temporary storage for vs->sq_cap slots. Grown like the queue (at least
+// doubling, up to one full round; not inside stream capture).
+int alloc_order(trn_viewset* vs, long long cap, cudaStream_t st) {
+  if (vs->sq && vs->sq_cap >= cap) return 0;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  TRN_CUDA_TRY(cudaStreamIsCapturing(st, &cs));
+  if (cs != cudaStreamCaptureStatusNone) {
+    set_error("boundary term: its sort buffers must be allocated before stream capture (run it once first)");
+    return -1;
+  }
+  const long long n = std::max(cap, std::min(2 * vs->sq_cap, kIndirectRound));
+  cub::DoubleBuffer<unsigned> k(nullptr, nullptr), v(nullptr, nullptr);
+  size_t tmp = 0;
+  TRN_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tmp, k, v, (int)n, 0, 32, st));
+  TRN_CUDA_TRY(cudaStreamSynchronize(st));
+  if (vs->sq) cudaFree(vs->sq);
+  vs->sq = nullptr;
+  vs->sq_cap = 0;
+  if (cudaMalloc(&vs->sq, (16 * (size_t)n + 255) / 256 * 256 + tmp) != cudaSuccess) {
+    set_error("boundary term: out of memory for its sort buffers");
+    return -1;
+  }
+  vs->sq_cap = n;
+  vs->sq_tmp = tmp;
+  return 0;
+}
+
+// Order buffers for this launch's rounds; returns 1 (run in slot order) when
+// the keys of this view set do not fit 32 bits.
+int ensure_order(trn_viewset* vs, const Params& P, long long cap, cudaStream_t st) {
+  if ((unsigned long long)P.nviews * (unsigned long long)(P.ne + 1) > 0xffffffffull) return 1;
+  return alloc_order(vs, cap, st);
+}
+
+// Edge-sorted run order of the round [P.order_first, P.total): keys, then a
+// stable radix sort over the bits the keys use; sets P.order.
+int order_round(trn_viewset* vs, Params& P, int term, cudaStream_t st) {
+  const long long n = P.total - P.order_first, cap = vs->sq_cap;
+  unsigned* base = static_cast<unsigned*>(vs->sq);
+  cub::DoubleBuffer<unsigned> k(base, base + cap), v(base + 2 * cap, base + 3 * cap);
+  P.order = nullptr;
+  const int grid = (int)std::min<long long>((n + 255) / 256, 16LL * sms());
+  k_edge_keys<<<grid, 256, 0, st>>>(P, term, k.Current(), v.Current());
+  count_launch(1);
+  const unsigned long long keys = (unsigned long long)P.nviews * (unsigned long long)(P.ne + 1);
+  int bits = 1;
+  while (bits < 32 && (1ull << bits) < keys) bits++;
+  void* tmp = reinterpret_cast<char*>(vs->sq) + (16 * (size_t)cap + 255) / 256 * 256;
+  size_t tb = vs->sq_tmp;
+  TRN_CUDA_TRY(cub::DeviceRadixSort::SortPairs(tmp, tb, k, v, (int)n, 0, bits, st));
+  P.order = v.Current();
+  return 0;
+}
+
 // The split direct term in rounds of at most kIndirectRound slots.
 int direct_split(trn_viewset* vs, Params P, const trn_launch* ln, long long total, cudaStream_t st) {
   const long long cap = std::min(total, kIndirectRound);
@@ -2472,8 +2646,12 @@ int direct_split(trn_viewset* vs, Params P, const trn_launch* ln, long long tota
   P.q_cap = cap;
   int grid, block;
   launch_dims(ln, cap, grid, block);
+  const int ordered = TRN_EDGE_ORDER ? ensure_order(vs, P, cap, st) : 1;
+  if (ordered < 0) return -1;
   for (long long first = 0; first < total; first += cap) {
     P.total = std::min(total, first + cap);
+    P.order_first = first;
+    if (!ordered && order_round(vs, P, TRN_DIRECT_EDGE, st)) return -1;
     k_indirect_round<<<1, 32, 0, st>>>(P.work, (unsigned long long)first, P.q_count);
     k_direct_setup<<<grid, block, 0, st>>>(P);
     k_direct_body<<<grid, block, 0, st>>>(P);
@@ -2492,8 +2670,12 @@ int primary_split(trn_viewset* vs, Params P, const trn_launch* ln, long long tot
   P.q_cap = cap;
   int grid, block;
   launch_dims(ln, cap, grid, block);
+  const int ordered = TRN_EDGE_ORDER ? ensure_order(vs, P, cap, st) : 1;
+  if (ordered < 0) return -1;
   for (long long first = 0; first < total; first += cap) {
     P.total = std::min(total, first + cap);
+    P.order_first = first;
+    if (!ordered && order_round(vs, P, TRN_PRIMARY_EDGE, st)) return -1;
     k_indirect_round<<<1, 32, 0, st>>>(P.work, (unsigned long long)first, P.q_count);
     k_primary_setup<<<grid, block, 0, st>>>(P);
     k_primary_body<<<grid, block, 0, st>>>(P);
@@ -2522,8 +2704,12 @@ int indirect_split(trn_viewset* vs, Params P, const trn_launch* ln, long long to
   P.q_cap = cap;
   int grid, block;
   launch_dims(ln, cap, grid, block);
+  const int ordered = TRN_EDGE_ORDER && TRN_INDIRECT_STAGES == 3 ? ensure_order(vs, P, cap, st) : 1;
+  if (ordered < 0) return -1;
   for (long long first = 0; first < total; first += cap) {
     P.total = std::min(total, first + cap);
+    P.order_first = first;
+    if (!ordered && order_round(vs, P, TRN_INDIRECT_EDGE, st)) return -1;
     k_indirect_round<<<1, 32, 0, st>>>(P.work, (unsigned long long)first, P.q_count);
     if (TRN_INDIRECT_STAGES == 3) {
       k_indirect_setup<<<grid, block, 0, st>>>(P);
@@ -2550,6 +2736,93 @@ int indirect_split(trn_viewset* vs, Params P, const trn_launch* ln, long long to
   return 0;
 }
 
+#ifndef TRN_PATH_CACHE
+#define TRN_PATH_CACHE 0
+#endif
+
+// What the interior paths of a launch depend on: the scene version, seed,
+// depth, slot count and, per view, camera, spp, seed, slot offset and depth.
+// (Weights, pixel offsets and buffers only enter the image write and dL/dI.)
+std::vector<char> path_key(const trn_viewset* vs, const trn_render_options* o, int spp_override, long long total) {
+  std::vector<char> k;
+  auto put = [&](const void* p, size_t n) {
+    const char* c = static_cast<const char*>(p);
+    k.insert(k.end(), c, c + n);
+  };
+  put(&vs->scene->version, sizeof(vs->scene->version));
+  put(&o->seed, sizeof(o->seed));
+  put(&o->max_bounces, sizeof(o->max_bounces));
+  put(&spp_override, sizeof(spp_override));
+  put(&total, sizeof(total));
+  for (const trn_view& v : vs->h_views) {
+    put(&v.camera, sizeof(v.camera));
+    put(&v.spp, sizeof(v.spp));
+    put(&v.seed, sizeof(v.seed));
+    put(&v.slot_offset, sizeof(v.slot_offset));
+    put(&v.max_bounces, sizeof(v.max_bounces));
+  }
+  return k;
+}
+
+bool capturing(cudaStream_t st) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  return cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone;
+}
+
+// Recording forward render of the interior term into the view set's path
+// cache. Returns 1 when the cache is not used (off, a sample table, stream
+// capture, above the limit, or no memory for it): the caller then renders
+// with k_path_fwd.
+int path_cache_fwd(trn_viewset* vs, Params P, const trn_launch* ln, const trn_render_options* o, int spp_override,
+                   long long total, cudaStream_t st) {
+  vs->pc_valid = false;
+  if (!TRN_PATH_CACHE || vs->pc_limit <= 0 || P.table || capturing(st)) return 1;
+  const bool shallow = vs->max_depth <= 8;
+  const size_t bytes = shallow ? path_soa_bytes<8>(total) : path_soa_bytes<kMaxDepth>(total);
+  if (bytes > (size_t)vs->pc_limit) return 1;
+  if (vs->pc_bytes < bytes || !vs->pc_count) {
+    TRN_CUDA_TRY(cudaStreamSynchronize(st));
+    if (vs->pc) cudaFree(vs->pc);
+    vs->pc = nullptr;
+    vs->pc_bytes = 0;
+    if (cudaMalloc(&vs->pc, bytes) != cudaSuccess ||
+        (!vs->pc_count && cudaMalloc(&vs->pc_count, sizeof(unsigned long long)) != cudaSuccess)) {
+      cudaGetLastError();  // out of memory: render without records
+      if (vs->pc) cudaFree(vs->pc);
+      vs->pc = nullptr;
+      return 1;
+    }
+    vs->pc_bytes = bytes;
+  }
+  TRN_CUDA_TRY(cudaMemsetAsync(vs->pc_count, 0, sizeof(unsigned long long), st));
+  P.queue = vs->pc;
+  P.q_count = vs->pc_count;
+  P.q_cap = total;
+  if (shallow) launch(k_path_fwd_rec<8>, ln, total, P, st); else launch(k_path_fwd_rec<kMaxDepth>, ln, total, P, st);
+  TRN_CUDA_TRY(cudaGetLastError());
+  vs->pc_key = path_key(vs, o, spp_override, total);
+  vs->pc_valid = true;
+  return 0;
+}
+
+// Reverse sweep over the cached records when they are the paths of this
+// gradient call. Returns 1 when they are not (the caller replays).
+int path_cache_grad(trn_viewset* vs, Params P, const trn_launch* ln, const trn_render_options* o, int spp_override,
+                    long long total, cudaStream_t st) {
+  if (!vs->pc_valid || P.table || capturing(st)) return 1;
+  if (vs->pc_key != path_key(vs, o, spp_override, total)) return 1;
+  P.queue = vs->pc;
+  P.q_count = vs->pc_count;
+  P.q_cap = total;
+  int grid, block;
+  launch_dims(ln, total, grid, block);
+  if (vs->max_depth <= 8) k_path_reverse<8, true><<<grid, block, 0, st>>>(P);
+  else k_path_reverse<kMaxDepth, true><<<grid, block, 0, st>>>(P);
+  count_launch(1);
+  TRN_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
 int render_views(trn_scene* s, trn_viewset* vs, const trn_render_options* o, int integrator,
                  const trn_samples* smp, const trn_launch* ln, int spp_override, bool forward, float* image,
                  const float* dLdI, cudaStream_t st) {
@@ -2568,6 +2841,8 @@ int render_views(trn_scene* s, trn_viewset* vs, const trn_render_options* o, int
     if (image) TRN_CUDA_TRY(cudaMemsetAsync(image, 0, sizeof(float) * 3 * vs->npix, st));
     if (integrator != TRN_PATH_TRACER || total == 0) return 0;  // edge terms have no primal image
     TRN_CUDA_TRY(cudaMemsetAsync(vs->work, 0, sizeof(unsigned long long), st));
+    const int cached = path_cache_fwd(vs, P, ln, o, spp_override, total, st);
+    if (cached <= 0) return cached;
     launch(k_path_fwd, ln, total, P, st);
     TRN_CUDA_TRY(cudaGetLastError());
     return 0;
@@ -2587,10 +2862,13 @@ int render_views(trn_scene* s, trn_viewset* vs, const trn_render_options* o, int
   TRN_CUDA_TRY(cudaMemsetAsync(vs->work, 0, sizeof(unsigned long long), st));
   const bool shallow = vs->max_depth <= 8;  // smaller per-thread path records
   switch (integrator) {
-    case TRN_PATH_TRACER:
+    case TRN_PATH_TRACER: {
+      const int cached = path_cache_grad(vs, P, ln, o, spp_override, total, st);
+      if (cached <= 0) return cached;
       if (TRN_PATHADJ_SPLIT) return path_adj_split(vs, P, ln, total, shallow, st);
       if (shallow) launch(k_path_adj<8>, ln, total, P, st); else launch(k_path_adj<kMaxDepth>, ln, total, P, st);
       break;
+    }
     case TRN_PRIMARY_EDGE:
       if (TRN_PRIMARY_SPLIT) return primary_split(vs, P, ln, total, st);
       launch(k_primary_adj, ln, total, P, st);
@@ -2686,6 +2964,7 @@ int single_view(trn_scene* s, const trn_camera* cam, trn_viewset** out) {
   } else if (trn_viewset_create(s, 1, &v, &s->single)) {
     return -1;
   }
+  s->single->pc_limit = s->single_path_cache;
   *out = s->single;
   return 0;
 }
@@ -2719,7 +2998,7 @@ int trn_viewset_update(trn_viewset* vs, int nviews, const trn_view* views) {
 int trn_viewset_destroy(trn_viewset* vs) {
   if (!vs) return 0;
   if (vs->copy_done) cudaEventSynchronize(vs->copy_done);
-  void* ptrs[] = {vs->views, vs->vbegin, vs->pbegin, vs->pfunc, vs->pcdf, vs->pint, vs->work, vs->iq, vs->iq_count};
+  void* ptrs[] = {vs->views, vs->vbegin, vs->pbegin, vs->pfunc, vs->pcdf, vs->pint, vs->work, vs->iq, vs->iq_count, vs->sq, vs->pc, vs->pc_count};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (vs->h_stage) cudaFreeHost(vs->h_stage);
@@ -2732,6 +3011,35 @@ int trn_viewset_destroy(trn_viewset* vs) {
 int trn_viewset_num_pixels(const trn_viewset* vs, long long* npix) {
   if (!vs || !npix) { set_error("trn_viewset_num_pixels: null argument"); return -1; }
   *npix = vs->npix;
+  return 0;
+}
+
+int trn_viewset_reserve(trn_viewset* vs, int max_bounces, cudaStream_t st) {
+  if (!vs) { set_error("trn_viewset_reserve: null view set"); return -1; }
+  if (max_bounces < 0 || max_bounces > kMaxDepth) { set_error("trn_viewset_reserve: max_bounces must be in [0, 16]"); return -1; }
+  if (ensure_queue(vs, full_queue_bytes(max_bounces <= 8), st)) return -1;
+  if (TRN_EDGE_ORDER && alloc_order(vs, kIndirectRound, st)) return -1;
+  return 0;
+}
+
+int trn_viewset_path_cache(trn_viewset* vs, long long max_bytes) {
+  if (!vs || max_bytes < 0) { set_error("trn_viewset_path_cache: invalid arguments"); return -1; }
+  vs->pc_limit = max_bytes;
+  vs->pc_valid = false;
+  if (max_bytes == 0 && vs->pc) {
+    if (vs->copy_done) cudaEventSynchronize(vs->copy_done);
+    TRN_CUDA_TRY(cudaDeviceSynchronize());
+    cudaFree(vs->pc);
+    vs->pc = nullptr;
+    vs->pc_bytes = 0;
+  }
+  return 0;
+}
+
+int trn_scene_path_cache(trn_scene* s, long long max_bytes) {
+  if (!s || max_bytes < 0) { set_error("trn_scene_path_cache: invalid arguments"); return -1; }
+  s->single_path_cache = max_bytes;
+  if (s->single) return trn_viewset_path_cache(s->single, max_bytes);
   return 0;
 }
 

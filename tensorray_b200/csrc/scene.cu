@@ -1056,9 +1056,9 @@ int trn_scene_configure(trn_scene* s, cudaStream_t st) {
     }
   }
   TRN_CUDA_TRY(cudaGetLastError());
-  TRN_CUDA_TRY(cudaGetLastError());
   s->configured = true;
   s->built = true;
+  s->version++;
   return 0;
 }
 
@@ -1074,6 +1074,7 @@ int trn_scene_refit(trn_scene* s, cudaStream_t st) {
   count_launch(1);
   TRN_CUDA_TRY(cudaGetLastError());
   s->configured = true;
+  s->version++;
   return 0;
 }
 
@@ -1081,18 +1082,21 @@ int trn_scene_set_translation(trn_scene* s, const float* t, cudaStream_t st) {
   if (!s || !t) { set_error("trn_scene_set_translation: null argument"); return -1; }
   TRN_CUDA_TRY(cudaMemcpyAsync(s->translation, t, sizeof(float) * 3 * s->nmesh, cudaMemcpyDeviceToDevice, st));
   s->configured = false;
+  s->version++;
   return 0;
 }
 int trn_scene_set_positions(trn_scene* s, const float* p, cudaStream_t st) {
   if (!s || !p) { set_error("trn_scene_set_positions: null argument"); return -1; }
   TRN_CUDA_TRY(cudaMemcpyAsync(s->raw_pos, p, sizeof(float) * 3 * s->nv, cudaMemcpyDeviceToDevice, st));
   s->configured = false;
+  s->version++;
   return 0;
 }
 int trn_scene_set_texels(trn_scene* s, const float* p, cudaStream_t st) {
   if (!s || !p) { set_error("trn_scene_set_texels: null argument"); return -1; }
   if (s->ntexel == 0) return 0;
   TRN_CUDA_TRY(cudaMemcpyAsync(s->texels, p, sizeof(float) * 3 * s->ntexel, cudaMemcpyDeviceToDevice, st));
+  s->version++;
   return 0;
 }
 

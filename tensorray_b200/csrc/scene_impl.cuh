@@ -11,6 +11,9 @@ struct trn_scene {
   // one-view set reused by trn_render_fwd / trn_render_grad (no per-call
   // allocation); created on the first single-view call
   trn_viewset* single = nullptr;
+  // bytes of interior path records the single-view calls may keep between a
+  // forward render and the gradient call of the same paths (0 = off)
+  long long single_path_cache = 16LL << 30;
   // ---- sizes -----------------------------------------------------------------
   int nv = 0, nt = 0, nuv = 0, nmesh = 0, nlight = 0, nbsdf = 0, ntex = 0, ne = 0;
   long long ntexel = 0;
@@ -94,6 +97,9 @@ struct trn_scene {
   bool configured = false;
   bool built = false;             // an LBVH topology exists (refit possible)
   bool grads_finalized = true;
+  // bumped by every change of parameters or geometry: path records of an
+  // older version are not reused
+  unsigned long long version = 0;
 
   trn::DeviceScene view() const {
     trn::DeviceScene s;

@@ -22,14 +22,18 @@ class InverseRenderer:
 
     integrators: ids of the terms whose gradients drive the step (the forward
     image is always the interior path tracer's). options: one RenderOptions for
-    every term (its seed advances each step so sample noise decorrelates)."""
+    every term (its seed advances each step so sample noise decorrelates).
+    path_cache_bytes: bound on the interior path records the forward render
+    keeps for the interior gradient of the same step (0 = re-trace them)."""
 
     def __init__(self, scene: api.Scene, cameras: list, spps: list, targets: torch.Tensor,
                  options: api.RenderOptions, integrators=(api.TRN_PATH_TRACER, api.TRN_PRIMARY_EDGE,
                                                           api.TRN_DIRECT_EDGE),
-                 lr: float = 1e-3, refit: bool = True, launch=None):
+                 lr: float = 1e-3, refit: bool = True, launch=None, path_cache_bytes: int = 0):
         self.scene = scene
         self.views = api.ViewSet(scene, cameras, spps)
+        if path_cache_bytes:
+            self.views.set_path_cache(path_cache_bytes)
         if targets.numel() != 3 * self.views.npix:
             raise RuntimeError("targets must hold npix x 3 values (all views concatenated)")
         self.targets = targets.reshape(-1, 3).to(scene.device, torch.float32).contiguous()

@@ -35,8 +35,10 @@ PHASE_FWD, PHASE_GRAD, PHASE_FINISH, PHASE_DONE = 0, 1, 2, 3
 
 # Device bytes a view set may hold for the queues of the split integrator
 # kernels (allocated by the library on first use; at most 2M path records of
-# about 620 bytes at depth <= 8, or 4M boundary samples).
-VIEWSET_QUEUE_BYTES = 1_400_000_000
+# about 620 bytes at depth <= 8, or 4M boundary samples) and for the boundary
+# set-up's run order (16 bytes per slot of a 4M-slot round plus the sort's
+# temporary storage).
+VIEWSET_QUEUE_BYTES = 1_500_000_000
 
 
 @dataclass
@@ -80,8 +82,11 @@ class ServerStats:
 
 class Server:
     def __init__(self, scenes: dict, hbm_budget_bytes: float = 120e9, chunk_spp: int = 8, max_active: int = 256,
-                 clock=time.perf_counter, iter_samples: int = 1 << 25):
+                 clock=time.perf_counter, iter_samples: int = 1 << 25, max_depth: int = 8):
         self.scenes = scenes
+        # gradient view sets reserve their round buffers for this depth when
+        # created (deeper requests still run; their first batch grows them)
+        self.max_depth = int(max_depth)
         # the forward and gradient view sets of every scene hold one queue each
         self.reserve = 2 * len(scenes) * VIEWSET_QUEUE_BYTES
         self.budget = int(hbm_budget_bytes) - self.reserve
@@ -117,6 +122,20 @@ class Server:
             raise RuntimeError(f"request {req.rid} needs {req.nbytes} bytes, above the HBM budget {self.budget}")
         self.pending.append(req)
         return req
+
+    def warmup(self) -> None:
+        """Serve one small request per scene, so that this server's view sets
+        exist (with their round buffers reserved) and every kernel has run
+        once before the first real request; then reset the statistics."""
+        for name, sc in self.scenes.items():
+            cam = api.Camera((0.0, 0.0, 4.0), (0.0, 0.0, 0.0), (0.0, 1.0, 0.0), 64, 64, 45.0)
+            self.submit(RenderRequest(name, cam, self.chunk_spp, 3, torch.zeros(64 * 64, 3, device=sc.device),
+                                      seed=999))
+        while not self.idle():
+            self.step()
+        torch.cuda.synchronize()
+        self.stats = ServerStats()
+        self._next_id = 0
 
     def idle(self) -> bool:
         return not self.pending and not self.active
@@ -231,6 +250,8 @@ class Server:
         vs = self.vsets.get(key)
         if vs is None:
             vs = api.ViewSet(self.scenes[name], cams, spps, views=arr)
+            if phase != PHASE_FWD:
+                vs.reserve(self.max_depth)
             self.vsets[key] = vs
         else:
             vs.update(cams, spps, arr)

@@ -115,3 +115,38 @@ def test_per_view_gradient_buffers(setup, integ):
         if float(ref.abs().sum()) == 0:
             continue
         assert rel_l2(bufs[i][0].cpu(), ref.cpu()) < 1e-4, f"view {i}: rel L2 {rel_l2(bufs[i][0].cpu(), ref.cpu()):.2e}"
+
+
+def test_reserved_set_allocates_nothing_later(setup):
+    """After ViewSet.reserve, gradient calls of every term allocate no device
+    memory and give the gradients of a set that allocates on first use."""
+    scene, cams, spps = setup
+    dev = scene.device
+    opts = api.RenderOptions(5, D, 0, 0, 0, 0, 0)
+    g = torch.Generator().manual_seed(4)
+    plain = api.ViewSet(scene, cams, spps)
+    dLdI = (torch.rand(plain.npix, 3, generator=g) - 0.3).to(dev)
+    ref = []
+    for integ in range(5):
+        scene.clear_grads()
+        plain.render_grad(integ, opts, dLdI)
+        ref.append(scene.get_grads()["positions"].clone())
+    vs = api.ViewSet(scene, cams, spps)
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    vs.reserve(D)
+    torch.cuda.synchronize()
+    free1 = torch.cuda.mem_get_info()[0]
+    assert 0 < free0 - free1 < 1.7e9, f"reserved {free0 - free1} bytes"
+    for integ in range(5):
+        scene.clear_grads()
+        torch.cuda.synchronize()
+        before = torch.cuda.mem_get_info()[0]
+        vs.render_grad(integ, opts, dLdI)
+        torch.cuda.synchronize()
+        assert torch.cuda.mem_get_info()[0] == before, f"term {integ} allocated"
+        got = scene.get_grads()["positions"]
+        if float(ref[integ].abs().sum()) > 0:
+            assert rel_l2(got.cpu(), ref[integ].cpu()) < 1e-4
+    with pytest.raises(RuntimeError):
+        vs.reserve(17)
