@@ -215,6 +215,8 @@ def main():
     spec = scenes.config2_scene(a.res, a.res, tris=a.tris)
     scene = api.Scene(spec)
     scene.configure()
+    if a.no_path_cache:
+        scene.set_path_cache(0)
     sphere = scene.shapes[0]
     D = a.depth
     from tensorray_b200 import dist as trd

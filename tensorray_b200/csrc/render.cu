@@ -78,6 +78,12 @@ constexpr int kMaxDepth = 16;
 #ifndef TRN_MINB_PATHADJ
 #define TRN_MINB_PATHADJ 2
 #endif
+#ifndef TRN_MINB_REVERSE
+#define TRN_MINB_REVERSE TRN_MINB_PATHADJ
+#endif
+#ifndef TRN_MINB_FWDREC
+#define TRN_MINB_FWDREC TRN_MINB_PATHADJ
+#endif
 #ifndef TRN_MINB_INDIRECT
 #define TRN_MINB_INDIRECT 3
 #endif
@@ -1071,7 +1077,7 @@ __global__ void __launch_bounds__(256, TRN_MINB_PATHADJ) k_path_replay(Params P)
 // and carry no dL/dI yet; each path reads its pixel's now and is skipped when
 // that is zero, as path_adj_setup skips it in the replaying form.
 template <int MAXD, bool CACHED = false>
-__global__ void __launch_bounds__(256, TRN_MINB_PATHADJ) k_path_reverse(Params P) {
+__global__ void __launch_bounds__(256, TRN_MINB_REVERSE) k_path_reverse(Params P) {
   Cnt cnt;
   stage_top(P.s);
   const unsigned long long n = min(*P.q_count, (unsigned long long)P.q_cap);
@@ -1094,7 +1100,7 @@ __global__ void __launch_bounds__(256, TRN_MINB_PATHADJ) k_path_reverse(Params P
 // call of the same paths then runs k_path_reverse<MAXD, true> over them
 // instead of tracing them again. Same image as k_path_fwd.
 template <int MAXD>
-__global__ void __launch_bounds__(256, TRN_MINB_PATHADJ) k_path_fwd_rec(Params P) {
+__global__ void __launch_bounds__(256, TRN_MINB_FWDREC) k_path_fwd_rec(Params P) {
   Cnt cnt;
   stage_top(P.s);
   int vhint = 0;
@@ -2039,6 +2045,10 @@ __global__ void k_edge_keys(Params P, int term, unsigned* keys, unsigned* vals) 
 }
 
 
+#ifndef TRN_PIXEL_INTERLEAVE
+#define TRN_PIXEL_INTERLEAVE 1
+#endif
+
 // ---------------------------------------------------------------------------
 // pixel boundary (BoundaryPixel.cpp:36-159, Edge.cpp:377-409, Camera.cpp:433-467)
 // ---------------------------------------------------------------------------
@@ -2049,11 +2059,20 @@ __global__ void k_edge_keys(Params P, int term, unsigned* keys, unsigned* vals) 
 TRN_D bool pixel_setup(const Params& P, long long gslot, EdgeState& st, int& vhint, Cnt& cnt) {
   const DeviceScene& s = P.s;
   const ViewDesc& V = view_of(P, gslot, vhint);
-  const long long p = gslot - V.begin;
   const CameraDesc& cam = V.cam;
   const int W_ = cam.w, WH = cam.w * cam.h;
   const F3 cpos = cam_pos(cam);
   const long long nanti = V.n / 4;
+#if TRN_PIXEL_INTERLEAVE
+  // Run order: the 4 antithetic copies of a slot take adjacent lanes. Their
+  // camera rays leave one pixel's border and share every later sample, so
+  // their paths stay close together (coherent traversal). Sample index p
+  // (copy * nanti + slot) and everything derived from it are unchanged.
+  const long long i = gslot - V.begin;
+  const long long p = (i & 3) * nanti + (i >> 2);
+#else
+  const long long p = gslot - V.begin;
+#endif
   const long long slot = p % nanti;
   const int anti = (int)(p / nanti);
   // the 4 antithetic copies of a slot share its samples (BoundaryPixel.cpp:135-138)
@@ -2737,7 +2756,7 @@ int indirect_split(trn_viewset* vs, Params P, const trn_launch* ln, long long to
 }
 
 #ifndef TRN_PATH_CACHE
-#define TRN_PATH_CACHE 0
+#define TRN_PATH_CACHE 1
 #endif
 
 // What the interior paths of a launch depend on: the scene version, seed,

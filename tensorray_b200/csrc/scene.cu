@@ -281,9 +281,10 @@ __device__ __forceinline__ float union_area(const float* a, const float* b) {
 
 // Nearest neighbour in the window; ties go to the smaller index, which keeps
 // at least one mutual pair (the smallest index among the closest pairs).
-__global__ void k_ploc_nn(const int* count, const float* cbox, int* nn) {
+__global__ void k_ploc_nn(int* count, const float* cbox, int* nn) {
   __shared__ float sb[(kPlocBlock + 2 * kPlocR) * 6];
   const int n = count[1];  // clusters of this round (the launch covers an upper bound)
+  if (blockIdx.x == 0 && threadIdx.x == 0 && n > 1) count[2] += 1;  // rounds that merge
   if ((int)(blockIdx.x * kPlocBlock) >= n) return;
   const int start = blockIdx.x * kPlocBlock - kPlocR;
   for (int t = threadIdx.x; t < (kPlocBlock + 2 * kPlocR) * 6; t += blockDim.x) {
@@ -893,7 +894,7 @@ int trn_scene_create(const trn_scene_desc* d, trn_scene** out) {
         dev_alloc_copy(&s->ploc_nn, (const int*)nullptr, (size_t)nt) ||
         dev_alloc_copy(&s->ploc_flag, (const int*)nullptr, (size_t)nt) ||
         dev_alloc_copy(&s->ploc_pos, (const int*)nullptr, (size_t)nt) ||
-        dev_alloc_copy(&s->ploc_count, (const int*)nullptr, 2) ||
+        dev_alloc_copy(&s->ploc_count, (const int*)nullptr, 3) ||
         cudaMalloc(&s->scan_tmp, std::max<size_t>(sb, 16)) != cudaSuccess) {
       set_error("trn_scene_create: out of memory");
       return fail();
@@ -959,7 +960,7 @@ int configure_geometry(trn_scene* s, cudaStream_t st) {
 constexpr int kPlocBatch = 32;
 
 __global__ void k_ploc_count_init(int* count, int n) {
-  if (threadIdx.x == 0) { count[0] = 0; count[1] = n; }
+  if (threadIdx.x == 0) { count[0] = 0; count[1] = n; count[2] = 0; }
 }
 
 __global__ void k_set_root_parent(int* parent) {
@@ -975,9 +976,13 @@ int ploc_build(trn_scene* s, cudaStream_t st) {
   k_ploc_init<<<nblk(nt), 256, 0, st>>>(nt, s->keys_alt, s->pos, s->idx, cur_node, cur_box);
   count_launch(1);
   int n = nt;  // upper bound of the device-side count
+  // The previous build of this scene needed s->ploc_rounds rounds: the first
+  // batch runs that many and a few more (over the full upper bound), so that
+  // a rebuild of similar geometry reads the count back once.
   for (int batch = 0; n > 1; batch++) {
     if (batch * kPlocBatch > 4 * nt + 64) { set_error("trn_scene_configure: PLOC did not converge"); return -1; }
-    for (int r = 0; r < kPlocBatch; r++) {
+    const int rounds = batch == 0 && s->ploc_rounds > 0 ? s->ploc_rounds + 4 : kPlocBatch;
+    for (int r = 0; r < rounds; r++) {
       k_ploc_nn<<<(n + kPlocBlock - 1) / kPlocBlock, kPlocBlock, 0, st>>>(s->ploc_count, cur_box, s->ploc_nn);
       k_ploc_merge<<<nblk(n), 256, 0, st>>>(nt, n, s->ploc_nn, cur_node, cur_box, tmp_node, tmp_box, s->ploc_flag,
                                             s->nodes, s->parent, s->ploc_count);
@@ -990,11 +995,12 @@ int ploc_build(trn_scene* s, cudaStream_t st) {
                                               s->ploc_count);
       count_launch(4);
     }
-    int counts[2];
+    int counts[3];
     TRN_CUDA_TRY(cudaMemcpyAsync(counts, s->ploc_count, sizeof(counts), cudaMemcpyDeviceToHost, st));
     TRN_CUDA_TRY(cudaStreamSynchronize(st));
     if (counts[1] >= n && n > 1) { set_error("trn_scene_configure: PLOC rounds merged nothing"); return -1; }
     n = counts[1];
+    s->ploc_rounds = counts[2];
   }
   k_set_root_parent<<<1, 32, 0, st>>>(s->parent);
   count_launch(1);

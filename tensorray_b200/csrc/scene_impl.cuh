@@ -76,7 +76,8 @@ struct trn_scene {
   int* ploc_nn = nullptr;         // [T]
   int* ploc_flag = nullptr;       // [T]
   int* ploc_pos = nullptr;        // [T]
-  int* ploc_count = nullptr;      // [2] merge counter, cluster count
+  int* ploc_count = nullptr;      // [3] merge counter, cluster count, rounds that merged
+  int ploc_rounds = 0;            // rounds the last build needed (0 = none yet)
   void* scan_tmp = nullptr;
   size_t scan_tmp_bytes = 0;
   float* bounds = nullptr;        // [6]
