@@ -401,6 +401,95 @@ __global__ void k_refit(int n, const unsigned long long* keys, const float* pos,
 
 
 // ---------------------------------------------------------------------------
+// Multi-triangle leaves: every subtree of the binary LBVH with at most
+// TRN_LEAF_MAX triangles becomes one leaf whose triangles are contiguous in
+// ctri. cnodes keeps the binary nodes (same indices and child boxes) with
+// such children re-encoded as leaves: ~(first | (count - 1) << 29). Nodes
+// inside a collapsed subtree are not reached. A ray meets the same triangles
+// or fewer node boxes; its result (closest (t, triangle id), or any hit)
+// does not depend on the tree.
+// ---------------------------------------------------------------------------
+__host__ __device__ constexpr int leaf_code(int first, int count) { return ~(first | ((count - 1) << 29)); }
+
+// subtree triangle counts, bottom-up from the leaves (the second child to
+// arrive at a node continues, as in k_refit)
+__global__ void k_leaf_counts(int n, const BvhNode* nodes, const int* parent, int* flags, int* cnt) {
+  const int leaf = blockIdx.x * blockDim.x + threadIdx.x;
+  if (leaf >= n) return;
+  int p = parent[n - 1 + leaf];
+  while (p >= 0) {
+    __threadfence();
+    if (atomicAdd(&flags[p], 1) == 0) return;
+    __threadfence();
+    const int4 d = nodes[p].d;
+    const volatile int* vc = cnt;
+    const int c = (d.x < 0 ? 1 : vc[d.x]) + (d.y < 0 ? 1 : vc[d.y]);
+    cnt[p] = c;
+    p = parent[p];
+  }
+}
+
+// triangles each reachable node's leaf children hold (0 inside a collapsed
+// subtree): the scan of this gives each node its first ctri slot
+__global__ void k_leaf_slots(int ninner, const BvhNode* nodes, const int* cnt, int* slots) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ninner) return;
+  if (cnt[i] <= TRN_LEAF_MAX) { slots[i] = 0; return; }
+  const int4 d = nodes[i].d;
+  int k = 0;
+  for (int side = 0; side < 2; side++) {
+    const int c = side ? d.y : d.x;
+    k += c < 0 ? 1 : (cnt[c] <= TRN_LEAF_MAX ? cnt[c] : 0);
+  }
+  slots[i] = k;
+}
+
+__device__ __forceinline__ void copy_tri(const float4* src, int leaf, float4* dst, int slot) {
+  dst[3 * slot + 0] = src[3 * leaf + 0];
+  dst[3 * slot + 1] = src[3 * leaf + 1];
+  dst[3 * slot + 2] = src[3 * leaf + 2];
+}
+
+__global__ void k_leaf_collapse(int ninner, const BvhNode* nodes, const int* cnt, const int* base,
+                                const float4* tri_verts, BvhNode* cnodes, float4* ctri) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ninner || cnt[i] <= TRN_LEAF_MAX) return;
+  BvhNode o = nodes[i];
+  int slot = base[i];
+  int child[2];
+  for (int side = 0; side < 2; side++) {
+    const int c = side ? o.d.y : o.d.x;
+    if (c < 0) {
+      copy_tri(tri_verts, ~c, ctri, slot);
+      child[side] = leaf_code(slot, 1);
+      slot += 1;
+    } else if (cnt[c] <= TRN_LEAF_MAX) {
+      // gather the subtree's triangles (at most TRN_LEAF_MAX leaves)
+      const int first = slot;
+      int stack[TRN_LEAF_MAX];
+      int sp = 0;
+      stack[sp++] = c;
+      while (sp > 0) {
+        const int4 d = nodes[stack[--sp]].d;
+        for (int k = 0; k < 2; k++) {  // (the order within a leaf is immaterial)
+          const int g = k ? d.y : d.x;
+          if (g < 0) {
+            copy_tri(tri_verts, ~g, ctri, slot++);
+          } else if (sp < TRN_LEAF_MAX) {
+            stack[sp++] = g;
+          }
+        }
+      }
+      child[side] = leaf_code(first, cnt[c]);
+    } else {
+      child[side] = c;
+    }
+  }
+  o.d = make_int4(child[0], child[1], 0, 0);
+  cnodes[i] = o;
+}
+
+// ---------------------------------------------------------------------------
 // collapse the binary LBVH into the 8-wide quantised BVH (top-down, one
 // level of wide nodes per launch). Each wide node takes the two children of
 // its binary node and repeatedly opens the internal child with the largest
@@ -859,6 +948,10 @@ int trn_scene_create(const trn_scene_desc* d, trn_scene** out) {
       dev_alloc_copy(&s->tri_verts, (const float4*)nullptr, 3 * (size_t)nt) ||
       dev_alloc_copy(&s->parent, (const int*)nullptr, 2 * (size_t)nt) ||
       dev_alloc_copy(&s->flags, (const int*)nullptr, std::max(1, nt - 1)) ||
+      (TRN_LEAF_MAX > 1 && nt > TRN_LEAF_MAX &&
+       (dev_alloc_copy(&s->cnodes, (const BvhNode*)nullptr, (size_t)nt - 1) ||
+        dev_alloc_copy(&s->ctri, (const float4*)nullptr, 3 * (size_t)nt) ||
+        dev_alloc_copy(&s->leaf_cnt, (const int*)nullptr, 3 * ((size_t)nt - 1)))) ||
       dev_alloc_copy(&s->keys, (const unsigned long long*)nullptr, (size_t)nt) ||
       dev_alloc_copy(&s->keys_alt, (const unsigned long long*)nullptr, (size_t)nt) ||
       dev_alloc_copy(&s->bounds, (const float*)nullptr, 6) ||
@@ -885,6 +978,15 @@ int trn_scene_create(const trn_scene_desc* d, trn_scene** out) {
   cub::DeviceRadixSort::SortKeys(nullptr, bytes, s->keys, s->keys_alt, nt);
   s->sort_tmp_bytes = bytes;
   if (cudaMalloc(&s->sort_tmp, bytes) != cudaSuccess) { set_error("trn_scene_create: out of memory"); return fail(); }
+  if (s->cnodes) {
+    size_t sb = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, sb, s->leaf_cnt, s->leaf_cnt, nt - 1);
+    s->leaf_scan_bytes = std::max<size_t>(sb, 16);
+    if (cudaMalloc(&s->leaf_scan_tmp, s->leaf_scan_bytes) != cudaSuccess) {
+      set_error("trn_scene_create: out of memory");
+      return fail();
+    }
+  }
   if (TRN_PLOC) {
     size_t sb = 0;
     cub::DeviceScan::ExclusiveSum(nullptr, sb, s->ploc_flag, s->ploc_pos, nt);
@@ -916,7 +1018,7 @@ int trn_scene_destroy(trn_scene* s) {
                   s->sort_tmp, s->bounds, s->g_pos, s->g_vnormal, s->g_texels, s->g_translation, s->err,
                   s->stats, s->wnodes, s->wtri, s->wqueue, s->wcount, s->aq_poly, s->aq_func, s->aq_cdf,
                   s->aq_int, s->ploc_node, s->ploc_box, s->ploc_nn, s->ploc_flag, s->ploc_pos, s->ploc_count,
-                  s->scan_tmp};
+                  s->scan_tmp, s->cnodes, s->ctri, s->leaf_cnt, s->leaf_scan_tmp};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   delete s;
@@ -953,6 +1055,29 @@ int configure_geometry(trn_scene* s, cudaStream_t st) {
   }
   return 0;
 }
+// Rebuild the collapsed arrays from the binary LBVH (after a build or refit).
+int leaf_collapse(trn_scene* s, cudaStream_t st) {
+  s->collapsed = false;
+  if (!s->cnodes) return 0;
+  const int nt = s->nt, ninner = nt - 1;
+  int* cnt = s->leaf_cnt;
+  int* slots = s->leaf_cnt + ninner;
+  int* base = s->leaf_cnt + 2 * ninner;
+  TRN_CUDA_TRY(cudaMemsetAsync(s->flags, 0, sizeof(int) * ninner, st));
+  k_leaf_counts<<<nblk(nt), 256, 0, st>>>(nt, s->nodes, s->parent, s->flags, cnt);
+  k_leaf_slots<<<nblk(ninner), 256, 0, st>>>(ninner, s->nodes, cnt, slots);
+  size_t sb = s->leaf_scan_bytes;
+  if (cub::DeviceScan::ExclusiveSum(s->leaf_scan_tmp, sb, slots, base, ninner, st) != cudaSuccess) {
+    set_error("trn_scene_configure: leaf scan failed");
+    return -1;
+  }
+  k_leaf_collapse<<<nblk(ninner), 256, 0, st>>>(ninner, s->nodes, cnt, base, s->tri_verts, s->cnodes, s->ctri);
+  count_launch(4);
+  TRN_CUDA_TRY(cudaGetLastError());
+  s->collapsed = true;
+  return 0;
+}
+
 // PLOC rounds until one cluster is left. The kernels read the round's cluster
 // count from the device (count[1]); the host launches for an upper bound and
 // reads the count back only every kPlocBatch rounds, so the GPU does not wait
@@ -1037,6 +1162,7 @@ int trn_scene_configure(trn_scene* s, cudaStream_t st) {
   }
   k_refit<<<nblk(nt), 256, 0, st>>>(nt, s->keys_alt, s->pos, s->idx, s->nodes, s->parent, s->flags, s->tri_verts);
   count_launch(1);
+  if (!TRN_WIDE_BVH && leaf_collapse(s, st)) return -1;
   // 8-wide quantised BVH
   s->n_wnodes = 0;
   if (TRN_WIDE_BVH && nt > 1) {
@@ -1078,6 +1204,7 @@ int trn_scene_refit(trn_scene* s, cudaStream_t st) {
   if (nt > 1) TRN_CUDA_TRY(cudaMemsetAsync(s->flags, 0, sizeof(int) * (nt - 1), st));
   k_refit<<<nblk(nt), 256, 0, st>>>(nt, s->keys_alt, s->pos, s->idx, s->nodes, s->parent, s->flags, s->tri_verts);
   count_launch(1);
+  if (leaf_collapse(s, st)) return -1;
   TRN_CUDA_TRY(cudaGetLastError());
   s->configured = true;
   s->version++;

@@ -64,6 +64,14 @@ struct trn_scene {
   // acceleration structure
   trn::BvhNode* nodes = nullptr;  // [T-1]
   float4* tri_verts = nullptr;    // [T][3]
+  // multi-triangle leaves (TRN_LEAF_MAX > 1): the traversal uses these when
+  // `collapsed`; leaf_cnt holds subtree counts, slots and slot bases [3][T-1]
+  trn::BvhNode* cnodes = nullptr; // [T-1]
+  float4* ctri = nullptr;         // [T][3]
+  int* leaf_cnt = nullptr;
+  void* leaf_scan_tmp = nullptr;
+  size_t leaf_scan_bytes = 0;
+  bool collapsed = false;
   int* parent = nullptr;          // [2T-1]
   int* flags = nullptr;           // [T-1]
   unsigned long long* keys = nullptr;     // [T]
@@ -111,7 +119,9 @@ struct trn_scene {
     s.light_func = light_func; s.light_cdf = light_cdf; s.light_integral = light_integral_dev;
     s.light_radiance = light_radiance;
     s.n_bsdf = nbsdf; s.bsdfs = bsdfs; s.texs = texs; s.texels = texels;
-    s.nodes = nodes; s.tri_verts = tri_verts; s.root_is_leaf = nt == 1;
+    s.nodes = collapsed ? cnodes : nodes;
+    s.tri_verts = collapsed ? ctri : tri_verts;
+    s.root_is_leaf = nt == 1;
     s.wnodes = wnodes; s.wtri = wtri; s.n_wnodes = n_wnodes;
     return s;
   }

@@ -62,6 +62,13 @@ constexpr int kTopNodes = 73;  // root + 8 + 64 wide nodes staged in shared memo
 
 // Traversal structure: the binary LBVH with child boxes in the parent (default;
 // measured faster on B200 for the scenes here) or the 8-wide quantised BVH.
+// most triangles in one leaf of the traversed LBVH (1 = the binary tree's
+// one-triangle leaves, the default: leaves of up to 2 measured the same, up
+// to 4 slower, because a leaf's box admits more rays than its triangles'
+// boxes did and each costs exact watertight tests)
+#ifndef TRN_LEAF_MAX
+#define TRN_LEAF_MAX 1
+#endif
 #ifndef TRN_WIDE_BVH
 #define TRN_WIDE_BVH 0
 #endif

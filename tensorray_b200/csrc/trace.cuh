@@ -233,6 +233,7 @@ __device__ __noinline__ bool trace_wide(const DeviceScene& s, const RayPre& r, f
 #ifndef TRN_ONE_LEAF_SITE
 #define TRN_ONE_LEAF_SITE 1
 #endif
+static_assert(TRN_ONE_LEAF_SITE || TRN_LEAF_MAX == 1, "multi-triangle leaves need the one-leaf-site traversal");
 
 template <bool ANY>
 TRN_D bool trace(const DeviceScene& s, const F3& o, const F3& d, float tmin, float tmax, Hit& hit,
@@ -266,7 +267,15 @@ TRN_D bool trace(const DeviceScene& s, const F3& o, const F3& d, float tmin, flo
     int cur = 0;
     for (;;) {
       if (cur < 0) {
-        if (test_leaf(~cur)) return true;
+        if (TRN_LEAF_MAX == 1) {
+          if (test_leaf(~cur)) return true;
+        } else {
+          // leaf: ~(first | (count - 1) << 29), count triangles from first
+          const int v = ~cur;
+          const int first = v & 0x1fffffff, count = (v >> 29) + 1;
+          for (int k = 0; k < count; k++)
+            if (test_leaf(first + k)) return true;
+        }
         if (sp == 0) break;
         cur = stack[--sp];
         continue;
