@@ -259,7 +259,7 @@ int trn_viewset_num_pixels(const trn_viewset* views, long long* npix);
  * them (each growth synchronises the stream and frees the old buffer). For a
  * serving loop, or before capturing render calls into a CUDA graph. No
  * counterpart in the reference (its tensor library allocates per call).
- * About 1.5 GB for max_bounces <= 8. */
+ * About 5.5 GB for max_bounces <= 8 (rounds of 16M boundary samples). */
 int trn_viewset_reserve(trn_viewset* views, int max_bounces, cudaStream_t stream);
 /* Path cache. A forward render of TRN_PATH_TRACER can keep the record of
  * every path it traced (hit points, light samples, throughputs: about 620

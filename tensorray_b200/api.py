@@ -475,7 +475,7 @@ class ViewSet:
         self.spps = [int(x) for x in spps]
 
     def reserve(self, max_bounces: int = 8) -> None:
-        """Allocate the split kernels' round buffers now (about 1.5 GB at
+        """Allocate the split kernels' round buffers now (about 5.5 GB at
         max_bounces <= 8), so that no later render call of this set allocates
         device memory or synchronises to grow them."""
         check(self.scene._lib.trn_viewset_reserve(self._h, int(max_bounces), C.c_void_p(_stream())),

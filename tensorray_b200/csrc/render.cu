@@ -1124,6 +1124,120 @@ __global__ void __launch_bounds__(256, TRN_MINB_FWDREC) k_path_fwd_rec(Params P)
   flush_cnt(cnt, P.stats);
 }
 
+// k_path_fwd_rec with path regeneration: lanes fetch slots until at least
+// TRN_COMPACT_MIN hold a path (as for_each_valid), then every lane with a
+// path takes one bounce; a lane whose path has ended writes its record's
+// totals and its pixel and takes the next slot at once. Each path runs
+// exactly the steps of path_replay.
+#ifndef TRN_FWD_REGEN
+#define TRN_FWD_REGEN 1
+#endif
+
+template <int MAXD>
+__global__ void __launch_bounds__(256, TRN_MINB_FWDREC) k_path_fwd_rec_regen(Params P) {
+  Cnt cnt;
+  stage_top(P.s);
+  const DeviceScene& s = P.s;
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;
+  int vhint = 0;
+  bool active = false, done = false;
+  const ViewDesc* V = nullptr;
+  long long gslot = 0, p = 0, kr = 0;
+  int pix = 0, b = 0, K = 1, D = 0;
+  unsigned mask = 0u;
+  SurfF x;
+  F3 T, rdir, L;
+  for (;;) {
+    // refill: fetch slots until enough lanes hold a path with a primary hit
+    for (;;) {
+      const unsigned need = __ballot_sync(0xffffffffu, !active && !done);
+      if (!need || __popc(__ballot_sync(0xffffffffu, active)) >= TRN_COMPACT_MIN) break;
+      const int leader = __ffs(need) - 1;
+      unsigned long long base = 0;
+      if (lane == leader) base = atomicAdd(P.work, (unsigned long long)__popc(need));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      AdjState st;
+      bool got = false;
+      if (!active && !done) {
+        const long long g = (long long)base + __popc(need & lt);
+        if (g >= P.total) done = true;
+        else got = path_adj_setup(P, g, st, vhint, cnt, false);
+      }
+      const unsigned gm = __ballot_sync(0xffffffffu, got);
+      if (!gm) continue;
+      const int gl = __ffs(gm) - 1;
+      unsigned long long rb = 0;
+      if (lane == gl) rb = atomicAdd(P.q_count, (unsigned long long)__popc(gm));
+      rb = __shfl_sync(0xffffffffu, rb, gl);
+      if (got) {
+        kr = (long long)(rb + __popc(gm & lt));
+        if (kr >= P.q_cap) {
+          atomicExch(P.err, 2);
+        } else {
+          V = st.V; gslot = st.gslot; p = st.p; pix = st.pix;
+          PathRecSoA<MAXD> r = path_soa<MAXD>(P.queue, P.q_cap, kr);
+          r.gslot = gslot; r.p = p; r.view = (int)(V - P.views); r.g = F3z();
+          x = post_intersect(s, st.h.tri, st.h.u, st.h.v);
+          r.vr[1] = {st.h.tri, st.h.u, st.h.v};
+          const F3 org = cam_pos(V->cam);
+          const float t1 = camera_factor<float>(V->cam, x.p, x.ng, 1.f);
+          T = F3(t1, t1, t1);
+          rdir = normalize(x.p - org);
+          r.Tk[1] = T;
+          F3 m1 = emitted(s, x, -rdir);
+          if (!finite3(T * m1)) m1 = F3z();
+          r.Mk[1] = m1;
+          L = T * m1;
+          K = 1;
+          D = min(V->D, MAXD);
+          mask = 0u;
+          b = 0;
+          active = true;
+        }
+      }
+    }
+    if (!__any_sync(0xffffffffu, active)) break;
+    if (active) {
+      PathRecSoA<MAXD> r = path_soa<MAXD>(P.queue, P.q_cap, kr);
+      bool fin = b >= D;
+      if (!fin) {
+        const PathSmp S{&P, V->seed, gslot, p + V->slot_off};
+        const int k = b + 1;
+        const int o = 2 + 5 * b;
+        F3 c;
+        BounceRec R;
+        const bool more = radiance_step_k<TRN_SHARED_STEPS_PATHADJ>(s, x, rdir, T, S(o), S(o + 1), S(o + 2),
+                                                                   S(o + 3), S(o + 4), c, &R, cnt);
+        if (R.nee_ok && !R.scrubbed) mask |= 1u << k;
+        L = L + c;
+        r.br[k] = {R.ltri, R.lu, R.lv, R.lpdf, R.lmis, R.prev_pdf};
+        if (!more) {
+          fin = true;
+        } else {
+          r.vr[k + 1] = {x.tri, x.u, x.v};
+          r.Tk[k + 1] = T;
+          r.Mk[k + 1] = (R.scrubbed || R.emis == 0.f) ? F3z() : R.eLe * R.emis;
+          K = k + 1;
+          if (T.x == 0.f && T.y == 0.f && T.z == 0.f) fin = true;
+        }
+        b++;
+        if (b >= D) fin = true;
+      }
+      if (fin) {
+        r.K = K;
+        r.D = D;
+        r.nee_mask = mask;
+        cnt.v[kCntPixel]++;
+        atomic_add3((V->image ? V->image : P.image + 3 * V->pix_off) + 3 * pix, L * V->inv_spp);
+        active = false;
+      }
+    }
+  }
+  flush_cnt(cnt, P.stats);
+}
+
+
 // ---------------------------------------------------------------------------
 // EvalImportance for one ray (Integrator.cpp:75-176)
 // ---------------------------------------------------------------------------
@@ -1429,6 +1543,80 @@ __global__ void __launch_bounds__(256, TRN_MINB_BODY) k_primary_body(Params P) {
     const SurfF x = post_intersect(P.s, it.x_tri, it.x_u, it.x_v);
     primary_body(P, P.views[it.view], it.gslot, it.p, x, it.rdir, F3(it.T0, it.T0, it.T0), it.w0, it.g, it.v0, it.v1,
                  it.sedge, it.p0, it.far_tri, it.n, cnt, it.dim0);
+  }
+  flush_cnt(cnt, P.stats);
+}
+
+// Path regeneration for the queue's bodies: a lane whose radiance path has
+// ended takes the next queue item at once instead of idling until the warp's
+// longest path ends (the boundary paths end after one or two bounces on
+// average, at most D). Each item runs exactly the steps of primary_body.
+#ifndef TRN_BODY_REGEN
+#define TRN_BODY_REGEN 1
+#endif
+
+__global__ void __launch_bounds__(256, TRN_MINB_BODY) k_primary_body_regen(Params P) {
+  Cnt cnt;
+  stage_top(P.s);
+  const DeviceScene& s = P.s;
+  const PrimaryItem* q = reinterpret_cast<const PrimaryItem*>(P.queue);
+  const unsigned long long n = min(*P.q_count, (unsigned long long)P.q_cap);
+  unsigned long long* next = P.q_count + 1;  // items handed out (zeroed with the round)
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;
+  bool active = false, done = false;
+  unsigned long long k = 0;
+  const ViewDesc* V = nullptr;
+  SurfF x;
+  F3 T, rdir, L;
+  int b = 0, D = 0;
+  for (;;) {
+    const unsigned need = __ballot_sync(0xffffffffu, !active && !done);
+    if (need) {
+      const int leader = __ffs(need) - 1;
+      unsigned long long base = 0;
+      if (lane == leader) base = atomicAdd(next, (unsigned long long)__popc(need));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      if (!active && !done) {
+        k = base + __popc(need & lt);
+        if (k >= n) {
+          done = true;
+        } else {
+          const PrimaryItem& it = q[k];
+          V = P.views + it.view;
+          D = V->D;
+          x = post_intersect(s, it.x_tri, it.x_u, it.x_v);
+          T = F3(it.T0, it.T0, it.T0);
+          rdir = it.rdir;
+          L = scrub(T * emitted(s, x, -rdir));
+          b = 0;
+          active = true;
+        }
+      }
+    }
+    if (!__any_sync(0xffffffffu, active)) break;
+    if (active) {
+      bool fin = b >= D;
+      if (!fin) {
+        const PrimaryItem& it = q[k];
+        const PathSmp S{&P, V->seed, it.gslot, it.p + V->slot_off};
+        const int o = it.dim0 + 5 * b;
+        F3 c;
+        const bool more = radiance_step_k<TRN_SHARED_STEPS_PRIMARY>(s, x, rdir, T, S(o), S(o + 1), S(o + 2),
+                                                                    S(o + 3), S(o + 4), c, nullptr, cnt);
+        L = L + c;
+        b++;
+        fin = !more || (T.x == 0.f && T.y == 0.f && T.z == 0.f) || b >= D;
+      }
+      if (fin) {
+        const PrimaryItem& it = q[k];
+        const float W = dot(it.g, L * it.w0);
+        if (W != 0.f && isfinite(W))
+          xdotn_vjp(P, *V, W, cam_pos(V->cam), false, -1, 0.f, 0.f, it.v0, it.v1, it.sedge, it.p0, it.far_tri, it.n,
+                    cnt);
+        active = false;
+      }
+    }
   }
   flush_cnt(cnt, P.stats);
 }
@@ -2492,7 +2680,14 @@ void launch(K kernel, const trn_launch* ln, long long total, const Params& P, cu
 #ifndef TRN_INDIRECT_SPLIT
 #define TRN_INDIRECT_SPLIT 1
 #endif
-constexpr long long kIndirectRound = 1LL << 22;  // slots per split round (queue of 4M items)
+// slots per round of the split boundary terms: 16M (one round for a 512² x
+// 64 spp term). Larger rounds give each edge more samples per sort and the
+// terms fewer kernel tails (measured: 4M 195.6, 8M 189.5, 16M 186.2 ms/step
+// on that workload), at about 5.5 GB of queue per view set.
+#ifndef TRN_ROUND_LOG2
+#define TRN_ROUND_LOG2 24
+#endif
+constexpr long long kIndirectRound = 1LL << TRN_ROUND_LOG2;
 constexpr long long kPathRound = 1LL << 21;  // paths per split round of the interior adjoint
 
 // Largest queue that any split term needs for one full round (depth <= 8
@@ -2585,7 +2780,8 @@ int pixel_split(trn_viewset* vs, Params P, const trn_launch* ln, long long total
     P.total = std::min(total, first + cap);
     k_indirect_round<<<1, 32, 0, st>>>(P.work, (unsigned long long)first, P.q_count);
     k_pixel_setup<<<grid, block, 0, st>>>(P);
-    k_primary_body<<<grid, block, 0, st>>>(P);
+    if (TRN_BODY_REGEN) k_primary_body_regen<<<grid, block, 0, st>>>(P);
+    else k_primary_body<<<grid, block, 0, st>>>(P);
     count_launch(3);
   }
   TRN_CUDA_TRY(cudaGetLastError());
@@ -2697,7 +2893,8 @@ int primary_split(trn_viewset* vs, Params P, const trn_launch* ln, long long tot
     if (!ordered && order_round(vs, P, TRN_PRIMARY_EDGE, st)) return -1;
     k_indirect_round<<<1, 32, 0, st>>>(P.work, (unsigned long long)first, P.q_count);
     k_primary_setup<<<grid, block, 0, st>>>(P);
-    k_primary_body<<<grid, block, 0, st>>>(P);
+    if (TRN_BODY_REGEN) k_primary_body_regen<<<grid, block, 0, st>>>(P);
+    else k_primary_body<<<grid, block, 0, st>>>(P);
     count_launch(3);
   }
   TRN_CUDA_TRY(cudaGetLastError());
@@ -2817,7 +3014,12 @@ int path_cache_fwd(trn_viewset* vs, Params P, const trn_launch* ln, const trn_re
   P.queue = vs->pc;
   P.q_count = vs->pc_count;
   P.q_cap = total;
-  if (shallow) launch(k_path_fwd_rec<8>, ln, total, P, st); else launch(k_path_fwd_rec<kMaxDepth>, ln, total, P, st);
+  if (TRN_FWD_REGEN) {
+    if (shallow) launch(k_path_fwd_rec_regen<8>, ln, total, P, st);
+    else launch(k_path_fwd_rec_regen<kMaxDepth>, ln, total, P, st);
+  } else {
+    if (shallow) launch(k_path_fwd_rec<8>, ln, total, P, st); else launch(k_path_fwd_rec<kMaxDepth>, ln, total, P, st);
+  }
   TRN_CUDA_TRY(cudaGetLastError());
   vs->pc_key = path_key(vs, o, spp_override, total);
   vs->pc_valid = true;

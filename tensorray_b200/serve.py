@@ -33,12 +33,11 @@ from ._abi import TRN_DIRECT_EDGE, TRN_PATH_TRACER, TRN_PRIMARY_EDGE, TrnView
 
 PHASE_FWD, PHASE_GRAD, PHASE_FINISH, PHASE_DONE = 0, 1, 2, 3
 
-# Device bytes a view set may hold for the queues of the split integrator
-# kernels (allocated by the library on first use; at most 2M path records of
-# about 620 bytes at depth <= 8, or 4M boundary samples) and for the boundary
-# set-up's run order (16 bytes per slot of a 4M-slot round plus the sort's
-# temporary storage).
-VIEWSET_QUEUE_BYTES = 1_500_000_000
+# Device bytes a gradient view set holds for the queues of the split
+# integrator kernels (one round: 16M boundary samples, at most about 312 bytes
+# each at depth <= 8) and for the boundary set-up's run order (16 bytes per
+# slot plus the sort's temporary storage). Forward view sets hold none.
+VIEWSET_QUEUE_BYTES = 5_600_000_000
 
 
 @dataclass
@@ -87,8 +86,8 @@ class Server:
         # gradient view sets reserve their round buffers for this depth when
         # created (deeper requests still run; their first batch grows them)
         self.max_depth = int(max_depth)
-        # the forward and gradient view sets of every scene hold one queue each
-        self.reserve = 2 * len(scenes) * VIEWSET_QUEUE_BYTES
+        # the gradient view set of every scene holds one round of queues
+        self.reserve = len(scenes) * VIEWSET_QUEUE_BYTES
         self.budget = int(hbm_budget_bytes) - self.reserve
         self.chunk_spp = chunk_spp
         self.iter_samples = int(iter_samples)

@@ -137,7 +137,7 @@ def test_reserved_set_allocates_nothing_later(setup):
     vs.reserve(D)
     torch.cuda.synchronize()
     free1 = torch.cuda.mem_get_info()[0]
-    assert 0 < free0 - free1 < 1.7e9, f"reserved {free0 - free1} bytes"
+    assert 0 < free0 - free1 < 6e9, f"reserved {free0 - free1} bytes"
     for integ in range(5):
         scene.clear_grads()
         torch.cuda.synchronize()
