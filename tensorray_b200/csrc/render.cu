@@ -50,7 +50,8 @@ struct Params {
   const float* aq_cdf;        // [E] leaf distribution
   const float* aq_int;        // [2] integral, sum of weight x volume
   // queues of the split kernels (nullptr = fused kernel): q_count[0] counts
-  // `queue`, q_count[1] counts `queue2` (the indirect term's second stage)
+  // `queue`, q_count[1] counts `queue2` (the indirect term's second stage),
+  // q_count[2] hands out the items of `queue` to a regenerating stage
   void* queue;
   void* queue2;
   unsigned long long* q_count;
@@ -2196,10 +2197,185 @@ __global__ void __launch_bounds__(256, TRN_MINB_INDIRECT) k_indirect_sensor_q(Pa
   flush_cnt(cnt, P.stats);
 }
 
+// k_indirect_sensor_q with path regeneration: a lane whose importance path
+// has ended queues its item (when a depth reached the image) and takes the
+// next set-up item at once. Each item runs exactly the steps of
+// indirect_sensor.
+#ifndef TRN_SENSOR_REGEN
+#define TRN_SENSOR_REGEN 1
+#endif
+
+template <int MAXD>
+__global__ void __launch_bounds__(256, TRN_MINB_INDIRECT) k_indirect_sensor_regen(Params P) {
+  Cnt cnt;
+  stage_top(P.s);
+  const DeviceScene& s = P.s;
+  const IndirectSetupItem* qa = reinterpret_cast<const IndirectSetupItem*>(P.queue);
+  IndirectItem<MAXD>* qb = reinterpret_cast<IndirectItem<MAXD>*>(P.queue2);
+  const unsigned long long n = min(P.q_count[0], (unsigned long long)P.q_cap);
+  unsigned long long* next = P.q_count + 2;
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;
+  bool active = false, done = false;
+  unsigned long long k = 0;
+  const ViewDesc* V = nullptr;
+  SurfF xx;
+  F3 T, rd;
+  F3 sc[MAXD];
+  int b = 0, D = 0, bmin = 0;
+  for (;;) {
+    const unsigned need = __ballot_sync(0xffffffffu, !active && !done);
+    if (need) {
+      const int leader = __ffs(need) - 1;
+      unsigned long long base = 0;
+      if (lane == leader) base = atomicAdd(next, (unsigned long long)__popc(need));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      if (!active && !done) {
+        k = base + __popc(need & lt);
+        if (k >= n) {
+          done = true;
+        } else {
+          const IndirectSetupItem& a = qa[k];
+          V = P.views + a.view;
+          D = min(V->D, MAXD);
+          xx = post_intersect(s, a.xs_tri, a.xs_u, a.xs_v);
+          rd = a.rdir;
+          T = F3(1.f, 1.f, 1.f);
+          for (int j = 0; j < D - 1; j++) sc[j] = F3z();
+          bmin = D;
+          b = 0;
+          active = true;
+        }
+      }
+    }
+    if (!__any_sync(0xffffffffu, active)) break;
+    bool fin = false;
+    if (active) {
+      fin = b >= D - 1;
+      if (!fin) {
+        const IndirectSetupItem& a = qa[k];
+        const PathSmp S{&P, V->seed, a.gslot, a.p + V->slot_off};
+        const int o = 3 + 5 * (D - 1) + 3 * b;
+        F3 c;
+        int pix;
+        const bool more = importance_step_shared(s, V->cam, xx, rd, T, S(o), S(o + 1), S(o + 2), c, pix, cnt);
+        if (pix >= 0) {
+          sc[b] = g_at(P, *V, pix) * c;
+          if (sc[b].x != 0.f || sc[b].y != 0.f || sc[b].z != 0.f) bmin = min(bmin, b);
+        }
+        b++;
+        fin = !more || b >= D - 1;
+      }
+    }
+    const bool push = fin && bmin < D - 1;
+    const unsigned m = __ballot_sync(0xffffffffu, push);
+    if (m) {
+      const int leader = __ffs(m) - 1;
+      unsigned long long base = 0;
+      if (lane == leader) base = atomicAdd(P.q_count + 1, (unsigned long long)__popc(m));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      const unsigned long long j = base + __popc(m & lt);
+      if (push && j >= (unsigned long long)P.q_cap) atomicExch(P.err, 2);
+      if (push && j < (unsigned long long)P.q_cap) {
+        const IndirectSetupItem& a = qa[k];
+        IndirectItem<MAXD>& it = qb[j];
+        it.gslot = a.gslot; it.p = a.p; it.view = a.view; it.jmax = D - 2 - bmin; it.D = D;
+        it.xe_tri = a.xe_tri; it.xe_u = a.xe_u; it.xe_v = a.xe_v;
+        it.xs_tri = a.xs_tri; it.xs_u = a.xs_u; it.xs_v = a.xs_v;
+        it.rdir = a.rdir; it.p0 = a.p0; it.n = a.n; it.w0 = a.w0; it.sedge = a.sedge;
+        it.v0 = a.v0; it.v1 = a.v1; it.far_tri = a.far_tri;
+        for (int q = 0; q < D - 1; q++) it.sc[q] = sc[q];
+      }
+    }
+    if (fin) active = false;
+  }
+  flush_cnt(cnt, P.stats);
+}
+
+// k_indirect_emitter with path regeneration (three-stage form): a lane whose
+// emitter-side path has ended adds the remaining depths' terms with its last
+// radiance, as the loop form does after the path dies, scatters, and takes
+// the next item at once. Each item runs exactly the steps and the
+// additions of indirect_emitter.
+#ifndef TRN_EMITTER_REGEN
+#define TRN_EMITTER_REGEN 1
+#endif
+
+template <int MAXD>
+__global__ void __launch_bounds__(256, TRN_MINB_INDIRECT) k_indirect_emitter_regen(Params P) {
+  Cnt cnt;
+  stage_top(P.s);
+  const DeviceScene& s = P.s;
+  const IndirectItem<MAXD>* q = reinterpret_cast<const IndirectItem<MAXD>*>(P.queue2);
+  const unsigned long long n = min(P.q_count[1], (unsigned long long)P.q_cap);
+  unsigned long long* next = P.q_count + 3;
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;
+  bool active = false, done = false;
+  unsigned long long k = 0;
+  const ViewDesc* V = nullptr;
+  SurfF xx;
+  F3 T, rd, cur;
+  float W = 0.f;
+  int j = 0;
+  for (;;) {
+    const unsigned need = __ballot_sync(0xffffffffu, !active && !done);
+    if (need) {
+      const int leader = __ffs(need) - 1;
+      unsigned long long base = 0;
+      if (lane == leader) base = atomicAdd(next, (unsigned long long)__popc(need));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      if (!active && !done) {
+        k = base + __popc(need & lt);
+        if (k >= n) {
+          done = true;
+        } else {
+          const IndirectItem<MAXD>& it = q[k];
+          V = P.views + it.view;
+          xx = post_intersect(s, it.xe_tri, it.xe_u, it.xe_v);
+          rd = -it.rdir;
+          T = F3(1.f, 1.f, 1.f);
+          cur = F3z();
+          W = 0.f;
+          j = 0;
+          active = true;
+        }
+      }
+    }
+    if (!__any_sync(0xffffffffu, active)) break;
+    if (active) {
+      const IndirectItem<MAXD>& it = q[k];
+      const int D = it.D, jmax = it.jmax;
+      bool alive = false;
+      if (j <= jmax) {
+        const PathSmp S{&P, V->seed, it.gslot, it.p + V->slot_off};
+        const int o = 3 + 5 * j;
+        F3 c;
+        alive = radiance_step_shared(s, xx, rd, T, S(o), S(o + 1), S(o + 2), S(o + 3), S(o + 4), c, nullptr, cnt);
+        cur = cur + c;
+        if (T.x == 0.f && T.y == 0.f && T.z == 0.f) alive = false;
+        W += dot(it.sc[D - 2 - j], cur) * it.w0;
+        j++;
+      }
+      if (!alive || j > jmax) {
+        // the path has ended: the remaining depths pair with the last radiance
+        for (; j <= jmax; j++) W += dot(it.sc[D - 2 - j], cur) * it.w0;
+        if (W != 0.f && isfinite(W)) {
+          const SurfF xs = post_intersect(s, it.xs_tri, it.xs_u, it.xs_v);
+          xdotn_vjp(P, *V, W, xs.p, true, it.xs_tri, it.xs_u, it.xs_v, it.v0, it.v1, it.sedge, it.p0, it.far_tri,
+                    it.n, cnt);
+        }
+        active = false;
+      }
+    }
+  }
+  flush_cnt(cnt, P.stats);
+}
+
 // Slot range of one split round: the work counter starts at `first`, the
 // queue is empty.
 __global__ void k_indirect_round(unsigned long long* work, unsigned long long first, unsigned long long* q_count) {
-  if (threadIdx.x == 0) { *work = first; q_count[0] = 0ull; q_count[1] = 0ull; }
+  if (threadIdx.x == 0) { *work = first; q_count[0] = 0ull; q_count[1] = 0ull; q_count[2] = 0ull; q_count[3] = 0ull; }
 }
 
 // Sort keys of one round of a split boundary set-up: view x (E + 1) + the
@@ -2726,7 +2902,7 @@ int ensure_queue(trn_viewset* vs, size_t need, cudaStream_t st) {
     if (cudaMalloc(&vs->iq, bytes) != cudaSuccess) { set_error("boundary term: out of memory for its queue"); return -1; }
     vs->iq_bytes = bytes;
   }
-  if (!vs->iq_count && cudaMalloc(&vs->iq_count, 2 * sizeof(unsigned long long)) != cudaSuccess) {
+  if (!vs->iq_count && cudaMalloc(&vs->iq_count, 4 * sizeof(unsigned long long)) != cudaSuccess) {
     set_error("boundary term: out of memory");
     return -1;
   }
@@ -2930,11 +3106,15 @@ int indirect_split(trn_viewset* vs, Params P, const trn_launch* ln, long long to
     if (TRN_INDIRECT_STAGES == 3) {
       k_indirect_setup<<<grid, block, 0, st>>>(P);
       if (shallow) {
-        k_indirect_sensor_q<8><<<grid, block, 0, st>>>(P);
-        k_indirect_emitter<8><<<grid, block, 0, st>>>(P);
+        if (TRN_SENSOR_REGEN) k_indirect_sensor_regen<8><<<grid, block, 0, st>>>(P);
+        else k_indirect_sensor_q<8><<<grid, block, 0, st>>>(P);
+        if (TRN_EMITTER_REGEN) k_indirect_emitter_regen<8><<<grid, block, 0, st>>>(P);
+        else k_indirect_emitter<8><<<grid, block, 0, st>>>(P);
       } else {
-        k_indirect_sensor_q<kMaxDepth><<<grid, block, 0, st>>>(P);
-        k_indirect_emitter<kMaxDepth><<<grid, block, 0, st>>>(P);
+        if (TRN_SENSOR_REGEN) k_indirect_sensor_regen<kMaxDepth><<<grid, block, 0, st>>>(P);
+        else k_indirect_sensor_q<kMaxDepth><<<grid, block, 0, st>>>(P);
+        if (TRN_EMITTER_REGEN) k_indirect_emitter_regen<kMaxDepth><<<grid, block, 0, st>>>(P);
+        else k_indirect_emitter<kMaxDepth><<<grid, block, 0, st>>>(P);
       }
       count_launch(4);
     } else {
@@ -3181,7 +3361,11 @@ int single_view(trn_scene* s, const trn_camera* cam, trn_viewset** out) {
   std::memset(&v, 0, sizeof(v));
   std::memcpy(&v.camera, cam, sizeof(trn_camera));
   if (s->single) {
-    if (set_views(s->single, 1, &v)) return -1;
+    // an unchanged camera keeps the uploaded table: no restaging, so the host
+    // does not wait for the previous call's upload and can run ahead
+    const bool same = s->single->nviews == 1 && s->single->h_views.size() == 1 &&
+                      std::memcmp(&s->single->h_views[0], &v, sizeof(v)) == 0;
+    if (!same && set_views(s->single, 1, &v)) return -1;
   } else if (trn_viewset_create(s, 1, &v, &s->single)) {
     return -1;
   }
