@@ -76,12 +76,19 @@ def parse():
 
 
 class Clocks:
-    """nvidia-smi sampling during the timed region."""
+    """nvidia-smi sampling during the timed region. start() may come before
+    the warm-up (nvidia-smi's own start-up then stays out of the timed
+    steps); mark() at the start of the timed region keeps only the samples
+    taken after it."""
 
     def __init__(self, index: int):
         self.index = index
         self.proc = None
+        self.t_mark = None
         self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+
+    def mark(self):
+        self.t_mark = time.time()
 
     def start(self):
         os.makedirs(os.path.dirname(self.path), exist_ok=True)
@@ -89,7 +96,7 @@ class Clocks:
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}",
-                 "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "--query-gpu=timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
                  "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
                  "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
                  "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
@@ -103,10 +110,18 @@ class Clocks:
         self.proc.wait()
         self.f.close()
         sm, smax, reasons = [], [], set()
+        from datetime import datetime
         for line in open(self.path):
             p = [x.strip() for x in line.split(",")]
-            if len(p) < 9:
+            if len(p) < 10:
                 continue
+            if self.t_mark is not None:
+                try:
+                    if datetime.strptime(p[0], "%Y/%m/%d %H:%M:%S.%f").timestamp() < self.t_mark:
+                        continue
+                except ValueError:
+                    pass
+            p = p[1:]
             try:
                 sm.append(float(p[1]))
                 smax.append(float(p[2]))
@@ -258,14 +273,18 @@ def main():
         gr = scene.get_grads(clear=True)
         return trd.allreduce_grads(gr)
 
+    # the clock sampler starts before the warm-up, so that nvidia-smi's own
+    # start-up does not fall into a timed step; only samples taken during the
+    # timed steps count
+    clocks = Clocks(local)
+    clocks.start()
     for _ in range(a.warmup):
         step()
     torch.cuda.synchronize()
 
     ev_keys = ["fwd"] + kernel_names[1:]
     per_kernel = {k: [] for k in ev_keys}
-    clocks = Clocks(local)
-    clocks.start()
+    clocks.mark()
     launches0 = lib.trn_kernel_launches()
     total_ms = 0.0
     step_ms = []
