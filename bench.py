@@ -24,6 +24,7 @@ import math
 import os
 import statistics
 import subprocess
+import tempfile
 import sys
 import time
 
@@ -85,7 +86,10 @@ class Clocks:
         self.index = index
         self.proc = None
         self.t_mark = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        # raw samples go to TRN_CLOCKS_DIR when set (kept for inspection),
+        # else to the temporary directory
+        d = os.environ.get("TRN_CLOCKS_DIR") or tempfile.gettempdir()
+        self.path = os.path.join(d, f"clocks_{os.getpid()}.csv")
 
     def mark(self):
         self.t_mark = time.time()
