@@ -232,10 +232,21 @@ int trn_render_grad(trn_scene* scene, const trn_camera* camera, const trn_render
  * array compiled into the library (about 8 MiB, held on every GPU that loads
  * the library until the process exits), and the call does not synchronise
  * the stream.
+ * - Speed: it runs each term as one fused kernel (no split stages, no queues,
+ *   no edge-sorted set-up order, since those need scratch that grows with
+ *   the launch), which is about 20-50 % slower per term than
+ *   trn_render_grad.
  * - Limit: for TRN_PRIMARY_EDGE the scene may have at most 1048576 edges;
  *   larger scenes are rejected with an error.
+ * - The scene's device must be the current device; otherwise the call
+ *   returns an error.
  * - The first call on each device looks up the array's device address
  *   (cudaGetSymbolAddress); make that first call before any stream capture.
+ *   The fused kernels keep large per-thread stack frames, so the first call
+ *   in a process may also make the CUDA driver enlarge its local-memory
+ *   reservation for the context (the driver's own allocation, not one by
+ *   this library); making the first call during set-up keeps that out of the
+ *   loop that must not allocate.
  * - Calls that overlap on the GPU (other streams or host threads, same
  *   device) share the array and race; the array keeps the last call's
  *   contents, and each call rewrites what it reads. */

@@ -87,6 +87,71 @@ def uniform_table(seed: int, dims: int, slots: int) -> torch.Tensor:
 
 
 # ---------------------------------------------------------------------------
+# deterministic trigonometry (the library's sincos_det / acos_det, csrc/common.cuh)
+# ---------------------------------------------------------------------------
+# binary64 evaluation with individually rounded operations, rounded once to
+# float32: Cody & Waite reduction by pi/2 plus Taylor polynomials for sin and
+# cos, the Maclaurin series of asin for acos. The GPU runs the identical
+# sequence of IEEE operations, so sampled directions agree bit for bit.
+_PI_D = 3.141592653589793
+_PIO2_D = 1.5707963267948966
+_TWO_OVER_PI_D = 0.6366197723675814
+_SIN_C = (-1.0 / 1307674368000.0, 1.0 / 6227020800.0, -1.0 / 39916800.0, 1.0 / 362880.0, -1.0 / 5040.0,
+          1.0 / 120.0, -1.0 / 6.0)
+_COS_C = (1.0 / 20922789888000.0, -1.0 / 87178291200.0, 1.0 / 479001600.0, -1.0 / 3628800.0, 1.0 / 40320.0,
+          -1.0 / 720.0, 1.0 / 24.0, -0.5)
+_ASIN_C = (0.0030578216492580306, 0.003297059503473485, 0.0035692053938259347, 0.003880964558837669,
+           0.004240907093679363, 0.004660143486915096, 0.005153309682319905, 0.005740037670841924,
+           0.006447210311889649, 0.0073125258735988454, 0.008390335809616815, 0.009761609529194078,
+           0.011551800896139705, 0.01396484375, 0.017352764423076924, 0.022372159090909092,
+           0.030381944444444444, 0.044642857142857144, 0.075, 0.16666666666666666)
+
+
+def _horner(c, z2):
+    p = np.full_like(z2, c[0])
+    for k in c[1:]:
+        p = k + z2 * p
+    return p
+
+
+def _np64(x):
+    if torch.is_tensor(x):
+        x = x.detach().cpu().numpy()
+    return np.asarray(x, np.float32).astype(np.float64)
+
+
+def sincos_det(x):
+    """sin and cos of a float32 tensor, bit-identical to the GPU's sincos_det."""
+    xd = _np64(x)
+    k = np.floor(xd * _TWO_OVER_PI_D + 0.5)
+    y = xd - k * _PIO2_D
+    y2 = y * y
+    sy = y + (y * y2) * _horner(_SIN_C, y2)
+    cy = 1.0 + y2 * _horner(_COS_C, y2)
+    q = k.astype(np.int64) & 3
+    sd = np.select([q == 0, q == 1, q == 2], [sy, cy, -sy], -cy)
+    cd = np.select([q == 0, q == 1, q == 2], [cy, -sy, -cy], sy)
+    return torch.from_numpy(sd.astype(np.float32)), torch.from_numpy(cd.astype(np.float32))
+
+
+def acos_det(x):
+    """acos of a float32 tensor, bit-identical to the GPU's acos_det."""
+    xd = _np64(x)
+    a = np.abs(xd)
+    with np.errstate(invalid="ignore"):
+        lo = np.minimum(a, 0.5)
+        t_lo = lo + (lo * (lo * lo)) * _horner(_ASIN_C, lo * lo)
+        r_lo = np.where(xd < 0, _PIO2_D + t_lo, _PIO2_D - t_lo)
+        z = np.sqrt(np.clip((1.0 - a) * 0.5, 0.0, None))
+        z = np.minimum(z, 0.5)
+        t_hi = 2.0 * (z + (z * (z * z)) * _horner(_ASIN_C, z * z))
+        r_hi = np.where(xd < 0, _PI_D - t_hi, t_hi)
+        r = np.where(a <= 0.5, r_lo, r_hi)
+        r = np.where(a <= 1.0, r, np.nan)
+    return torch.from_numpy(r.astype(np.float32))
+
+
+# ---------------------------------------------------------------------------
 # small vector helpers on [N, 3] tensors
 # ---------------------------------------------------------------------------
 def dot(a, b):
@@ -594,7 +659,8 @@ def cosine_hemisphere(s0, s1):
     zero = (r1 == 0) & (r2 == 0)
     r = torch.where(zero, torch.zeros_like(r), r)
     phi = torch.where(zero, torch.zeros_like(phi), phi)
-    x, y = r * torch.cos(phi), r * torch.sin(phi)
+    sp, cp = sincos_det(phi)
+    x, y = r * cp, r * sp
     z = torch.sqrt(torch.clamp(1.0 - x * x - y * y, min=1e-4))
     return torch.stack([x, y, z], -1)
 
@@ -607,7 +673,8 @@ def disk_concentric(s0, s1):
     rp = torch.where(q13, x, y)
     phi_ = 0.25 * PI * rp / r
     phi = torch.where(is_zero, torch.zeros_like(phi_), torch.where(q13, 0.5 * PI - phi_, phi_))
-    return r * torch.cos(phi), r * torch.sin(phi)
+    sp, cp = sincos_det(phi)
+    return r * cp, r * sp
 
 
 def vndf_sample(v, alpha, s0, s1):
@@ -1114,15 +1181,17 @@ def indirect_edge(scene, cam, spp, D, smp):
     z = torch.clamp(1.0 - 2.0 * r1, max=np.float32(1.0 - EDGE_EPS))
     r = torch.sqrt(torch.clamp(1.0 - z * z, min=0.0))
     phi = 2.0 * PI * r2
-    dir_b = tg * (r * torch.cos(phi))[:, None] + bt * (r * torch.sin(phi))[:, None] + nrm * z[:, None]
+    sp, cp = sincos_det(phi)
+    dir_b = tg * (r * cp)[:, None] + bt * (r * sp)[:, None] + nrm * z[:, None]
     # interior edges: two-sided wedge
-    phi0 = torch.acos(dot(n0, n1))
+    phi0 = acos_det(dot(n0, n1))
     zz = normalize(n0 + n1)
     yy = normalize(cross(n0, zz))
     xx = cross(yy, zz)
     ph = (r1 - 0.5) * phi0
     ph = torch.minimum(torch.maximum(ph, -0.5 * phi0 + EDGE_EPS), 0.5 * phi0 - EDGE_EPS)
-    x1 = xx * torch.cos(ph)[:, None] + zz * torch.sin(ph)[:, None]
+    sp, cp = sincos_det(ph)
+    x1 = xx * cp[:, None] + zz * sp[:, None]
     m0 = r2 > 0.5
     bq = 4.0 * r2 - torch.where(m0, torch.full_like(r2, 3.0), torch.ones_like(r2))
     aq = torch.sqrt(1.0 - bq * bq) * (1.0 - m0.to(F32) * 2.0)

@@ -26,15 +26,127 @@ constexpr float kInvPi = 0.31830988618379067154f;
 constexpr float kPiOver2 = 1.57079632679489661923f;
 constexpr float kPiOver4 = 0.78539816339744830962f;
 
+// ---- deterministic trigonometry for the sampling code ----------------------
+// The directions a path takes depend on sin/cos (cosine-weighted hemisphere,
+// concentric disk, edge-wedge sampling) and acos (wedge angle). CUDA's cosf
+// and the CPU's libm round differently in the last ulp, and one ulp in a
+// sampled direction can send a grazing ray to another triangle. These
+// versions are evaluated in binary64 with individually rounded operations
+// only (explicit _rn intrinsics on the device; no contraction on the host),
+// then rounded once to float, so the CPU restatement reproduces every bit
+// with numpy float64. Methods (no library code involved):
+//   * sin/cos: reduction by the nearest multiple k of pi/2 (Cody & Waite,
+//     "Software Manual for the Elementary Functions", 1980; one binary64 pi/2
+//     is exact enough for |x| < 64), then the Taylor polynomials of sin and
+//     cos, coefficients (-1)^j/(2j+1)! and (-1)^j/(2j)!, to degree 15 and 16
+//     on |y| <= pi/4 (truncation below 2e-14);
+//   * acos: the Maclaurin series of asin, coefficients
+//     (2n)! / (4^n (n!)^2 (2n+1)), n <= 20, on [0, 1/2] (truncation below
+//     1e-15), and acos(a) = 2 asin(sqrt((1 - a)/2)) for a > 1/2.
+// Inputs outside [-1, 1] give NaN from acos_det, as acosf does.
+#ifdef __CUDA_ARCH__
+#define TRN_DMUL(a, b) __dmul_rn((a), (b))
+#define TRN_DADD(a, b) __dadd_rn((a), (b))
+#define TRN_DSUB(a, b) __dsub_rn((a), (b))
+#define TRN_DSQRT(a) __dsqrt_rn((a))
+#else
+#define TRN_DMUL(a, b) ((a) * (b))
+#define TRN_DADD(a, b) ((a) + (b))
+#define TRN_DSUB(a, b) ((a) - (b))
+#define TRN_DSQRT(a) sqrt((a))
+#endif
+constexpr double kPiD = 3.141592653589793;
+constexpr double kPiOver2D = 1.5707963267948966;
+constexpr double kTwoOverPiD = 0.6366197723675814;
+
+TRN_HD double sin_poly_d(double y) {  // |y| <= pi/4
+  const double y2 = TRN_DMUL(y, y);
+  double p = -1.0 / 1307674368000.0;
+  p = TRN_DADD(1.0 / 6227020800.0, TRN_DMUL(y2, p));
+  p = TRN_DADD(-1.0 / 39916800.0, TRN_DMUL(y2, p));
+  p = TRN_DADD(1.0 / 362880.0, TRN_DMUL(y2, p));
+  p = TRN_DADD(-1.0 / 5040.0, TRN_DMUL(y2, p));
+  p = TRN_DADD(1.0 / 120.0, TRN_DMUL(y2, p));
+  p = TRN_DADD(-1.0 / 6.0, TRN_DMUL(y2, p));
+  return TRN_DADD(y, TRN_DMUL(TRN_DMUL(y, y2), p));
+}
+TRN_HD double cos_poly_d(double y) {  // |y| <= pi/4
+  const double y2 = TRN_DMUL(y, y);
+  double p = 1.0 / 20922789888000.0;
+  p = TRN_DADD(-1.0 / 87178291200.0, TRN_DMUL(y2, p));
+  p = TRN_DADD(1.0 / 479001600.0, TRN_DMUL(y2, p));
+  p = TRN_DADD(-1.0 / 3628800.0, TRN_DMUL(y2, p));
+  p = TRN_DADD(1.0 / 40320.0, TRN_DMUL(y2, p));
+  p = TRN_DADD(-1.0 / 720.0, TRN_DMUL(y2, p));
+  p = TRN_DADD(1.0 / 24.0, TRN_DMUL(y2, p));
+  p = TRN_DADD(-0.5, TRN_DMUL(y2, p));
+  return TRN_DADD(1.0, TRN_DMUL(y2, p));
+}
+TRN_HD void sincos_det(float x, float& s, float& c) {
+  const double xd = (double)x;
+  const double k = floor(TRN_DADD(TRN_DMUL(xd, kTwoOverPiD), 0.5));
+  const double y = TRN_DSUB(xd, TRN_DMUL(k, kPiOver2D));
+  const double sy = sin_poly_d(y), cy = cos_poly_d(y);
+  const int q = ((int)k) & 3;
+  double sd, cd;
+  if (q == 0) { sd = sy; cd = cy; }
+  else if (q == 1) { sd = cy; cd = -sy; }
+  else if (q == 2) { sd = -sy; cd = -cy; }
+  else { sd = -cy; cd = sy; }
+  s = (float)sd;
+  c = (float)cd;
+}
+TRN_HD double asin_series_d(double z) {  // 0 <= z <= 1/2
+  const double z2 = TRN_DMUL(z, z);
+  double p = 0.0030578216492580306;
+  p = TRN_DADD(0.003297059503473485, TRN_DMUL(z2, p));
+  p = TRN_DADD(0.0035692053938259347, TRN_DMUL(z2, p));
+  p = TRN_DADD(0.003880964558837669, TRN_DMUL(z2, p));
+  p = TRN_DADD(0.004240907093679363, TRN_DMUL(z2, p));
+  p = TRN_DADD(0.004660143486915096, TRN_DMUL(z2, p));
+  p = TRN_DADD(0.005153309682319905, TRN_DMUL(z2, p));
+  p = TRN_DADD(0.005740037670841924, TRN_DMUL(z2, p));
+  p = TRN_DADD(0.006447210311889649, TRN_DMUL(z2, p));
+  p = TRN_DADD(0.0073125258735988454, TRN_DMUL(z2, p));
+  p = TRN_DADD(0.008390335809616815, TRN_DMUL(z2, p));
+  p = TRN_DADD(0.009761609529194078, TRN_DMUL(z2, p));
+  p = TRN_DADD(0.011551800896139705, TRN_DMUL(z2, p));
+  p = TRN_DADD(0.01396484375, TRN_DMUL(z2, p));
+  p = TRN_DADD(0.017352764423076924, TRN_DMUL(z2, p));
+  p = TRN_DADD(0.022372159090909092, TRN_DMUL(z2, p));
+  p = TRN_DADD(0.030381944444444444, TRN_DMUL(z2, p));
+  p = TRN_DADD(0.044642857142857144, TRN_DMUL(z2, p));
+  p = TRN_DADD(0.075, TRN_DMUL(z2, p));
+  p = TRN_DADD(0.16666666666666666, TRN_DMUL(z2, p));
+  return TRN_DADD(z, TRN_DMUL(TRN_DMUL(z, z2), p));
+}
+TRN_HD float acos_det(float x) {
+  const double xd = (double)x;
+  const double a = xd < 0.0 ? -xd : xd;
+  if (!(a <= 1.0)) return nanf("");
+  double r;
+  if (a <= 0.5) {
+    const double t = asin_series_d(a);
+    r = xd < 0.0 ? TRN_DADD(kPiOver2D, t) : TRN_DSUB(kPiOver2D, t);
+  } else {
+    const double z = TRN_DSQRT(TRN_DMUL(TRN_DSUB(1.0, a), 0.5));
+    const double t = TRN_DMUL(2.0, asin_series_d(z));
+    r = xd < 0.0 ? TRN_DSUB(kPiD, t) : t;
+  }
+  return (float)r;
+}
+TRN_HD float cos_det(float x) { float s, c; sincos_det(x, s, c); return c; }
+TRN_HD float sin_det(float x) { float s, c; sincos_det(x, s, c); return s; }
+
 // ---- scalar helpers that dispatch on float / dual --------------------------
 TRN_HD float val(float x) { return x; }
 TRN_HD float sqrt_(float x) { return sqrtf(x); }
 TRN_HD float abs_(float x) { return fabsf(x); }
 TRN_HD float exp_(float x) { return expf(x); }
 TRN_HD float log_(float x) { return logf(x); }
-TRN_HD float cos_(float x) { return cosf(x); }
-TRN_HD float sin_(float x) { return sinf(x); }
-TRN_HD float acos_(float x) { return acosf(x); }
+TRN_HD float cos_(float x) { return cos_det(x); }
+TRN_HD float sin_(float x) { return sin_det(x); }
+TRN_HD float acos_(float x) { return acos_det(x); }
 TRN_HD float detach(float x) { return x; }
 TRN_HD float fmax_(float a, float b) { return fmaxf(a, b); }
 TRN_HD float fmin_(float a, float b) { return fminf(a, b); }

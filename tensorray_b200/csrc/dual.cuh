@@ -126,19 +126,19 @@ template <int N> TRN_HD Dual<N> log_(const Dual<N>& a) {
   return r;
 }
 template <int N> TRN_HD Dual<N> cos_(const Dual<N>& a) {
-  Dual<N> r; float s, c; sincosf(a.v, &s, &c); r.v = c;
+  Dual<N> r; float s, c; sincos_det(a.v, s, c); r.v = c;
 #pragma unroll
   for (int i = 0; i < N; i++) r.d[i] = -s * a.d[i];
   return r;
 }
 template <int N> TRN_HD Dual<N> sin_(const Dual<N>& a) {
-  Dual<N> r; float s, c; sincosf(a.v, &s, &c); r.v = s;
+  Dual<N> r; float s, c; sincos_det(a.v, s, c); r.v = s;
 #pragma unroll
   for (int i = 0; i < N; i++) r.d[i] = c * a.d[i];
   return r;
 }
 template <int N> TRN_HD Dual<N> acos_(const Dual<N>& a) {
-  Dual<N> r; r.v = acosf(a.v);
+  Dual<N> r; r.v = acos_det(a.v);
   float k = -1.f / sqrtf(1.f - a.v * a.v);
 #pragma unroll
   for (int i = 0; i < N; i++) r.d[i] = k * a.d[i];

@@ -1926,18 +1926,22 @@ TRN_D bool indirect_setup(const Params& P, long long gslot, EdgeState& st, int& 
     const float z = fminf(1.f - 2.f * r1, 1.f - kEdgeEps);
     const float r = sqrtf(fmaxf(0.f, 1.f - z * z));
     const float phi = 2.f * kPi * r2;
-    dir = tg * (r * cosf(phi)) + bt * (r * sinf(phi)) + nrm * z;
+    float sp, cp;
+    sincos_det(phi, sp, cp);
+    dir = tg * (r * cp) + bt * (r * sp) + nrm * z;
     pdf_d = 0.25f / kPi;
   } else {
     const F3 n1 = load3(s.fnormal, f1);
-    const float phi0 = acosf(dot(n0, n1));
+    const float phi0 = acos_det(dot(n0, n1));
     pdf_d = 0.25f / phi0;
     const F3 zz = normalize(n0 + n1);
     const F3 yy = normalize(cross(n0, zz));
     const F3 xx = cross(yy, zz);
     float phi = (r1 - 0.5f) * phi0;
     phi = fminf(fmaxf(phi, -0.5f * phi0 + kEdgeEps), 0.5f * phi0 - kEdgeEps);
-    const F3 x1 = xx * cosf(phi) + zz * sinf(phi);
+    float sp, cp;
+    sincos_det(phi, sp, cp);
+    const F3 x1 = xx * cp + zz * sp;
     const bool m0 = r2 > 0.5f;
     const float bq = 4.f * r2 - (m0 ? 3.f : 1.f);
     const float aq = sqrtf(1.f - bq * bq) * (1.f - (m0 ? 1.f : 0.f) * 2.f);
@@ -3531,10 +3535,24 @@ std::atomic<unsigned char*> g_noalloc_base[kNoAllocMaxDevices];
 // the array's name only stands in for it, so the address comes from
 // cudaGetSymbolAddress, once per device (this may load the module on that
 // device, which is why the first call must not run inside stream capture).
-unsigned char* noalloc_scratch() {
+// The scene's buffers must live on the current device: the address looked up
+// is that device's copy of the array, and kernels launched there would
+// otherwise read another GPU's scene.
+unsigned char* noalloc_scratch(const trn_scene* s) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) {
     set_error("trn_render_grad_noalloc: no usable current device");
+    return nullptr;
+  }
+  cudaPointerAttributes pa;
+  if (cudaPointerGetAttributes(&pa, s->pos) != cudaSuccess || pa.type != cudaMemoryTypeDevice) {
+    cudaGetLastError();
+    set_error("trn_render_grad_noalloc: cannot tell which device holds the scene");
+    return nullptr;
+  }
+  if (pa.device != dev) {
+    set_error("trn_render_grad_noalloc: the scene lives on device " + std::to_string(pa.device) +
+              " but device " + std::to_string(dev) + " is current; make the scene's device current");
     return nullptr;
   }
   unsigned char* p = g_noalloc_base[dev].load(std::memory_order_acquire);
@@ -3582,7 +3600,7 @@ int trn_render_grad_noalloc(trn_scene* s, const trn_camera* cam, const trn_rende
     set_error("pixel boundary needs W*H*spp divisible by 4");
     return -1;
   }
-  unsigned char* base = noalloc_scratch();
+  unsigned char* base = noalloc_scratch(s);
   if (!base) return -1;
   ViewDesc* table = (ViewDesc*)base;
   long long* vbegin = (long long*)(base + kNoAllocHeader - 3 * 256);

@@ -187,8 +187,10 @@ TRN_HD void disk_concentric(float sx, float sy, float& ox, float& oy) {
   const float rp = q13 ? x : y;
   const float phi_ = 0.25f * kPi * rp / r;
   const float phi = is_zero ? 0.f : (q13 ? 0.5f * kPi - phi_ : phi_);
-  ox = r * cosf(phi);
-  oy = r * sinf(phi);
+  float sp, cp;
+  sincos_det(phi, sp, cp);
+  ox = r * cp;
+  oy = r * sp;
 }
 // BSDF::GGX_VNDF_Sample / SampleVisible11, BSDF.cpp:272-302
 TRN_HD F3 ggx_vndf_sample(const F3& v, float alpha, float s0, float s1) {
@@ -236,7 +238,9 @@ TRN_HD F3 cosine_hemisphere(float s0, float s1) {
   const float phi = cond ? kPiOver4 * (r2 / r1) : kPiOver2 - (r1 / r2) * kPiOver4;
   const bool zero = r1 == 0.f && r2 == 0.f;
   const float rr = zero ? 0.f : r, pp = zero ? 0.f : phi;
-  const float x = rr * cosf(pp), y = rr * sinf(pp);
+  float sp, cp;
+  sincos_det(pp, sp, cp);
+  const float x = rr * cp, y = rr * sp;
   const float z = sqrtf(fmaxf(1e-4f, 1.f - x * x - y * y));
   return F3(x, y, z);
 }

@@ -1,17 +1,24 @@
 """GPU parity of the trn CUDA path against the CPU oracle (same inputs, same
-uniform sample tables), called through the C-ABI via the Python mirror."""
+uniform sample tables), called through the C-ABI via the Python mirror.
+
+Tolerance: every pixel within 1e-4 relative, gradients within 1e-4 relative
+L2 and 1e-4 of the largest element (the float atomics of the scatter add in
+another order than the oracle's index_add). Paths agree exactly: the
+sampling arithmetic is evaluated with the same IEEE operations on both
+sides (no multiply-add contraction, deterministic sin/cos/acos)."""
 import numpy as np
 import pytest
 import torch
 
 from oracle import tr_oracle as O
 from tensorray_b200 import api, scenes
-from tests.helpers import oracle_camera_from, rel_l2, sample_table
+from tests.helpers import assert_grad_parity, assert_image_parity, oracle_camera_from, sample_table
 
 pytestmark = pytest.mark.gpu
 
 W = H = 32
 D = 3
+DEPTHS = [3, 5]  # 5 is the depth of the single-view benchmark
 
 
 @pytest.fixture(scope="module")
@@ -92,43 +99,37 @@ def test_hash_sampler_matches_numpy(cfg1):
     torch.testing.assert_close(img_hash, img_tab, rtol=1e-6, atol=1e-7)
 
 
-def test_path_forward_parity(cfg1):
+@pytest.mark.parametrize("depth", DEPTHS)
+def test_path_forward_parity(cfg1, depth):
     spec, scene, osc, cam = cfg1
     spp = 4
-    smp = sample_table(0, W, H, spp, D, 1)
-    img_g = api.PathTracer().renderC(scene, api.RenderOptions(0, D, spp, 0, 0, 0, 0), samples=smp.to(scene.device))
+    smp = sample_table(0, W, H, spp, depth, 1)
+    img_g = api.PathTracer().renderC(scene, api.RenderOptions(0, depth, spp, 0, 0, 0, 0),
+                                     samples=smp.to(scene.device))
     with torch.no_grad():
         osc.configure()
-        img_o = O.path_tracer(osc, cam, spp, D, smp)
-    a = img_g.reshape(-1, 3).cpu().double()
-    b = img_o.double()
-    assert float(b.sum()) > 0
-    err = (a - b).abs()
-    tol = 1e-4 * torch.maximum(a.abs(), b.abs()) + 1e-6
-    bad = (err > tol).any(-1).float().mean()
-    assert bad <= 0.01, f"{float(bad):.4f} of pixels differ"
-    assert abs(float(a.sum() - b.sum())) <= 1e-3 * float(b.sum())
+        img_o = O.path_tracer(osc, cam, spp, depth, smp)
+    assert_image_parity(img_g, img_o, f"cfg1 {W}x{H} D{depth} forward")
 
 
+@pytest.mark.parametrize("depth", DEPTHS)
 @pytest.mark.parametrize("integrator", [0, 1, 2, 3, 4])
-def test_grad_parity(cfg1, integrator):
+def test_grad_parity(cfg1, integrator, depth):
     spec, scene, osc, cam = cfg1
-    spp = {0: 4, 1: 4, 2: 4, 3: 4, 4: 4}[integrator]
-    smp = sample_table(integrator, W, H, spp, D, 2)
+    spp = 4
+    smp = sample_table(integrator, W, H, spp, depth, 2)
     g = torch.Generator().manual_seed(11)
     dLdI = torch.rand(W * H, 3, generator=g) - 0.3
     cls = [api.PathTracer, api.PrimaryEdgeIntegrator, api.DirectEdgeIntegrator, api.IndirectEdgeIntegrator,
            api.PixelBoundaryIntegrator][integrator]
-    opts = api.RenderOptions(0, D, spp, spp, spp, spp, spp)
+    opts = api.RenderOptions(0, depth, spp, spp, spp, spp, spp)
     scene.clear_grads()
     cls().renderD(scene, opts, dLdI.reshape(H, W, 3).to(scene.device), samples=smp.to(scene.device))
     gg = scene.get_grads()
-    go, _ = O.grads(osc, cam, integrator, spp, D, smp, dLdI)
-    t_g, t_o = gg["translation"].cpu(), go["translation"].detach()
-    p_g, p_o = gg["positions"].cpu(), go["positions"].detach()
-    assert float(p_o.abs().sum()) > 0
-    assert rel_l2(p_g, p_o) < 2e-3, f"vertex grads rel L2 {rel_l2(p_g, p_o):.2e}"
-    assert rel_l2(t_g, t_o) < 2e-3, f"translation grads {t_g.tolist()} vs {t_o.tolist()}"
+    go, _ = O.grads(osc, cam, integrator, spp, depth, smp, dLdI)
+    label = f"cfg1 {W}x{H} D{depth} term {integrator}"
+    assert_grad_parity(gg["positions"], go["positions"], label + " vertices")
+    assert_grad_parity(gg["translation"], go["translation"], label + " translation")
 
 
 @pytest.mark.parametrize("eps", [0.01, 0.5])
@@ -148,7 +149,6 @@ def test_guided_direct_grad_parity(cfg1, eps):
                                        samples=smp.to(scene.device))
     gg = scene.get_grads()
     go, _ = O.grads(osc, cam, api.TRN_DIRECT_EDGE, spp, D, smp, dLdI, guiding=(5, gspp, eps))
-    p_g, p_o = gg["positions"].cpu(), go["positions"].detach()
-    assert float(p_o.abs().sum()) > 0
-    assert rel_l2(p_g, p_o) < 2e-3, f"vertex grads rel L2 {rel_l2(p_g, p_o):.2e}"
-    assert rel_l2(gg["translation"].cpu(), go["translation"].detach()) < 2e-3
+    label = f"cfg1 {W}x{H} D{D} guided direct eps {eps}"
+    assert_grad_parity(gg["positions"], go["positions"], label + " vertices")
+    assert_grad_parity(gg["translation"], go["translation"], label + " translation")

@@ -60,6 +60,37 @@ def test_noalloc_grad_matches_allocating_entry_point(setup, integrator, guided):
         assert rel_l2(t, ref_t) < TOL, f"translation grads {t.tolist()} vs {ref_t.tolist()}"
 
 
+def _call_noalloc(scene, integrator, dLdI):
+    lib = scene._lib
+    o = api.RenderOptions(3, D, SPP, SPP, SPP, SPP, SPP)
+    opts = o._c()
+    smp = TrnSamples(None, 0)
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    check(lib.trn_render_grad_noalloc(scene.handle, C.byref(scene.cameras[0].c), C.byref(opts), integrator,
+                                      C.byref(smp), C.c_void_p(dLdI.data_ptr()), stream), "noalloc")
+
+
+def test_noalloc_allocates_nothing(setup):
+    """Free device memory stays the same across calls, including the first
+    calls on a scene that never rendered through trn_render_grad (so no
+    per-scene buffer is created lazily either). One earlier call per term on
+    another scene has looked up the scratch address and let the driver size
+    its local memory for the fused kernels."""
+    scene, dLdI = setup
+    for integ in range(5):
+        _call_noalloc(scene, integ, dLdI)
+    torch.cuda.synchronize()
+    fresh = api.Scene(scenes.config1_scene(W, H))
+    fresh.configure()
+    torch.cuda.synchronize()
+    before = torch.cuda.mem_get_info()[0]
+    for _ in range(3):
+        for integ in range(5):
+            _call_noalloc(fresh, integ, dLdI)
+        torch.cuda.synchronize()
+        assert torch.cuda.mem_get_info()[0] == before, "trn_render_grad_noalloc allocated device memory"
+
+
 def test_noalloc_rejects_bad_arguments(setup):
     scene, dLdI = setup
     lib = scene._lib
