@@ -154,6 +154,15 @@ def acos_det(x):
 # ---------------------------------------------------------------------------
 # small vector helpers on [N, 3] tensors
 # ---------------------------------------------------------------------------
+def sqrt_rn(x):
+    """Correctly rounded float32 square root (IEEE 754, as the GPU's sqrtf and
+    numpy compute it): torch's vectorised CPU sqrt is off by one ulp on some
+    small arguments (e.g. 5.9935515e-11), which flips threshold tests on the
+    tiny triangles of a 100K-triangle mesh. The float64 root of a float32
+    argument rounds to the correctly rounded float32 root."""
+    return torch.sqrt(x.to(torch.float64)).to(x.dtype)
+
+
 def dot(a, b):
     return a[..., 0] * b[..., 0] + a[..., 1] * b[..., 1] + a[..., 2] * b[..., 2]
 
@@ -166,7 +175,7 @@ def cross(a, b):
 
 def length(a):
     # VectorLength (Tensor.cpp:695-702): Sqrt(X^2 + Y^2 + Z^2)
-    return torch.sqrt(dot(a, a))
+    return sqrt_rn(dot(a, a))
 
 
 def normalize(a):
@@ -232,7 +241,7 @@ def camera_ray_dir(cam, ix, iy, sx, sy):
     row = lambda r: ((m[4 * r] * rx + m[4 * r + 1] * ry) + m[4 * r + 2] * zero) + m[4 * r + 3]
     hx, hy, hz, hw = row(0), row(1), row(2), row(3)
     cx, cy, cz = hx / hw, hy / hw, hz / hw
-    ln = torch.sqrt((cx * cx + cy * cy) + cz * cz)
+    ln = sqrt_rn((cx * cx + cy * cy) + cz * cz)
     dx, dy, dz = cx / ln, cy / ln, cz / ln
     vr = lambda r: (v[4 * r] * dx + v[4 * r + 1] * dy) + v[4 * r + 2] * dz
     return torch.stack([vr(0), vr(1), vr(2)], -1)
@@ -264,7 +273,7 @@ def sample_direct(cam, p):
     cpos = torch.from_numpy(cam["pos"])
     d = p.detach() - cpos
     dist2 = dot(d, d)
-    d = d / torch.sqrt(dist2)[:, None]
+    d = d / sqrt_rn(dist2)[:, None]
     cos_t = dot(torch.from_numpy(cam["dir"]).expand_as(d), d)
     ic = 1.0 / cos_t
     sval = 1.0 / dist2 * ic * ic * ic * float(cam["inv_area"])
@@ -452,7 +461,7 @@ class OracleScene:
     # --- merged area light (Light.cpp:134-184) ----------------------------------
     def light_sample(self, s0, s1):
         e, pmf, reuse = sample_discrete(self.light_cdf, self.light_integral, self.light_func, s0)
-        t = torch.sqrt(reuse)
+        t = sqrt_rn(reuse)
         bu = 1.0 - t
         bv = t * s1
         tri = self.emit_tris[e]
@@ -561,8 +570,8 @@ def coordinate_system(n):
     """CoordinateSystem (Utils.cpp:118-140)."""
     nx, ny, nz = n[:, 0], n[:, 1], n[:, 2]
     cond = nx.abs() > ny.abs()
-    inv_a = 1.0 / torch.sqrt(torch.clamp(nx * nx + nz * nz, min=1e-3))
-    inv_b = 1.0 / torch.sqrt(torch.clamp(ny * ny + nz * nz, min=1e-3))
+    inv_a = 1.0 / sqrt_rn(torch.clamp(nx * nx + nz * nz, min=1e-3))
+    inv_b = 1.0 / sqrt_rn(torch.clamp(ny * ny + nz * nz, min=1e-3))
     zero = torch.zeros_like(nx)
     ta = torch.stack([-nz * inv_a, zero, nx * inv_a], -1)
     tb = torch.stack([zero, nz * inv_b, -ny * inv_b], -1)
@@ -628,7 +637,7 @@ def ggx_D(wh, alpha):
 def smith_G(v, wh, alpha):
     tan2 = _tan2(wh)
     root = alpha * alpha * tan2
-    G = 2.0 / (1.0 + torch.sqrt(1.0 + root * root))
+    G = 2.0 / (1.0 + sqrt_rn(1.0 + root * root))
     G = torch.where(tan2 < 3.402823466e38, G, torch.zeros_like(G))
     G = torch.where(tan2 == 0, torch.ones_like(G), G)
     return torch.where(dot(v, wh) * v[:, 2] <= 0, torch.zeros_like(G), G)
@@ -661,7 +670,7 @@ def cosine_hemisphere(s0, s1):
     phi = torch.where(zero, torch.zeros_like(phi), phi)
     sp, cp = sincos_det(phi)
     x, y = r * cp, r * sp
-    z = torch.sqrt(torch.clamp(1.0 - x * x - y * y, min=1e-4))
+    z = sqrt_rn(torch.clamp(1.0 - x * x - y * y, min=1e-4))
     return torch.stack([x, y, z], -1)
 
 
@@ -680,16 +689,16 @@ def disk_concentric(s0, s1):
 def vndf_sample(v, alpha, s0, s1):
     """GGX_VNDF_Sample / SampleVisible11 (BSDF.cpp:272-302)."""
     V = normalize(torch.stack([v[:, 0] * alpha, v[:, 1] * alpha, v[:, 2]], -1))
-    sinT = torch.sqrt(torch.clamp(1.0 - V[:, 2] * V[:, 2], min=0.0))
+    sinT = sqrt_rn(torch.clamp(1.0 - V[:, 2] * V[:, 2], min=0.0))
     sin_phi = torch.where(sinT == 0, torch.zeros_like(sinT), torch.clamp(V[:, 1] / sinT, -1.0, 1.0))
     cos_phi = torch.where(sinT == 0, torch.ones_like(sinT), torch.clamp(V[:, 0] / sinT, -1.0, 1.0))
     ct = V[:, 2]
     px, py = disk_concentric(s0, s1)
     s = 0.5 * (1.0 + ct)
-    a = torch.sqrt(torch.clamp(1.0 - px * px, min=0.0))
+    a = sqrt_rn(torch.clamp(1.0 - px * px, min=0.0))
     y = (1.0 - s) * a + s * py
-    z = torch.sqrt(torch.clamp(1.0 - (px * px + py * py), min=0.0))
-    st = torch.sqrt(torch.clamp(1.0 - ct * ct, min=0.0))
+    z = sqrt_rn(torch.clamp(1.0 - (px * px + py * py), min=0.0))
+    st = sqrt_rn(torch.clamp(1.0 - ct * ct, min=0.0))
     norm = 1.0 / (st * y + ct * z)
     slx, sly = (ct * y - st * z) * norm, px * norm
     sx = (cos_phi * slx - sin_phi * sly) * alpha
@@ -761,7 +770,7 @@ def radiance_direct(scene, surf, rdir, T, l0, l1, b0, b1, b2):
         wo = -rd
         wi = L["p"] - sx["p"]
         d2 = dot(wi, wi)
-        d = torch.sqrt(d2)
+        d = sqrt_rn(d2)
         wi = wi / d[:, None]
         dotSh, dotGeo = dot(sx["ns"], wi), dot(sx["ng"], wi)
         stable = (d > SHADOW_EPS) & (dotSh.abs() > EDGE_EPS)
@@ -786,7 +795,7 @@ def radiance_direct(scene, surf, rdir, T, l0, l1, b0, b1, b2):
             nx = scene.post_intersect(tri[hit], u[hit], v[hit])
             dr = nx["p"] - sh["p"]
             dist2 = dot(dr, dr)
-            dr = dr / torch.sqrt(dist2)[:, None]
+            dr = dr / sqrt_rn(dist2)[:, None]
             Gn = dot(nx["ng"], -dr).abs() / dist2
             fr_h = tuple(f[hit] for f in frame)
             bvn = bsdf_eval(bsdf, fr_h, sh["ng"], kd[hit], wo[hit], dr, False) * dot(sh["ns"], dr).abs()[:, None]
@@ -1106,7 +1115,7 @@ def direct_edge(scene, cam, spp, D, smp, guide=None):
     p0, p2, nL = es["p0"], ls["p"], ls["n"]
     ev = p2.detach() - p0.detach()
     dsq = dot(ev, ev)
-    dist = torch.sqrt(dsq)
+    dist = sqrt_rn(dsq)
     en = ev / dist[:, None]
     cos_t = dot(nL.detach(), -en)
     E = es["E"]
@@ -1179,7 +1188,7 @@ def indirect_edge(scene, cam, spp, D, smp):
     nrm = cross(n0, edge)
     tg, bt = coordinate_system(nrm)
     z = torch.clamp(1.0 - 2.0 * r1, max=np.float32(1.0 - EDGE_EPS))
-    r = torch.sqrt(torch.clamp(1.0 - z * z, min=0.0))
+    r = sqrt_rn(torch.clamp(1.0 - z * z, min=0.0))
     phi = 2.0 * PI * r2
     sp, cp = sincos_det(phi)
     dir_b = tg * (r * cp)[:, None] + bt * (r * sp)[:, None] + nrm * z[:, None]
@@ -1194,7 +1203,7 @@ def indirect_edge(scene, cam, spp, D, smp):
     x1 = xx * cp[:, None] + zz * sp[:, None]
     m0 = r2 > 0.5
     bq = 4.0 * r2 - torch.where(m0, torch.full_like(r2, 3.0), torch.ones_like(r2))
-    aq = torch.sqrt(1.0 - bq * bq) * (1.0 - m0.to(F32) * 2.0)
+    aq = sqrt_rn(1.0 - bq * bq) * (1.0 - m0.to(F32) * 2.0)
     dir_i = x1 * aq[:, None] + yy * bq[:, None]
     dirv = torch.where(isb[:, None], dir_b, dir_i).detach()
     pdf_d = torch.where(isb, torch.full_like(r1, 0.25 / PI), 0.25 / phi0)
