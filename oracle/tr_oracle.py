@@ -922,9 +922,33 @@ def ray_intersect_ad(d, org, p0, e1, e2):
     return u, v
 
 
+class _SampleGuard(torch.autograd.Function):
+    """Identity on per-sample rows; in the backward pass a sample (row) whose
+    gradient is not finite in any of the inputs contributes zero to all of
+    them. The CUDA path skips such a sample's xDotN scatter (a line parallel
+    to the far triangle, or a receiver on the edge point); the reference has
+    no guard there and would turn the whole gradient into NaN."""
+
+    @staticmethod
+    def forward(ctx, *xs):
+        return tuple(x.clone() for x in xs)
+
+    @staticmethod
+    def backward(ctx, *gs):
+        bad = None
+        for g in gs:
+            if g is not None:
+                b = ~torch.isfinite(g).all(-1)
+                bad = b if bad is None else bad | b
+        if bad is None or not bool(bad.any()):
+            return gs
+        return tuple(None if g is None else torch.where(bad[:, None], torch.zeros_like(g), g) for g in gs)
+
+
 def _xdotn(scene, org, target, tri, n):
     i0, i1, i2 = (scene.idx[tri, k] for k in range(3))
     P0, P1, P2 = scene.pos[i0], scene.pos[i1], scene.pos[i2]
+    org, target, P0, P1, P2 = _SampleGuard.apply(org, target, P0, P1, P2)
     u, v = ray_intersect_ad(normalize(target - org), org, P0, P1 - P0, P2 - P0)
     w = 1.0 - u - v
     u2 = w[:, None] * P0.detach() + u[:, None] * P1.detach() + v[:, None] * P2.detach()

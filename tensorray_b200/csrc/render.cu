@@ -1356,6 +1356,12 @@ TRN_D void xdotn_vjp(const Params& P, const ViewDesc& V, float W, const F3& org,
   }
   F3 gorg, gt, g0, g1, g2;
   xdotn_grad(org, target, P0, P1, P2, n, W, gorg, gt, g0, g1, g2);
+  // a degenerate sample (the line org -> target parallel to the far
+  // triangle, or org == target) has no finite derivative; it contributes
+  // nothing instead of turning the whole gradient buffer into NaN
+  if (!(finite3(g0) && finite3(g1) && finite3(g2) && (!edge_attached || finite3(gt)) &&
+        (!org_attached || finite3(gorg))))
+    return;
   agg_add3(V.gpos, i0, g0);
   agg_add3(V.gpos, i1, g1);
   agg_add3(V.gpos, i2, g2);
