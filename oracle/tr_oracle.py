@@ -24,13 +24,17 @@ Differences that are deliberate and shared with the GPU path:
   * the edge CDFs keep zero-weight entries instead of compacting the edge
     list first (the same distribution).
 
-Parity status: the reference cannot be built or run here (it needs OptiX 7.4
-and MSVC-only code). No reference test pins render outputs. This oracle is
-pinned by closed-form answers (Lambert's polygon irradiance for direct light
-from a quad emitter, a clamped-cosine furnace), by the reference's
-finite-difference-vs-AD validation pattern (Tensor.h:2968-3021) and by the
-reference's own comment goldens for the primitive ops it restates. Relative
-to the reference's own outputs, parity is unpinned.
+  * a boundary sample whose xDotN derivative is not finite contributes
+    nothing (_SampleGuard); the reference would turn the whole gradient NaN;
+  * square roots are correctly rounded (sqrt_rn), like the GPU's.
+
+Parity status: parity unpinned. The reference cannot be built or run here:
+it needs OptiX 7.4, MSVC-only headers (crtdbg.h, ppl.h), and its JIT reads
+its own source tree at run time. No reference test pins render outputs. This
+oracle is pinned by closed-form answers (Lambert's polygon irradiance for
+direct light from a quad emitter, a clamped-cosine furnace) and by the
+reference's finite-difference-vs-AD validation pattern (Tensor.h:2968-3021)
+applied to its render path.
 """
 from __future__ import annotations
 

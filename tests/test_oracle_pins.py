@@ -109,12 +109,6 @@ def test_vector_cross_golden():
     assert O.cross(a, b).tolist() == [[-3.0, 6.0, -3.0]]
 
 
-def test_standard_deviation_golden():
-    # Utils.cpp UtilityTest "Test 3" comment golden: std(LinSpace(0,10,10)) = 3.19143
-    a = torch.linspace(0, 10, 10)
-    assert abs(float(a.std(unbiased=False)) - 3.19143) < 1e-4
-
-
 def test_watertight_shared_edge_hits_exactly_once():
     # two triangles sharing the edge x = 0 in the plane z = 0
     P0 = torch.tensor([[0.0, -1.0, 0.0], [0.0, -1.0, 0.0]])
