@@ -64,6 +64,8 @@ def parse():
     ap.add_argument("--tris", type=int, default=100_000)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the batched-views and served-requests legs of the default run")
     ap.add_argument("--quick", action="store_true", help="small smoke-sized run")
     ap.add_argument("--no-path-cache", action="store_true",
                     help="gradient calls re-trace the interior paths instead of reusing the forward's records")
@@ -216,6 +218,45 @@ def main():
         return run_inverse(a)
     if a.workload == "serve":
         return run_serve(a)
+    line, world = run_single(a)
+    if line is not None and world == 1 and not a.no_extra:
+        # the metric's comparison legs at N=1: the batched multi-view
+        # configuration and the served request stream, each against the plain
+        # per-view / one-at-a-time form of the same kernels
+        import copy
+        import gc
+        ax = copy.copy(a)
+        ax.steps, ax.warmup = min(a.steps, 10), max(3, min(a.warmup, 5))
+        gc.collect()
+        torch.cuda.empty_cache()
+        v = run_views(ax, quiet=True)
+        line["batched_vs_plain"] = {
+            "workload": v["config"]["workload"], "batched_over_plain": v["batched_over_plain"],
+            "batched": {"value": v["value"], "unit": v["unit"], "ms_per_step": v["ms_per_step"]},
+            "plain_per_view": {"value": v["plain_per_view"]["value"], "unit": v["unit"],
+                               "ms_per_step": v["plain_per_view"]["ms_per_step"]},
+            "split_ms": v["split_ms"], "graph_vs_eager_grad_rel_l2": v["graph_vs_eager_grad_rel_l2"],
+            "steps": ax.steps, "warmup": ax.warmup}
+        gc.collect()
+        torch.cuda.empty_cache()
+        sv = run_serve(ax, quiet=True)
+        pl = sv["plain_one_at_a_time"]
+        line["served_vs_plain"] = {
+            "workload": sv["config"]["workload"],
+            "served": {"latency_s": sv["latency_s"], "value": sv["value"], "unit": sv["unit"],
+                       "requests_per_s": sv["requests_per_s"]},
+            "plain_one_at_a_time": {"latency_s": pl["latency_s"], "value": pl["value"], "unit": sv["unit"],
+                                    "requests_per_s": pl["requests_per_s"]},
+            "throughput_over_plain": sv["value"] / pl["value"],
+            "p50_plain_over_served": pl["latency_s"]["p50"] / sv["latency_s"]["p50"],
+            "clocks": sv["clocks"]}
+    if line is not None:
+        print(json.dumps(line), flush=True)
+
+
+def run_single(a):
+    """The 100K-triangle single-view configuration (the headline line);
+    returns (line on rank 0 else None, world size)."""
     import torch.distributed as dist
     from tensorray_b200 import api, scenes
     from tensorray_b200 import autograd as tra
@@ -243,7 +284,20 @@ def main():
     opts = api.RenderOptions(base_seed, D, a.spp, a.spp, a.spp, a.spp, a.spp)
     integrators = [api.PathTracer(), api.PrimaryEdgeIntegrator(), api.DirectEdgeIntegrator(),
                    api.IndirectEdgeIntegrator(), api.PixelBoundaryIntegrator()]
-    kernel_names = ["k_path_fwd", "k_path_adj", "k_primary_adj", "k_direct_adj", "k_indirect_adj", "k_pixel_adj"]
+    # timed spans: the interior forward and one span per renderD call; each
+    # span is the term's production kernels (set-up rounds, edge keys and
+    # their radix sort, body stages)
+    kernel_names = ["interior_fwd", "interior_adj", "primary", "direct", "indirect", "pixel"]
+    term_kernels = {
+        "interior_fwd": ["k_path_fwd_rec_regen"] if not a.no_path_cache else ["k_path_fwd"],
+        "interior_adj": (["k_path_reverse<8,true> (over the forward's path records)"] if not a.no_path_cache
+                         else ["k_path_replay", "k_path_reverse"]),
+        "primary": ["k_edge_keys", "cub radix sort", "k_primary_setup", "k_primary_body_regen"],
+        "direct": ["k_edge_keys", "cub radix sort", "k_direct_setup", "k_direct_body"],
+        "indirect": ["k_edge_keys", "cub radix sort", "k_indirect_setup", "k_indirect_sensor_regen",
+                     "k_indirect_emitter_regen"],
+        "pixel": ["k_pixel_setup", "k_primary_body_regen"],
+    }
     units_per_step = a.res * a.res * a.spp * 5
     V0 = scene._raw_positions.clone()
     tex0 = torch.as_tensor(np.ascontiguousarray(spec.textures[0]), device=dev).reshape(-1, 3).clone()
@@ -265,9 +319,9 @@ def main():
         scene.set_vertex_positions(V0)
         scene.set_texels(tex0)
         scene.configure()
-        if ev: ev["fwd"][0].record(stream)
+        if ev: ev["interior_fwd"][0].record(stream)
         img = integrators[0].renderC(scene, opts)
-        if ev: ev["fwd"][1].record(stream)
+        if ev: ev["interior_fwd"][1].record(stream)
         dLdI = img - target
         scene.clear_grads()
         for i, it in enumerate(integrators):
@@ -286,7 +340,7 @@ def main():
         step()
     torch.cuda.synchronize()
 
-    ev_keys = ["fwd"] + kernel_names[1:]
+    ev_keys = kernel_names
     per_kernel = {k: [] for k in ev_keys}
     clocks.mark()
     launches0 = lib.trn_kernel_launches()
@@ -372,7 +426,7 @@ def main():
     scene.configure()
     img = integrators[0].renderC(scene, opts)
     lib.trn_stats_read(scene.handle, buf, 1, C.c_void_p(stream.cuda_stream))
-    counts["fwd"] = dict(zip(CNT_NAMES, list(buf)[:10]))
+    counts["interior_fwd"] = dict(zip(CNT_NAMES, list(buf)[:10]))
     dLdI = img - target
     for i, it in enumerate(integrators):
         it.renderD(scene, opts, dLdI)
@@ -400,11 +454,11 @@ def main():
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
         try:
-            traffic = json.load(open(tpath)).get(dom.replace("fwd", "k_path_fwd"))
+            traffic = json.load(open(tpath)).get(dom)
         except Exception:
             traffic = None
     roofline = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
-                "traffic": traffic, "kernel": dom if dom != "fwd" else "k_path_fwd",
+                "traffic": traffic, "kernel": f"{dom} term: " + " + ".join(term_kernels[dom]),
                 "peak_source": peak_src}
 
     cpu = None
@@ -413,6 +467,7 @@ def main():
         cpu = {"value": rate, "unit": "grad path-samples/s", "cores": cores, "kind": "port",
                "sample": f"{units} grad path-samples in {dt:.1f}s: 8x8 px, 1 spp per term, 5 terms, same scene"}
 
+    line = None
     if rank == 0:
         line = {
             "metric": "grad path-samples/sec", "value": value, "unit": "grad path-samples/s", "n_gpus": world,
@@ -422,20 +477,21 @@ def main():
                        "res": a.res, "spp_per_term": a.spp, "depth": D, "triangles": scene.num_triangles,
                        "l2": "flushed between timed steps (256 MB write)", "parallelism": f"seeds x{world}"},
             "e2e": e2e, "gpu_launches": int(launches), "clocks": clk, "roofline": roofline, "step_ms": step_ms,
-            "kernels": {k: {"ms": v["ms"], "GB/s": v["gbs"], "counts": v["counts"]} for k, v in per_kernel_roof.items()},
+            "kernels": {k: {"ms": v["ms"], "GB/s": v["gbs"], "launches_of": term_kernels[k], "counts": v["counts"]}
+                        for k, v in per_kernel_roof.items()},
             "cpu_baseline": cpu,
         }
-        print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+    return line, world
 
 
 # ---------------------------------------------------------------------------
 # batched multi-view workload: one graph-captured launch per integrator for
 # all views vs the same kernels launched one view at a time
 # ---------------------------------------------------------------------------
-def run_views(a):
+def run_views(a, quiet: bool = False):
     from tensorray_b200 import api, autotune, scenes
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     rng = np.random.default_rng(0)
@@ -480,15 +536,19 @@ def run_views(a):
     tgt_v = [vs.view_image(targets, i).reshape(-1, 3).contiguous() for i in range(nviews)]
 
     def plain_step():
+        # the reference's multi-view loop (pyTensorRay/renderer_multi_view.py:
+        # 53-98): per view a forward, its loss, every integrator's renderD
+        # and get_grads, summed into the vertex gradient
         losses = []
+        gsum = torch.zeros(scene.num_vertices, 3, device=scene.device)
         for i, sv in enumerate(singles):
             im = sv.render(api.TRN_PATH_TRACER, opts)
             d = torch.empty_like(im)
             losses.append(sv.loss(im, tgt_v[i], d))
             for t in terms:
                 sv.render_grad(t, opts, d)
-        g = scene.get_grads(clear=True)
-        return losses, g["positions"]
+            gsum += scene.get_grads(clear=True)["positions"]
+        return losses, gsum
 
     for _ in range(a.warmup):
         batched_step()
@@ -578,7 +638,9 @@ def run_views(a):
                        "fwd": [ln_f.block, ln_f.blocks_per_sm, ln_f.chunk] if ln_f else "default",
                        **{str(t): ([ln_g[t].block, ln_g[t].blocks_per_sm, ln_g[t].chunk] if ln_g[t] else "default")
                           for t in terms}}}
-    print(json.dumps(line), flush=True)
+    if not quiet:
+        print(json.dumps(line), flush=True)
+    return line
 
 
 # ---------------------------------------------------------------------------
@@ -672,7 +734,7 @@ def run_inverse(a):
 # served workload: Poisson arrivals of render+gradient requests over four
 # resident scenes, continuous batching vs one request at a time
 # ---------------------------------------------------------------------------
-def run_serve(a):
+def run_serve(a, quiet: bool = False):
     from tensorray_b200 import api, scenes, serve
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     rng = np.random.default_rng(0)
@@ -749,7 +811,9 @@ def run_serve(a):
                                     "latency_s": {"p50": serve.percentile(plain_lat, 50),
                                                   "p99": serve.percentile(plain_lat, 99)}},
             "peak_request_bytes": stats.peak_bytes, "iterations": stats.iterations, "clocks": clk}
-    print(json.dumps(line), flush=True)
+    if not quiet:
+        print(json.dumps(line), flush=True)
+    return line
 
 
 if __name__ == "__main__":
