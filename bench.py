@@ -247,6 +247,7 @@ def main():
                        "requests_per_s": sv["requests_per_s"]},
             "plain_one_at_a_time": {"latency_s": pl["latency_s"], "value": pl["value"], "unit": sv["unit"],
                                     "requests_per_s": pl["requests_per_s"]},
+            "plain_one_at_a_time_path_cache": sv["plain_one_at_a_time_path_cache"],
             "throughput_over_plain": sv["value"] / pl["value"],
             "p50_plain_over_served": pl["latency_s"]["p50"] / sv["latency_s"]["p50"],
             "clocks": sv["clocks"]}
@@ -778,26 +779,36 @@ def run_serve(a, quiet: bool = False):
     clk = clocks.stop()
     lat = [r.latency for r in stats.completed]
     samples = sum(r.samples() for r in stats.completed)
-    # plain: one request at a time through the single-view API, no batching
-    plain_lat = []
-    t1 = time.perf_counter()
-    tq = 0.0
-    for r, at in zip(reqs, arrivals):
-        start = max(at, tq)
-        sc = world[r.scene]
-        e0 = time.perf_counter()
-        opts = api.RenderOptions(r.seed, r.depth, r.spp, r.spp, r.spp, 0, 0)
-        img = api.PathTracer().renderC(sc, opts, camera=r.camera)
-        d = img.reshape(-1, 3) - r.target
-        sc.clear_grads()
-        for it in (api.PathTracer(), api.PrimaryEdgeIntegrator(), api.DirectEdgeIntegrator()):
-            it.renderD(sc, opts, d.reshape(img.shape), camera=r.camera)
-        sc.get_grads()
-        torch.cuda.synchronize()
-        dur = time.perf_counter() - e0
-        tq = start + dur
-        plain_lat.append(tq - at)
-    plain_wall = time.perf_counter() - t1
+    # plain: one request at a time through the single-view API, no batching.
+    # Like the server (and the reference's RenderD) its gradient call
+    # re-traces the interior paths; a second pass lets the single-view calls
+    # keep the forward's path records (not possible across the server's
+    # interleaved chunks, whose forward completes before any gradient chunk)
+    def one_at_a_time(path_cache: bool):
+        for sc in world.values():
+            sc.set_path_cache((16 << 30) if path_cache else 0)
+        lat = []
+        t1 = time.perf_counter()
+        tq = 0.0
+        for r, at in zip(reqs, arrivals):
+            start = max(at, tq)
+            sc = world[r.scene]
+            e0 = time.perf_counter()
+            opts = api.RenderOptions(r.seed, r.depth, r.spp, r.spp, r.spp, 0, 0)
+            img = api.PathTracer().renderC(sc, opts, camera=r.camera)
+            d = img.reshape(-1, 3) - r.target
+            sc.clear_grads()
+            for it in (api.PathTracer(), api.PrimaryEdgeIntegrator(), api.DirectEdgeIntegrator()):
+                it.renderD(sc, opts, d.reshape(img.shape), camera=r.camera)
+            sc.get_grads()
+            torch.cuda.synchronize()
+            dur = time.perf_counter() - e0
+            tq = start + dur
+            lat.append(tq - at)
+        return lat, time.perf_counter() - t1
+
+    plain_lat, plain_wall = one_at_a_time(False)
+    cached_lat, cached_wall = one_at_a_time(True)
     line = {"metric": "grad path-samples/sec", "value": samples / wall, "unit": "grad path-samples/s", "n_gpus": 1,
             "steps": 1, "warmup": 1, "ms_per_step": 1e3 * wall, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scenes, Poisson arrivals)",
@@ -810,6 +821,9 @@ def run_serve(a, quiet: bool = False):
             "plain_one_at_a_time": {"requests_per_s": nreq / plain_wall, "value": samples / plain_wall,
                                     "latency_s": {"p50": serve.percentile(plain_lat, 50),
                                                   "p99": serve.percentile(plain_lat, 99)}},
+            "plain_one_at_a_time_path_cache": {"requests_per_s": nreq / cached_wall, "value": samples / cached_wall,
+                                               "latency_s": {"p50": serve.percentile(cached_lat, 50),
+                                                             "p99": serve.percentile(cached_lat, 99)}},
             "peak_request_bytes": stats.peak_bytes, "iterations": stats.iterations, "clocks": clk}
     if not quiet:
         print(json.dumps(line), flush=True)

@@ -114,7 +114,7 @@ constexpr int kMaxDepth = 16;
 #define TRN_SETUP_SHARED_DIRECT 0
 #endif
 #ifndef TRN_SETUP_SHARED_PIXEL
-#define TRN_SETUP_SHARED_PIXEL 1
+#define TRN_SETUP_SHARED_PIXEL 0
 #endif
 
 // Per-thread work counters behind the roofline's algorithmic-byte model:
@@ -308,7 +308,7 @@ TRN_D void vadj_zero(VAdj& a) { a.p = F3z(); a.ns = F3z(); a.ng = F3z(); a.J = 0
 // J = A / Detach(A) with c = cross(P1 - P0, P2 - P0), shading normal
 // w n0 + u n1 + v n2 (Scene.cpp:668-730, Primitive.cpp:299-340).
 #ifndef TRN_SHARED_SCATTER
-#define TRN_SHARED_SCATTER 1
+#define TRN_SHARED_SCATTER 0
 #endif
 #if TRN_SHARED_SCATTER
 #define TRN_SCATTER_FN __device__ __noinline__
@@ -451,10 +451,12 @@ TRN_D bool radiance_step(const DeviceScene& s, SurfF& x, F3& rdir, F3& T, float 
 }
 
 // One shared (non-inlined) copy of each per-bounce step, with the traversal
-// inlined inside it. Kernels that run both kinds of steps in one body (the
-// indirect boundary term) or many of them call these: inlining every step at
-// every call site inflates those kernels past the instruction cache. The
-// other kernels choose per kernel (measured) between this and the inlined step.
+// inlined inside it. A shared copy keeps a kernel's code small (the fused
+// kernels are instruction-fetch bound), but every object it takes by
+// reference lives in local memory: about 0.6-1 KB of stack per thread, which
+// at 512-768 threads per SM spills out of L1 and L2 into DRAM. Each kernel
+// chooses (measured) between this and the inlined step; the split stage
+// kernels are small enough to inline.
 #ifndef TRN_SHARED_STEPS_PRIMARY
 #define TRN_SHARED_STEPS_PRIMARY 0
 #endif
@@ -468,7 +470,11 @@ TRN_D bool radiance_step(const DeviceScene& s, SurfF& x, F3& rdir, F3& T, float 
 #define TRN_SHARED_STEPS_DIRECT 0
 #endif
 #ifndef TRN_SHARED_STEPS_PATHADJ
-#define TRN_SHARED_STEPS_PATHADJ 1
+#define TRN_SHARED_STEPS_PATHADJ 0
+#endif
+// the indirect term's regenerating sensor and emitter stages
+#ifndef TRN_SHARED_STEPS_INDIRECT
+#define TRN_SHARED_STEPS_INDIRECT 0
 #endif
 __device__ __noinline__ bool radiance_step_shared(const DeviceScene& s, SurfF& x, F3& rdir, F3& T, float l0, float l1,
                                                   float b0, float b1, float b2, F3& contrib, BounceRec* rec, Cnt& cnt) {
@@ -696,7 +702,7 @@ TRN_HD void tangent_vjp(const F3& n, const F3& g_t, F3& g_n) {
 // Reverse mode of F above for the output adjoint `adj`; accumulates into the
 // gradient outputs (g_prev only if need_prev, g_kd only if need_kd).
 #ifndef TRN_SHARED_FACTOR_VJP
-#define TRN_SHARED_FACTOR_VJP 1
+#define TRN_SHARED_FACTOR_VJP 0
 #endif
 #if TRN_SHARED_FACTOR_VJP
 #define TRN_FACTOR_FN __host__ __device__ __noinline__
@@ -2268,7 +2274,8 @@ __global__ void __launch_bounds__(256, TRN_MINB_INDIRECT) k_indirect_sensor_rege
         const int o = 3 + 5 * (D - 1) + 3 * b;
         F3 c;
         int pix;
-        const bool more = importance_step_shared(s, V->cam, xx, rd, T, S(o), S(o + 1), S(o + 2), c, pix, cnt);
+        const bool more = importance_step_k<TRN_SHARED_STEPS_INDIRECT>(s, V->cam, xx, rd, T, S(o), S(o + 1),
+                                                                        S(o + 2), c, pix, cnt);
         if (pix >= 0) {
           sc[b] = g_at(P, *V, pix) * c;
           if (sc[b].x != 0.f || sc[b].y != 0.f || sc[b].z != 0.f) bmin = min(bmin, b);
@@ -2361,7 +2368,8 @@ __global__ void __launch_bounds__(256, TRN_MINB_INDIRECT) k_indirect_emitter_reg
         const PathSmp S{&P, V->seed, it.gslot, it.p + V->slot_off};
         const int o = 3 + 5 * j;
         F3 c;
-        alive = radiance_step_shared(s, xx, rd, T, S(o), S(o + 1), S(o + 2), S(o + 3), S(o + 4), c, nullptr, cnt);
+        alive = radiance_step_k<TRN_SHARED_STEPS_INDIRECT>(s, xx, rd, T, S(o), S(o + 1), S(o + 2), S(o + 3),
+                                                           S(o + 4), c, nullptr, cnt);
         cur = cur + c;
         if (T.x == 0.f && T.y == 0.f && T.z == 0.f) alive = false;
         W += dot(it.sc[D - 2 - j], cur) * it.w0;
