@@ -650,8 +650,18 @@ def run_views(a, quiet: bool = False):
 # lr 1e-3; a step = refit + batched forward + loss + batched adjoints + Adam
 # ---------------------------------------------------------------------------
 def run_inverse(a):
+    """The inverse-rendering loop. Under torchrun (N > 1) every rank holds a
+    replica of the scene and renders its cost-balanced share of the views;
+    the vertex gradient is summed with one NCCL all-reduce per step."""
+    import torch.distributed as dist
     from tensorray_b200 import api, inverse, scenes
-    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
     tris, nviews, res, D = (20_000, 4, 128, 4) if a.quick else (2_000_000, 16, 1024, 8)
     spp = 2 if a.quick else min(a.spp, 4)
     spec = scenes.served_scene(tris, seed=5)
@@ -674,6 +684,10 @@ def run_inverse(a):
     inv = inverse.InverseRenderer(scene, cams, [spp] * nviews, targets, opts, lr=1e-3,
                                   path_cache_bytes=0 if a.no_path_cache else 64 << 30)
     units = inv.samples_per_step()
+    if world > 1:
+        u = torch.tensor([float(units)], device="cuda")
+        dist.all_reduce(u)
+        units = int(u.item())
     losses = []
     for _ in range(a.warmup):
         losses.append(float(inv.step().sum()))
@@ -694,13 +708,14 @@ def run_inverse(a):
     st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
     lib.trn_stats_read(scene.handle, buf, 1, st)
     work = {}
-    inv.views.render(api.TRN_PATH_TRACER, inv.options, out=inv.image)
-    lib.trn_stats_read(scene.handle, buf, 1, st)
-    work["forward"] = dict(zip(CNT_NAMES, list(buf)[:10]))
-    for i in inv.integrators:
-        inv.views.render_grad(i, inv.options, inv.dLdI)
+    if inv.views is not None:
+        inv.views.render(api.TRN_PATH_TRACER, inv.options, out=inv.image)
         lib.trn_stats_read(scene.handle, buf, 1, st)
-        work[f"grad_{i}"] = dict(zip(CNT_NAMES, list(buf)[:10]))
+        work["forward"] = dict(zip(CNT_NAMES, list(buf)[:10]))
+        for i in inv.integrators:
+            inv.views.render_grad(i, inv.options, inv.dLdI)
+            lib.trn_stats_read(scene.handle, buf, 1, st)
+            work[f"grad_{i}"] = dict(zip(CNT_NAMES, list(buf)[:10]))
     lib.trn_stats_enable(scene.handle, 0)
     scene.clear_grads()
     torch.cuda.synchronize()
@@ -708,6 +723,8 @@ def run_inverse(a):
     clk.start()
     ms = []
     for _ in range(a.steps):
+        if world > 1:
+            dist.barrier()
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
@@ -718,14 +735,23 @@ def run_inverse(a):
         losses.append(float(l.sum()))
     clocks = clk.stop()
     mean_ms = sum(ms) / len(ms)
+    if world > 1:
+        t = torch.tensor([mean_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        mean_ms = float(t.item())
+        dist.barrier()
+        dist.destroy_process_group()
+        if rank != 0:
+            return
     line = {"metric": "grad path-samples/sec", "value": units / (mean_ms / 1e3), "unit": "grad path-samples/s",
-            "n_gpus": 1, "steps": a.steps, "warmup": a.warmup, "ms_per_step": mean_ms, "higher_is_better": True,
+            "n_gpus": world, "steps": a.steps, "warmup": a.warmup, "ms_per_step": mean_ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded displaced sphere target, seeded vertex perturbation)",
             "config": {"workload": f"inverse rendering, {tris} tris target, {nviews} views {res}^2, {spp} spp x "
                                    f"3 terms (interior+primary+guided direct), depth {D}, Adam lr 1e-3, "
                                    "LBVH refit per step; inputs larger than L2",
-                       "samples_per_step": units},
+                       "samples_per_step": units,
+                       "parallelism": f"views sharded by cost over {world} rank(s), gradient all-reduce"},
             "loss": {"first": losses[0], "last": losses[-1], "per_step": losses},
             "phases_ms": probe, "work": work, "clocks": clocks}
     print(json.dumps(line), flush=True)

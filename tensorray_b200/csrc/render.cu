@@ -472,6 +472,11 @@ TRN_D bool radiance_step(const DeviceScene& s, SurfF& x, F3& rdir, F3& T, float 
 #ifndef TRN_SHARED_STEPS_PATHADJ
 #define TRN_SHARED_STEPS_PATHADJ 0
 #endif
+// path_replay (k_path_replay, the fused k_path_adj and the loop-form recording
+// forward); TRN_SHARED_STEPS_PATHADJ is the regenerating recording forward
+#ifndef TRN_SHARED_STEPS_REPLAY
+#define TRN_SHARED_STEPS_REPLAY 1
+#endif
 // the indirect term's regenerating sensor and emitter stages
 #ifndef TRN_SHARED_STEPS_INDIRECT
 #define TRN_SHARED_STEPS_INDIRECT 0
@@ -882,7 +887,7 @@ TRN_D F3 path_replay(const Params& P, const AdjState& st, Rec& r, Cnt& cnt) {
     const int o = 2 + 5 * b;
     F3 c;
     BounceRec R;
-    const bool more = radiance_step_k<TRN_SHARED_STEPS_PATHADJ>(s, x, rdir, T, S(o), S(o + 1), S(o + 2),
+    const bool more = radiance_step_k<TRN_SHARED_STEPS_REPLAY>(s, x, rdir, T, S(o), S(o + 1), S(o + 2),
                                     S(o + 3), S(o + 4), c, &R, cnt);
     // a scrubbed (non-finite) bounce contributes nothing and carries no gradient
     if (R.nee_ok && !R.scrubbed) mask |= 1u << k;

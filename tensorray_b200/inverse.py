@@ -15,6 +15,7 @@ from __future__ import annotations
 import torch
 
 from . import api
+from . import dist as trd
 
 
 class InverseRenderer:
@@ -24,19 +25,36 @@ class InverseRenderer:
     image is always the interior path tracer's). options: one RenderOptions for
     every term (its seed advances each step so sample noise decorrelates).
     path_cache_bytes: bound on the interior path records the forward render
-    keeps for the interior gradient of the same step (0 = re-trace them)."""
+    keeps for the interior gradient of the same step (0 = re-trace them).
+
+    With an initialised torch.distributed process group (one process per GPU,
+    each with its own replica of the scene), the views are split over the
+    ranks by cost (trd.ViewShard); each rank renders its views, the vertex
+    gradient is summed over ranks with one all-reduce before the identical
+    Adam update on every rank, and step() returns the losses of all views."""
 
     def __init__(self, scene: api.Scene, cameras: list, spps: list, targets: torch.Tensor,
                  options: api.RenderOptions, integrators=(api.TRN_PATH_TRACER, api.TRN_PRIMARY_EDGE,
                                                           api.TRN_DIRECT_EDGE),
-                 lr: float = 1e-3, refit: bool = True, launch=None, path_cache_bytes: int = 0):
+                 lr: float = 1e-3, refit: bool = True, launch=None, path_cache_bytes: int = 0, group=None):
         self.scene = scene
-        self.views = api.ViewSet(scene, cameras, spps)
-        if path_cache_bytes:
-            self.views.set_path_cache(path_cache_bytes)
-        if targets.numel() != 3 * self.views.npix:
+        self.group = group
+        npix_all = sum(c.width * c.height for c in cameras)
+        if targets.numel() != 3 * npix_all:
             raise RuntimeError("targets must hold npix x 3 values (all views concatenated)")
-        self.targets = targets.reshape(-1, 3).to(scene.device, torch.float32).contiguous()
+        self.shard = trd.ViewShard.of(cameras, spps, options.max_bounces, group)
+        offs = [0]
+        for c in cameras:
+            offs.append(offs[-1] + c.width * c.height)
+        tg = targets.reshape(-1, 3).to(scene.device, torch.float32)
+        self.targets = torch.cat([tg[offs[i]:offs[i + 1]] for i in self.shard.local]).contiguous() \
+            if self.shard.local else tg[:0].contiguous()
+        # every view keeps its global index as its seed: the sharded run draws
+        # the samples of the unsharded one
+        self.views = api.ViewSet(scene, self.shard.pick(cameras), self.shard.pick(spps), seeds=list(self.shard.local)) \
+            if self.shard.local else None
+        if path_cache_bytes and self.views is not None:
+            self.views.set_path_cache(path_cache_bytes)
         self.options = options
         self.integrators = tuple(integrators)
         self.refit = refit
@@ -44,13 +62,16 @@ class InverseRenderer:
         dev = scene.device
         self.x = scene._raw_positions.detach().clone().requires_grad_(True)
         self.opt = torch.optim.Adam([self.x], lr=lr)
-        self.image = torch.empty(self.views.npix, 3, device=dev)
-        self.dLdI = torch.empty(self.views.npix, 3, device=dev)
+        npix = self.views.npix if self.views is not None else 0
+        self.image = torch.empty(npix, 3, device=dev)
+        self.dLdI = torch.empty(npix, 3, device=dev)
         self.loss = torch.zeros(len(cameras), device=dev)
         self.steps = 0
 
     def samples_per_step(self) -> int:
-        """Grad path-samples of one step: every view's W*H*spp per term."""
+        """Grad path-samples of one step on this rank: its views' W*H*spp per term."""
+        if self.views is None:
+            return 0
         n = sum(c.width * c.height * s for c, s in zip(self.views.cameras, self.views.spps))
         return n * len(self.integrators)
 
@@ -70,15 +91,23 @@ class InverseRenderer:
         sc.configure(refit=self.refit and self.steps > 0)
         mark("configure")
         self.options.seed = self.steps
-        self.views.render(api.TRN_PATH_TRACER, self.options, launch=self.launch, out=self.image)
-        mark("forward")
-        self.loss = self.views.loss(self.image, self.targets, self.dLdI)
         sc.clear_grads()
-        for i in self.integrators:
-            self.views.render_grad(i, self.options, self.dLdI, launch=self.launch)
-            mark(f"grad_{i}")
+        if self.views is not None:
+            self.views.render(api.TRN_PATH_TRACER, self.options, launch=self.launch, out=self.image)
+            mark("forward")
+            local_loss = self.views.loss(self.image, self.targets, self.dLdI)
+            for i in self.integrators:
+                self.views.render_grad(i, self.options, self.dLdI, launch=self.launch)
+                mark(f"grad_{i}")
+        else:
+            local_loss = torch.zeros(0, device=sc.device)
         g = sc.get_grads()["positions"]
-        self.x.grad = torch.nan_to_num(g, nan=0.0, posinf=0.0, neginf=0.0)
+        # non-finite entries are zeroed, as the reference's multi-view bridge
+        # does (pyTensorRay/renderer_multi_view.py:94)
+        g = torch.nan_to_num(g, nan=0.0, posinf=0.0, neginf=0.0)
+        self.x.grad = trd.allreduce_grads({"positions": g}, self.group)["positions"]
+        self.loss = trd.gather_view_values(self.shard, local_loss, self.group)
+        mark("exchange")
         self.opt.step()
         mark("update")
         self.steps += 1

@@ -53,3 +53,122 @@ def test_rank_seeds_are_disjoint_and_views_balance():
 def test_single_process_allreduce_is_identity():
     g = {"positions": torch.ones(3, 3)}
     assert trd.allreduce_grads(g) is g
+
+
+# ---- view-sharded inverse-rendering step, render stubbed on the CPU ----------
+class _FakeCamera:
+    def __init__(self, w, h):
+        self.width, self.height = w, h
+
+
+class _FakeScene:
+    """Stands in for api.Scene: raw positions, a gradient buffer that the
+    fake view sets accumulate into, and a log of every rendered view."""
+
+    def __init__(self, nv):
+        self.device = torch.device("cpu")
+        self._raw_positions = torch.linspace(-1.0, 1.0, nv * 3).reshape(nv, 3)
+        self.grad = torch.zeros(nv, 3)
+        self.rendered = []
+
+    def set_vertex_positions(self, x):
+        self._raw_positions = x.detach().clone()
+
+    def configure(self, refit=False):
+        pass
+
+    def clear_grads(self):
+        self.grad.zero_()
+
+    def get_grads(self):
+        return {"positions": self.grad.clone()}
+
+
+class _FakeViewSet:
+    """Stands in for api.ViewSet: view i of the set is global view seeds[i];
+    its image, loss and gradient depend only on that index and the positions."""
+
+    def __init__(self, scene, cameras, spps, seeds=None):
+        self.scene, self.cameras, self.spps = scene, list(cameras), list(spps)
+        self.seeds = list(seeds if seeds is not None else range(len(cameras)))
+        self.npix = sum(c.width * c.height for c in cameras)
+
+    def _slices(self):
+        off = 0
+        for c in self.cameras:
+            n = c.width * c.height
+            yield slice(off, off + n)
+            off += n
+
+    def render(self, integrator, options, launch=None, out=None):
+        for v, sl in zip(self.seeds, self._slices()):
+            out[sl] = float(v + 1) * self.scene._raw_positions.sum() / 10.0
+            self.scene.rendered.append(("fwd", v))
+        return out
+
+    def loss(self, image, targets, dLdI):
+        dLdI.copy_(image - targets)
+        return torch.stack([0.5 * (dLdI[sl] ** 2).sum() for sl in self._slices()])
+
+    def render_grad(self, integrator, options, dLdI, launch=None):
+        nv = self.scene.grad.shape[0]
+        for v, sl in zip(self.seeds, self._slices()):
+            self.scene.grad[v % nv] += dLdI[sl].sum(0) * (integrator + 1)
+            self.scene.rendered.append(("grad", integrator, v))
+
+
+def _views_setup():
+    cams = [_FakeCamera(w, w) for w in (4, 2, 3, 5, 1, 2, 4)]
+    spps = [8, 64, 16, 4, 32, 8, 16]
+    npix = sum(c.width * c.height for c in cams)
+    targets = torch.arange(npix * 3, dtype=torch.float32).reshape(npix, 3) / npix
+    return cams, spps, targets
+
+
+def _run_inverse(steps):
+    from tensorray_b200 import api, inverse
+    cams, spps, targets = _views_setup()
+    scene = _FakeScene(5)
+    real = api.ViewSet
+    api.ViewSet = _FakeViewSet
+    try:
+        inv = inverse.InverseRenderer(scene, cams, spps, targets, api.RenderOptions(0, 3, 0, 0, 0, 0, 0), lr=1e-2)
+        losses = [inv.step().clone() for _ in range(steps)]
+    finally:
+        api.ViewSet = real
+    return inv, scene, losses
+
+
+def _sharded_worker(rank, world, port, out):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    inv, scene, losses = _run_inverse(3)
+    out[rank] = (list(inv.shard.local), scene.rendered, [l.tolist() for l in losses], inv.x.detach().clone(),
+                 inv.x.grad.clone())
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_view_sharded_inverse_step_matches_one_rank():
+    """Two gloo ranks split the views by cost; every view is rendered exactly
+    once per step, the summed gradient, the per-view losses and the Adam
+    update equal those of a single process rendering every view."""
+    world = 2
+    port = _free_port()
+    mgr = mp.Manager()
+    out = mgr.dict()
+    mp.start_processes(_sharded_worker, args=(world, port, out), nprocs=world, join=True, start_method="spawn")
+    inv1, scene1, losses1 = _run_inverse(3)
+    nviews = len(_views_setup()[0])
+    locals_ = [out[r][0] for r in range(world)]
+    assert sorted(sum(locals_, [])) == list(range(nviews)) and all(locals_)
+    # three steps: every view's forward once per step, and its gradient once
+    # per step and integrator, on one rank or the other
+    fwd = sorted(e[1] for r in range(world) for e in out[r][1] if e[0] == "fwd")
+    assert fwd == sorted(list(range(nviews)) * 3)
+    grads = sorted((e[1], e[2]) for r in range(world) for e in out[r][1] if e[0] == "grad")
+    assert grads == sorted([(i, v) for i in (0, 1, 2) for v in range(nviews)] * 3)
+    for r in range(world):
+        assert out[r][2] == [l.tolist() for l in losses1]
+        torch.testing.assert_close(out[r][3], inv1.x.detach(), rtol=1e-6, atol=1e-7)
+        torch.testing.assert_close(out[r][4], inv1.x.grad, rtol=1e-6, atol=1e-6)
