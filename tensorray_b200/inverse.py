@@ -16,6 +16,8 @@ import torch
 
 from . import api
 from . import dist as trd
+from . import loss as trl
+from . import optim as tro
 
 
 class InverseRenderer:
@@ -27,6 +29,12 @@ class InverseRenderer:
     path_cache_bytes: bound on the interior path records the forward render
     keeps for the interior gradient of the same step (0 = re-trace them).
 
+    loss: "l2" (0.5 |I - T|^2 per view in one launch, the default), or "l1",
+    "pyramid_l1", "pyramid_l2" (pyTensorRay/loss.py:41-83, evaluated per view
+    on the device by tensorray_b200.loss). optimizer: "adam" (torch Adam, the
+    default) or "largesteps" (tensorray_b200.optim.LargeSteps over the whole
+    scene's mesh, pyTensorRay/optimizer.py:149-180, with `lmbda`).
+
     With an initialised torch.distributed process group (one process per GPU,
     each with its own replica of the scene), the views are split over the
     ranks by cost (trd.ViewShard); each rank renders its views, the vertex
@@ -36,8 +44,12 @@ class InverseRenderer:
     def __init__(self, scene: api.Scene, cameras: list, spps: list, targets: torch.Tensor,
                  options: api.RenderOptions, integrators=(api.TRN_PATH_TRACER, api.TRN_PRIMARY_EDGE,
                                                           api.TRN_DIRECT_EDGE),
-                 lr: float = 1e-3, refit: bool = True, launch=None, path_cache_bytes: int = 0, group=None):
+                 lr: float = 1e-3, refit: bool = True, launch=None, path_cache_bytes: int = 0, group=None,
+                 loss: str = "l2", optimizer: str = "adam", lmbda: float = 0.1):
+        if loss not in ("l2",) + tuple(trl.LOSSES):
+            raise ValueError(f"unknown loss {loss!r}")
         self.scene = scene
+        self.loss_kind = loss
         self.group = group
         npix_all = sum(c.width * c.height for c in cameras)
         if targets.numel() != 3 * npix_all:
@@ -61,12 +73,39 @@ class InverseRenderer:
         self.launch = launch
         dev = scene.device
         self.x = scene._raw_positions.detach().clone().requires_grad_(True)
-        self.opt = torch.optim.Adam([self.x], lr=lr)
+        if optimizer == "adam":
+            self.opt = torch.optim.Adam([self.x], lr=lr)
+        elif optimizer == "largesteps":
+            faces = torch.as_tensor(scene.spec.arrays()["indices"], device=dev).reshape(-1, 3)
+            self.opt = tro.LargeSteps(self.x, faces, lr=lr, lmbda=lmbda)
+        else:
+            raise ValueError(f"unknown optimizer {optimizer!r}")
+        # target pyramids of the pyramid losses, per local view
+        self._target_levels = None
+        if loss.startswith("pyramid"):
+            self._target_levels = [trl.build_pyramid(self._view(self.targets, i)) for i in range(len(self.shard.local))]
         npix = self.views.npix if self.views is not None else 0
         self.image = torch.empty(npix, 3, device=dev)
         self.dLdI = torch.empty(npix, 3, device=dev)
         self.loss = torch.zeros(len(cameras), device=dev)
         self.steps = 0
+
+    def _view(self, flat: torch.Tensor, i: int) -> torch.Tensor:
+        """Local view i of a concatenated [npix, 3] buffer as (H, W, 3)."""
+        c = self.views.cameras[i]
+        off = self.views.offsets[i]
+        return flat[off:off + c.width * c.height].view(c.height, c.width, 3)
+
+    def _loss_and_dLdI(self) -> torch.Tensor:
+        if self.loss_kind == "l2":
+            return self.views.loss(self.image, self.targets, self.dLdI)
+        losses = []
+        for i in range(len(self.views.cameras)):
+            tgt = self._target_levels[i] if self._target_levels is not None else self._view(self.targets, i)
+            l, g = trl.loss_and_grad(self.loss_kind, self._view(self.image, i), tgt)
+            self._view(self.dLdI, i).copy_(g)
+            losses.append(l)
+        return torch.stack(losses)
 
     def samples_per_step(self) -> int:
         """Grad path-samples of one step on this rank: its views' W*H*spp per term."""
@@ -95,7 +134,7 @@ class InverseRenderer:
         if self.views is not None:
             self.views.render(api.TRN_PATH_TRACER, self.options, launch=self.launch, out=self.image)
             mark("forward")
-            local_loss = self.views.loss(self.image, self.targets, self.dLdI)
+            local_loss = self._loss_and_dLdI()
             for i in self.integrators:
                 self.views.render_grad(i, self.options, self.dLdI, launch=self.launch)
                 mark(f"grad_{i}")

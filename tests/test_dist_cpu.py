@@ -92,6 +92,7 @@ class _FakeViewSet:
         self.scene, self.cameras, self.spps = scene, list(cameras), list(spps)
         self.seeds = list(seeds if seeds is not None else range(len(cameras)))
         self.npix = sum(c.width * c.height for c in cameras)
+        self.offsets = [sum(c.width * c.height for c in cameras[:i]) for i in range(len(cameras))]
 
     def _slices(self):
         off = 0
@@ -172,3 +173,44 @@ def test_view_sharded_inverse_step_matches_one_rank():
         assert out[r][2] == [l.tolist() for l in losses1]
         torch.testing.assert_close(out[r][3], inv1.x.detach(), rtol=1e-6, atol=1e-7)
         torch.testing.assert_close(out[r][4], inv1.x.grad, rtol=1e-6, atol=1e-6)
+
+
+class _FakeSpec:
+    def __init__(self, faces):
+        self.faces = faces
+
+    def arrays(self):
+        return {"indices": self.faces}
+
+
+def test_inverse_step_pyramid_loss_and_largesteps_plumbing():
+    """One process, render stubbed: the pyramid loss's dL/dI per view is the
+    reverse mode of pyTensorRay/loss.py's pyramid L1 of that view, and the
+    LargeSteps option updates the positions as optim.LargeSteps does."""
+    from tensorray_b200 import api, inverse, loss as trl, optim
+    cams, spps, targets = _views_setup()
+    scene = _FakeScene(5)
+    faces = torch.tensor([[0, 1, 2], [0, 2, 3], [0, 3, 4], [0, 4, 1]], dtype=torch.int32)
+    scene.spec = _FakeSpec(faces.numpy())
+    real = api.ViewSet
+    api.ViewSet = _FakeViewSet
+    try:
+        inv = inverse.InverseRenderer(scene, cams, spps, targets, api.RenderOptions(0, 3, 0, 0, 0, 0, 0), lr=1e-2,
+                                      loss="pyramid_l1", optimizer="largesteps", lmbda=0.5)
+        x0 = inv.x.detach().clone()
+        losses = inv.step()
+    finally:
+        api.ViewSet = real
+    assert losses.shape == (len(cams),)
+    for i, c in enumerate(cams):
+        sl = slice(inv.views.offsets[i], inv.views.offsets[i] + c.width * c.height)
+        img = inv.image[sl].view(c.height, c.width, 3)
+        tgt = targets[sl].view(c.height, c.width, 3)
+        ref_loss, ref_g = trl.loss_and_grad("pyramid_l1", img, trl.build_pyramid(tgt))
+        torch.testing.assert_close(inv.dLdI[sl].view(c.height, c.width, 3), ref_g)
+        assert abs(float(losses[i]) - float(ref_loss)) <= 1e-6 * abs(float(ref_loss)) + 1e-7
+    ref = x0.clone().requires_grad_(True)
+    opt = optim.LargeSteps(ref, torch.as_tensor(faces), lr=1e-2, lmbda=0.5)
+    ref.grad = inv.x.grad.clone()
+    opt.step()
+    torch.testing.assert_close(inv.x.detach(), ref.detach())
