@@ -1,0 +1,118 @@
+"""XML scene ingest (SceneLoader.cpp:36-408) on the CPU: the supported
+elements, transforms, bitmap textures and error reporting, and an XML copy
+of the icosphere configuration that loads to the same scene arrays as the
+programmatic one."""
+import os
+
+import numpy as np
+import pytest
+
+from tensorray_b200 import scene_xml, scenes
+
+
+def write_obj(path, P, F, uv=None):
+    with open(path, "w") as f:
+        for p in P:
+            f.write("v %.9g %.9g %.9g\n" % tuple(float(x) for x in p))
+        if uv is not None:
+            for t in uv:
+                f.write("vt %.9g %.9g\n" % (float(t[0]), 1.0 - float(t[1])))
+        for tri in F:
+            if uv is None:
+                f.write("f %d %d %d\n" % tuple(int(i) + 1 for i in tri))
+            else:
+                f.write("f %s\n" % " ".join(f"{int(i) + 1}/{int(i) + 1}" for i in tri))
+
+
+def config1_xml(d, width=64, height=48):
+    """The icosphere configuration as an XML scene with three OBJ files."""
+    spec = scenes.config1_scene(width, height)
+    names = ["sphere.obj", "ground.obj", "light.obj"]
+    for m, n in zip(spec.meshes, names):
+        write_obj(os.path.join(d, n), m.positions, m.faces)
+    xml = f"""<?xml version="1.0"?>
+<scene version="0.5.0">
+  <bsdf type="diffuse" id="sphere_mat"><rgb name="reflectance" value="0.7"/></bsdf>
+  <bsdf type="diffuse" id="gray"><spectrum name="reflectance" value="0.5, 0.5, 0.5"/></bsdf>
+  <shape type="obj" id="sphere">
+    <string name="filename" value="{names[0]}"/>
+    <boolean name="face_normals" value="false"/>
+    <ref id="sphere_mat"/>
+  </shape>
+  <shape type="obj" id="ground"><string name="filename" value="{names[1]}"/><ref id="gray"/></shape>
+  <shape type="obj" id="light">
+    <string name="filename" value="{names[2]}"/>
+    <ref id="gray"/>
+    <emitter type="area"><rgb name="radiance" value="10"/></emitter>
+  </shape>
+  <sensor type="perspective">
+    <float name="fov" value="45"/>
+    <transform name="to_world"><lookat origin="0, 0, 4" target="0, 0, 0" up="0, 1, 0"/></transform>
+    <film type="hdrfilm"><integer name="width" value="{width}"/><integer name="height" value="{height}"/></film>
+  </sensor>
+</scene>
+"""
+    path = os.path.join(d, "scene.xml")
+    with open(path, "w") as f:
+        f.write(xml)
+    return path, spec
+
+
+def test_xml_copy_of_the_icosphere_configuration_loads_the_same_arrays(tmp_path):
+    path, ref = config1_xml(str(tmp_path))
+    spec = scene_xml.load_xml(path)
+    a, b = spec.arrays(), ref.arrays()
+    for k in ("positions", "indices", "mesh_bsdf", "mesh_light", "mesh_smooth", "light_radiance"):
+        np.testing.assert_array_equal(a[k], b[k], err_msg=k)
+    # albedos as the renderer reads them: float32
+    assert [(x.type, tuple(np.float32(x.albedo))) for x in spec.bsdfs] == \
+        [(x.type, tuple(np.float32(x.albedo))) for x in ref.bsdfs]
+    assert spec.cameras == ref.cameras
+
+
+def test_transforms_textures_microfacet_and_errors(tmp_path):
+    d = str(tmp_path)
+    P = np.array([[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0]], np.float32)
+    F = np.array([[0, 1, 2], [0, 2, 3]])
+    write_obj(os.path.join(d, "quad.obj"), P, F, uv=P[:, :2])
+    from PIL import Image
+    tex = (np.arange(4 * 5 * 3).reshape(4, 5, 3) * 4).astype(np.uint8)
+    Image.fromarray(tex).save(os.path.join(d, "tex.png"))
+    xml = """<scene>
+  <bsdf type="diffuse" id="t"><texture type="bitmap" name="reflectance"><string name="filename" value="tex.png"/></texture></bsdf>
+  <bsdf type="microfacet" id="g"><float name="roughness" value="0.3"/>
+    <spectrum name="diffuseReflectance" value="0.2 0.3 0.4"/><spectrum name="specularReflectance" value="0.04"/></bsdf>
+  <shape type="obj"><string name="filename" value="quad.obj"/><ref id="t"/>
+    <transform name="toWorld"><scale x="2"/><rotate z="1" angle="90"/><translate x="1" y="2" z="3"/></transform>
+  </shape>
+  <shape type="obj"><string name="filename" value="quad.obj"/><ref id="g"/></shape>
+</scene>"""
+    with open(os.path.join(d, "s.xml"), "w") as f:
+        f.write(xml)
+    spec = scene_xml.load_xml(os.path.join(d, "s.xml"))
+    np.testing.assert_allclose(spec.textures[0], (tex / 255.0) ** 2.2, rtol=1e-6)
+    assert spec.bsdfs[0].texture == 0
+    g = spec.bsdfs[1]
+    assert g.type == scenes.MICROFACET and g.roughness == pytest.approx(0.3)
+    assert g.albedo == pytest.approx((0.2, 0.3, 0.4)) and g.specular == pytest.approx((0.04, 0.04, 0.04))
+    # scale x2, then 90 degrees about z, then translate (1, 2, 3)
+    q = P.astype(np.float64) * [2, 1, 1]
+    q = np.stack([-q[:, 1], q[:, 0], q[:, 2]], 1) + [1, 2, 3]
+    np.testing.assert_allclose(spec.meshes[0].positions, q, atol=1e-6)
+    np.testing.assert_array_equal(spec.meshes[1].positions, P)
+    assert spec.meshes[0].smooth is False and spec.meshes[0].uvs is not None
+    for bad, msg in [('<bsdf type="roughconductor" id="r"/>', "unsupported BSDF"),
+                     ('<shape type="obj"><string name="filename" value="quad.obj"/><ref id="nope"/></shape>',
+                      "unknown BSDF id"),
+                     ('<shape type="sphere"/>', "unsupported shape")]:
+        with open(os.path.join(d, "bad.xml"), "w") as f:
+            f.write("<scene>" + bad + "</scene>")
+        with pytest.raises(scene_xml.SceneXmlError, match=msg):
+            scene_xml.load_xml(os.path.join(d, "bad.xml"))
+
+
+def test_parse_vector_repeats_the_last_component():
+    np.testing.assert_array_equal(scene_xml.parse_vector("0.5", 3, allow_empty=True), [0.5, 0.5, 0.5])
+    np.testing.assert_array_equal(scene_xml.parse_vector("1, 2 3"), [1, 2, 3])
+    with pytest.raises(scene_xml.SceneXmlError):
+        scene_xml.parse_vector("1 2")
