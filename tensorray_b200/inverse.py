@@ -32,8 +32,12 @@ class InverseRenderer:
     loss: "l2" (0.5 |I - T|^2 per view in one launch, the default), or "l1",
     "pyramid_l1", "pyramid_l2" (pyTensorRay/loss.py:41-83, evaluated per view
     on the device by tensorray_b200.loss). optimizer: "adam" (torch Adam, the
-    default) or "largesteps" (tensorray_b200.optim.LargeSteps over the whole
-    scene's mesh, pyTensorRay/optimizer.py:149-180, with `lmbda`).
+    default) or "largesteps" (tensorray_b200.optim.LargeSteps,
+    pyTensorRay/optimizer.py:149-180, with `lmbda`). shapes: indices of the
+    meshes whose vertices are optimised (None: every vertex). The reference
+    optimises one shape's vertices (DiffAllVertexPos, Primitive.cpp:385-388);
+    LargeSteps needs this, since its uniform second moment would otherwise be
+    set by the largest gradient anywhere in the scene.
 
     With an initialised torch.distributed process group (one process per GPU,
     each with its own replica of the scene), the views are split over the
@@ -45,7 +49,7 @@ class InverseRenderer:
                  options: api.RenderOptions, integrators=(api.TRN_PATH_TRACER, api.TRN_PRIMARY_EDGE,
                                                           api.TRN_DIRECT_EDGE),
                  lr: float = 1e-3, refit: bool = True, launch=None, path_cache_bytes: int = 0, group=None,
-                 loss: str = "l2", optimizer: str = "adam", lmbda: float = 0.1):
+                 loss: str = "l2", optimizer: str = "adam", lmbda: float = 0.1, shapes=None):
         if loss not in ("l2",) + tuple(trl.LOSSES):
             raise ValueError(f"unknown loss {loss!r}")
         self.scene = scene
@@ -73,11 +77,29 @@ class InverseRenderer:
         self.launch = launch
         dev = scene.device
         self.x = scene._raw_positions.detach().clone().requires_grad_(True)
+        # the optimised vertices: all, or those of the chosen meshes
+        self._sel = None
+        self._xs = self.x
+        faces = None
+        if shapes is not None:
+            meshes = scene.spec.meshes
+            starts = [0]
+            for m in meshes:
+                starts.append(starts[-1] + len(m.positions))
+            sel, fl, base = [], [], 0
+            for i in shapes:
+                sel.append(torch.arange(starts[i], starts[i + 1]))
+                fl.append(torch.as_tensor(meshes[i].faces, dtype=torch.int64) + base)
+                base += starts[i + 1] - starts[i]
+            self._sel = torch.cat(sel).to(dev)
+            faces = torch.cat(fl).to(dev)
+            self._xs = self.x.detach()[self._sel].clone().requires_grad_(True)
         if optimizer == "adam":
-            self.opt = torch.optim.Adam([self.x], lr=lr)
+            self.opt = torch.optim.Adam([self._xs], lr=lr)
         elif optimizer == "largesteps":
-            faces = torch.as_tensor(scene.spec.arrays()["indices"], device=dev).reshape(-1, 3)
-            self.opt = tro.LargeSteps(self.x, faces, lr=lr, lmbda=lmbda)
+            if faces is None:
+                faces = torch.as_tensor(scene.spec.arrays()["indices"], device=dev).reshape(-1, 3)
+            self.opt = tro.LargeSteps(self._xs, faces, lr=lr, lmbda=lmbda)
         else:
             raise ValueError(f"unknown optimizer {optimizer!r}")
         # target pyramids of the pyramid losses, per local view
@@ -147,7 +169,13 @@ class InverseRenderer:
         self.x.grad = trd.allreduce_grads({"positions": g}, self.group)["positions"]
         self.loss = trd.gather_view_values(self.shard, local_loss, self.group)
         mark("exchange")
-        self.opt.step()
+        if self._sel is None:
+            self.opt.step()
+        else:
+            self._xs.grad = self.x.grad[self._sel]
+            self.opt.step()
+            with torch.no_grad():
+                self.x[self._sel] = self._xs.detach()
         mark("update")
         self.steps += 1
         return self.loss
