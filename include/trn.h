@@ -100,12 +100,15 @@ typedef struct {
   int sppe0;      /* pixel boundary */
   /* AQ guiding of the direct boundary term (RenderOptions::g_*,
    * Integrator.h:72-77; AdaptiveQuadratureDistribution, AQ_distrb.h:62-197).
-   * g_direct != 0 builds a depth-0 guiding distribution per direct-boundary
-   * call from g_direct_spp samples per secondary edge and mixes it with
-   * g_eps. Guided samples use one extra sample dimension (3 + 3*max_bounces).
-   * g_direct_depth, g_direct_max_size and g_direct_thold are accepted for
-   * interface parity; like the reference, only depth 0 is built, and the leaf
-   * arrays are sized by the edge count rather than by g_direct_max_size. */
+   * g_direct != 0 builds a guiding distribution per direct-boundary call:
+   * one leaf per secondary edge (depth 0), then g_direct_depth refinement
+   * passes that evaluate 36 points per leaf and split the leaves whose error
+   * exceeds g_direct_thold (the reference's gen_eval_point / cut_tree,
+   * NEE.cu:91-396, whose loop it keeps commented out, AQ_distrb.h:121-136),
+   * up to max(edges, g_direct_max_size) leaves; leaf weights come from
+   * g_direct_spp samples per leaf, mixed with g_eps. Guided samples use one
+   * extra sample dimension (3 + 3*max_bounces). A refining call allocates
+   * the tree's arrays on first use. */
   int g_direct;
   int g_direct_depth;
   int g_direct_max_size;

@@ -1082,37 +1082,156 @@ def _guide_base_val(scene, x, y, z):
     return out
 
 
-def aq_guide(scene, seed, g_spp, eps):
-    """AdaptiveQuadratureDistribution::setup at tree depth 0 (AQ_distrb.h:83-173,
-    NEE.cu:70-89 build_tree): one leaf per secondary edge, box
-    [cdf[i-1], cdf[i]] x [0,1] x [0,1] of the (edge, light) sample cube; the
-    leaf weight is the mean |baseVal| of g_spp uniform samples in the box,
-    normalised to sum 1, mixed with eps, and the leaf distribution is
-    weight x box volume. Leaves of non-secondary edges (zero length in the
+REFINE_TERM = 6   # hash-sampler term of the refinement's random points
+AQ_POINTS = 36
+
+
+def _f32(x):
+    return np.asarray(x, np.float32)
+
+
+def _aq_points(box, stream):
+    """The 36 evaluation points of every leaf for one refinement pass
+    (gen_eval_point, NEE.cu:91-240, with the box midpoint m = (p0 + p1) / 2):
+    corners and edge midpoints of the x = p0 and x = p1 faces (0-15), corners
+    of the x = m section (16-19), two random points per octant (20-35; octant
+    bits x, y, z = bits 2, 1, 0 of k - 20; the second eight use 1 - r).
+    box is [6, n] float32; returns [n, 36, 3] float32."""
+    lo, hi = box[0:3], box[3:6]
+    mid = _f32((lo + hi) * np.float32(0.5))
+    n = lo.shape[1]
+    pts = np.zeros((n, AQ_POINTS, 3), np.float32)
+    sel = [lo, hi, mid]
+    yz16 = [(0, 0), (0, 1), (0, 2), (1, 0), (1, 1), (1, 2), (2, 0), (2, 1)]
+    yz4 = [(0, 0), (0, 1), (1, 0), (1, 1)]
+    for k in range(20):
+        sx = 0 if k < 8 else (1 if k < 16 else 2)
+        yz = yz16[k & 7] if k < 16 else yz4[k - 16]
+        pts[:, k, 0] = sel[sx][0]
+        pts[:, k, 1] = sel[yz[0]][1]
+        pts[:, k, 2] = sel[yz[1]][2]
+    half = _f32(mid - lo)
+    leaves = np.arange(n, dtype=np.uint64)
+    for k in range(20, 36):
+        o = (k - 20) & 7
+        for a in range(3):
+            r = hash_uniform(stream, REFINE_TERM, 3 * (k - 20) + a, leaves)
+            if k >= 28:
+                r = _f32(np.float32(1.0) - r)
+            base = mid[a] if (o >> (2 - a)) & 1 else lo[a]
+            pts[:, k, a] = _f32(base + _f32(half[a] * r))
+    return pts
+
+
+def _avg8(e, idx):
+    s = _f32(e[:, idx[0]] + e[:, idx[1]])
+    for j in idx[2:]:
+        s = _f32(s + e[:, j])
+    return _f32(s / np.float32(8.0))
+
+
+def _aq_refine(box, edge, ev, thold, stream, limit):
+    """One cut_tree pass (NEE.cu:243-396): split the leaves whose corner and
+    Monte Carlo averages disagree by more than thold (times the box volume)
+    along the axis whose halves disagree most (a random axis on ties). New
+    leaves take the upper half and are appended in leaf order, up to `limit`."""
+    n = box.shape[1]
+    vol = _f32(_f32(_f32(box[3] - box[0]) * _f32(box[4] - box[1])) * _f32(box[5] - box[2]))
+    lag = _avg8(ev, [0, 1, 3, 4, 8, 9, 11, 12])
+    mc = np.zeros(n, np.float32)
+    for k in range(20, 36):
+        mc = _f32(mc + ev[:, k])
+    mc = _f32(mc / np.float32(16.0))
+    err = _f32(np.abs(_f32(lag - mc)) * vol)
+    split = err > np.float32(thold)
+    ad = lambda a, b: np.abs(_f32(a - b))
+    e0 = np.abs(_f32(ad(_avg8(ev, [0, 1, 3, 4, 16, 17, 18, 19]), _avg8(ev, [20, 21, 22, 23, 28, 29, 30, 31])) -
+                     ad(_avg8(ev, [8, 9, 11, 12, 16, 17, 18, 19]), _avg8(ev, [24, 25, 26, 27, 32, 33, 34, 35]))))
+    e1 = np.abs(_f32(ad(_avg8(ev, [0, 1, 6, 7, 8, 9, 14, 15]), _avg8(ev, [20, 21, 24, 25, 28, 29, 32, 33])) -
+                     ad(_avg8(ev, [3, 4, 6, 7, 11, 12, 14, 15]), _avg8(ev, [22, 23, 26, 27, 30, 31, 34, 35]))))
+    e2 = np.abs(_f32(ad(_avg8(ev, [0, 2, 3, 5, 8, 10, 11, 13]), _avg8(ev, [20, 22, 24, 26, 28, 30, 32, 34])) -
+                     ad(_avg8(ev, [1, 2, 4, 5, 9, 10, 12, 13]), _avg8(ev, [21, 23, 25, 27, 29, 31, 33, 35]))))
+    r = _f32(hash_uniform(stream, REFINE_TERM, 48, np.arange(n, dtype=np.uint64)) * np.float32(3.0))
+    axis = np.where(r < 1.0, 0, np.where(r < 2.0, 1, 2))
+    axis = np.where((e2 > e0) & (e2 > e1), 2, axis)
+    axis = np.where((e1 > e0) & (e1 > e2), 1, axis)
+    axis = np.where((e0 > e1) & (e0 > e2), 0, axis)
+    new_box, new_edge = [], []
+    box = box.copy()
+    for leaf in np.nonzero(split)[0]:
+        if n + len(new_box) >= limit:
+            break
+        a = axis[leaf]
+        mid = _f32((box[a, leaf] + box[3 + a, leaf]) * np.float32(0.5))
+        nb = box[:, leaf].copy()
+        nb[a] = mid
+        box[3 + a, leaf] = mid
+        new_box.append(nb)
+        new_edge.append(edge[leaf])
+    if new_box:
+        box = np.concatenate([box, np.stack(new_box, 1)], 1)
+        edge = np.concatenate([edge, np.array(new_edge, edge.dtype)])
+    return box, edge
+
+
+def aq_guide(scene, seed, g_spp, eps, depth=0, max_size=100000, thold=0.01):
+    """AdaptiveQuadratureDistribution::setup (AQ_distrb.h:83-173). The depth-0
+    tree (build_tree, NEE.cu:70-89) has one leaf per secondary edge, box
+    [cdf[i-1], cdf[i]] x [0,1] x [0,1] of the (edge, light) sample cube.
+    `depth` refinement passes then evaluate 36 points per leaf and split
+    leaves (the loop the reference keeps commented out, AQ_distrb.h:121-136;
+    see _aq_points, _aq_refine); the tree holds at most max(E, max_size)
+    leaves. The leaf weight is the mean |baseVal| of g_spp uniform samples in
+    the box, normalised to sum 1, mixed with eps, and the leaf distribution is
+    weight x box volume. Leaves on non-secondary edges (zero length in the
     edge distribution) get weight 0 and zero volume, as if absent.
-    Returns (weight, cdf, integral, sum of weight x volume)."""
+    Returns a dict: box [6, n], poly, cdf, integral, fsum (sum of weight x
+    volume)."""
     E = scene.edges.shape[0]
-    cdf = scene.sec_cdf
-    lo = torch.cat([torch.zeros(1), cdf[:-1]])
-    hi = cdf
-    live = scene.sec_func.detach() > 0
-    poly = torch.zeros(E)
-    leaf = torch.arange(E)
+    cdf = scene.sec_cdf.numpy().astype(np.float32)
+    box = np.zeros((6, E), np.float32)
+    box[0, 1:] = cdf[:-1]
+    box[3] = cdf
+    box[4] = 1.0
+    box[5] = 1.0
+    edge = np.arange(E)
+    efunc = scene.sec_func.detach().numpy()
+    live_scene = float(scene.sec_integral) > 0
     stream = (seed * 1000003) & 0xFFFFFFFF
+    limit = max(E, max_size) if depth > 0 else E
+    for p in range(depth):
+        ps = (stream + p) & 0xFFFFFFFF
+        pts = _aq_points(box, ps)
+        n = box.shape[1]
+        flat = torch.from_numpy(pts.reshape(-1, 3))
+        live = np.repeat((efunc[edge] > 0) & live_scene, AQ_POINTS)
+        ev = np.zeros(n * AQ_POINTS, np.float32)
+        if live.any():
+            m = np.nonzero(live)[0]
+            ev[m] = _guide_base_val(scene, flat[m, 0], flat[m, 1], flat[m, 2]).numpy()
+        box, edge = _aq_refine(box, edge, ev.reshape(n, AQ_POINTS), thold, ps, limit)
+    n = box.shape[1]
+    live = torch.from_numpy((efunc[edge] > 0) & live_scene)
+    tb = torch.from_numpy(box)
+    poly = torch.zeros(n)
+    leaf = torch.arange(n)
     for k in range(g_spp):
         slot = (leaf * g_spp + k).numpy().astype(np.uint64)
         r = [torch.from_numpy(hash_uniform(stream, GUIDE_TERM, d, slot)) for d in range(3)]
-        x = lo + r[0] * (hi - lo)
-        bv = _guide_base_val(scene, x, r[1], r[2])
+        x = tb[0] + r[0] * (tb[3] - tb[0])
+        y = tb[1] + r[1] * (tb[4] - tb[1])
+        z = tb[2] + r[2] * (tb[5] - tb[2])
+        bv = _guide_base_val(scene, x, y, z)
         poly = poly + torch.where(live, bv, torch.zeros_like(bv)) / np.float32(g_spp)
     tot = float(poly.double().sum())
     if tot > 0:
         poly = poly / np.float32(tot)
     poly = np.float32(eps) + np.float32(1.0 - eps) * poly
-    func = poly * (hi - lo)
+    vol = ((tb[3] - tb[0]) * (tb[4] - tb[1])) * (tb[5] - tb[2])
+    func = poly * vol
     gcdf, gint = cdf_of(func)
     fsum = torch.tensor(float(func.double().sum()), dtype=F32)
-    return poly, gcdf, gint, fsum
+    return {"box": tb, "edge": torch.from_numpy(edge), "poly": poly, "cdf": gcdf, "integral": gint, "fsum": fsum}
 
 
 def direct_edge(scene, cam, spp, D, smp, guide=None):
@@ -1129,17 +1248,19 @@ def direct_edge(scene, cam, spp, D, smp, guide=None):
     slots = torch.arange(N)
     r0 = smp[0][slots]
     pdf_b = torch.ones(N)
+    r1, r2 = smp[1][slots], smp[2][slots]
     if guide is not None:
-        poly, gcdf, gint, fsum = guide
-        if not gint > 0:
+        gcdf = guide["cdf"]
+        if not guide["integral"] > 0:
             return img
         leaf = torch.searchsorted(gcdf, smp[3 + 3 * D][slots], right=False).clamp(0, gcdf.shape[0] - 1)
-        cdf = scene.sec_cdf
-        lo = torch.where(leaf > 0, cdf[(leaf - 1).clamp(min=0)], torch.zeros_like(r0))
-        r0 = lo + r0 * (cdf[leaf] - lo)
-        pdf_b = poly[leaf] / fsum
+        b = guide["box"][:, leaf]
+        r0 = b[0] + r0 * (b[3] - b[0])
+        r1 = b[1] + r1 * (b[4] - b[1])
+        r2 = b[2] + r2 * (b[5] - b[2])
+        pdf_b = guide["poly"][leaf] / guide["fsum"]
     es = _edge_point(scene, scene.sec_func, scene.sec_cdf, scene.sec_integral, r0)
-    ls = scene.light_sample(smp[1][slots], smp[2][slots])
+    ls = scene.light_sample(r1, r2)
     p0, p2, nL = es["p0"], ls["p"], ls["n"]
     ev = p2.detach() - p0.detach()
     dsq = dot(ev, ev)
@@ -1354,7 +1475,7 @@ INTEGRATORS = {0: path_tracer, 1: primary_edge, 2: direct_edge, 3: indirect_edge
 
 
 def render(scene, cam, integrator, spp, D, smp, guiding=None):
-    """guiding = (seed, g_direct_spp, g_eps) turns on AQ guiding of the direct
+    """guiding = (seed, g_direct_spp, g_eps[, depth, max_size, thold]) turns on AQ guiding of the direct
     boundary term."""
     if integrator == 2 and guiding is not None:
         return direct_edge(scene, cam, spp, D, smp, guide=aq_guide(scene, *guiding))

@@ -46,9 +46,13 @@ struct Params {
   int* err;
   unsigned long long* stats;  // optional work counters (see Cnt), nullptr = off
   // AQ guiding of the direct boundary term (nullptr = unguided)
-  const float* aq_poly;       // [E] leaf weights
-  const float* aq_cdf;        // [E] leaf distribution
+  const float* aq_poly;       // [leaves] leaf weights
+  const float* aq_cdf;        // [leaves] leaf distribution
   const float* aq_int;        // [2] integral, sum of weight x volume
+  const float* aq_box;        // [6][aq_cap] leaf boxes (x0, y0, z0, x1, y1, z1)
+  const int* aq_edge;         // [leaves] the secondary edge a leaf lies on
+  const int* aq_n;            // leaf count
+  long long aq_cap;
   // queues of the split kernels (nullptr = fused kernel): q_count[0] counts
   // `queue`, q_count[1] counts `queue2` (the indirect term's second stage),
   // q_count[2] hands out the items of `queue` to a regenerating stage
@@ -1642,6 +1646,12 @@ __global__ void __launch_bounds__(256, TRN_MINB_BODY) k_primary_body_regen(Param
 // ---------------------------------------------------------------------------
 // direct boundary (BoundaryDirect.cpp:38-143, Edge.cpp:90-144, 201-309)
 // ---------------------------------------------------------------------------
+// coordinate `axis` of a point placed by r in [0, 1) in guiding leaf `leaf`
+TRN_D float aq_lerp(const float* box, long long cap, int leaf, int axis, float r) {
+  const float lo = __ldg(box + axis * cap + leaf), hi = __ldg(box + (3 + axis) * cap + leaf);
+  return __fadd_rn(lo, __fmul_rn(r, __fsub_rn(hi, lo)));
+}
+
 // Direct boundary set-up (SampleBoundarySegmentDirect, Edge.cpp:108-144, with
 // AQ guiding when enabled; EvalBoundarySegmentDirect's geometry,
 // Edge.cpp:201-291). Returns false for a rejected sample.
@@ -1650,20 +1660,21 @@ TRN_D bool direct_setup(const Params& P, long long gslot, EdgeState& st, int& vh
   const ViewDesc& V = view_of(P, gslot, vhint);
   const long long p = gslot - V.begin;
   const PathSmp S{&P, V.seed, gslot, p + V.slot_off};
-  float r0 = S(0);
-  const float r1 = S(1), r2 = S(2);
+  float r0 = S(0), r1 = S(1), r2 = S(2);
   float reuse;
   const float integral = __ldg(P.eint);
   if (!(integral > 0.f)) return false;
   float pdf_b = 1.f;
   if (P.aq_cdf) {
     // AdaptiveQuadratureDistribution::sample (AQ_distrb.h:176-195): pick a
-    // leaf with the extra uniform, then place the edge coordinate in its box
+    // leaf with the extra uniform, then place the (edge, light) sample point
+    // uniformly in its box
     if (!(__ldg(P.aq_int) > 0.f)) return false;
     float unused;
-    const int leaf = sample_discrete(P.aq_cdf, P.ne, S(3 + 3 * V.D), unused);
-    const float lo = leaf > 0 ? __ldg(P.ecdf + leaf - 1) : 0.f, hi = __ldg(P.ecdf + leaf);
-    r0 = __fadd_rn(lo, __fmul_rn(r0, __fsub_rn(hi, lo)));
+    const int leaf = sample_discrete(P.aq_cdf, __ldg(P.aq_n), S(3 + 3 * V.D), unused);
+    r0 = aq_lerp(P.aq_box, P.aq_cap, leaf, 0, r0);
+    r1 = aq_lerp(P.aq_box, P.aq_cap, leaf, 1, r1);
+    r2 = aq_lerp(P.aq_box, P.aq_cap, leaf, 2, r2);
     pdf_b = __fdiv_rn(__ldg(P.aq_poly + leaf), __ldg(P.aq_int + 1));
   }
   const int e = sample_discrete(P.ecdf, P.ne, r0, reuse);
@@ -1847,24 +1858,186 @@ TRN_D float guide_base_val(const Params& P, float x, float y, float z) {
   return isfinite(bv) ? bv : 0.f;
 }
 
-// Leaf weight = mean |baseVal| over gspp uniform samples in the leaf box
-// [cdf[i-1], cdf[i]] x [0,1]^2. Leaves of non-secondary edges (zero length in
-// the edge distribution) do not exist in the reference's compacted edge list
-// and get weight 0 here.
-__global__ void k_aq_poly(Params P, uint32_t stream, int gspp, float* poly) {
+constexpr uint32_t kRefineTerm = 6;  // hash-sampler term of the refinement's random points
+constexpr int kAqPoints = 36;        // evaluation points per leaf and refinement pass
+
+// Depth-0 tree (build_tree, NEE.cu:70-89, with one y and one z cell): leaf i
+// is edge i's interval of the secondary-edge CDF times [0, 1]^2.
+__global__ void k_aq_init(int ne, const float* ecdf, float* box, int* edge, int* count, long long cap) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= P.ne) return;
+  if (i == 0) { count[0] = ne; count[1] = ne; }
+  if (i >= ne) return;
+  box[i] = i > 0 ? ecdf[i - 1] : 0.f;
+  box[cap + i] = 0.f;
+  box[2 * cap + i] = 0.f;
+  box[3 * cap + i] = ecdf[i];
+  box[4 * cap + i] = 1.f;
+  box[5 * cap + i] = 1.f;
+  edge[i] = i;
+}
+
+// Evaluation point k of a leaf for a refinement pass (gen_eval_point,
+// NEE.cu:91-240, with the box midpoint m = (p0 + p1) / 2): k < 16 are the
+// corners and edge midpoints of the x = p0 and x = p1 faces, 16..19 the
+// corners of the x = m section, and 20..35 two random points in each octant
+// (octant bits x, y, z = bits 2, 1, 0 of k - 20; the second eight use 1 - r).
+TRN_D void aq_point(const float* box, long long cap, int leaf, int k, uint32_t stream, float out[3]) {
+  float lo[3], hi[3], mid[3];
+  for (int a = 0; a < 3; a++) {
+    lo[a] = box[a * cap + leaf];
+    hi[a] = box[(3 + a) * cap + leaf];
+    mid[a] = __fmul_rn(__fadd_rn(lo[a], hi[a]), 0.5f);
+  }
+  if (k < 20) {
+    // (y, z) of the face points: low, high or middle per axis
+    const unsigned char yz16[8][2] = {{0, 0}, {0, 1}, {0, 2}, {1, 0}, {1, 1}, {1, 2}, {2, 0}, {2, 1}};
+    const unsigned char yz4[4][2] = {{0, 0}, {0, 1}, {1, 0}, {1, 1}};
+    const int sx = k < 8 ? 0 : (k < 16 ? 1 : 2);
+    const unsigned char* yz = k < 16 ? yz16[k & 7] : yz4[k - 16];
+    auto pick = [&](int a, int c) { return c == 0 ? lo[a] : (c == 1 ? hi[a] : mid[a]); };
+    out[0] = pick(0, sx);
+    out[1] = pick(1, yz[0]);
+    out[2] = pick(2, yz[1]);
+    return;
+  }
+  const int o = (k - 20) & 7;
+  for (int a = 0; a < 3; a++) {
+    float r = hash_uniform(stream, kRefineTerm, (uint32_t)(3 * (k - 20) + a), (uint32_t)leaf);
+    if (k >= 28) r = __fsub_rn(1.f, r);
+    const float base = ((o >> (2 - a)) & 1) ? mid[a] : lo[a];
+    out[a] = __fadd_rn(base, __fmul_rn(__fsub_rn(mid[a], lo[a]), r));
+  }
+}
+
+// One thread per (leaf, point): |baseVal| at the refinement's evaluation
+// points (GuideDirectBoundary_Helper, AQ_distrb.h:65-79).
+__global__ void k_aq_eval(Params P, uint32_t stream, const float* box, const int* edge, const int* count,
+                          long long cap, float* eval) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const int leaf = (int)(t / kAqPoints), k = (int)(t % kAqPoints);
+  if (leaf >= __ldg(count)) return;
+  float v = 0.f;
+  if (P.efunc[edge[leaf]] > 0.f && __ldg(P.eint) > 0.f) {
+    float x[3];
+    aq_point(box, cap, leaf, k, stream, x);
+    v = guide_base_val(P, x[0], x[1], x[2]);
+  }
+  eval[t] = v;
+}
+
+// sum of the 8 listed evaluation values of a leaf, added in list order, over 8
+TRN_D float aq_avg8(const float* e, int a, int b, int c, int d, int f, int g, int h, int i) {
+  float s = __fadd_rn(e[a], e[b]);
+  s = __fadd_rn(s, e[c]);
+  s = __fadd_rn(s, e[d]);
+  s = __fadd_rn(s, e[f]);
+  s = __fadd_rn(s, e[g]);
+  s = __fadd_rn(s, e[h]);
+  s = __fadd_rn(s, e[i]);
+  return __fdiv_rn(s, 8.f);
+}
+
+// Split decision per leaf (cut_tree, NEE.cu:243-396): the leaf's error is
+// |corner average - Monte Carlo average| x volume; above `thold` it splits
+// along the axis whose two halves disagree most between their corner and
+// Monte Carlo averages (a random axis on ties). flag = 0 (keep) or 1 + axis.
+__global__ void k_aq_flag(const float* box, const int* count, long long cap, const float* eval, float thold,
+                          uint32_t stream, int* flag) {
+  const int leaf = blockIdx.x * blockDim.x + threadIdx.x;
+  if (leaf >= __ldg(count)) return;
+  const float* e = eval + (long long)leaf * kAqPoints;
+  const float vol = __fmul_rn(__fmul_rn(__fsub_rn(box[3 * cap + leaf], box[leaf]),
+                                        __fsub_rn(box[4 * cap + leaf], box[cap + leaf])),
+                              __fsub_rn(box[5 * cap + leaf], box[2 * cap + leaf]));
+  const float lag = aq_avg8(e, 0, 1, 3, 4, 8, 9, 11, 12);
+  float mc = 0.f;
+  for (int k = 20; k < 36; k++) mc = __fadd_rn(mc, e[k]);
+  mc = __fdiv_rn(mc, 16.f);
+  const float err = __fmul_rn(fabsf(__fsub_rn(lag, mc)), vol);
+  int f = 0;
+  if (err > thold) {
+    const float d1a = aq_avg8(e, 0, 1, 3, 4, 16, 17, 18, 19), d1b = aq_avg8(e, 8, 9, 11, 12, 16, 17, 18, 19);
+    const float d2a = aq_avg8(e, 0, 1, 6, 7, 8, 9, 14, 15), d2b = aq_avg8(e, 3, 4, 6, 7, 11, 12, 14, 15);
+    const float d3a = aq_avg8(e, 0, 2, 3, 5, 8, 10, 11, 13), d3b = aq_avg8(e, 1, 2, 4, 5, 9, 10, 12, 13);
+    const float m1a = aq_avg8(e, 20, 21, 22, 23, 28, 29, 30, 31), m1b = aq_avg8(e, 24, 25, 26, 27, 32, 33, 34, 35);
+    const float m2a = aq_avg8(e, 20, 21, 24, 25, 28, 29, 32, 33), m2b = aq_avg8(e, 22, 23, 26, 27, 30, 31, 34, 35);
+    const float m3a = aq_avg8(e, 20, 22, 24, 26, 28, 30, 32, 34), m3b = aq_avg8(e, 21, 23, 25, 27, 29, 31, 33, 35);
+    const float e0 = fabsf(__fsub_rn(fabsf(__fsub_rn(d1a, m1a)), fabsf(__fsub_rn(d1b, m1b))));
+    const float e1 = fabsf(__fsub_rn(fabsf(__fsub_rn(d2a, m2a)), fabsf(__fsub_rn(d2b, m2b))));
+    const float e2 = fabsf(__fsub_rn(fabsf(__fsub_rn(d3a, m3a)), fabsf(__fsub_rn(d3b, m3b))));
+    int axis;
+    if (e0 > e1 && e0 > e2) axis = 0;
+    else if (e1 > e0 && e1 > e2) axis = 1;
+    else if (e2 > e0 && e2 > e1) axis = 2;
+    else {
+      const float r = __fmul_rn(hash_uniform(stream, kRefineTerm, 48u, (uint32_t)leaf), 3.f);
+      axis = r < 1.f ? 0 : (r < 2.f ? 1 : 2);
+    }
+    f = 1 + axis;
+  }
+  flag[leaf] = f;
+}
+
+// Exclusive prefix count of the split flags in leaf order (one block), so
+// that new leaves are appended in a fixed order; count[1] = leaves after the
+// pass, at most `limit`.
+__global__ void k_aq_scan(const int* count, const int* flag, int* prefix, int* count_out, int limit) {
+  __shared__ int part[1024];
+  const int n = __ldg(count);
+  const int T = blockDim.x, tid = threadIdx.x;
+  const int chunk = (n + T - 1) / T;
+  const int a = min(n, tid * chunk), b = min(n, a + chunk);
+  int acc = 0;
+  for (int i = a; i < b; i++) acc += flag[i] != 0;
+  part[tid] = acc;
+  __syncthreads();
+  if (tid == 0) {
+    int run = 0;
+    for (int i = 0; i < T; i++) { const int x = part[i]; part[i] = run; run += x; }
+    count_out[1] = min(n + run, limit);
+  }
+  __syncthreads();
+  int run = part[tid];
+  for (int i = a; i < b; i++) { prefix[i] = run; run += flag[i] != 0; }
+}
+
+// Split the flagged leaves: the leaf keeps the lower half along its axis and
+// the new leaf n + prefix takes the upper half (cut_tree's split).
+__global__ void k_aq_split(const int* count, const int* flag, const int* prefix, float* box, int* edge,
+                           long long cap) {
+  const int leaf = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = __ldg(count);
+  if (leaf >= n || flag[leaf] == 0) return;
+  const int idx = n + prefix[leaf];
+  if (idx >= __ldg(count + 1)) return;
+  const int axis = flag[leaf] - 1;
+  const float lo = box[axis * cap + leaf], hi = box[(3 + axis) * cap + leaf];
+  const float mid = __fmul_rn(__fadd_rn(lo, hi), 0.5f);
+  for (int c = 0; c < 6; c++) box[c * cap + idx] = box[c * cap + leaf];
+  box[axis * cap + idx] = mid;
+  box[(3 + axis) * cap + leaf] = mid;
+  edge[idx] = edge[leaf];
+}
+
+__global__ void k_aq_commit(int* count) { count[0] = count[1]; }
+
+// Leaf weight = mean |baseVal| over gspp uniform samples in the leaf box
+// (AQ_distrb.h:150-161). Leaves on non-secondary edges (zero length in the
+// edge distribution) do not exist in the reference's compacted edge list and
+// get weight 0 here.
+__global__ void k_aq_poly(Params P, uint32_t stream, int gspp, const float* box, const int* edge, const int* count,
+                          long long cap, float* poly) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= __ldg(count)) return;
   float acc = 0.f;
-  if (P.efunc[i] > 0.f && __ldg(P.eint) > 0.f) {
-    const float lo = i > 0 ? P.ecdf[i - 1] : 0.f, hi = P.ecdf[i];
+  if (P.efunc[edge[i]] > 0.f && __ldg(P.eint) > 0.f) {
     const float fs = (float)gspp;
     for (int k = 0; k < gspp; k++) {
       const uint32_t slot = (uint32_t)i * (uint32_t)gspp + (uint32_t)k;
-      const float r0 = hash_uniform(stream, kGuideTerm, 0, slot);
-      const float r1 = hash_uniform(stream, kGuideTerm, 1, slot);
-      const float r2 = hash_uniform(stream, kGuideTerm, 2, slot);
-      const float x = __fadd_rn(lo, __fmul_rn(r0, __fsub_rn(hi, lo)));
-      acc = __fadd_rn(acc, __fdiv_rn(guide_base_val(P, x, r1, r2), fs));
+      const float x = aq_lerp(box, cap, i, 0, hash_uniform(stream, kGuideTerm, 0, slot));
+      const float y = aq_lerp(box, cap, i, 1, hash_uniform(stream, kGuideTerm, 1, slot));
+      const float z = aq_lerp(box, cap, i, 2, hash_uniform(stream, kGuideTerm, 2, slot));
+      acc = __fadd_rn(acc, __fdiv_rn(guide_base_val(P, x, y, z), fs));
     }
   }
   poly[i] = acc;
@@ -1873,8 +2046,10 @@ __global__ void k_aq_poly(Params P, uint32_t stream, int gspp, float* poly) {
 // poly /= sum(poly); poly = eps + (1 - eps) poly; func = poly x leaf volume;
 // out[1] = sum(func) (the pdf normaliser of AQ_distrb.h:194). One block of
 // 1024 threads.
-__global__ void k_aq_mix(int n, float* poly, const float* ecdf, float eps, float* func, float* out) {
+__global__ void k_aq_mix(const int* count, float* poly, const float* box, long long cap, float eps, float* func,
+                         float* out) {
   __shared__ double part[1024];
+  const int n = __ldg(count);
   const int tid = threadIdx.x, T = blockDim.x;
   double acc = 0.0;
   for (int i = tid; i < n; i += T) acc += (double)poly[i];
@@ -1893,8 +2068,9 @@ __global__ void k_aq_mix(int n, float* poly, const float* ecdf, float eps, float
     float p = poly[i];
     if (tot > 0.0) p = __fdiv_rn(p, ftot);
     p = __fadd_rn(eps, __fmul_rn(one_m, p));
-    const float lo = i > 0 ? ecdf[i - 1] : 0.f;
-    const float f = __fmul_rn(p, __fsub_rn(ecdf[i], lo));
+    const float vol = __fmul_rn(__fmul_rn(__fsub_rn(box[3 * cap + i], box[i]), __fsub_rn(box[4 * cap + i], box[cap + i])),
+                                __fsub_rn(box[5 * cap + i], box[2 * cap + i]));
+    const float f = __fmul_rn(p, vol);
     poly[i] = p;
     func[i] = f;
     acc += (double)f;
@@ -2422,7 +2598,7 @@ __global__ void k_edge_keys(Params P, int term, unsigned* keys, unsigned* vals) 
       if (__ldg(V.pint) > 0.f) e = sample_discrete(V.pcdf, P.ne, S(0), reuse);
     } else if (__ldg(P.eint) > 0.f && (term != TRN_INDIRECT_EDGE || V.D >= 2)) {
       if (term == TRN_DIRECT_EDGE && P.aq_cdf)
-        e = sample_discrete(P.aq_cdf, P.ne, S(3 + 3 * V.D), reuse);
+        e = __ldg(P.aq_edge + sample_discrete(P.aq_cdf, __ldg(P.aq_n), S(3 + 3 * V.D), reuse));
       else
         e = sample_discrete(P.ecdf, P.ne, S(0), reuse);
     }
@@ -2579,12 +2755,10 @@ __global__ void k_prim_edges_views(int ne, const int* edges, const float* pos, c
 }
 
 // Distribution1D::SetFunction for one block per view (prefix sums in double)
-__global__ void k_cdf_views(int n, const float* func_all, float* cdf_all, float* integral_all) {
+// Distribution1D::SetFunction over n weights by one block (see k_cdf).
+TRN_D void cdf_block(int n, const float* func, float* cdf, float* integral_out) {
   __shared__ double part[1024];
   __shared__ float integral;
-  const int v = blockIdx.x;
-  const float* func = func_all + (long long)v * n;
-  float* cdf = cdf_all + (long long)v * n;
   const int T = blockDim.x, tid = threadIdx.x;
   const int chunk = (n + T - 1) / T;
   const int a = min(n, tid * chunk), b = min(n, a + chunk);
@@ -2598,9 +2772,20 @@ __global__ void k_cdf_views(int n, const float* func_all, float* cdf_all, float*
   double run = part[tid];
   for (int i = a; i < b; i++) { run += (double)func[i]; cdf[i] = (float)run * inv_size; }
   __syncthreads();
-  if (tid == 0) { integral = n > 0 ? cdf[n - 1] : 0.f; integral_all[v] = integral; }
+  if (tid == 0) { integral = n > 0 ? cdf[n - 1] : 0.f; *integral_out = integral; }
   __syncthreads();
   if (integral > 0.f) for (int i = a; i < b; i++) cdf[i] = cdf[i] / integral;
+}
+
+// one distribution per block: view v's n weights at func_all + v n
+__global__ void k_cdf_views(int n, const float* func_all, float* cdf_all, float* integral_all) {
+  const int v = blockIdx.x;
+  cdf_block(n, func_all + (long long)v * n, cdf_all + (long long)v * n, integral_all + v);
+}
+
+// one distribution whose length is in device memory (the guiding tree's leaves)
+__global__ void k_cdf_count(const int* count, const float* func, float* cdf, float* integral) {
+  cdf_block(__ldg(count), func, cdf, integral);
 }
 
 // 0.5 |I - T|^2 per view and dL/dI = I - T (pyTensorRay/loss.py:34-38)
@@ -2811,6 +2996,9 @@ Params base_params(trn_scene* s, trn_viewset* vs, const trn_render_options* o, i
   P.err = s->err;
   P.stats = s->stats_on ? s->stats : nullptr;
   P.aq_poly = P.aq_cdf = P.aq_int = nullptr;
+  P.aq_box = nullptr;
+  P.aq_edge = P.aq_n = nullptr;
+  P.aq_cap = 0;
   P.queue = nullptr;
   P.queue2 = nullptr;
   P.q_count = nullptr;
@@ -2820,29 +3008,98 @@ Params base_params(trn_scene* s, trn_viewset* vs, const trn_render_options* o, i
   return P;
 }
 
+// Grow the guiding tree's arrays to `cap` leaves (the first refining call, or
+// a larger g_direct_max_size); the depth-0 arrays are allocated with the scene.
+int aq_reserve(trn_scene* s, long long cap) {
+  if (cap <= s->aq_cap && s->aq_eval) return 0;
+  cap = std::max(cap, s->aq_cap);
+  float* f[4] = {nullptr, nullptr, nullptr, nullptr};
+  int* i3[3] = {nullptr, nullptr, nullptr};
+  float* eval = nullptr;
+  const size_t n = (size_t)cap;
+  bool ok = cudaMalloc(&f[0], n * sizeof(float)) == cudaSuccess && cudaMalloc(&f[1], n * sizeof(float)) == cudaSuccess &&
+            cudaMalloc(&f[2], n * sizeof(float)) == cudaSuccess && cudaMalloc(&f[3], 6 * n * sizeof(float)) == cudaSuccess &&
+            cudaMalloc(&i3[0], n * sizeof(int)) == cudaSuccess && cudaMalloc(&i3[1], n * sizeof(int)) == cudaSuccess &&
+            cudaMalloc(&i3[2], n * sizeof(int)) == cudaSuccess &&
+            cudaMalloc(&eval, (size_t)kAqPoints * n * sizeof(float)) == cudaSuccess;
+  if (!ok) {
+    for (float* p : f) if (p) cudaFree(p);
+    for (int* p : i3) if (p) cudaFree(p);
+    if (eval) cudaFree(eval);
+    cudaGetLastError();
+    set_error("guiding: cannot allocate the refined tree (g_direct_max_size leaves)");
+    return -1;
+  }
+  void* old[] = {s->aq_poly, s->aq_func, s->aq_cdf, s->aq_box, s->aq_edge, s->aq_flag, s->aq_prefix, s->aq_eval};
+  for (void* p : old) if (p) cudaFree(p);
+  s->aq_poly = f[0]; s->aq_func = f[1]; s->aq_cdf = f[2]; s->aq_box = f[3];
+  s->aq_edge = i3[0]; s->aq_flag = i3[1]; s->aq_prefix = i3[2]; s->aq_eval = eval;
+  s->aq_cap = cap;
+  return 0;
+}
+
 // AdaptiveQuadratureDistribution::setup (AQ_distrb.h:83-173) for one
-// direct-boundary call: leaf weights from g_direct_spp samples per leaf, eps
-// mixing, leaf distribution. The set-up samples come from the counter hash
-// (its own term), also when the call's samples come from a table.
-int guide_setup(trn_scene* s, const trn_render_options* o, Params& P, cudaStream_t st) {
+// direct-boundary call: the depth-0 tree, g_direct_depth refinement passes
+// (the loop the reference keeps commented out, AQ_distrb.h:121-136, with
+// gen_eval_point and cut_tree of NEE.cu:91-396), leaf weights from
+// g_direct_spp samples per leaf, eps mixing, leaf distribution. The tree
+// holds at most max(E, g_direct_max_size) leaves. The set-up samples come
+// from the counter hash (their own terms), also when the call's samples come
+// from a table. may_alloc = false (the allocation-free entry point) refuses
+// a refinement that would need larger arrays than the scene holds.
+int guide_setup(trn_scene* s, const trn_render_options* o, Params& P, cudaStream_t st, bool may_alloc = true) {
   if (!o->g_direct || s->ne == 0) return 0;
   if (o->g_direct_spp <= 0) { set_error("g_direct_spp must be positive when g_direct is set"); return -1; }
   if (!(o->g_eps >= 0.f && o->g_eps <= 1.f)) { set_error("g_eps must be in [0, 1]"); return -1; }
-  if ((long long)s->ne * o->g_direct_spp > 0xFFFFFFFFLL) {
-    set_error("guiding: edges x g_direct_spp exceeds 2^32 set-up samples");
+  if (o->g_direct_depth < 0) { set_error("g_direct_depth must be >= 0"); return -1; }
+  const int depth = o->g_direct_depth;
+  const long long limit = depth > 0 ? std::max<long long>(s->ne, o->g_direct_max_size) : s->ne;
+  if (limit > 0x7FFFFFFFLL / kAqPoints) { set_error("guiding: g_direct_max_size is too large"); return -1; }
+  if (limit * o->g_direct_spp > 0xFFFFFFFFLL) {
+    set_error("guiding: leaves x g_direct_spp exceeds 2^32 set-up samples");
     return -1;
+  }
+  if (depth > 0) {
+    if (!(o->g_direct_thold >= 0.f)) { set_error("g_direct_thold must be >= 0"); return -1; }
+    if ((limit > s->aq_cap || !s->aq_eval) && !may_alloc) {
+      set_error("refining the guiding tree (g_direct_depth > 0) allocates its arrays on first use; call "
+                "trn_render_grad once with the same options first");
+      return -1;
+    }
+    if (aq_reserve(s, limit)) return -1;
   }
   Params G = P;
   G.table = nullptr;
   G.stats = nullptr;
-  k_aq_poly<<<(s->ne + 255) / 256, 256, 0, st>>>(G, (uint32_t)o->seed * 1000003u, o->g_direct_spp, s->aq_poly);
-  k_aq_mix<<<1, 1024, 0, st>>>(s->ne, s->aq_poly, s->sec_cdf, o->g_eps, s->aq_func, s->aq_int);
-  k_cdf_views<<<1, 1024, 0, st>>>(s->ne, s->aq_func, s->aq_cdf, s->aq_int);
-  count_launch(3);
+  const long long cap = s->aq_cap;
+  const uint32_t stream = (uint32_t)o->seed * 1000003u;
+  k_aq_init<<<(s->ne + 255) / 256, 256, 0, st>>>(s->ne, s->sec_cdf, s->aq_box, s->aq_edge, s->aq_count, cap);
+  int launches = 1;
+  for (int pass = 0; pass < depth; pass++) {
+    const uint32_t ps = stream + (uint32_t)pass;
+    k_aq_eval<<<(unsigned)((limit * kAqPoints + 255) / 256), 256, 0, st>>>(G, ps, s->aq_box, s->aq_edge, s->aq_count,
+                                                                           cap, s->aq_eval);
+    k_aq_flag<<<(unsigned)((limit + 255) / 256), 256, 0, st>>>(s->aq_box, s->aq_count, cap, s->aq_eval,
+                                                               o->g_direct_thold, ps, s->aq_flag);
+    k_aq_scan<<<1, 1024, 0, st>>>(s->aq_count, s->aq_flag, s->aq_prefix, s->aq_count, (int)limit);
+    k_aq_split<<<(unsigned)((limit + 255) / 256), 256, 0, st>>>(s->aq_count, s->aq_flag, s->aq_prefix, s->aq_box,
+                                                                s->aq_edge, cap);
+    k_aq_commit<<<1, 1, 0, st>>>(s->aq_count);
+    launches += 5;
+  }
+  k_aq_poly<<<(unsigned)((limit + 255) / 256), 256, 0, st>>>(G, stream, o->g_direct_spp, s->aq_box, s->aq_edge,
+                                                              s->aq_count, cap, s->aq_poly);
+  k_aq_mix<<<1, 1024, 0, st>>>(s->aq_count, s->aq_poly, s->aq_box, cap, o->g_eps, s->aq_func, s->aq_int);
+  k_cdf_count<<<1, 1024, 0, st>>>(s->aq_count, s->aq_func, s->aq_cdf, s->aq_int);
+  count_launch(launches + 3);
   TRN_CUDA_TRY(cudaGetLastError());
   P.aq_poly = s->aq_poly;
   P.aq_cdf = s->aq_cdf;
   P.aq_int = s->aq_int;
+  P.aq_box = s->aq_box;
+  P.aq_edge = s->aq_edge;
+  P.aq_n = s->aq_count;
+  P.aq_cap = cap;
   return 0;
 }
 
@@ -3674,7 +3931,8 @@ int trn_render_grad_noalloc(trn_scene* s, const trn_camera* cam, const trn_rende
     count_launch(2);
   }
   // the guiding distribution lives in buffers the scene allocated at creation
-  if (integrator == TRN_DIRECT_EDGE && guide_setup(s, o, P, st)) return -1;
+  // (a refined tree in those of an earlier allocating call)
+  if (integrator == TRN_DIRECT_EDGE && guide_setup(s, o, P, st, false)) return -1;
   const bool shallow = o->max_bounces <= 8;
   switch (integrator) {
     case TRN_PATH_TRACER:

@@ -944,6 +944,9 @@ int trn_scene_create(const trn_scene_desc* d, trn_scene** out) {
       dev_alloc_copy(&s->aq_func, (const float*)nullptr, std::max<size_t>(1, (size_t)s->ne)) ||
       dev_alloc_copy(&s->aq_cdf, (const float*)nullptr, std::max<size_t>(1, (size_t)s->ne)) ||
       dev_alloc_copy(&s->aq_int, (const float*)nullptr, 2) ||
+      dev_alloc_copy(&s->aq_box, (const float*)nullptr, 6 * std::max<size_t>(1, (size_t)s->ne)) ||
+      dev_alloc_copy(&s->aq_edge, (const int*)nullptr, std::max<size_t>(1, (size_t)s->ne)) ||
+      dev_alloc_copy(&s->aq_count, (const int*)nullptr, 4) ||
       dev_alloc_copy(&s->nodes, (const BvhNode*)nullptr, std::max(1, nt - 1)) ||
       dev_alloc_copy(&s->tri_verts, (const float4*)nullptr, 3 * (size_t)nt) ||
       dev_alloc_copy(&s->parent, (const int*)nullptr, 2 * (size_t)nt) ||
@@ -966,6 +969,7 @@ int trn_scene_create(const trn_scene_desc* d, trn_scene** out) {
       dev_alloc_copy(&s->err, (const int*)nullptr, 1) ||
       dev_alloc_copy(&s->stats, (const unsigned long long*)nullptr, 16))
     return fail();
+  s->aq_cap = std::max<long long>(1, s->ne);
   if (d->uvs && d->uv_indices && d->num_uvs > 0) {
     s->nuv = d->num_uvs;
     if (dev_alloc_copy(&s->uv, d->uvs, 2 * (size_t)d->num_uvs) ||
@@ -1017,7 +1021,7 @@ int trn_scene_destroy(trn_scene* s) {
                   s->sec_integral_dev, s->nodes, s->tri_verts, s->parent, s->flags, s->keys, s->keys_alt,
                   s->sort_tmp, s->bounds, s->g_pos, s->g_vnormal, s->g_texels, s->g_translation, s->err,
                   s->stats, s->wnodes, s->wtri, s->wqueue, s->wcount, s->aq_poly, s->aq_func, s->aq_cdf,
-                  s->aq_int, s->ploc_node, s->ploc_box, s->ploc_nn, s->ploc_flag, s->ploc_pos, s->ploc_count,
+                  s->aq_int, s->aq_box, s->aq_edge, s->aq_count, s->aq_eval, s->aq_flag, s->aq_prefix, s->ploc_node, s->ploc_box, s->ploc_nn, s->ploc_flag, s->ploc_pos, s->ploc_count,
                   s->scan_tmp, s->cnodes, s->ctri, s->leaf_cnt, s->leaf_scan_tmp};
   for (void* p : ptrs)
     if (p) cudaFree(p);

@@ -61,6 +61,18 @@ struct trn_scene {
   float* aq_func = nullptr;       // [E] weight x leaf volume
   float* aq_cdf = nullptr;        // [E]
   float* aq_int = nullptr;        // [2] integral of aq_func/E, sum of aq_func
+  // leaf boxes of the guiding tree: [6][aq_cap] (x0, y0, z0, x1, y1, z1) in
+  // the (edge, light u, light v) sample cube, each leaf's edge, and the leaf
+  // count (aq_count[0]; [1] is the count after the pass being built)
+  float* aq_box = nullptr;
+  int* aq_edge = nullptr;
+  int* aq_count = nullptr;
+  long long aq_cap = 0;           // leaves the aq_* arrays hold
+  // refinement passes (g_direct_depth > 0): 36 evaluations per leaf, split
+  // flags and their prefix sums; allocated by the first refining call
+  float* aq_eval = nullptr;
+  int* aq_flag = nullptr;
+  int* aq_prefix = nullptr;
   // acceleration structure
   trn::BvhNode* nodes = nullptr;  // [T-1]
   float4* tri_verts = nullptr;    // [T][3]

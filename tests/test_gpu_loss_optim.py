@@ -57,11 +57,11 @@ def test_inverse_rendering_with_pyramid_loss_and_largesteps(built_lib):
     scene.set_vertex_positions(start)
     scene.configure()
     inv = inverse.InverseRenderer(scene, cams, [4] * len(cams), target, api.RenderOptions(0, 3, 4, 4, 4, 0, 0),
-                                  lr=5e-3, loss="pyramid_l2", optimizer="largesteps", lmbda=2.0, shapes=(0,))
+                                  lr=5e-2, loss="pyramid_l2", optimizer="largesteps", lmbda=2.0, shapes=(0,))
     losses = [float(inv.step().sum()) for _ in range(30)]
     assert all(torch.isfinite(torch.tensor(losses)))
     r = inv.x.detach()[:nv].norm(dim=1).mean().item()
-    assert r < 1.08, f"mean radius {r:.4f}, losses {losses[0]:.4g} .. {losses[-1]:.4g}"
+    assert r < 1.07, f"mean radius {r:.4f}, losses {losses[0]:.4g} .. {losses[-1]:.4g}"
     assert sum(losses[-5:]) < sum(losses[:5])
     # only the sphere's vertices are optimised
     torch.testing.assert_close(inv.x.detach()[nv:].cpu(), start[nv:])

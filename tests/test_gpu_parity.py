@@ -132,10 +132,13 @@ def test_grad_parity(cfg1, integrator, depth):
     assert_grad_parity(gg["translation"], go["translation"], label + " translation")
 
 
-@pytest.mark.parametrize("eps", [0.01, 0.5])
-def test_guided_direct_grad_parity(cfg1, eps):
+@pytest.mark.parametrize("eps,depth,max_size,thold", [(0.01, 0, 0, 0.0), (0.5, 0, 0, 0.0),
+                                                      (0.01, 2, 3000, 1e-4), (0.5, 1, 2100, 1e-5)])
+def test_guided_direct_grad_parity(cfg1, eps, depth, max_size, thold):
     """AQ-guided direct boundary term (AdaptiveQuadratureDistribution,
-    AQ_distrb.h:83-195): same leaf weights, same guided samples, same grads."""
+    AQ_distrb.h:83-195): same tree, same leaf weights, same guided samples,
+    same grads. depth > 0 refines the tree (36 evaluations per leaf and pass,
+    splits appended in leaf order); the last case fills the leaf limit."""
     spec, scene, osc, cam = cfg1
     spp, gspp = 4, 4
     dims = api.sample_dims(api.TRN_DIRECT_EDGE, D, guided=True)
@@ -144,11 +147,13 @@ def test_guided_direct_grad_parity(cfg1, eps):
     dLdI = torch.rand(W * H, 3, generator=g) - 0.3
     opts = api.RenderOptions(5, D, spp, spp, spp, spp, spp)
     opts.g_direct, opts.g_direct_spp, opts.g_eps = True, gspp, eps
+    opts.g_direct_depth, opts.g_direct_max_size, opts.g_direct_thold = depth, max_size, thold
     scene.clear_grads()
     api.DirectEdgeIntegrator().renderD(scene, opts, dLdI.reshape(H, W, 3).to(scene.device),
                                        samples=smp.to(scene.device))
     gg = scene.get_grads()
-    go, _ = O.grads(osc, cam, api.TRN_DIRECT_EDGE, spp, D, smp, dLdI, guiding=(5, gspp, eps))
-    label = f"cfg1 {W}x{H} D{D} guided direct eps {eps}"
+    go, _ = O.grads(osc, cam, api.TRN_DIRECT_EDGE, spp, D, smp, dLdI,
+                    guiding=(5, gspp, eps, depth, max_size, thold))
+    label = f"cfg1 {W}x{H} D{D} guided direct eps {eps} depth {depth}"
     assert_grad_parity(gg["positions"], go["positions"], label + " vertices")
     assert_grad_parity(gg["translation"], go["translation"], label + " translation")
