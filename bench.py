@@ -70,8 +70,11 @@ def parse():
     ap.add_argument("--no-path-cache", action="store_true",
                     help="gradient calls re-trace the interior paths instead of reusing the forward's records")
     ap.add_argument("--requests", type=int, default=48, help="serve workload: number of requests")
-    ap.add_argument("--workload", default="single", choices=["single", "views", "serve", "inverse"],
-                    help="single: the 100K-triangle single-view config; views: 32 batched views "
+    ap.add_argument("--guide-depth", type=int, default=0,
+                    help="inverse workload: refinement passes of the direct boundary's guiding tree")
+    ap.add_argument("--workload", default="single", choices=["single", "icosphere", "views", "serve", "inverse"],
+                    help="single: the 100K-triangle single-view config; icosphere: the 1280-triangle "
+                         "config (translation gradient); views: 32 batched views "
                          "of the icosphere scene against the plain per-view form; serve: Poisson "
                          "render+gradient requests over four resident scenes; inverse: the 2M-triangle "
                          "16-view inverse-rendering loop (refit + guided direct boundary + Adam)")
@@ -218,6 +221,8 @@ def main():
         return run_inverse(a)
     if a.workload == "serve":
         return run_serve(a)
+    if a.workload == "icosphere":
+        return run_icosphere(a)
     line, world = run_single(a)
     if line is not None and world == 1 and not a.no_extra:
         # the metric's comparison legs at N=1: the batched multi-view
@@ -227,6 +232,11 @@ def main():
         import gc
         ax = copy.copy(a)
         ax.steps, ax.warmup = min(a.steps, 10), max(3, min(a.warmup, 5))
+        gc.collect()
+        torch.cuda.empty_cache()
+        ic = run_icosphere(ax, quiet=True)
+        line["icosphere_plain"] = {"workload": ic["config"]["workload"], "value": ic["value"], "unit": ic["unit"],
+                                   "ms_per_step": ic["ms_per_step"], "e2e": ic["e2e"]}
         gc.collect()
         torch.cuda.empty_cache()
         v = run_views(ax, quiet=True)
@@ -649,6 +659,80 @@ def run_views(a, quiet: bool = False):
 # AQ-guided direct boundary, start = target + N(0, 0.02^2) per vertex, Adam
 # lr 1e-3; a step = refit + batched forward + loss + batched adjoints + Adam
 # ---------------------------------------------------------------------------
+def run_icosphere(a, quiet: bool = False):
+    """The icosphere configuration: 1280-triangle Lambertian icosphere over the
+    ground quad, 256x256, 16 spp, depth 3, interior + primary + direct terms,
+    gradient of the L2 image loss w.r.t. the sphere's 3-float translation.
+    A step = translation upload + Scene::Configure + renderC + dL/dI + renderD
+    of the three integrators + get_grads. `value` times it on resident
+    inputs; `e2e` copies the translation from pinned host memory and the
+    gradient and loss back every step."""
+    from tensorray_b200 import api, scenes
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    res, spp, D = (64, 4, 3) if a.quick else (256, 16, 3)
+    scene = api.Scene(scenes.config1_scene(res, res))
+    scene.configure()
+    dev = scene.device
+    sphere = scene.shapes[0]
+    its = [api.PathTracer(), api.PrimaryEdgeIntegrator(), api.DirectEdgeIntegrator()]
+    opts = api.RenderOptions(1, D, spp, spp, spp, 0, 0)
+    sphere.translation = torch.tensor([0.05, -0.03, 0.02])
+    scene.configure()
+    target = its[0].renderC(scene, api.RenderOptions(777, D, 4 * spp, 0, 0, 0, 0)).clone()
+    t0 = torch.zeros(3, device=dev)
+    units = res * res * spp * len(its)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+
+    def step(t):
+        scene._translation[0].copy_(t)
+        scene.configure()
+        img = its[0].renderC(scene, opts)
+        dLdI = img - target
+        loss = 0.5 * (dLdI * dLdI).sum()
+        scene.clear_grads()
+        for it in its:
+            it.renderD(scene, opts, dLdI)
+        return loss, scene.get_grads(clear=True)["translation"][0]
+
+    th = torch.zeros(3).pin_memory()
+    gh = torch.empty(3).pin_memory()
+    lh = torch.empty(1).pin_memory()
+
+    def e2e_step():
+        loss, g = step(th.to(dev, non_blocking=True))
+        gh.copy_(g, non_blocking=True)
+        lh.copy_(loss.reshape(1), non_blocking=True)
+
+    def timed(fn):
+        for _ in range(a.warmup):
+            fn()
+        tot = []
+        for _ in range(a.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            tot.append(e0.elapsed_time(e1))
+        return sum(tot) / len(tot)
+
+    ms = timed(lambda: step(t0))
+    ms_e2e = timed(e2e_step)
+    line = {"metric": "grad path-samples/sec", "value": units / (ms / 1e3), "unit": "grad path-samples/s",
+            "n_gpus": 1, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
+            "config": {"workload": f"icosphere 1280 tris + ground, {res}x{res}, {spp} spp x 3 terms "
+                                   f"(interior+primary+direct), depth {D}, grad: sphere translation",
+                       "samples_per_step": units, "l2": "flushed between timed steps (256 MB write)"},
+            "e2e": {"value": units / (ms_e2e / 1e3), "unit": "grad path-samples/s", "ms_per_step": ms_e2e,
+                    "h2d_bytes_per_step": 12, "d2h_bytes_per_step": 16}}
+    if not quiet:
+        print(json.dumps(line), flush=True)
+    return line
+
+
 def run_inverse(a):
     """The inverse-rendering loop. Under torchrun (N > 1) every rank holds a
     replica of the scene and renders its cost-balanced share of the views;
@@ -679,6 +763,7 @@ def run_inverse(a):
     scene.configure()
     opts = api.RenderOptions(0, D, spp, spp, spp, 0, 0)
     opts.g_direct, opts.g_direct_spp, opts.g_eps = True, 16, 0.01
+    opts.g_direct_depth = a.guide_depth
     # the forward render keeps its interior path records for the interior
     # gradient of the same step (about 42 GB at 16 x 1024^2 x 4 spp, depth 8)
     inv = inverse.InverseRenderer(scene, cams, [spp] * nviews, targets, opts, lr=1e-3,
@@ -748,7 +833,7 @@ def run_inverse(a):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded displaced sphere target, seeded vertex perturbation)",
             "config": {"workload": f"inverse rendering, {tris} tris target, {nviews} views {res}^2, {spp} spp x "
-                                   f"3 terms (interior+primary+guided direct), depth {D}, Adam lr 1e-3, "
+                                   f"3 terms (interior+primary+guided direct, guiding tree depth {a.guide_depth}), depth {D}, Adam lr 1e-3, "
                                    "LBVH refit per step; inputs larger than L2",
                        "samples_per_step": units,
                        "parallelism": f"views sharded by cost over {world} rank(s), gradient all-reduce"},
