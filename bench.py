@@ -153,7 +153,10 @@ def workload_name(a) -> str:
 # ---------------------------------------------------------------------------
 # reference arm: the CPU oracle on a bounded sample
 # ---------------------------------------------------------------------------
-def cpu_oracle_rate(a, budget_s: float = 20.0, res: int = 8, spp: int = 1):
+CPU_RES = 32  # pixel window of the bounded CPU sample (1 spp per term)
+
+
+def cpu_oracle_rate(a, budget_s: float = 20.0, res: int = CPU_RES, spp: int = 1):
     from oracle import tr_oracle as O
     from tensorray_b200 import api, scenes
     torch.set_num_threads(os.cpu_count() or 1)
@@ -194,7 +197,7 @@ def run_reference(a):
         tot_units += units
         t_all += dt
     value = tot_units / t_all
-    sample = f"{tot_units // a.steps} grad path-samples per step: 8x8 px, 1 spp per term, 5 terms, same scene"
+    sample = f"{tot_units // a.steps} grad path-samples per step: {CPU_RES}x{CPU_RES} px, 1 spp per term, 5 terms, same scene"
     line = {"metric": "grad path-samples/sec", "value": value, "unit": "grad path-samples/s",
             "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * t_all / a.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -476,7 +479,7 @@ def run_single(a):
     if rank == 0 and world == 1 and not a.no_cpu:
         rate, units, dt, cores = cpu_oracle_rate(a, budget_s=15.0)
         cpu = {"value": rate, "unit": "grad path-samples/s", "cores": cores, "kind": "port",
-               "sample": f"{units} grad path-samples in {dt:.1f}s: 8x8 px, 1 spp per term, 5 terms, same scene"}
+               "sample": f"{units} grad path-samples in {dt:.1f}s: {CPU_RES}x{CPU_RES} px, 1 spp per term, 5 terms, same scene"}
 
     line = None
     if rank == 0:

@@ -44,6 +44,7 @@ import numpy as np
 import torch
 
 SHADOW_EPS = 1e-2   # Config.h:35
+CULL_MIN_TRIANGLES = 4096  # scenes this large cull ray queries by triangle clusters
 EDGE_EPS = 1e-8     # Config.h:34
 EPS = 1e-6          # Config.h:33
 RAY_MAX = 1e32
@@ -484,12 +485,72 @@ class OracleScene:
     # --- ray queries --------------------------------------------------------------
     def intersect(self, org, dir, tmin, tmax, any_hit=False):
         p = self.pos.detach()
-        return intersect_brute(p[self.idx[:, 0]], p[self.idx[:, 1]], p[self.idx[:, 2]], org.detach(),
-                               dir.detach(), tmin, tmax)
+        P0, P1, P2 = p[self.idx[:, 0]], p[self.idx[:, 1]], p[self.idx[:, 2]]
+        if P0.shape[0] < CULL_MIN_TRIANGLES:
+            return intersect_brute(P0, P1, P2, org.detach(), dir.detach(), tmin, tmax)
+        key = p.data_ptr(), p._version
+        if getattr(self, "_clusters_key", None) != key:
+            self._clusters = TriangleClusters(P0, P1, P2)
+            self._clusters_key = key
+        return intersect_culled(self._clusters, P0, P1, P2, org.detach(), dir.detach(), tmin, tmax)
 
     def occluded(self, org, dir, tmin, tmax):
         tri, _, _, _ = self.intersect(org, dir, tmin, tmax)
         return tri >= 0
+
+
+def _ray_frame(dir):
+    """Per-ray permutation and shear of the watertight test (Woop et al. 2013,
+    section 3): kz = the largest |d| axis, kx/ky the others (swapped when
+    d[kz] < 0), and the shear constants."""
+    n = dir.shape[0]
+    ad = dir.abs()
+    kz = torch.zeros(n, dtype=torch.long)
+    kz = torch.where(ad[:, 1] > ad[:, 0], torch.ones_like(kz), kz)
+    m = torch.gather(ad, 1, kz[:, None])[:, 0]
+    kz = torch.where(ad[:, 2] > m, torch.full_like(kz, 2), kz)
+    kx = (kz + 1) % 3
+    ky = (kx + 1) % 3
+    dkz = torch.gather(dir, 1, kz[:, None])[:, 0]
+    swap = dkz < 0
+    kx, ky = torch.where(swap, ky, kx), torch.where(swap, kx, ky)
+    g = lambda a, k: torch.gather(a, 1, k[:, None])[:, 0]
+    sx = g(dir, kx) / dkz
+    sy = g(dir, ky) / dkz
+    sz = torch.ones_like(dkz) / dkz
+    return kx, ky, kz, sx, sy, sz
+
+
+def _watertight(A, B, Cc, KX, KY, KZ, SX, SY, SZ, tmin, tmax):
+    """The watertight test on triangles given relative to the ray origins
+    (A, B, Cc: [..., 3]), with the ray frame broadcast to the same leading
+    shape; returns (hit, t, u, v)."""
+    gk = lambda X, K: torch.gather(X, -1, K[..., None])[..., 0]
+    Akz, Bkz, Ckz = gk(A, KZ), gk(B, KZ), gk(Cc, KZ)
+    Ax = gk(A, KX) - SX * Akz
+    Ay = gk(A, KY) - SY * Akz
+    Bx = gk(B, KX) - SX * Bkz
+    By = gk(B, KY) - SY * Bkz
+    Cx = gk(Cc, KX) - SX * Ckz
+    Cy = gk(Cc, KY) - SY * Ckz
+    U = Cx * By - Cy * Bx
+    V = Ax * Cy - Ay * Cx
+    W = Bx * Ay - By * Ax
+    z = (U == 0) | (V == 0) | (W == 0)
+    if bool(z.any()):
+        d = lambda a: a.double()
+        U = torch.where(z, (d(Cx) * d(By) - d(Cy) * d(Bx)).float(), U)
+        V = torch.where(z, (d(Ax) * d(Cy) - d(Ay) * d(Cx)).float(), V)
+        W = torch.where(z, (d(Bx) * d(Ay) - d(By) * d(Ax)).float(), W)
+    neg = (U < 0) | (V < 0) | (W < 0)
+    pos = (U > 0) | (V > 0) | (W > 0)
+    det = (U + V) + W
+    Az, Bz, Cz = SZ * Akz, SZ * Bkz, SZ * Ckz
+    Tt = (U * Az + V * Bz) + W * Cz
+    rcp = torch.ones_like(det) / det
+    t = Tt * rcp
+    ok = ~(neg & pos) & (det != 0) & (t > tmin) & (t < tmax)
+    return ok, t, V * rcp, W * rcp
 
 
 def intersect_brute(P0, P1, P2, org, dir, tmin, tmax, chunk=None):
@@ -505,65 +566,121 @@ def intersect_brute(P0, P1, P2, org, dir, tmin, tmax, chunk=None):
         return out_tri, out_u, out_v, out_t
     tmin = torch.as_tensor(tmin, dtype=F32).expand(n).contiguous()
     tmax = torch.as_tensor(tmax, dtype=F32).expand(n).contiguous()
-    ad = dir.abs()
-    kz = torch.zeros(n, dtype=torch.long)
-    kz = torch.where(ad[:, 1] > ad[:, 0], torch.ones_like(kz), kz)
-    m = torch.gather(ad, 1, kz[:, None])[:, 0]
-    kz = torch.where(ad[:, 2] > m, torch.full_like(kz, 2), kz)
-    kx = (kz + 1) % 3
-    ky = (kx + 1) % 3
-    dkz = torch.gather(dir, 1, kz[:, None])[:, 0]
-    swap = dkz < 0
-    kx, ky = torch.where(swap, ky, kx), torch.where(swap, kx, ky)
-    g = lambda a, k: torch.gather(a, 1, k[:, None])[:, 0]
-    sx = g(dir, kx) / dkz
-    sy = g(dir, ky) / dkz
-    sz = torch.ones_like(dkz) / dkz
+    kx, ky, kz, sx, sy, sz = _ray_frame(dir)
     tri_ids = torch.arange(T)
     for s in range(0, n, chunk):
         e = min(n, s + chunk)
         o = org[s:e, None, :]
         A, B, Cc = P0[None] - o, P1[None] - o, P2[None] - o
-        KX, KY, KZ = kx[s:e, None, None].expand(-1, T, 1), ky[s:e, None, None].expand(-1, T, 1), \
-            kz[s:e, None, None].expand(-1, T, 1)
-        gk = lambda X, K: torch.gather(X, 2, K)[..., 0]
-        Akz, Bkz, Ckz = gk(A, KZ), gk(B, KZ), gk(Cc, KZ)
-        SX, SY, SZ = sx[s:e, None], sy[s:e, None], sz[s:e, None]
-        Ax = gk(A, KX) - SX * Akz
-        Ay = gk(A, KY) - SY * Akz
-        Bx = gk(B, KX) - SX * Bkz
-        By = gk(B, KY) - SY * Bkz
-        Cx = gk(Cc, KX) - SX * Ckz
-        Cy = gk(Cc, KY) - SY * Ckz
-        U = Cx * By - Cy * Bx
-        V = Ax * Cy - Ay * Cx
-        W = Bx * Ay - By * Ax
-        z = (U == 0) | (V == 0) | (W == 0)
-        if bool(z.any()):
-            d = lambda a: a.double()
-            U = torch.where(z, (d(Cx) * d(By) - d(Cy) * d(Bx)).float(), U)
-            V = torch.where(z, (d(Ax) * d(Cy) - d(Ay) * d(Cx)).float(), V)
-            W = torch.where(z, (d(Bx) * d(Ay) - d(By) * d(Ax)).float(), W)
-        neg = (U < 0) | (V < 0) | (W < 0)
-        pos = (U > 0) | (V > 0) | (W > 0)
-        det = (U + V) + W
-        Az, Bz, Cz = SZ * Akz, SZ * Bkz, SZ * Ckz
-        Tt = (U * Az + V * Bz) + W * Cz
-        rcp = torch.ones_like(det) / det
-        t = Tt * rcp
-        ok = ~(neg & pos) & (det != 0) & (t > tmin[s:e, None]) & (t < tmax[s:e, None])
+        ex = lambda k: k[s:e, None].expand(-1, T)
+        ok, t, uu_all, vv_all = _watertight(A, B, Cc, ex(kx), ex(ky), ex(kz), sx[s:e, None], sy[s:e, None],
+                                            sz[s:e, None], tmin[s:e, None], tmax[s:e, None])
         tt = torch.where(ok, t, torch.full_like(t, float("inf")))
         best_t = tt.min(1).values
         cand = ok & (tt == best_t[:, None])
         idx = torch.where(cand, tri_ids[None].expand_as(cand), torch.full_like(cand, T, dtype=torch.long)).min(1).values
         hit = idx < T
         idc = idx.clamp(max=T - 1)
-        uu = torch.gather(V * rcp, 1, idc[:, None])[:, 0]
-        vv = torch.gather(W * rcp, 1, idc[:, None])[:, 0]
+        uu = torch.gather(uu_all, 1, idc[:, None])[:, 0]
+        vv = torch.gather(vv_all, 1, idc[:, None])[:, 0]
         out_tri[s:e] = torch.where(hit, idx, torch.full_like(idx, -1))
         out_u[s:e] = torch.where(hit, uu, torch.zeros_like(uu))
         out_v[s:e] = torch.where(hit, vv, torch.zeros_like(vv))
         out_t[s:e] = torch.where(hit, best_t, torch.full_like(best_t, -1.0))
+    return out_tri, out_u, out_v, out_t
+
+
+def _morton3(q):
+    """Interleave the low 10 bits of three integer coordinates [n, 3]."""
+    key = torch.zeros(q.shape[0], dtype=torch.long)
+    for b in range(10):
+        for a in range(3):
+            key |= ((q[:, a] >> b) & 1) << (3 * b + a)
+    return key
+
+
+class TriangleClusters:
+    """Culling structure of the oracle's ray queries: the triangles in
+    Morton order of their centroids, cut into clusters of `size`, each with
+    a padded float64 box. A ray's candidate triangles are those of the
+    clusters whose box it crosses within [tmin, tmax]. The padding (1e-4 of
+    the scene extent) and the float64 slab test keep the culling
+    conservative, so the exact test over the candidates returns what the
+    brute-force test over every triangle returns."""
+
+    def __init__(self, P0, P1, P2, size=64):
+        T = P0.shape[0]
+        cent = (P0.double() + P1.double() + P2.double()) / 3.0
+        lo, hi = cent.min(0).values, cent.max(0).values
+        q = ((cent - lo) / (hi - lo).clamp_min(1e-30) * 1023.0).long().clamp(0, 1023)
+        order = torch.argsort(_morton3(q), stable=True)
+        nc = (T + size - 1) // size
+        members = torch.full((nc * size,), -1, dtype=torch.long)
+        members[:T] = order
+        self.members = members.view(nc, size)
+        V = torch.stack([P0, P1, P2], 1).double()[order]            # [T, 3, 3]
+        pad_rows = nc * size - T
+        if pad_rows:
+            V = torch.cat([V, V[-1:].expand(pad_rows, 3, 3)], 0)
+        V = V.view(nc, size * 3, 3)
+        ext = float((V.amax((0, 1)) - V.amin((0, 1))).max())
+        eps = 1e-4 * max(ext, 1e-30) + 1e-12
+        self.lo = V.amin(1) - eps
+        self.hi = V.amax(1) + eps
+
+    def candidates(self, org, dir, tmin, tmax, chunk=2048):
+        """(ray index, triangle index) pairs whose cluster box the ray crosses."""
+        rays, tris = [], []
+        for s in range(0, org.shape[0], chunk):
+            o = org[s:s + chunk].double()[:, None, :]
+            d = dir[s:s + chunk].double()[:, None, :]
+            with np.errstate(all="ignore"):
+                inv = 1.0 / d
+                t0 = (self.lo[None] - o) * inv
+                t1 = (self.hi[None] - o) * inv
+            tn = torch.minimum(t0, t1).nan_to_num(nan=-float("inf"))
+            tf = torch.maximum(t0, t1).nan_to_num(nan=float("inf"))
+            near = torch.maximum(tn.amax(-1), tmin[s:s + chunk].double()[:, None])
+            far = torch.minimum(tf.amin(-1), tmax[s:s + chunk].double()[:, None])
+            r, c = torch.nonzero(near <= far * (1 + 1e-9) + 1e-9, as_tuple=True)
+            m = self.members[c]                                      # [pairs, size]
+            rr = (r + s)[:, None].expand_as(m)
+            keep = m >= 0
+            rays.append(rr[keep])
+            tris.append(m[keep])
+        return torch.cat(rays), torch.cat(tris)
+
+
+def intersect_culled(clusters, P0, P1, P2, org, dir, tmin, tmax):
+    """intersect_brute's result (same arithmetic, same (t, id) order) over the
+    candidate triangles of TriangleClusters."""
+    n = org.shape[0]
+    out_tri = torch.full((n,), -1, dtype=torch.long)
+    out_u, out_v, out_t = torch.zeros(n), torch.zeros(n), torch.full((n,), -1.0)
+    if n == 0:
+        return out_tri, out_u, out_v, out_t
+    tmin = torch.as_tensor(tmin, dtype=F32).expand(n).contiguous()
+    tmax = torch.as_tensor(tmax, dtype=F32).expand(n).contiguous()
+    r, tri = clusters.candidates(org, dir, tmin, tmax)
+    if r.numel() == 0:
+        return out_tri, out_u, out_v, out_t
+    kx, ky, kz, sx, sy, sz = _ray_frame(dir)
+    o = org[r]
+    ok, t, uu, vv = _watertight(P0[tri] - o, P1[tri] - o, P2[tri] - o, kx[r], ky[r], kz[r], sx[r], sy[r], sz[r],
+                                tmin[r], tmax[r])
+    tt = torch.where(ok, t, torch.full_like(t, float("inf")))
+    best_t = torch.full((n,), float("inf")).scatter_reduce(0, r, tt, "amin")
+    cand = ok & (tt == best_t[r])
+    big = torch.iinfo(torch.long).max
+    best_id = torch.full((n,), big, dtype=torch.long).scatter_reduce(
+        0, r, torch.where(cand, tri, torch.full_like(tri, big)), "amin")
+    hit = best_id < big
+    pick = cand & (tri == best_id[r])
+    pr = r[pick]
+    out_tri[hit] = best_id[hit]
+    out_t[hit] = best_t[hit]
+    out_u[pr] = uu[pick]
+    out_v[pr] = vv[pick]
     return out_tri, out_u, out_v, out_t
 
 

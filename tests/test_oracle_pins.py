@@ -161,3 +161,26 @@ def test_camera_center_ray_points_at_target():
     assert float(d0[0, 0]) < 0 and float(d0[0, 1]) > 0
     half = math.atan2(float(d0[0, 1]), -float(d0[0, 2]))
     assert abs(half - math.radians(22.5)) < 1e-5
+
+
+def test_culled_ray_queries_equal_brute_force():
+    """The oracle's cluster culling (TriangleClusters) is conservative: the
+    same hits, barycentrics and distances as the test over every triangle,
+    for random rays and for rays leaving surface points (the set-up rays of
+    the boundary terms)."""
+    from tensorray_b200 import scenes
+    osc = O.OracleScene(scenes.config2_scene(8, 8, tris=20000), requires_grad=())
+    g = torch.Generator().manual_seed(1)
+    org = (torch.rand(600, 3, generator=g) - 0.5) * 4
+    p = osc.pos.detach()
+    tri = torch.randint(0, osc.idx.shape[0], (600,), generator=g)
+    surf = (p[osc.idx[tri, 0]] + p[osc.idx[tri, 1]] + p[osc.idx[tri, 2]]) / 3
+    org = torch.cat([org, surf])
+    d = torch.nn.functional.normalize(torch.randn(1200, 3, generator=g), dim=1)
+    assert osc.idx.shape[0] >= O.CULL_MIN_TRIANGLES
+    P = [p[osc.idx[:, k]] for k in range(3)]
+    culled = osc.intersect(org, d, O.SHADOW_EPS, O.RAY_MAX)
+    brute = O.intersect_brute(*P, org, d, O.SHADOW_EPS, O.RAY_MAX)
+    assert int((brute[0] >= 0).sum()) > 300
+    for a, b in zip(culled, brute):
+        assert torch.equal(a, b)
