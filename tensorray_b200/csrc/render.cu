@@ -81,16 +81,16 @@ constexpr int kMaxDepth = 16;
 #define TRN_MINB 3
 #endif
 #ifndef TRN_MINB_PATHADJ
-#define TRN_MINB_PATHADJ 2
+#define TRN_MINB_PATHADJ 3
 #endif
 #ifndef TRN_MINB_REVERSE
-#define TRN_MINB_REVERSE TRN_MINB_PATHADJ
+#define TRN_MINB_REVERSE 2
 #endif
 #ifndef TRN_MINB_FWDREC
-#define TRN_MINB_FWDREC TRN_MINB_PATHADJ
+#define TRN_MINB_FWDREC 4
 #endif
 #ifndef TRN_MINB_INDIRECT
-#define TRN_MINB_INDIRECT 3
+#define TRN_MINB_INDIRECT 4
 #endif
 // the split forms' set-up kernels are latency-bound with little state: four
 // blocks per SM (64 registers) hide more of it (measured)
@@ -98,7 +98,7 @@ constexpr int kMaxDepth = 16;
 #define TRN_MINB_SETUP 4
 #endif
 #ifndef TRN_MINB_BODY
-#define TRN_MINB_BODY 2
+#define TRN_MINB_BODY 4
 #endif
 // the indirect kernel's two set-up rays use the shared traversal
 #ifndef TRN_INDIRECT_SETUP_SHARED
