@@ -29,9 +29,14 @@ from dataclasses import dataclass, field
 import torch
 
 from . import api
-from ._abi import TRN_DIRECT_EDGE, TRN_PATH_TRACER, TRN_PRIMARY_EDGE, TrnView
+from ._abi import (TRN_DIRECT_EDGE, TRN_INDIRECT_EDGE, TRN_PATH_TRACER, TRN_PIXEL_EDGE, TRN_PRIMARY_EDGE,
+                   TrnView)
 
 PHASE_FWD, PHASE_GRAD, PHASE_FINISH, PHASE_DONE = 0, 1, 2, 3
+
+# the gradient terms a request may ask for (RenderRequest.terms): the
+# interior path tracer and the four boundary terms
+ALL_TERMS = (TRN_PATH_TRACER, TRN_PRIMARY_EDGE, TRN_DIRECT_EDGE, TRN_INDIRECT_EDGE, TRN_PIXEL_EDGE)
 
 # Device bytes a gradient view set holds for the queues of the split
 # integrator kernels (one round: 16M boundary samples, at most about 312 bytes

@@ -25,13 +25,20 @@ def _req(world, scene, pos, res, spp, depth, seed):
     return serve.RenderRequest(scene, cam, spp, depth, tgt, seed=seed)
 
 
-def _probe(world):
-    return _req(world, "ico", (0.3, 0.5, 4.0), 32, 12, 3, seed=7)
+def _probe(world, terms=None):
+    r = _req(world, "ico", (0.3, 0.5, 4.0), 32, 12, 3, seed=7)
+    if terms is not None:
+        r.terms = tuple(terms)
+    return r
 
 
-def test_alone_equals_in_the_mix(world):
+TERM_SETS = [None, serve.ALL_TERMS]
+
+
+@pytest.mark.parametrize("terms", TERM_SETS, ids=["three_terms", "all_terms"])
+def test_alone_equals_in_the_mix(world, terms):
     alone = serve.Server(world, chunk_spp=4)
-    r0 = alone.submit(_probe(world))
+    r0 = alone.submit(_probe(world, terms))
     while not alone.idle():
         alone.step()
     mix = serve.Server(world, chunk_spp=4)
@@ -41,7 +48,7 @@ def test_alone_equals_in_the_mix(world):
     for o in others[:3]:
         mix.submit(o)
     mix.step()  # the probe arrives while others are already on the GPU
-    r1 = mix.submit(_probe(world))
+    r1 = mix.submit(_probe(world, terms))
     for o in others[3:]:
         mix.submit(o)
     while not mix.idle():
@@ -54,9 +61,10 @@ def test_alone_equals_in_the_mix(world):
     assert abs(float(r1.loss) - float(r0.loss)) <= 1e-5 * abs(float(r0.loss)) + 1e-7
 
 
-def test_server_equals_direct_views(world):
+@pytest.mark.parametrize("terms", TERM_SETS, ids=["three_terms", "all_terms"])
+def test_server_equals_direct_views(world, terms):
     srv = serve.Server(world, chunk_spp=64)   # one chunk per phase
-    r = srv.submit(_probe(world))
+    r = srv.submit(_probe(world, terms))
     while not srv.idle():
         srv.step()
     sc = world["ico"]
