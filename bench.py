@@ -650,7 +650,7 @@ def run_views(a, quiet: bool = False):
             "split_ms": {"batched": split_b, "batched_default_shape": split_bd, "plain": split_p},
             "launch": {"shape": best, "ms_by_shape": shape_ms,
                        "fwd": [ln_f.block, ln_f.blocks_per_sm, ln_f.chunk] if ln_f else "default",
-                       **{str(t): ([ln_g[t].block, ln_g[t].blocks_per_sm, ln_g[t].chunk] if ln_g[t] else "default")
+                       **{str(t): ([ln_g[t].block, ln_g[t].blocks_per_sm, ln_g[t].chunk, ln_g[t].round_log2] if ln_g[t] else "default")
                           for t in terms}}}
     if not quiet:
         print(json.dumps(line), flush=True)

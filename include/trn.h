@@ -127,13 +127,16 @@ typedef struct {
 } trn_samples;
 
 /* Launch shape of the persistent integrator kernels (0 = library default):
- * threads per block, resident blocks per SM, and sample slots each lane takes
- * per fetch from the work queue. Chosen by the autotuner
+ * threads per block, resident blocks per SM, sample slots each lane takes
+ * per fetch from the work queue, and the sample slots (boundary terms) or
+ * paths (interior adjoint) per round of the split kernels, log2, at most the
+ * default (boundary 24, interior 21), at least 16. Chosen by the autotuner
  * (tensorray_b200/autotune.py). */
 typedef struct {
   int block;
   int blocks_per_sm;
   int chunk;
+  int round_log2;
 } trn_launch;
 
 /* One camera view of a batched render (the reference renders one view per

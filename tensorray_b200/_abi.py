@@ -65,7 +65,7 @@ class TrnSamples(C.Structure):
 
 
 class TrnLaunch(C.Structure):
-    _fields_ = [("block", C.c_int), ("blocks_per_sm", C.c_int), ("chunk", C.c_int)]
+    _fields_ = [("block", C.c_int), ("blocks_per_sm", C.c_int), ("chunk", C.c_int), ("round_log2", C.c_int)]
 
 
 class TrnView(C.Structure):

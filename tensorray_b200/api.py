@@ -530,5 +530,5 @@ class ViewSet:
         return images[o:o + c.width * c.height].reshape(c.height, c.width, 3)
 
 
-def launch_config(block: int = 0, blocks_per_sm: int = 0, chunk: int = 0) -> TrnLaunch:
-    return TrnLaunch(int(block), int(blocks_per_sm), int(chunk))
+def launch_config(block: int = 0, blocks_per_sm: int = 0, chunk: int = 0, round_log2: int = 0) -> TrnLaunch:
+    return TrnLaunch(int(block), int(blocks_per_sm), int(chunk), int(round_log2))

@@ -3,6 +3,10 @@
 For one (view set, integrator) pair it times every candidate launch shape --
 threads per block, resident blocks per SM, and the number of sample slots a
 lane takes per work-queue fetch -- with CUDA events and keeps the fastest.
+For the gradient calls it then times the round size of the split kernels
+(sample slots per set-up/body round of the boundary terms, paths per round
+of the interior adjoint: smaller rounds need smaller queues, larger ones give
+each edge more samples per sort and fewer kernel tails) with that shape.
 Results are cached per (integrator, slot-count bucket, scene size bucket).
 Gradient passes write into the scene's gradient buffers, so the caller clears
 them after tuning (tune() does it).
@@ -18,6 +22,7 @@ from . import api
 BLOCKS = (128, 256)
 PER_SM = (2, 4, 8)
 CHUNKS = (1, 4)
+ROUND_LOG2 = (20, 22)   # tried against the library default (16M boundary slots, 2M paths)
 
 _cache: dict = {}
 
@@ -45,6 +50,24 @@ def tune(vs: api.ViewSet, integrator: int, options: api.RenderOptions, dLdI: tor
     for b, p, c in cands:
         ln = api.launch_config(b, p, c)
         run(ln)  # warm
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            run(ln)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        if ms < best_ms:
+            best, best_ms = ln, ms
+    # round size of the split kernels, with the best shape (only sizes below
+    # the call's slot count change anything)
+    slots = vs.slots(integrator)
+    for r in ROUND_LOG2:
+        if (1 << r) >= slots:
+            continue
+        ln = api.launch_config(best.block, best.blocks_per_sm, best.chunk, r)
+        run(ln)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()

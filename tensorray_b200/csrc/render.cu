@@ -3122,6 +3122,10 @@ int validate_launch(const trn_launch* ln) {
     set_error("launch blocks_per_sm must be in [0, 64] and chunk in [0, 64]");
     return -1;
   }
+  if (ln->round_log2 != 0 && (ln->round_log2 < 16 || ln->round_log2 > 40)) {
+    set_error("launch round_log2 must be 0 (default) or in [16, 40]");
+    return -1;
+  }
   return 0;
 }
 
@@ -3145,6 +3149,13 @@ void launch(K kernel, const trn_launch* ln, long long total, const Params& P, cu
 #endif
 constexpr long long kIndirectRound = 1LL << TRN_ROUND_LOG2;
 constexpr long long kPathRound = 1LL << 21;  // paths per split round of the interior adjoint
+
+// Slots (or paths) per round: the launch's round_log2 when set, never above
+// the default that the queues are sized for.
+long long round_cap(const trn_launch* ln, long long dflt) {
+  if (ln && ln->round_log2 > 0) return std::min(dflt, 1LL << ln->round_log2);
+  return dflt;
+}
 
 // Largest queue that any split term needs for one full round (depth <= 8
 // when shallow, else up to kMaxDepth).
@@ -3196,7 +3207,7 @@ int ensure_queue(trn_viewset* vs, size_t need, cudaStream_t st) {
 // The split interior adjoint in rounds of at most kPathRound paths (a queue
 // of about 1.3 GB at depth <= 8).
 int path_adj_split(trn_viewset* vs, Params P, const trn_launch* ln, long long total, bool shallow, cudaStream_t st) {
-  const long long cap = std::min(total, kPathRound);
+  const long long cap = std::min(total, round_cap(ln, kPathRound));
   if (ensure_queue(vs, shallow ? path_soa_bytes<8>(cap) : path_soa_bytes<kMaxDepth>(cap), st)) return -1;
   P.queue = vs->iq;
   P.q_count = vs->iq_count;
@@ -3225,7 +3236,7 @@ int path_adj_split(trn_viewset* vs, Params P, const trn_launch* ln, long long to
 
 // The split pixel boundary term in rounds of at most kIndirectRound samples.
 int pixel_split(trn_viewset* vs, Params P, const trn_launch* ln, long long total, cudaStream_t st) {
-  const long long cap = std::min(total, kIndirectRound);
+  const long long cap = std::min(total, round_cap(ln, kIndirectRound));
   if (ensure_queue(vs, sizeof(PrimaryItem) * (size_t)cap, st)) return -1;
   P.queue = vs->iq;
   P.q_count = vs->iq_count;
@@ -3310,7 +3321,7 @@ int order_round(trn_viewset* vs, Params& P, int term, cudaStream_t st) {
 
 // The split direct term in rounds of at most kIndirectRound slots.
 int direct_split(trn_viewset* vs, Params P, const trn_launch* ln, long long total, cudaStream_t st) {
-  const long long cap = std::min(total, kIndirectRound);
+  const long long cap = std::min(total, round_cap(ln, kIndirectRound));
   if (ensure_queue(vs, sizeof(DirectItem) * (size_t)cap, st)) return -1;
   P.queue = vs->iq;
   P.q_count = vs->iq_count;
@@ -3334,7 +3345,7 @@ int direct_split(trn_viewset* vs, Params P, const trn_launch* ln, long long tota
 
 // The split primary term in rounds of at most kIndirectRound slots.
 int primary_split(trn_viewset* vs, Params P, const trn_launch* ln, long long total, cudaStream_t st) {
-  const long long cap = std::min(total, kIndirectRound);
+  const long long cap = std::min(total, round_cap(ln, kIndirectRound));
   if (ensure_queue(vs, sizeof(PrimaryItem) * (size_t)cap, st)) return -1;
   P.queue = vs->iq;
   P.q_count = vs->iq_count;
@@ -3365,7 +3376,7 @@ int primary_split(trn_viewset* vs, Params P, const trn_launch* ln, long long tot
 // stages (set-up + sensor side, emitter side) or three (set-up, sensor side,
 // emitter side; the default).
 int indirect_split(trn_viewset* vs, Params P, const trn_launch* ln, long long total, bool shallow, cudaStream_t st) {
-  const long long cap = std::min(total, kIndirectRound);
+  const long long cap = std::min(total, round_cap(ln, kIndirectRound));
   const size_t item = shallow ? sizeof(IndirectItem<8>) : sizeof(IndirectItem<kMaxDepth>);
   const size_t item_a = TRN_INDIRECT_STAGES == 3 ? sizeof(IndirectSetupItem) : 0;
   const size_t bytes_a = (item_a * (size_t)cap + 255) / 256 * 256;

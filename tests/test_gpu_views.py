@@ -87,6 +87,27 @@ def test_launch_configs_give_same_image(setup):
 
 
 @pytest.mark.parametrize("integ", [0, 1, 2, 3, 4])
+def test_round_size_does_not_change_gradients(setup, integ):
+    """Split kernels in rounds of 2^16 slots (paths) give the gradients of the
+    default rounds: a slot's samples do not depend on its round."""
+    scene = setup[0]
+    cams = [api.Camera(c.pos, c.target, c.up, c.width, c.height, c.fov)
+            for c in scenes.fibonacci_cameras(2, 4.0, [256], seed=4)]
+    vs = api.ViewSet(scene, cams, [4, 4])
+    g = torch.Generator().manual_seed(5)
+    dLdI = (torch.rand(vs.npix, 3, generator=g) - 0.3).to(scene.device)
+    opts = api.RenderOptions(2, D, 0, 0, 0, 0, 0)
+    out = []
+    for ln in (None, api.launch_config(0, 0, 0, 16)):
+        scene.clear_grads()
+        vs.render_grad(integ, opts, dLdI, launch=ln)
+        out.append(scene.get_grads()["positions"].clone())
+    assert vs.slots(integ) > (1 << 16)
+    assert float(out[0].abs().sum()) > 0
+    assert rel_l2(out[1].cpu(), out[0].cpu()) < 1e-5
+
+
+@pytest.mark.parametrize("integ", [0, 1, 2, 3, 4])
 def test_per_view_gradient_buffers(setup, integ):
     """Views with their own gradient buffers in one launch: each buffer holds
     exactly its view's gradient (the warp-aggregated scatter must not merge
