@@ -100,6 +100,11 @@ constexpr int kMaxDepth = 16;
 #ifndef TRN_MINB_BODY
 #define TRN_MINB_BODY 4
 #endif
+// the indirect set-up traces the sensor-side ray first (1) or the
+// emitter-side ray first (0); a miss of the first skips the second
+#ifndef TRN_INDIRECT_SENSOR_FIRST
+#define TRN_INDIRECT_SENSOR_FIRST 0
+#endif
 // the indirect kernel's two set-up rays use the shared traversal
 #ifndef TRN_INDIRECT_SETUP_SHARED
 #define TRN_INDIRECT_SETUP_SHARED 1
@@ -2143,8 +2148,13 @@ TRN_D bool indirect_setup(const Params& P, long long gslot, EdgeState& st, int& 
   const float pdf = pdf_e * pdf_d;
   Hit he, hs;
   cnt.v[kCntClosest] += 2;
+#if TRN_INDIRECT_SENSOR_FIRST
+  if (!trace_k<TRN_INDIRECT_SETUP_SHARED, false>(s, p0, dir, kShadowEps, kRayMax, hs, P.err)) return false;
+  if (!trace_k<TRN_INDIRECT_SETUP_SHARED, false>(s, p0, -dir, kShadowEps, kRayMax, he, P.err)) return false;
+#else
   if (!trace_k<TRN_INDIRECT_SETUP_SHARED, false>(s, p0, -dir, kShadowEps, kRayMax, he, P.err)) return false;
   if (!trace_k<TRN_INDIRECT_SETUP_SHARED, false>(s, p0, dir, kShadowEps, kRayMax, hs, P.err)) return false;
+#endif
   const SurfF xe = post_intersect(s, he.tri, he.u, he.v);
   const SurfF xs = post_intersect(s, hs.tri, hs.u, hs.v);
   const float dl = length(xe.p - xs.p);
