@@ -716,16 +716,20 @@ TRN_HD void tangent_vjp(const F3& n, const F3& g_t, F3& g_n) {
 // Reverse mode of F above for the output adjoint `adj`; accumulates into the
 // gradient outputs (g_prev only if need_prev, g_kd only if need_kd).
 #ifndef TRN_SHARED_FACTOR_VJP
-#define TRN_SHARED_FACTOR_VJP 0
+#define TRN_SHARED_FACTOR_VJP 2
 #endif
-#if TRN_SHARED_FACTOR_VJP
+// 0: inlined at each call; 1: one shared copy with reference parameters (its
+// callers keep every argument in local memory); 2: one shared copy that takes
+// its inputs by value and returns its gradient increments
+#if TRN_SHARED_FACTOR_VJP == 1
 #define TRN_FACTOR_FN __host__ __device__ __noinline__
 #else
 #define TRN_FACTOR_FN TRN_HD
 #endif
-TRN_FACTOR_FN F3 factor_vjp(const BsdfDesc& b, bool need_prev, bool need_kd, const F3& xprev, const F3& x, const F3& ns,
-                      const F3& kd, const F3& z, const F3& nz, float J, const F3& K, const F3& adj, F3& g_prev,
-                      F3& g_x, F3& g_ns, F3& g_kd, F3& g_z, F3& g_nz, float& g_J) {
+TRN_FACTOR_FN F3 factor_vjp_acc(const BsdfDesc& b, bool need_prev, bool need_kd, const F3& xprev, const F3& x,
+                                const F3& ns, const F3& kd, const F3& z, const F3& nz, float J, const F3& K,
+                                const F3& adj, F3& g_prev, F3& g_x, F3& g_ns, F3& g_kd, F3& g_z, F3& g_nz,
+                                float& g_J) {
   const F3 v0 = x - xprev;
   const float L0 = length(v0);
   const F3 n0 = v0 / L0;
@@ -778,6 +782,36 @@ TRN_FACTOR_FN F3 factor_vjp(const BsdfDesc& b, bool need_prev, bool need_kd, con
   g_x = g_x + g_v0;
   if (need_prev) g_prev = g_prev - g_v0;
   return F;
+}
+
+#if TRN_SHARED_FACTOR_VJP == 2
+struct FactorGrad {
+  F3 F, g_prev, g_x, g_ns, g_kd, g_z, g_nz;
+  float g_J;
+};
+__host__ __device__ __noinline__ FactorGrad factor_vjp_byval(BsdfDesc b, bool need_prev, bool need_kd, F3 xprev, F3 x,
+                                                            F3 ns, F3 kd, F3 z, F3 nz, float J, F3 K, F3 adj) {
+  FactorGrad r;
+  r.g_prev = r.g_x = r.g_ns = r.g_kd = r.g_z = r.g_nz = F3z();
+  r.g_J = 0.f;
+  r.F = factor_vjp_acc(b, need_prev, need_kd, xprev, x, ns, kd, z, nz, J, K, adj, r.g_prev, r.g_x, r.g_ns, r.g_kd,
+                       r.g_z, r.g_nz, r.g_J);
+  return r;
+}
+#endif
+
+TRN_HD F3 factor_vjp(const BsdfDesc& b, bool need_prev, bool need_kd, const F3& xprev, const F3& x, const F3& ns,
+                     const F3& kd, const F3& z, const F3& nz, float J, const F3& K, const F3& adj, F3& g_prev,
+                     F3& g_x, F3& g_ns, F3& g_kd, F3& g_z, F3& g_nz, float& g_J) {
+#if TRN_SHARED_FACTOR_VJP == 2
+  const FactorGrad r = factor_vjp_byval(b, need_prev, need_kd, xprev, x, ns, kd, z, nz, J, K, adj);
+  g_prev = g_prev + r.g_prev; g_x = g_x + r.g_x; g_ns = g_ns + r.g_ns; g_kd = g_kd + r.g_kd;
+  g_z = g_z + r.g_z; g_nz = g_nz + r.g_nz; g_J += r.g_J;
+  return r.F;
+#else
+  return factor_vjp_acc(b, need_prev, need_kd, xprev, x, ns, kd, z, nz, J, K, adj, g_prev, g_x, g_ns, g_kd, g_z,
+                        g_nz, g_J);
+#endif
 }
 
 // Gradient of the NEE factor w.r.t. (xprev, x, ns, kd, y, nl, Jl).
