@@ -244,6 +244,9 @@ int trn_render_grad(trn_scene* scene, const trn_camera* camera, const trn_render
  *   trn_render_grad.
  * - Limit: for TRN_PRIMARY_EDGE the scene may have at most 1048576 edges;
  *   larger scenes are rejected with an error.
+ * - A guided direct term with g_direct_depth > 0 needs the refined tree's
+ *   arrays, which the first refining trn_render_grad call allocates; before
+ *   that call it is rejected with an error.
  * - The scene's device must be the current device; otherwise the call
  *   returns an error.
  * - The first call on each device looks up the array's device address
