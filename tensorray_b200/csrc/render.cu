@@ -74,6 +74,19 @@ TRN_D long long slot_at(const Params& P, long long i) {
 
 constexpr int kMaxDepth = 16;
 
+// The integrator kernels' parameter block. Its members (the scene above all)
+// are passed by reference into non-inlined functions; a plain by-value
+// kernel parameter whose address is taken is first copied into every
+// thread's local memory, a __grid_constant__ one is addressed in place.
+#ifndef TRN_GRID_CONSTANT
+#define TRN_GRID_CONSTANT 1
+#endif
+#if TRN_GRID_CONSTANT
+#define TRN_KPARAMS const __grid_constant__ Params P
+#else
+#define TRN_KPARAMS Params P
+#endif
+
 // Minimum resident 256-thread blocks per SM the integrator kernels are
 // compiled for (caps registers per thread at 65536 / (256 * minimum)); the
 // values below are the measured best per kernel family.
@@ -117,7 +130,7 @@ constexpr int kMaxDepth = 16;
 #define TRN_SETUP_SHARED_PATHADJ 0
 #endif
 #ifndef TRN_SETUP_SHARED_PRIMARY
-#define TRN_SETUP_SHARED_PRIMARY 0
+#define TRN_SETUP_SHARED_PRIMARY 1
 #endif
 #ifndef TRN_SETUP_SHARED_DIRECT
 #define TRN_SETUP_SHARED_DIRECT 0
@@ -563,7 +576,7 @@ struct FwdState {
   F3 T, rdir, L;
 };
 
-__global__ void __launch_bounds__(256, TRN_MINB) k_path_fwd(Params P) {
+__global__ void __launch_bounds__(256, TRN_MINB) k_path_fwd(TRN_KPARAMS) {
   Cnt cnt;
   stage_top(P.s);
   int vhint = 0;
@@ -1036,7 +1049,7 @@ TRN_D void path_reverse(const Params& P, const Rec& r, Cnt& cnt) {
 }
 
 template <int MAXD>
-__global__ void __launch_bounds__(256, TRN_MINB_PATHADJ) k_path_adj(Params P) {
+__global__ void __launch_bounds__(256, TRN_MINB_PATHADJ) k_path_adj(TRN_KPARAMS) {
   Cnt cnt;
   stage_top(P.s);
   int vhint = 0;
@@ -1107,7 +1120,7 @@ TRN_D PathRecSoA<MAXD> path_soa(void* base, long long cap, long long i) {
 // half of the fused kernel's code (the fused kernel is instruction-fetch
 // bound).
 template <int MAXD>
-__global__ void __launch_bounds__(256, TRN_MINB_PATHADJ) k_path_replay(Params P) {
+__global__ void __launch_bounds__(256, TRN_MINB_PATHADJ) k_path_replay(TRN_KPARAMS) {
   Cnt cnt;
   stage_top(P.s);
   int vhint = 0;
@@ -1132,7 +1145,7 @@ __global__ void __launch_bounds__(256, TRN_MINB_PATHADJ) k_path_replay(Params P)
 // and carry no dL/dI yet; each path reads its pixel's now and is skipped when
 // that is zero, as path_adj_setup skips it in the replaying form.
 template <int MAXD, bool CACHED = false>
-__global__ void __launch_bounds__(256, TRN_MINB_REVERSE) k_path_reverse(Params P) {
+__global__ void __launch_bounds__(256, TRN_MINB_REVERSE) k_path_reverse(TRN_KPARAMS) {
   Cnt cnt;
   stage_top(P.s);
   const unsigned long long n = min(*P.q_count, (unsigned long long)P.q_cap);
@@ -1155,7 +1168,7 @@ __global__ void __launch_bounds__(256, TRN_MINB_REVERSE) k_path_reverse(Params P
 // call of the same paths then runs k_path_reverse<MAXD, true> over them
 // instead of tracing them again. Same image as k_path_fwd.
 template <int MAXD>
-__global__ void __launch_bounds__(256, TRN_MINB_FWDREC) k_path_fwd_rec(Params P) {
+__global__ void __launch_bounds__(256, TRN_MINB_FWDREC) k_path_fwd_rec(TRN_KPARAMS) {
   Cnt cnt;
   stage_top(P.s);
   int vhint = 0;
@@ -1189,7 +1202,7 @@ __global__ void __launch_bounds__(256, TRN_MINB_FWDREC) k_path_fwd_rec(Params P)
 #endif
 
 template <int MAXD>
-__global__ void __launch_bounds__(256, TRN_MINB_FWDREC) k_path_fwd_rec_regen(Params P) {
+__global__ void __launch_bounds__(256, TRN_MINB_FWDREC) k_path_fwd_rec_regen(TRN_KPARAMS) {
   Cnt cnt;
   stage_top(P.s);
   const DeviceScene& s = P.s;
@@ -1534,7 +1547,7 @@ TRN_D void primary_body(const Params& P, const ViewDesc& V, long long gslot, lon
   xdotn_vjp(P, V, W, cam_pos(V.cam), false, -1, 0.f, 0.f, v0, v1, sedge, p0, far_tri, n, cnt);
 }
 
-__global__ void __launch_bounds__(256, TRN_MINB) k_primary_adj(Params P) {
+__global__ void __launch_bounds__(256, TRN_MINB) k_primary_adj(TRN_KPARAMS) {
   Cnt cnt;
   stage_top(P.s);
   int vhint = 0;
@@ -1559,7 +1572,7 @@ struct PrimaryItem {
   F3 rdir, p0, n, g;
 };
 
-__global__ void __launch_bounds__(256, TRN_MINB_SETUP) k_primary_setup(Params P) {
+__global__ void __launch_bounds__(256, TRN_MINB_SETUP) k_primary_setup(TRN_KPARAMS) {
   Cnt cnt;
   stage_top(P.s);
   int vhint = 0;
@@ -1593,7 +1606,7 @@ __global__ void __launch_bounds__(256, TRN_MINB_SETUP) k_primary_setup(Params P)
   flush_cnt(cnt, P.stats);
 }
 
-__global__ void __launch_bounds__(256, TRN_MINB_BODY) k_primary_body(Params P) {
+__global__ void __launch_bounds__(256, TRN_MINB_BODY) k_primary_body(TRN_KPARAMS) {
   Cnt cnt;
   stage_top(P.s);
   const PrimaryItem* q = reinterpret_cast<const PrimaryItem*>(P.queue);
@@ -1616,7 +1629,7 @@ __global__ void __launch_bounds__(256, TRN_MINB_BODY) k_primary_body(Params P) {
 #define TRN_BODY_REGEN 1
 #endif
 
-__global__ void __launch_bounds__(256, TRN_MINB_BODY) k_primary_body_regen(Params P) {
+__global__ void __launch_bounds__(256, TRN_MINB_BODY) k_primary_body_regen(TRN_KPARAMS) {
   Cnt cnt;
   stage_top(P.s);
   const DeviceScene& s = P.s;
@@ -1789,7 +1802,7 @@ TRN_D void direct_body(const Params& P, const ViewDesc& V, long long gslot, long
   xdotn_vjp(P, V, W, x0.p, true, x0.tri, x0.u, x0.v, v0, v1, sedge, p0, far_tri, n, cnt);
 }
 
-__global__ void __launch_bounds__(256, TRN_MINB) k_direct_adj(Params P) {
+__global__ void __launch_bounds__(256, TRN_MINB) k_direct_adj(TRN_KPARAMS) {
   Cnt cnt;
   stage_top(P.s);
   int vhint = 0;
@@ -1811,7 +1824,7 @@ struct DirectItem {
   F3 rdir, ev0, p0, n;
 };
 
-__global__ void __launch_bounds__(256, TRN_MINB_SETUP) k_direct_setup(Params P) {
+__global__ void __launch_bounds__(256, TRN_MINB_SETUP) k_direct_setup(TRN_KPARAMS) {
   Cnt cnt;
   stage_top(P.s);
   int vhint = 0;
@@ -1844,7 +1857,7 @@ __global__ void __launch_bounds__(256, TRN_MINB_SETUP) k_direct_setup(Params P) 
   flush_cnt(cnt, P.stats);
 }
 
-__global__ void __launch_bounds__(256, TRN_MINB_BODY) k_direct_body(Params P) {
+__global__ void __launch_bounds__(256, TRN_MINB_BODY) k_direct_body(TRN_KPARAMS) {
   Cnt cnt;
   stage_top(P.s);
   const DirectItem* q = reinterpret_cast<const DirectItem*>(P.queue);
@@ -1950,7 +1963,7 @@ TRN_D void aq_point(const float* box, long long cap, int leaf, int k, uint32_t s
 
 // One thread per (leaf, point): |baseVal| at the refinement's evaluation
 // points (GuideDirectBoundary_Helper, AQ_distrb.h:65-79).
-__global__ void k_aq_eval(Params P, uint32_t stream, const float* box, const int* edge, const int* count,
+__global__ void k_aq_eval(TRN_KPARAMS, uint32_t stream, const float* box, const int* edge, const int* count,
                           long long cap, float* eval) {
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const int leaf = (int)(t / kAqPoints), k = (int)(t % kAqPoints);
@@ -2064,7 +2077,7 @@ __global__ void k_aq_commit(int* count) { count[0] = count[1]; }
 // (AQ_distrb.h:150-161). Leaves on non-secondary edges (zero length in the
 // edge distribution) do not exist in the reference's compacted edge list and
 // get weight 0 here.
-__global__ void k_aq_poly(Params P, uint32_t stream, int gspp, const float* box, const int* edge, const int* count,
+__global__ void k_aq_poly(TRN_KPARAMS, uint32_t stream, int gspp, const float* box, const int* edge, const int* count,
                           long long cap, float* poly) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= __ldg(count)) return;
@@ -2258,7 +2271,7 @@ TRN_D float indirect_emitter(const Params& P, const ViewDesc& V, long long gslot
 }
 
 template <int MAXD>
-__global__ void __launch_bounds__(256, TRN_MINB_INDIRECT) k_indirect_adj(Params P) {
+__global__ void __launch_bounds__(256, TRN_MINB_INDIRECT) k_indirect_adj(TRN_KPARAMS) {
   Cnt cnt;
   stage_top(P.s);
   int vhint = 0;
@@ -2299,7 +2312,7 @@ struct IndirectItem {
 };
 
 template <int MAXD>
-__global__ void __launch_bounds__(256, TRN_MINB_INDIRECT) k_indirect_sensor(Params P) {
+__global__ void __launch_bounds__(256, TRN_MINB_INDIRECT) k_indirect_sensor(TRN_KPARAMS) {
   Cnt cnt;
   stage_top(P.s);
   int vhint = 0;
@@ -2326,7 +2339,7 @@ __global__ void __launch_bounds__(256, TRN_MINB_INDIRECT) k_indirect_sensor(Para
 }
 
 template <int MAXD>
-__global__ void __launch_bounds__(256, TRN_MINB_INDIRECT) k_indirect_emitter(Params P) {
+__global__ void __launch_bounds__(256, TRN_MINB_INDIRECT) k_indirect_emitter(TRN_KPARAMS) {
   Cnt cnt;
   stage_top(P.s);
   // two-stage form: the queue and its count; three-stage form: the second queue
@@ -2357,7 +2370,7 @@ struct IndirectSetupItem {
   F3 rdir, p0, n;
 };
 
-__global__ void __launch_bounds__(256, TRN_MINB_SETUP) k_indirect_setup(Params P) {
+__global__ void __launch_bounds__(256, TRN_MINB_SETUP) k_indirect_setup(TRN_KPARAMS) {
   Cnt cnt;
   stage_top(P.s);
   int vhint = 0;
@@ -2393,7 +2406,7 @@ __global__ void __launch_bounds__(256, TRN_MINB_SETUP) k_indirect_setup(Params P
 }
 
 template <int MAXD>
-__global__ void __launch_bounds__(256, TRN_MINB_INDIRECT) k_indirect_sensor_q(Params P) {
+__global__ void __launch_bounds__(256, TRN_MINB_INDIRECT) k_indirect_sensor_q(TRN_KPARAMS) {
   Cnt cnt;
   stage_top(P.s);
   const IndirectSetupItem* qa = reinterpret_cast<const IndirectSetupItem*>(P.queue);
@@ -2447,7 +2460,7 @@ __global__ void __launch_bounds__(256, TRN_MINB_INDIRECT) k_indirect_sensor_q(Pa
 #endif
 
 template <int MAXD>
-__global__ void __launch_bounds__(256, TRN_MINB_INDIRECT) k_indirect_sensor_regen(Params P) {
+__global__ void __launch_bounds__(256, TRN_MINB_INDIRECT) k_indirect_sensor_regen(TRN_KPARAMS) {
   Cnt cnt;
   stage_top(P.s);
   const DeviceScene& s = P.s;
@@ -2544,7 +2557,7 @@ __global__ void __launch_bounds__(256, TRN_MINB_INDIRECT) k_indirect_sensor_rege
 #endif
 
 template <int MAXD>
-__global__ void __launch_bounds__(256, TRN_MINB_INDIRECT) k_indirect_emitter_regen(Params P) {
+__global__ void __launch_bounds__(256, TRN_MINB_INDIRECT) k_indirect_emitter_regen(TRN_KPARAMS) {
   Cnt cnt;
   stage_top(P.s);
   const DeviceScene& s = P.s;
@@ -2629,7 +2642,7 @@ __global__ void k_indirect_round(unsigned long long* work, unsigned long long fi
 // The edge pick restates the set-up functions' first step: primary_setup
 // (view silhouette table), direct_setup (scene table, or the AQ leaf when
 // guided), indirect_setup (scene table).
-__global__ void k_edge_keys(Params P, int term, unsigned* keys, unsigned* vals) {
+__global__ void k_edge_keys(TRN_KPARAMS, int term, unsigned* keys, unsigned* vals) {
   const long long first = P.order_first, n = P.total - first;
   int vhint = 0;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
@@ -2728,7 +2741,7 @@ TRN_D bool pixel_setup(const Params& P, long long gslot, EdgeState& st, int& vhi
   return true;
 }
 
-__global__ void __launch_bounds__(256, TRN_MINB) k_pixel_adj(Params P) {
+__global__ void __launch_bounds__(256, TRN_MINB) k_pixel_adj(TRN_KPARAMS) {
   Cnt cnt;
   stage_top(P.s);
   int vhint = 0;
@@ -2744,7 +2757,7 @@ __global__ void __launch_bounds__(256, TRN_MINB) k_pixel_adj(Params P) {
 
 // Split form: k_pixel_setup queues the accepted samples as PrimaryItem
 // (dimension 1 onwards, no edge vertices); k_primary_body runs them.
-__global__ void __launch_bounds__(256, TRN_MINB_SETUP) k_pixel_setup(Params P) {
+__global__ void __launch_bounds__(256, TRN_MINB_SETUP) k_pixel_setup(TRN_KPARAMS) {
   Cnt cnt;
   stage_top(P.s);
   int vhint = 0;
