@@ -184,3 +184,31 @@ def test_culled_ray_queries_equal_brute_force():
     assert int((brute[0] >= 0).sum()) > 300
     for a, b in zip(culled, brute):
         assert torch.equal(a, b)
+
+
+def test_guiding_tree_refinement_partitions_the_sample_cube():
+    """AQ refinement (the oracle's _aq_points / _aq_refine): after two passes
+    the leaves still tile the (edge, light) sample cube, i.e. their volumes
+    sum to the depth-0 tree's and every leaf lies inside its edge's
+    interval; the leaf limit holds; and a threshold nothing exceeds leaves the
+    depth-0 tree unchanged."""
+    from tensorray_b200 import scenes
+    osc = O.OracleScene(scenes.config1_scene(16, 16), requires_grad=())
+    with torch.no_grad():
+        osc.configure()
+    E = osc.edges.shape[0]
+    g0 = O.aq_guide(osc, 3, 2, 0.1)
+    g2 = O.aq_guide(osc, 3, 2, 0.1, depth=2, max_size=E + 150, thold=1e-5)
+    b0, b2 = g0["box"].double(), g2["box"].double()
+    vol = lambda b: ((b[3] - b[0]) * (b[4] - b[1]) * (b[5] - b[2])).sum()
+    n2 = b2.shape[1]
+    assert E < n2 <= E + 150
+    assert abs(float(vol(b2)) - float(vol(b0))) < 1e-6
+    cdf = osc.sec_cdf.double()
+    lo = torch.cat([torch.zeros(1, dtype=torch.float64), cdf[:-1]])
+    e = g2["edge"]
+    assert bool((b2[0] >= lo[e] - 1e-7).all() and (b2[3] <= cdf[e] + 1e-7).all())
+    assert bool((b2[1] >= 0).all() and (b2[4] <= 1).all() and (b2[2] >= 0).all() and (b2[5] <= 1).all())
+    assert bool((b2[3] >= b2[0]).all() and (b2[4] > b2[1]).all() and (b2[5] > b2[2]).all())
+    same = O.aq_guide(osc, 3, 2, 0.1, depth=2, max_size=E + 150, thold=1e30)
+    assert torch.equal(same["box"], g0["box"]) and torch.equal(same["cdf"], g0["cdf"])
