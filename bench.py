@@ -383,6 +383,34 @@ def run_single(a):
     ms_per_step = float(ms)
     value = units_per_step * world / (ms_per_step / 1e3)
 
+    # ---- the replay form: the gradient calls re-trace the interior paths
+    # from their seeds instead of reading the forward's path records ----
+    replay = None
+    if not a.no_path_cache:
+        scene.set_path_cache(0)
+        rsteps = min(a.steps, 10)
+        for _ in range(2):
+            step()
+        tot = 0.0
+        for _ in range(rsteps):
+            if world > 1:
+                dist.barrier()
+            flush.zero_()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            step()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            tot += e0.elapsed_time(e1)
+        t = torch.tensor([tot / rsteps], device=dev)
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        replay = {"value": units_per_step * world / (float(t) / 1e3), "unit": "grad path-samples/s",
+                  "ms_per_step": float(t), "steps": rsteps,
+                  "kernels": {"interior_fwd": ["k_path_fwd"], "interior_adj": ["k_path_replay", "k_path_reverse"]}}
+        scene.set_path_cache(16 << 30)
+
     # ---- e2e: through the autograd.Function with host buffers ----
     e2e = None
     if not a.no_e2e:
@@ -491,6 +519,7 @@ def run_single(a):
                        "res": a.res, "spp_per_term": a.spp, "depth": D, "triangles": scene.num_triangles,
                        "l2": "flushed between timed steps (256 MB write)", "parallelism": f"seeds x{world}"},
             "e2e": e2e, "gpu_launches": int(launches), "clocks": clk, "roofline": roofline, "step_ms": step_ms,
+            "replay_form": replay,
             "kernels": {k: {"ms": v["ms"], "GB/s": v["gbs"], "launches_of": term_kernels[k], "counts": v["counts"]}
                         for k, v in per_kernel_roof.items()},
             "cpu_baseline": cpu,
