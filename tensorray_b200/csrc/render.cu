@@ -91,10 +91,10 @@ constexpr int kMaxDepth = 16;
 // compiled for (caps registers per thread at 65536 / (256 * minimum)); the
 // values below are the measured best per kernel family.
 #ifndef TRN_MINB
-#define TRN_MINB 3
+#define TRN_MINB 4
 #endif
 #ifndef TRN_MINB_PATHADJ
-#define TRN_MINB_PATHADJ 3
+#define TRN_MINB_PATHADJ 4
 #endif
 #ifndef TRN_MINB_REVERSE
 #define TRN_MINB_REVERSE 2
