@@ -214,3 +214,40 @@ def test_inverse_step_pyramid_loss_and_largesteps_plumbing():
     ref.grad = inv.x.grad.clone()
     opt.step()
     torch.testing.assert_close(inv.x.detach(), ref.detach())
+
+
+def _one_view_worker(rank, world, port, out):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    from tensorray_b200 import api, inverse
+    cams = [_FakeCamera(3, 3)]
+    targets = torch.zeros(9, 3)
+    scene = _FakeScene(5)
+    real = api.ViewSet
+    api.ViewSet = _FakeViewSet
+    try:
+        inv = inverse.InverseRenderer(scene, cams, [4], targets, api.RenderOptions(0, 3, 0, 0, 0, 0, 0), lr=1e-2)
+        losses = [inv.step().clone() for _ in range(2)]
+    finally:
+        api.ViewSet = real
+    out[rank] = (list(inv.shard.local), inv.views is None, inv.samples_per_step(), [l.tolist() for l in losses],
+                 inv.x.detach().clone())
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_rank_without_views_still_joins_the_exchange():
+    """More ranks than views: the rank that holds no view renders nothing,
+    reports no samples, and still takes part in the gradient and loss
+    all-reduces, so every rank ends with the same losses and positions."""
+    world = 2
+    port = _free_port()
+    mgr = mp.Manager()
+    out = mgr.dict()
+    mp.start_processes(_one_view_worker, args=(world, port, out), nprocs=world, join=True, start_method="spawn")
+    holders = [r for r in range(world) if out[r][0]]
+    assert len(holders) == 1
+    empty = 1 - holders[0]
+    assert out[empty][1] and out[empty][2] == 0
+    assert out[0][3] == out[1][3]
+    torch.testing.assert_close(out[0][4], out[1][4])
