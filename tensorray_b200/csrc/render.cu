@@ -2642,7 +2642,14 @@ __global__ void k_indirect_round(unsigned long long* work, unsigned long long fi
 // The edge pick restates the set-up functions' first step: primary_setup
 // (view silhouette table), direct_setup (scene table, or the AQ leaf when
 // guided), indirect_setup (scene table).
-__global__ void k_edge_keys(TRN_KPARAMS, int term, unsigned* keys, unsigned* vals) {
+// bits_r1 + bits_r2 > 0 (indirect term) appends a direction bin below the
+// edge: the set-up rays of one edge leave one point, and sorting them by the
+// two samples that pick their direction (Edge.cpp:152-195) puts rays that
+// head the same way into one warp. r2 is the major part: it picks the
+// quadrant and the angle along the edge (or the azimuth of a boundary edge);
+// r1 sweeps the wedge between the face normals, which is narrow on a smooth
+// mesh (or the polar angle of a boundary edge).
+__global__ void k_edge_keys(TRN_KPARAMS, int term, int bits_r1, int bits_r2, unsigned* keys, unsigned* vals) {
   const long long first = P.order_first, n = P.total - first;
   int vhint = 0;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
@@ -2659,7 +2666,13 @@ __global__ void k_edge_keys(TRN_KPARAMS, int term, unsigned* keys, unsigned* val
       else
         e = sample_discrete(P.ecdf, P.ne, S(0), reuse);
     }
-    keys[i] = (unsigned)(&V - P.views) * (unsigned)(P.ne + 1) + (unsigned)e;
+    unsigned key = (unsigned)(&V - P.views) * (unsigned)(P.ne + 1) + (unsigned)e;
+    if (bits_r1 + bits_r2 > 0) {
+      const unsigned b1 = min((unsigned)(S(1) * (float)(1 << bits_r1)), (1u << bits_r1) - 1u);
+      const unsigned b2 = min((unsigned)(S(2) * (float)(1 << bits_r2)), (1u << bits_r2) - 1u);
+      key = (key << (bits_r1 + bits_r2)) | (b2 << bits_r1) | b1;
+    }
+    keys[i] = key;
     vals[i] = (unsigned)i;
   }
 }
@@ -3320,6 +3333,16 @@ int pixel_split(trn_viewset* vs, Params P, const trn_launch* ln, long long total
 #define TRN_EDGE_ORDER 1
 #endif
 
+// Direction bins per edge in the indirect term's run order: bits of the sort
+// key below the edge index taken from the samples r1 and r2 (0 and 0 sort by
+// edge alone).
+#ifndef TRN_INDIRECT_DIR_R1_BITS
+#define TRN_INDIRECT_DIR_R1_BITS 2
+#endif
+#ifndef TRN_INDIRECT_DIR_R2_BITS
+#define TRN_INDIRECT_DIR_R2_BITS 6
+#endif
+
 // Buffers of the edge-sorted run order for rounds of up to `cap` slots: keys
 // and values double-buffered (16 bytes per slot) plus the radix sort's
 // temporary storage for vs->sq_cap slots. Grown like the queue (at least
@@ -3364,9 +3387,16 @@ int order_round(trn_viewset* vs, Params& P, int term, cudaStream_t st) {
   cub::DoubleBuffer<unsigned> k(base, base + cap), v(base + 2 * cap, base + 3 * cap);
   P.order = nullptr;
   const int grid = (int)std::min<long long>((n + 255) / 256, 16LL * sms());
-  k_edge_keys<<<grid, 256, 0, st>>>(P, term, k.Current(), v.Current());
+  unsigned long long keys = (unsigned long long)P.nviews * (unsigned long long)(P.ne + 1);
+  // direction bits of the indirect term, r2's given up last, as many as fit
+  // the 32-bit key
+  int bits_r1 = term == TRN_INDIRECT_EDGE ? TRN_INDIRECT_DIR_R1_BITS : 0;
+  int bits_r2 = term == TRN_INDIRECT_EDGE ? TRN_INDIRECT_DIR_R2_BITS : 0;
+  while (bits_r1 > 0 && (keys << (bits_r1 + bits_r2)) > 0x100000000ull) bits_r1--;
+  while (bits_r2 > 0 && (keys << bits_r2) > 0x100000000ull) bits_r2--;
+  keys <<= bits_r1 + bits_r2;
+  k_edge_keys<<<grid, 256, 0, st>>>(P, term, bits_r1, bits_r2, k.Current(), v.Current());
   count_launch(1);
-  const unsigned long long keys = (unsigned long long)P.nviews * (unsigned long long)(P.ne + 1);
   int bits = 1;
   while (bits < 32 && (1ull << bits) < keys) bits++;
   void* tmp = reinterpret_cast<char*>(vs->sq) + (16 * (size_t)cap + 255) / 256 * 256;
