@@ -175,6 +175,17 @@ const char* trn_version(void);
 int trn_camera_init(trn_camera* out, const float pos[3], const float target[3], const float up[3],
                     int width, int height, float fov_deg);
 
+/* The edge list of a triangle mesh, host-only (no device work). Replaces
+ * ObjMesh::processEdges (EDXUtil/Graphics/ObjMesh.cpp:584-632), which the
+ * secondary and primary edge lists start from: one row (v0, v1, f0, f1, v2)
+ * per unique undirected edge, v0 < v1, rows in (v0, v1) order. f0 is the first
+ * face (in face order) that has the edge and v2 that face's third vertex; f1
+ * is the second face when exactly two faces share the edge, else -1.
+ * indices: [num_triangles*3]. Writes min(rows, cap) rows of 5 ints to out and
+ * returns the number of rows (call with cap = 0 to size out), or -1 on
+ * invalid arguments. */
+long long trn_mesh_edges(int num_triangles, const int* indices, int* out, long long cap);
+
 /* Scene lifetime. Replaces Scene::Configure (Scene.cpp:522-533): create
  * uploads the description; configure runs Primitive::Configure, face/vertex
  * normals, light distribution, secondary edge list and the LBVH build. */

@@ -28,13 +28,22 @@ Differences that are deliberate and shared with the GPU path:
     nothing (_SampleGuard); the reference would turn the whole gradient NaN;
   * square roots are correctly rounded (sqrt_rn), like the GPU's.
 
-Parity status: parity unpinned. The reference cannot be built or run here:
-it needs OptiX 7.4, MSVC-only headers (crtdbg.h, ppl.h), and its JIT reads
-its own source tree at run time. No reference test pins render outputs. This
-oracle is pinned by closed-form answers (Lambert's polygon irradiance for
-direct light from a quad emitter, a clamped-cosine furnace) and by the
-reference's finite-difference-vs-AD validation pattern (Tensor.h:2968-3021)
-applied to its render path.
+Parity status: partly pinned to the reference's own outputs.
+  * Pinned by the reference's code: the edge lists (build_edges equals
+    ObjMesh::processEdges row for row) and the camera (camera_matrices within
+    1e-6 relative of EDX::Camera and the renderer's derived matrices). The
+    reference's EDXUtil mesh and camera sources are plain C++ and are built
+    into oracle/_ref/edx_probe (oracle/edx/Makefile); its outputs on seeded
+    inputs are the fixtures in tests/golden/edx_pins.json.
+  * Unpinned by the reference's code: the integrators. Their sources cannot
+    be built or run here: they need OptiX 7.4 for every ray query and the
+    reference's tensor library, whose JIT compiles kernels at run time from
+    the reference's source tree and which includes MSVC-only headers (ppl.h
+    for concurrency::parallel_for). No reference test pins render outputs.
+    The integrators are pinned by closed-form answers (Lambert's polygon
+    irradiance for direct light from a quad emitter, a clamped-cosine
+    furnace) and by the reference's finite-difference-vs-AD validation
+    pattern (Tensor.h:2968-3021) applied to this render path.
 """
 from __future__ import annotations
 

@@ -80,6 +80,7 @@ _SIGNATURES = {
     "trn_version": (C.c_char_p, []),
     "trn_camera_init": (C.c_int, [C.POINTER(TrnCamera), C.POINTER(C.c_float), C.POINTER(C.c_float),
                                   C.POINTER(C.c_float), C.c_int, C.c_int, C.c_float]),
+    "trn_mesh_edges": (C.c_longlong, [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_longlong]),
     "trn_scene_create": (C.c_int, [C.POINTER(TrnSceneDesc), C.POINTER(C.c_void_p)]),
     "trn_scene_configure": (C.c_int, [C.c_void_p, C.c_void_p]),
     "trn_scene_destroy": (C.c_int, [C.c_void_p]),

@@ -418,6 +418,22 @@ def sample_dims(integrator_id: int, max_bounces: int, guided: bool = False) -> i
             TRN_INDIRECT_EDGE: 3 + 8 * max(D - 1, 0), TRN_PIXEL_EDGE: 1 + 5 * D}[integrator_id]
 
 
+def mesh_edges(faces: np.ndarray) -> np.ndarray:
+    """The edge list the library builds for a triangle mesh (trn_mesh_edges,
+    ObjMesh::processEdges): int32 rows (v0, v1, f0, f1, v2), v0 < v1, in
+    (v0, v1) order. Host-only."""
+    lib = _abi.load()
+    F = np.ascontiguousarray(np.asarray(faces, np.int32).reshape(-1, 3))
+    ip = F.ctypes.data_as(C.POINTER(C.c_int))
+    n = lib.trn_mesh_edges(len(F), ip, None, 0)
+    _abi.check(-1 if n < 0 else 0, "trn_mesh_edges")
+    out = np.empty((n, 5), np.int32)
+    if n:
+        _abi.check(0 if lib.trn_mesh_edges(len(F), ip, out.ctypes.data_as(C.POINTER(C.c_int)), n) == n else -1,
+                   "trn_mesh_edges")
+    return out
+
+
 def sample_slots(integrator_id: int, width: int, height: int, spp: int) -> int:
     n = width * height * spp
     return n // 4 if integrator_id == TRN_PIXEL_EDGE else n

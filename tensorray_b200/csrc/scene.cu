@@ -832,6 +832,18 @@ int trn_camera_init(trn_camera* out, const float pos[3], const float target[3], 
   return 0;
 }
 
+long long trn_mesh_edges(int num_triangles, const int* indices, int* out, long long cap) {
+  if (num_triangles < 0 || (num_triangles > 0 && !indices) || cap < 0 || (cap > 0 && !out)) {
+    set_error("trn_mesh_edges: invalid arguments");
+    return -1;
+  }
+  std::vector<int> rows;
+  build_edges(num_triangles, indices, rows);
+  const long long n = (long long)(rows.size() / 5);
+  if (cap > 0) std::copy(rows.begin(), rows.begin() + 5 * std::min(n, cap), out);
+  return n;
+}
+
 int trn_scene_create(const trn_scene_desc* d, trn_scene** out) {
   if (!d || !out) { set_error("trn_scene_create: null argument"); return -1; }
   *out = nullptr;

@@ -306,18 +306,49 @@ def fibonacci_cameras(n: int, radius: float, resolutions, seed: int = 0):
     return cams
 
 
+_LIBC = None
+
+
+def _strtof(token: str) -> np.float32:
+    global _LIBC
+    if _LIBC is None:
+        import ctypes
+        _LIBC = ctypes.CDLL(None)
+        _LIBC.strtof.restype = ctypes.c_float
+        _LIBC.strtof.argtypes = [ctypes.c_char_p, ctypes.c_void_p]
+    return np.float32(_LIBC.strtof(token.encode(), None))
+
+
+def parse_f32(tokens) -> np.ndarray:
+    """Decimal strings -> float32, rounded once, as C's strtof (behind the
+    reference's fscanf("%f")) rounds them. Python parses to the nearest
+    double, and rounding that to float32 can differ from a single rounding
+    only when the double lies exactly halfway between two float32 values;
+    those few are parsed again by the C library."""
+    d = np.asarray([float(t) for t in tokens], np.float64)
+    f = d.astype(np.float32)
+    tie = (d.view(np.uint64) & np.uint64((1 << 29) - 1)) == np.uint64(1 << 28)
+    for i in np.flatnonzero(tie):
+        f[i] = _strtof(tokens[i])
+    return f
+
+
 def load_obj(path: str, bsdf: int = 0, smooth: bool = True, light: int = -1,
              translation=(0.0, 0.0, 0.0)) -> MeshSpec:
     """Wavefront OBJ -> MeshSpec, following ObjMesh::LoadFromObj
     (EDXUtil/Graphics/ObjMesh.cpp:39-345) with makeLeftHanded = false, as every
     reference Primitive loads meshes (Renderer/Primitive.cpp:213-245):
-    `v` positions as given, `vt` texture coordinates with v flipped to 1 - v,
-    faces of 3 or 4 corners in the forms i, i/t, i/t/n, i//n with 1-based or
-    negative (relative) indices, quads split into (0, 1, 2) and (3, 0, 2).
-    Normals (`vn`), smoothing groups and materials are not used by the
-    renderer and are skipped. The reference leaves the texture indices of a
-    quad's second triangle unset; here they follow its position corners."""
-    pos, uv, faces, uvf = [], [], [], []
+    `v` positions as given, `vt` texture coordinates with v flipped to
+    1.0f - v in float32 arithmetic (ObjMesh.cpp:73-78), numbers rounded to
+    float32 as strtof rounds them, faces of 3 or 4 corners in the forms i,
+    i/t, i/t/n, i//n with 1-based or negative (relative) indices, quads split
+    into (0, 1, 2) and (3, 0, 2). Normals (`vn`), smoothing groups and
+    materials are not used by the renderer and are skipped. The reference
+    leaves the texture indices of a quad's second triangle unset; here they
+    follow its position corners. A comment line is skipped whole; the
+    reference reads the tokens after a lone '#' as commands, so a comment
+    such as "# v 1 2 3" would add a vertex there."""
+    pos, us, vs, faces, uvf = [], [], [], [], []
     textured = False
     with open(path, "r") as f:
         for raw in f:
@@ -326,9 +357,14 @@ def load_obj(path: str, bsdf: int = 0, smooth: bool = True, light: int = -1,
                 continue
             tag = parts[0]
             if tag == "v":
-                pos.append([float(x) for x in parts[1:4]])
+                if len(parts) < 4:
+                    raise ValueError(f"{path}: a vertex needs 3 coordinates: {raw.strip()!r}")
+                pos.extend(parts[1:4])
             elif tag == "vt":
-                uv.append([float(parts[1]), 1.0 - float(parts[2])])
+                if len(parts) < 3:
+                    raise ValueError(f"{path}: a texture coordinate needs 2 values: {raw.strip()!r}")
+                us.append(parts[1])
+                vs.append(parts[2])
                 textured = True
             elif tag == "f":
                 corners = parts[1:]
@@ -338,10 +374,10 @@ def load_obj(path: str, bsdf: int = 0, smooth: bool = True, light: int = -1,
                 for c in corners:
                     fields = c.split("/")
                     p = int(fields[0])
-                    pi.append(p - 1 if p > 0 else len(pos) + p)
+                    pi.append(p - 1 if p > 0 else len(pos) // 3 + p)
                     if len(fields) > 1 and fields[1]:
                         t = int(fields[1])
-                        ti.append(t - 1 if t > 0 else len(uv) + t)
+                        ti.append(t - 1 if t > 0 else len(us) + t)
                     else:
                         ti.append(0)
                 faces.append([pi[0], pi[1], pi[2]])
@@ -349,12 +385,12 @@ def load_obj(path: str, bsdf: int = 0, smooth: bool = True, light: int = -1,
                 if len(corners) == 4:
                     faces.append([pi[3], pi[0], pi[2]])
                     uvf.append([ti[3], ti[0], ti[2]])
-    P = np.asarray(pos, np.float32).reshape(-1, 3)
+    P = parse_f32(pos).reshape(-1, 3)
     F = np.asarray(faces, np.int32).reshape(-1, 3)
     if F.size and (F.min() < 0 or F.max() >= len(P)):
         raise ValueError(f"{path}: face index out of range")
     m = MeshSpec(P, F, bsdf=bsdf, light=light, smooth=smooth, translation=tuple(translation))
     if textured:
-        m.uvs = np.asarray(uv, np.float32).reshape(-1, 2)
+        m.uvs = np.stack([parse_f32(us), np.float32(1.0) - parse_f32(vs)], 1).astype(np.float32)
         m.uv_faces = np.asarray(uvf, np.int32).reshape(-1, 3)
     return m

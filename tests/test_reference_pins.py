@@ -1,0 +1,191 @@
+"""Pins against the reference's own code, on the CPU.
+
+tests/golden/edx_pins.json holds what the reference's EDXUtil computes on
+seeded inputs, written by tests/golden/make_edx_goldens.py from
+oracle/_ref/edx_probe (a g++ build of EDXUtil/Graphics/ObjMesh.cpp,
+BaseCamera.cpp and EDXUtil/Math/Matrix.cpp from the reference's sources):
+
+- OBJ ingest, ObjMesh::LoadFromObj (ObjMesh.cpp:39-345) as every Primitive
+  calls it: scenes.load_obj must give the same float32 bits for positions and
+  texture coordinates and the same face indices;
+- edge lists, ObjMesh::processEdges (ObjMesh.cpp:584-632): the oracle's
+  build_edges and the library's trn_mesh_edges must give the same rows;
+- the camera, EDX::Camera::Init (BaseCamera.cpp:45-88) and the quantities the
+  renderer's Camera::Resize derives (Camera.cpp:105-137): the library's
+  trn_camera_init and the oracle's camera_matrices must agree with it within
+  CAMERA_TOL relative per quantity (scaled by its largest entry).
+
+The camera cannot agree bit for bit. The reference normalises vectors with the
+SSE reciprocal-square-root estimate and one Newton step (EDXMath.h:223-229,
+Vec3.h:256-259), whose bits differ between CPU vendors, and inverts its
+matrices in float32; the library and the oracle compute in double and round
+once. The largest difference seen is 3.3e-7 (inv_area).
+"""
+import json
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from oracle import tr_oracle as O
+from tensorray_b200 import api, scenes
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GOLDEN = os.path.join(HERE, "golden", "edx_pins.json")
+PROBE = os.path.join(os.path.dirname(HERE), "oracle", "_ref", "edx_probe")
+CAMERA_TOL = 1e-6
+CAMERA_KEYS = ("pos", "dir", "raster_to_camera", "view_inv", "world_to_sample", "sample_to_camera", "raster_to_world",
+               "inv_area", "plane_len_x", "plane_len_y")
+
+
+@pytest.fixture(scope="module")
+def pins():
+    with open(GOLDEN) as f:
+        return json.load(f)
+
+
+def _f32(bits) -> np.ndarray:
+    return np.asarray(bits, np.uint32).view(np.float32)
+
+
+def _load(text, tmp_path, name):
+    path = tmp_path / f"{name}.obj"
+    path.write_text(text)
+    return scenes.load_obj(str(path)), str(path)
+
+
+def _quad_second_rows(text):
+    """Rows of the faces list that are the second triangle of a quad."""
+    rows, k = [], 0
+    for line in text.splitlines():
+        parts = line.split()
+        if parts and parts[0] == "f":
+            k += 1
+            if len(parts) == 5:
+                rows.append(k)
+                k += 1
+    return rows
+
+
+def _reference_edges(r):
+    return np.stack([r["edge_vertex0"], r["edge_vertex1"], r["edge_face0"], r["edge_face1"], r["edge_vertex2"]], 1)
+
+
+def test_fixture_covers_the_edge_cases(pins):
+    objs = pins["obj"]
+    edges = np.concatenate([_reference_edges(c["reference"]) for c in objs.values()])
+    assert (edges[:, 3] == -1).any() and (edges[:, 3] >= 0).any()
+    # non-manifold edges: three or more faces on one (v0, v1)
+    soup = objs["soup"]["reference"]
+    F = np.asarray(soup["face_positions"]).reshape(-1, 3)
+    und = np.sort(np.stack([F, np.roll(F, -1, 1)], 2).reshape(-1, 2), 1)
+    _, cnt = np.unique(und, axis=0, return_counts=True)
+    assert cnt.max() >= 3
+    assert any("-" in c["text"] for c in objs.values())          # relative indices
+    assert any(c["reference"]["textured"] for c in objs.values())
+    assert len(pins["camera"]) >= 8
+
+
+@pytest.mark.parametrize("name", ["tetra_vt_vn", "quads_untextured_forms", "quads_textured", "icosphere_level2",
+                                  "soup"])
+def test_obj_ingest_matches_reference_bits(pins, tmp_path, name):
+    case = pins["obj"][name]
+    r = case["reference"]
+    m, _ = _load(case["text"], tmp_path, name)
+    P = _f32(r["positions"]).reshape(-1, 3)
+    assert m.positions.dtype == np.float32
+    assert np.array_equal(m.positions.view(np.uint32), P.view(np.uint32))
+    assert np.array_equal(m.faces, np.asarray(r["face_positions"]).reshape(-1, 3))
+    assert r["triangle_count"] == len(m.faces) and r["vertex_count"] == len(m.positions)
+    if r["textured"]:
+        T = _f32(r["texcoords"]).reshape(-1, 2)
+        assert np.array_equal(m.uvs.view(np.uint32), T.view(np.uint32))
+        FT = np.asarray(r["face_texcoords"]).reshape(-1, 3)
+        # the reference leaves a textured quad's second triangle's texture
+        # indices unset (ObjMesh.cpp:221-262); every other row must agree
+        keep = np.ones(len(FT), bool)
+        keep[_quad_second_rows(case["text"])] = False
+        assert np.array_equal(m.uv_faces[keep], FT[keep])
+    else:
+        assert m.uvs is None
+
+
+@pytest.mark.parametrize("name", ["tetra_vt_vn", "quads_untextured_forms", "quads_textured", "icosphere_level2",
+                                  "soup"])
+def test_edge_lists_match_processEdges(pins, tmp_path, name):
+    r = pins["obj"][name]["reference"]
+    F = np.asarray(r["face_positions"]).reshape(-1, 3)
+    ref = _reference_edges(r)
+    assert r["num_edges"] == len(ref)
+    assert np.array_equal(O.build_edges(F), ref)
+    assert np.array_equal(api.mesh_edges(F), ref)
+
+
+def test_mesh_edges_rejects_bad_arguments():
+    lib = api._abi.load()
+    assert lib.trn_mesh_edges(-1, None, None, 0) == -1
+    assert "trn_mesh_edges" in lib.trn_last_error().decode()
+    assert lib.trn_mesh_edges(1, None, None, 0) == -1
+    assert api.mesh_edges(np.zeros((0, 3), np.int32)).shape == (0, 5)
+
+
+def test_parse_f32_rounds_once_like_strtof():
+    # 1 + 2^-24 is halfway between the float32 values 1 and 1 + 2^-23; the
+    # decimal just above it is nearest to that double, so a parse through
+    # double and then float32 rounds to even (1.0) where strtof gives 1 + 2^-23
+    above = "1.0000000596046447753906250000001"
+    below = "1.0000000596046447753906249999999"
+    f = scenes.parse_f32([above, below, "0.1", "-2.5e-3"])
+    assert f[0] == np.float32(1.0) + np.float32(2.0 ** -23)
+    assert f[1] == np.float32(1.0)
+    assert f[2] == np.float32(0.1) and f[3] == np.float32(-2.5e-3)
+
+
+def _rel(a, r):
+    a = np.asarray(a, np.float64).reshape(-1)
+    r = np.asarray(r, np.float64).reshape(-1)
+    return float(np.abs(a - r).max() / max(np.abs(r).max(), 1e-30))
+
+
+def test_camera_matches_reference(pins):
+    worst = 0.0
+    for case in pins["camera"]:
+        a, r = case["args"], case["reference"]
+        v = [float(x) for x in a[:9]]
+        w, h, fov = int(a[9]), int(a[10]), float(a[11])
+        lib_cam = api.Camera(v[0:3], v[3:6], v[6:9], w, h, fov).matrices()
+        ora_cam = O.camera_matrices(v[0:3], v[3:6], v[6:9], w, h, fov)
+        assert (lib_cam["width"], lib_cam["height"]) == (r["width"], r["height"])
+        for k in CAMERA_KEYS:
+            ref = _f32(r[k])
+            for got in (lib_cam[k], ora_cam[k]):
+                e = _rel(got, ref)
+                worst = max(worst, e)
+                assert e <= CAMERA_TOL, (a, k, e)
+    assert worst > 0.0        # the float32/rsqrt path is not the double one
+
+
+@pytest.mark.skipif(not os.path.exists(PROBE), reason="the reference probe is built only where the reference is")
+def test_fixture_is_what_the_reference_computes(pins, tmp_path):
+    """Replays the mesh inputs through the probe itself. Mesh ingest and edge
+    lists are integer and parse work, the same on every CPU; the camera is
+    replayed against the same tolerance as above (the SSE estimate's bits are
+    the CPU's)."""
+    for name, case in pins["obj"].items():
+        _, path = _load(case["text"], tmp_path, name)
+        live = json.loads(subprocess.run([PROBE, "obj", path], capture_output=True, text=True, check=True).stdout)
+        r = case["reference"]
+        keep = np.ones(len(r["face_texcoords"]), bool)
+        for row in _quad_second_rows(case["text"]) if r["textured"] else []:
+            keep[3 * row:3 * row + 3] = False
+        for k, v in r.items():
+            if k == "face_texcoords":
+                assert np.array_equal(np.asarray(live[k])[keep], np.asarray(v)[keep]), name
+            else:
+                assert live[k] == v, (name, k)
+    for case in pins["camera"]:
+        live = json.loads(subprocess.run([PROBE, "camera", *case["args"]], capture_output=True, text=True,
+                                         check=True).stdout)
+        for k in CAMERA_KEYS:
+            assert _rel(_f32(live[k]), _f32(case["reference"][k])) <= CAMERA_TOL
