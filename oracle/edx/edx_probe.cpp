@@ -12,6 +12,14 @@
 //     texture indices, and the edge lists processEdges built
 //     (EDXUtil/Graphics/ObjMesh.cpp:584-632).
 //
+//   edx_probe bitmap FILE
+//     Bitmap::ReadFromFile<float>(FILE, ..., 3), the call the renderer's
+//     ImageTexture makes (Renderer/BSDF.cpp:57-70). That function is one call
+//     of stbi_loadf with 3 required channels (EDXUtil/Windows/Bitmap.cpp:
+//     187-190) into the stb_image the reference compiles inside Bitmap.cpp
+//     (stb_image.h v2.02 with STB_IMAGE_IMPLEMENTATION, in C++), which is what
+//     this file compiles too.
+//
 //   edx_probe camera PX PY PZ TX TY TZ UX UY UZ W H FOV
 //     EDX::Camera::Init (EDXUtil/Graphics/BaseCamera.cpp:45-88) with the
 //     clip planes of the renderer's Camera::Init (Renderer/Camera.cpp:89-103),
@@ -27,6 +35,9 @@
 
 #include "Graphics/BaseCamera.h"
 #include "Graphics/ObjMesh.h"
+
+#define STB_IMAGE_IMPLEMENTATION
+#include "Windows/stb_image.h"
 
 namespace {
 
@@ -84,6 +95,20 @@ int probe_obj(const char* path) {
   put_ints("edge_face1", e.indexFace1);
   put_ints("edge_vertex2", e.indexVertex2, true);
   std::printf("}\n");
+  return 0;
+}
+
+int probe_bitmap(const char* path) {
+  int w = 0, h = 0, c = 0;
+  float* px = stbi_loadf(path, &w, &h, &c, 3);
+  if (!px) {
+    std::printf("{\n\"error\": \"%s\"\n}\n", stbi_failure_reason());
+    return 0;
+  }
+  std::printf("{\n\"width\": %d,\n\"height\": %d,\n\"channels_in_file\": %d,\n", w, h, c);
+  put_floats("texels", px, (size_t)w * h * 3, true);
+  std::printf("}\n");
+  stbi_image_free(px);
   return 0;
 }
 
@@ -151,9 +176,11 @@ int probe_camera(char** a) {
 
 int main(int argc, char** argv) {
   if (argc == 3 && !std::strcmp(argv[1], "obj")) return probe_obj(argv[2]);
+  if (argc == 3 && !std::strcmp(argv[1], "bitmap")) return probe_bitmap(argv[2]);
   if (argc == 14 && !std::strcmp(argv[1], "camera")) return probe_camera(argv + 2);
   std::fprintf(stderr,
                "usage: edx_probe obj FILE\n"
+               "       edx_probe bitmap FILE\n"
                "       edx_probe camera PX PY PZ TX TY TZ UX UY UZ W H FOV\n");
   return 2;
 }

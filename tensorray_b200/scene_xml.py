@@ -84,21 +84,142 @@ def _resolve(path: str, base: str) -> str:
     return cand
 
 
+_GAMMA_LUT = None
+
+# the image formats stb_image 2.02 reads that PIL decodes to the same 8-bit
+# values (JPEG: see load_bitmap)
+_STB_8BIT_FORMATS = ("PNG", "BMP", "TGA", "PPM", "GIF", "JPEG")
+
+
+def _gamma_lut() -> np.ndarray:
+    """stb_image's 8-bit to float conversion (stbi__ldr_to_hdr, stb_image.h
+    v2.02 as the reference builds it inside Bitmap.cpp, a C++ unit):
+    powf(v / 255.0f, 2.2f) * 1.0f for each 8-bit value v, with the C
+    library's powf (a vectorised float32 power can differ in the last bit)."""
+    global _GAMMA_LUT
+    if _GAMMA_LUT is None:
+        import ctypes
+        import ctypes.util
+        libm = ctypes.CDLL(ctypes.util.find_library("m"))
+        libm.powf.restype = ctypes.c_float
+        libm.powf.argtypes = [ctypes.c_float, ctypes.c_float]
+        x = np.arange(256, dtype=np.float32) / np.float32(255.0)
+        g = float(np.float32(2.2))
+        _GAMMA_LUT = np.array([libm.powf(float(v), g) for v in x], np.float32)
+    return _GAMMA_LUT
+
+
+def _read_radiance(path: str) -> np.ndarray:
+    """Radiance RGBE (.hdr) -> [H, W, 3] float32, as stbi__hdr_load
+    (stb_image.h v2.02) decodes it with 3 channels: a "#?RADIANCE" first line,
+    a header that must hold "FORMAT=32-bit_rle_rgbe" and ends at an empty
+    line, a "-Y H +X W" resolution line, then the pixels: flat RGBE when
+    W < 8 or W >= 32768, else run-length-encoded scanlines (2, 2, W >> 8,
+    W & 255, then each channel as runs (count > 128: count - 128 copies of one
+    byte) and dumps (count literal bytes)). A scanline without that marker
+    makes stb decode the whole image again as flat RGBE from that point.
+    Channel value c with exponent e becomes c * ldexp(1.0f, e - 136) in
+    float32; e = 0 is black. Corrupt data that stb would loop on or overrun
+    is an error here."""
+    with open(path, "rb") as f:
+        data = f.read()
+    pos = 0
+
+    def line() -> bytes:
+        nonlocal pos
+        end = data.find(b"\n", pos)
+        end = len(data) if end < 0 else end
+        out = data[pos:end]
+        pos = end + 1
+        return out
+
+    _require(line() == b"#?RADIANCE", f"{path}: not a Radiance HDR image")
+    valid = False
+    while pos < len(data):
+        tok = line()
+        if not tok:
+            break
+        valid |= tok == b"FORMAT=32-bit_rle_rgbe"
+    _require(valid, f"{path}: unsupported HDR format")
+    res = line().decode("latin-1").split()
+    _require(len(res) == 4 and res[0] == "-Y" and res[2] == "+X", f"{path}: unsupported HDR data layout")
+    H, W = int(res[1]), int(res[3])
+    _require(H > 0 and W > 0, f"{path}: bad HDR resolution")
+
+    def flat(at: int) -> np.ndarray:
+        _require(at + H * W * 4 <= len(data), f"{path}: truncated HDR data")
+        return np.frombuffer(data, np.uint8, H * W * 4, at).reshape(H, W, 4)
+
+    if W < 8 or W >= 32768:
+        rgbe = flat(pos)
+    else:
+        rgbe = np.empty((H, W, 4), np.uint8)
+        for j in range(H):
+            _require(pos + 4 <= len(data), f"{path}: truncated HDR data")
+            c1, c2, hi = data[pos], data[pos + 1], data[pos + 2]
+            if c1 != 2 or c2 != 2 or hi & 0x80:
+                rgbe = flat(pos)
+                break
+            _require(((hi << 8) | data[pos + 3]) == W, f"{path}: invalid decoded scanline length")
+            pos += 4
+            for k in range(4):
+                i = 0
+                while i < W:
+                    _require(pos < len(data), f"{path}: truncated HDR data")
+                    count = data[pos]
+                    pos += 1
+                    if count > 128:
+                        n = count - 128
+                        _require(i + n <= W and pos < len(data), f"{path}: corrupt HDR run")
+                        rgbe[j, i:i + n, k] = data[pos]
+                        pos += 1
+                    else:
+                        n = count
+                        _require(0 < n and i + n <= W and pos + n <= len(data), f"{path}: corrupt HDR dump")
+                        rgbe[j, i:i + n, k] = np.frombuffer(data, np.uint8, n, pos)
+                        pos += n
+                    i += n
+    e = rgbe[..., 3].astype(np.int64)
+    scale = np.ldexp(np.float64(1.0), e - 136).astype(np.float32)
+    out = rgbe[..., :3].astype(np.float32) * scale[..., None]
+    out[e == 0] = 0.0
+    return np.ascontiguousarray(out, np.float32)
+
+
 def load_bitmap(path: str) -> np.ndarray:
-    """[H, W, 3] float32 texels, top row first (stbi_loadf semantics)."""
+    """[H, W, 3] float32 texels, top row first, as the reference's texture
+    load gives them: Bitmap::ReadFromFile<float>(path, ..., 3)
+    (EDXUtil/Windows/Bitmap.cpp:187-190, called by ImageTexture,
+    Renderer/BSDF.cpp:57-70), one stbi_loadf call of stb_image 2.02.
+
+    - 8-bit images (PNG, BMP, TGA, binary PPM/PGM, GIF, JPEG): gray is
+      replicated, alpha dropped, and each value v becomes powf(v/255, 2.2).
+    - Radiance .hdr: linear RGBE (_read_radiance).
+    - 16-bit PNGs and other formats are refused, as stb_image 2.02 refuses
+      them.
+    - .npy [H, W, 3] arrays are taken as they are (this package's own format
+      for generated textures).
+
+    JPEG is decoded by PIL (libjpeg), whose IDCT and chroma upsampling are not
+    stb_image's: its values can differ from the reference's by a few 8-bit
+    levels. Every other format gives the reference's bits."""
     if path.endswith(".npy"):
         a = np.load(path).astype(np.float32)
         _require(a.ndim == 3 and a.shape[2] == 3, f"{path}: expected an [H, W, 3] array")
         return np.ascontiguousarray(a)
+    with open(path, "rb") as f:
+        head = f.read(32)
+    if head.startswith(b"#?RADIANCE"):
+        return _read_radiance(path)
+    _require(not (head.startswith(b"\x89PNG\r\n\x1a\n") and len(head) > 24 and head[24] == 16),
+             f"{path}: 16-bit PNGs are not loaded (the reference's stb_image 2.02 reads 8-bit PNGs only)")
     from PIL import Image
     img = Image.open(path)
-    if img.mode in ("F", "I", "I;16", "I;16B"):
-        a = np.asarray(img, np.float32)
-        if img.mode.startswith("I;16"):
-            a = (a / 65535.0) ** 2.2
-        return np.ascontiguousarray(np.repeat(a[:, :, None], 3, axis=2))
-    a = np.asarray(img.convert("RGB"), np.float32) / 255.0
-    return np.ascontiguousarray((a ** 2.2).astype(np.float32))
+    _require(img.format in _STB_8BIT_FORMATS and img.mode in ("1", "L", "LA", "P", "PA", "RGB", "RGBA"),
+             f"{path}: {img.format} {img.mode} images are not loaded (the reference's stb_image 2.02 reads "
+             "8-bit JPEG, PNG, BMP, TGA, PNM, GIF and Radiance HDR)")
+    a = np.asarray(img.convert("RGB"), np.uint8)
+    return np.ascontiguousarray(_gamma_lut()[a])
 
 
 def _transform(node) -> np.ndarray:

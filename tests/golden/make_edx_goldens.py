@@ -1,14 +1,17 @@
 """Writes tests/golden/edx_pins.json: what the reference's own EDXUtil code
-computes for the mesh ingest, the edge lists and the camera, on seeded inputs.
+computes for the mesh ingest, the edge lists, the texture images and the
+camera, on seeded inputs.
 
 The outputs come from oracle/_ref/edx_probe, which oracle/edx/Makefile builds
 from the reference's sources (EDXUtil/Graphics/ObjMesh.cpp, BaseCamera.cpp,
-EDXUtil/Math/Matrix.cpp). The inputs (OBJ text, camera arguments) are stored
+EDXUtil/Math/Matrix.cpp, EDXUtil/Windows/stb_image.h). The inputs (OBJ text,
+image file bytes, camera arguments) are stored
 beside the outputs, so tests/test_reference_pins.py replays them without the
 reference. Run it where the reference checkout is present:
 
     python tests/golden/make_edx_goldens.py [REFERENCE_ROOT]
 """
+import base64
 import json
 import os
 import subprocess
@@ -127,6 +130,79 @@ def obj_cases():
     }
 
 
+def _hdr_bytes(rgbe: np.ndarray, rle: bool) -> bytes:
+    """A Radiance file of the given [H, W, 4] RGBE bytes: flat, or with
+    run-length-encoded scanlines (runs of 3 or more equal bytes, dumps of at
+    most 128 between them)."""
+    H, W, _ = rgbe.shape
+    out = bytearray(b"#?RADIANCE\n# seeded test image\nFORMAT=32-bit_rle_rgbe\n\n" + f"-Y {H} +X {W}\n".encode())
+    if not rle:
+        return bytes(out + rgbe.tobytes())
+    for j in range(H):
+        out += bytes([2, 2, W >> 8, W & 255])
+        for k in range(4):
+            row = rgbe[j, :, k]
+            i = 0
+            while i < W:
+                n = 1
+                while i + n < W and n < 127 and row[i + n] == row[i]:
+                    n += 1
+                if n >= 3:
+                    out += bytes([128 + n, int(row[i])])
+                    i += n
+                    continue
+                s0 = i
+                while i < W and i - s0 < 128 and not (i + 2 < W and row[i] == row[i + 1] == row[i + 2]):
+                    i += 1
+                out += bytes([i - s0]) + row[s0:i].tobytes()
+    return bytes(out)
+
+
+def bitmap_cases():
+    """Seeded images in every format the reference's stb_image reads and PIL
+    writes, as file bytes."""
+    import io
+
+    from PIL import Image
+    rng = np.random.default_rng(5)
+    rgb = (np.arange(16 * 16 * 3) % 256).astype(np.uint8).reshape(16, 16, 3)   # every 8-bit value
+    rgb[8:] = rng.integers(0, 256, (8, 16, 3), dtype=np.uint8)
+
+    def enc(img, fmt):
+        b = io.BytesIO()
+        img.save(b, fmt)
+        return b.getvalue()
+
+    cases = {
+        "rgb.png": enc(Image.fromarray(rgb, "RGB"), "PNG"),
+        "gray.png": enc(Image.fromarray(rgb[:, :, 0], "L"), "PNG"),
+        "gray_alpha.png": enc(Image.fromarray(rgb[:, :, :2].copy(), "LA"), "PNG"),
+        "rgba.png": enc(Image.fromarray(np.concatenate([rgb, rgb[:, :, :1]], 2), "RGBA"), "PNG"),
+        "palette.png": enc(Image.fromarray(rgb, "RGB").convert("P"), "PNG"),
+        "gray16.png": enc(Image.fromarray(rng.integers(0, 65536, (8, 8), dtype=np.uint16)), "PNG"),
+        "rgb.bmp": enc(Image.fromarray(rgb, "RGB"), "BMP"),
+        "rgb.tga": enc(Image.fromarray(rgb, "RGB"), "TGA"),
+        "rgb.ppm": enc(Image.fromarray(rgb, "RGB"), "PPM"),
+        "gray.pgm": enc(Image.fromarray(rgb[:, :, 0], "L"), "PPM"),
+        "palette.gif": enc(Image.fromarray(rgb, "RGB").convert("P"), "GIF"),
+        "rgb.jpg": enc(Image.fromarray(rgb, "RGB"), "JPEG"),
+    }
+    e = rng.integers(100, 160, (5, 4, 1), dtype=np.uint8)
+    e[0, 0] = 0
+    flat = np.concatenate([rng.integers(0, 256, (5, 4, 3), dtype=np.uint8), e], 2)
+    cases["flat_w4.hdr"] = _hdr_bytes(flat, False)
+    blocks = np.repeat(np.repeat(rng.integers(0, 256, (3, 4, 4), dtype=np.uint8), 2, 0), 4, 1)   # 6 x 16, runs
+    blocks[..., 3] = np.where(blocks[..., 3] < 8, 0, blocks[..., 3] // 2 + 1)   # low exponents: subnormal scales
+    blocks[1, 3:9] = rng.integers(0, 256, (6, 4), dtype=np.uint8)                # a stretch to dump
+    blocks[4, 0:4] = [[1, 17, 255, 1], [3, 5, 7, 2], [200, 1, 9, 3], [255, 255, 255, 1]]   # subnormal results
+    blocks[5, 4:8, 3] = 0                                                          # exponent 0: black
+    cases["rle_w16.hdr"] = _hdr_bytes(blocks, True)
+    unmarked = np.concatenate([rng.integers(3, 256, (3, 12, 3), dtype=np.uint8),
+                               rng.integers(120, 140, (3, 12, 1), dtype=np.uint8)], 2)
+    cases["unmarked_w12.hdr"] = _hdr_bytes(unmarked, False)
+    return cases
+
+
 def camera_cases():
     cams = [
         ((0.0, 0.0, 4.0), (0.0, 0.0, 0.0), (0.0, 1.0, 0.0), 256, 256, 45.0),
@@ -155,12 +231,19 @@ def main():
             with open(path, "w") as f:
                 f.write(text)
             out["obj"][name] = {"text": text, "reference": _probe("obj", path)}
+    out["bitmap"] = {}
+    with tempfile.TemporaryDirectory() as d:
+        for name, raw in bitmap_cases().items():
+            path = os.path.join(d, name)
+            with open(path, "wb") as f:
+                f.write(raw)
+            out["bitmap"][name] = {"bytes": base64.b64encode(raw).decode(), "reference": _probe("bitmap", path)}
     for pos, tgt, up, w, h, fov in camera_cases():
         args = [repr(float(np.float32(x))) for x in (*pos, *tgt, *up)] + [str(w), str(h), repr(float(fov))]
         out["camera"].append({"args": args, "reference": _probe("camera", *args)})
     with open(OUT, "w") as f:
         json.dump(out, f, separators=(",", ":"))
-    print(f"wrote {OUT}: {len(out['obj'])} meshes, {len(out['camera'])} cameras")
+    print(f"wrote {OUT}: {len(out['obj'])} meshes, {len(out['bitmap'])} images, {len(out['camera'])} cameras")
 
 
 if __name__ == "__main__":

@@ -10,6 +10,12 @@ BaseCamera.cpp and EDXUtil/Math/Matrix.cpp from the reference's sources):
   texture coordinates and the same face indices;
 - edge lists, ObjMesh::processEdges (ObjMesh.cpp:584-632): the oracle's
   build_edges and the library's trn_mesh_edges must give the same rows;
+- texture images, Bitmap::ReadFromFile<float>(path, ..., 3) (Bitmap.cpp:
+  187-190, one stbi_loadf call of stb_image 2.02): scene_xml.load_bitmap must
+  give the same float32 bits for 8-bit PNG, BMP, TGA, PNM and GIF images and
+  for flat, run-length-encoded and unmarked Radiance HDR files, and refuse the
+  16-bit PNG the reference cannot load; JPEG goes through another decoder
+  (libjpeg) and is held to a bound instead;
 - the camera, EDX::Camera::Init (BaseCamera.cpp:45-88) and the quantities the
   renderer's Camera::Resize derives (Camera.cpp:105-137): the library's
   trn_camera_init and the oracle's camera_matrices must agree with it within
@@ -21,6 +27,7 @@ Vec3.h:256-259), whose bits differ between CPU vendors, and inverts its
 matrices in float32; the library and the oracle compute in double and round
 once. The largest difference seen is 3.3e-7 (inv_area).
 """
+import base64
 import json
 import os
 import subprocess
@@ -29,7 +36,7 @@ import numpy as np
 import pytest
 
 from oracle import tr_oracle as O
-from tensorray_b200 import api, scenes
+from tensorray_b200 import api, scene_xml, scenes
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 GOLDEN = os.path.join(HERE, "golden", "edx_pins.json")
@@ -142,6 +149,43 @@ def test_parse_f32_rounds_once_like_strtof():
     assert f[2] == np.float32(0.1) and f[3] == np.float32(-2.5e-3)
 
 
+BITMAPS = ["rgb.png", "gray.png", "gray_alpha.png", "rgba.png", "palette.png", "gray16.png", "rgb.bmp", "rgb.tga",
+           "rgb.ppm", "gray.pgm", "palette.gif", "rgb.jpg", "flat_w4.hdr", "rle_w16.hdr", "unmarked_w12.hdr"]
+
+
+@pytest.mark.parametrize("name", BITMAPS)
+def test_texture_images_match_reference_bits(pins, tmp_path, name):
+    case = pins["bitmap"][name]
+    r = case["reference"]
+    path = tmp_path / name
+    path.write_bytes(base64.b64decode(case["bytes"]))
+    if "error" in r:
+        with pytest.raises(scene_xml.SceneXmlError):
+            scene_xml.load_bitmap(str(path))
+        return
+    ref = _f32(r["texels"]).reshape(r["height"], r["width"], 3)
+    got = scene_xml.load_bitmap(str(path))
+    assert got.dtype == np.float32 and got.shape == ref.shape
+    if name.endswith(".jpg"):
+        # libjpeg's IDCT and chroma upsampling are not stb_image's
+        d = np.abs(got.astype(np.float64) - ref)
+        assert d.max() <= 0.03 and d.mean() <= 2e-3, (d.max(), d.mean())
+    else:
+        assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
+
+
+def test_hdr_fixtures_cover_the_decoder_paths(pins):
+    raw = {n: base64.b64decode(pins["bitmap"][n]["bytes"]) for n in ("flat_w4.hdr", "rle_w16.hdr",
+                                                                      "unmarked_w12.hdr")}
+    body = {n: b[b.index(b"+X"):].split(b"\n", 1)[1] for n, b in raw.items()}
+    assert body["rle_w16.hdr"][:4] == bytes([2, 2, 0, 16])
+    assert body["unmarked_w12.hdr"][:2] != bytes([2, 2])
+    ref = _f32(pins["bitmap"]["rle_w16.hdr"]["reference"]["texels"])
+    tiny = ref[(ref > 0) & (ref < np.finfo(np.float32).tiny)]
+    assert tiny.size > 0          # subnormal results from the low exponents
+    assert (ref == 0).any()       # exponent 0 is black
+
+
 def _rel(a, r):
     a = np.asarray(a, np.float64).reshape(-1)
     r = np.asarray(r, np.float64).reshape(-1)
@@ -184,6 +228,12 @@ def test_fixture_is_what_the_reference_computes(pins, tmp_path):
                 assert np.array_equal(np.asarray(live[k])[keep], np.asarray(v)[keep]), name
             else:
                 assert live[k] == v, (name, k)
+    for name, case in pins["bitmap"].items():
+        path = tmp_path / name
+        path.write_bytes(base64.b64decode(case["bytes"]))
+        live = json.loads(subprocess.run([PROBE, "bitmap", str(path)], capture_output=True, text=True,
+                                         check=True).stdout)
+        assert live == case["reference"], name
     for case in pins["camera"]:
         live = json.loads(subprocess.run([PROBE, "camera", *case["args"]], capture_output=True, text=True,
                                          check=True).stdout)
