@@ -2905,15 +2905,24 @@ __global__ void k_occluded(DeviceScene s, int n, const float* org, const float* 
 
 using namespace trn;
 
+// Pinned staging slots of a view set's table uploads. An upload waits only
+// for the upload this many before it to have left its slot, so a loop that
+// changes its views every call (a serving loop) runs that many uploads ahead
+// of the device instead of waiting for the previous call's kernels.
+constexpr int kStageRing = 4;
+
 // A set of camera views rendered by one launch per integrator: the device view
 // table plus per-view silhouette-edge workspace.
 struct trn_viewset {
   trn_scene* scene = nullptr;
   int nviews = 0;
   int cap = 0;                    // allocated view capacity
-  ViewDesc* h_stage = nullptr;    // pinned staging of the view table
+  // pinned staging of the view table: kStageRing slots of `cap` views and
+  // 2 * `cap` offsets (view begins, then pixel begins) each
+  ViewDesc* h_stage = nullptr;
   long long* h_stage_begin = nullptr;
-  cudaEvent_t copy_done = nullptr;
+  cudaEvent_t stage_done[kStageRing] = {};
+  int stage_next = 0;
   bool pbegin_dirty = true;
   long long npix = 0;
   std::vector<trn_view> h_views;
@@ -2981,6 +2990,20 @@ int spp_of(const trn_render_options* o, int integrator) {
 
 // Upload the view table for one integrator: per-view spp comes from the view
 // (spp_override < 0) or from the options (single-view calls).
+// The next staging slot, once the upload that last used it has left it.
+int next_stage(trn_viewset* vs) {
+  const int k = vs->stage_next;
+  vs->stage_next = (k + 1) % kStageRing;
+  if (vs->stage_done[k]) cudaEventSynchronize(vs->stage_done[k]);
+  return k;
+}
+
+// Every staging slot free (before the staging is freed or reallocated).
+void wait_stages(trn_viewset* vs) {
+  for (cudaEvent_t e : vs->stage_done)
+    if (e) cudaEventSynchronize(e);
+}
+
 int upload_views(trn_viewset* vs, const trn_render_options* o, int integrator, int spp_override, long long& total,
                  cudaStream_t st) {
   (void)o;
@@ -3005,9 +3028,9 @@ int upload_views(trn_viewset* vs, const trn_render_options* o, int integrator, i
   for (int v = 0; v < vs->nviews; v++)
     vs->max_depth = std::max(vs->max_depth, vs->h_views[v].max_bounces > 0 ? vs->h_views[v].max_bounces
                                                                             : o->max_bounces);
-  if (vs->copy_done) cudaEventSynchronize(vs->copy_done);  // previous upload has left the staging buffer
-  ViewDesc* d = vs->h_stage;
-  long long* begin = vs->h_stage_begin;
+  const int slot = next_stage(vs);
+  ViewDesc* d = vs->h_stage + (size_t)slot * vs->cap;
+  long long* begin = vs->h_stage_begin + (size_t)slot * 2 * vs->cap;
   total = 0;
   for (int v = 0; v < vs->nviews; v++) {
     const trn_view& hv = vs->h_views[v];
@@ -3040,7 +3063,7 @@ int upload_views(trn_viewset* vs, const trn_render_options* o, int integrator, i
   }
   TRN_CUDA_TRY(cudaMemcpyAsync(vs->views, d, sizeof(ViewDesc) * vs->nviews, cudaMemcpyHostToDevice, st));
   TRN_CUDA_TRY(cudaMemcpyAsync(vs->vbegin, begin, sizeof(long long) * vs->nviews, cudaMemcpyHostToDevice, st));
-  TRN_CUDA_TRY(cudaEventRecord(vs->copy_done, st));
+  TRN_CUDA_TRY(cudaEventRecord(vs->stage_done[slot], st));
   vs->uploaded_key = key;
   vs->total = total;
   return 0;
@@ -3686,8 +3709,8 @@ int set_views(trn_viewset* vs, int nviews, const trn_view* views) {
     pb.push_back(off);
     pix = std::max(pix, off + (long long)hv.camera.width * hv.camera.height);
   }
-  if (vs->copy_done) cudaEventSynchronize(vs->copy_done);  // staging buffers are free again
   if (nviews > vs->cap) {
+    wait_stages(vs);
     void* old[] = {vs->views, vs->vbegin, vs->pbegin, vs->pfunc, vs->pcdf, vs->pint};
     for (void* q : old) if (q) cudaFree(q);
     if (vs->h_stage) cudaFreeHost(vs->h_stage);
@@ -3699,8 +3722,8 @@ int set_views(trn_viewset* vs, int nviews, const trn_view* views) {
               cudaMalloc(&vs->vbegin, sizeof(long long) * cap) == cudaSuccess &&
               cudaMalloc(&vs->pbegin, sizeof(long long) * cap) == cudaSuccess &&
               cudaMalloc(&vs->pint, sizeof(float) * cap) == cudaSuccess &&
-              cudaMallocHost(&vs->h_stage, sizeof(ViewDesc) * cap) == cudaSuccess &&
-              cudaMallocHost(&vs->h_stage_begin, sizeof(long long) * 2 * cap) == cudaSuccess;
+              cudaMallocHost(&vs->h_stage, sizeof(ViewDesc) * cap * kStageRing) == cudaSuccess &&
+              cudaMallocHost(&vs->h_stage_begin, sizeof(long long) * 2 * cap * kStageRing) == cudaSuccess;
     if (ok && vs->ne > 0)
       ok = cudaMalloc(&vs->pfunc, sizeof(float) * (size_t)cap * vs->ne) == cudaSuccess &&
            cudaMalloc(&vs->pcdf, sizeof(float) * (size_t)cap * vs->ne) == cudaSuccess;
@@ -3720,18 +3743,18 @@ int set_views(trn_viewset* vs, int nviews, const trn_view* views) {
 // upload the per-view pixel offsets (used by the loss kernel) when they changed
 int upload_pbegin(trn_viewset* vs, cudaStream_t st) {
   if (!vs->pbegin_dirty) return 0;
-  if (vs->copy_done) cudaEventSynchronize(vs->copy_done);
-  long long* stage = vs->h_stage_begin + vs->cap;
+  const int slot = next_stage(vs);
+  long long* stage = vs->h_stage_begin + (size_t)slot * 2 * vs->cap + vs->cap;
   std::memcpy(stage, vs->h_pbegin.data(), sizeof(long long) * vs->nviews);
   TRN_CUDA_TRY(cudaMemcpyAsync(vs->pbegin, stage, sizeof(long long) * vs->nviews, cudaMemcpyHostToDevice, st));
-  TRN_CUDA_TRY(cudaEventRecord(vs->copy_done, st));
+  TRN_CUDA_TRY(cudaEventRecord(vs->stage_done[slot], st));
   vs->pbegin_dirty = false;
   return 0;
 }
 
 // The scene's cached one-view set, re-pointed at `cam`: the first call
-// allocates it, later calls only restage the view table (pinned staging,
-// guarded by the set's copy event), so single-view calls neither allocate nor
+// allocates it, later calls only restage the view table (a pinned slot of
+// the set's staging ring), so single-view calls neither allocate nor
 // synchronise the stream.
 int single_view(trn_scene* s, const trn_camera* cam, trn_viewset** out) {
   if (!cam) { set_error("null camera"); return -1; }
@@ -3762,8 +3785,9 @@ int trn_viewset_create(trn_scene* s, int nviews, const trn_view* views, trn_view
   trn_viewset* vs = new trn_viewset();
   vs->scene = s;
   vs->ne = s->ne;
-  if (cudaMalloc(&vs->work, sizeof(unsigned long long)) != cudaSuccess ||
-      cudaEventCreateWithFlags(&vs->copy_done, cudaEventDisableTiming) != cudaSuccess) {
+  bool ok = cudaMalloc(&vs->work, sizeof(unsigned long long)) == cudaSuccess;
+  for (cudaEvent_t& e : vs->stage_done) ok = ok && cudaEventCreateWithFlags(&e, cudaEventDisableTiming) == cudaSuccess;
+  if (!ok) {
     set_error("trn_viewset_create: out of memory");
     trn_viewset_destroy(vs);
     return -1;
@@ -3780,13 +3804,14 @@ int trn_viewset_update(trn_viewset* vs, int nviews, const trn_view* views) {
 
 int trn_viewset_destroy(trn_viewset* vs) {
   if (!vs) return 0;
-  if (vs->copy_done) cudaEventSynchronize(vs->copy_done);
+  wait_stages(vs);
   void* ptrs[] = {vs->views, vs->vbegin, vs->pbegin, vs->pfunc, vs->pcdf, vs->pint, vs->work, vs->iq, vs->iq_count, vs->sq, vs->pc, vs->pc_count};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (vs->h_stage) cudaFreeHost(vs->h_stage);
   if (vs->h_stage_begin) cudaFreeHost(vs->h_stage_begin);
-  if (vs->copy_done) cudaEventDestroy(vs->copy_done);
+  for (cudaEvent_t e : vs->stage_done)
+    if (e) cudaEventDestroy(e);
   delete vs;
   return 0;
 }
@@ -3810,7 +3835,7 @@ int trn_viewset_path_cache(trn_viewset* vs, long long max_bytes) {
   vs->pc_limit = max_bytes;
   vs->pc_valid = false;
   if (max_bytes == 0 && vs->pc) {
-    if (vs->copy_done) cudaEventSynchronize(vs->copy_done);
+    wait_stages(vs);
     TRN_CUDA_TRY(cudaDeviceSynchronize());
     cudaFree(vs->pc);
     vs->pc = nullptr;
