@@ -466,11 +466,20 @@ class ViewSet:
         npix = C.c_longlong()
         check(scene._lib.trn_viewset_num_pixels(self._h, C.byref(npix)), "trn_viewset_num_pixels")
         self.npix = npix.value
-        self.offsets = []
-        off = 0
-        for c in cameras:
-            self.offsets.append(off)
-            off += c.width * c.height
+        self.offsets = self._offsets(arr, n)
+
+    @staticmethod
+    def _offsets(arr, n: int) -> list:
+        """First pixel of each view in the concatenated image, as the library
+        places them (set_views): a view's own pixel_offset when it gives one,
+        else right after the views before it."""
+        offs, pix = [], 0
+        for i in range(n):
+            v = arr[i]
+            off = int(v.pixel_offset) if v.pixel_offset >= 0 else pix
+            offs.append(off)
+            pix = max(pix, off + int(v.camera.width) * int(v.camera.height))
+        return offs
 
     def __del__(self):
         try:
@@ -487,6 +496,7 @@ class ViewSet:
         npix = C.c_longlong()
         check(self.scene._lib.trn_viewset_num_pixels(self._h, C.byref(npix)), "trn_viewset_num_pixels")
         self.npix = npix.value
+        self.offsets = self._offsets(views, len(cameras))
         self.cameras = list(cameras)
         self.spps = [int(x) for x in spps]
 

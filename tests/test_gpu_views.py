@@ -5,6 +5,7 @@ import torch
 
 from oracle import tr_oracle as O
 from tensorray_b200 import api, scenes
+from tensorray_b200._abi import TrnView
 from tests.helpers import rel_l2
 
 pytestmark = pytest.mark.gpu
@@ -27,6 +28,41 @@ def _tables(integ, cams, spps, seed):
     per = [O.uniform_table(seed + 17 * i, api.sample_dims(integ, D), api.sample_slots(integ, c.width, c.height, s))
            for i, (c, s) in enumerate(zip(cams, spps))]
     return per, torch.cat(per, 1).contiguous()
+
+
+def test_updates_every_call_run_ahead_of_the_device(setup):
+    """A set whose views change on every call, as in the serving loop, stages
+    each table upload in its own pinned slot. Renders and losses issued back
+    to back with no synchronisation between them, more of them than there are
+    slots and with one growth of the set in between, give the images and
+    losses of fresh sets of the same views."""
+    scene, cams, spps = setup
+    opts = api.RenderOptions(5, D, 0, 0, 0, 0, 0)
+    plan = [[0], [1, 2], [3, 4, 0], [2], [4, 1], [0, 3], [1], [2, 3, 4], [0, 1, 2, 3, 4], [3], [4, 2], [1]]
+
+    def pick(idx):
+        arr = (TrnView * len(idx))()
+        for j, v in enumerate(idx):
+            arr[j] = TrnView(cams[v].c, spps[v], 100 + v, -1, 0, 0.0, 0, None, None, None, None, None)
+        return [cams[v] for v in idx], [spps[v] for v in idx], arr
+
+    vs = api.ViewSet(scene, *pick(plan[2])[:2], seeds=[100 + v for v in plan[2]])
+    out = []
+    for idx in plan:
+        c, s, arr = pick(idx)
+        vs.update(c, s, arr)
+        img = vs.render(0, opts)
+        loss = vs.loss(img, torch.zeros_like(img))
+        out.append((idx, img, loss, [vs.view_image(img, j) for j in range(len(idx))]))
+    torch.cuda.synchronize()
+    for idx, img, loss, views in out:
+        c, s, _ = pick(idx)
+        fresh = api.ViewSet(scene, c, s, seeds=[100 + v for v in idx])
+        ref = fresh.render(0, opts)
+        torch.testing.assert_close(img, ref, rtol=1e-5, atol=1e-6)
+        torch.testing.assert_close(loss, fresh.loss(ref, torch.zeros_like(ref)), rtol=1e-5, atol=1e-6)
+        for j in range(len(idx)):
+            torch.testing.assert_close(views[j], fresh.view_image(ref, j), rtol=1e-5, atol=1e-6)
 
 
 def test_batched_forward_equals_per_view(setup):
