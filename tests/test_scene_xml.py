@@ -116,3 +116,60 @@ def test_parse_vector_repeats_the_last_component():
     np.testing.assert_array_equal(scene_xml.parse_vector("1, 2 3"), [1, 2, 3])
     with pytest.raises(scene_xml.SceneXmlError):
         scene_xml.parse_vector("1 2")
+
+
+def _hdr(rows, header=b"FORMAT=32-bit_rle_rgbe\n", res=None, body=None):
+    """A flat Radiance file of the given RGBE rows."""
+    a = np.asarray(rows, np.uint8)
+    H, W = a.shape[:2]
+    res = res if res is not None else f"-Y {H} +X {W}\n".encode()
+    return b"#?RADIANCE\n" + header + b"\n" + res + (a.tobytes() if body is None else body)
+
+
+def test_radiance_textures_load_linear_and_through_xml(tmp_path):
+    d = str(tmp_path)
+    # (r, g, b, e): value = c * 2^(e - 136); e = 0 is black
+    rows = [[[128, 64, 32, 129], [255, 0, 1, 136], [9, 9, 9, 0]]]
+    with open(os.path.join(d, "sky.hdr"), "wb") as f:
+        f.write(_hdr(rows))
+    t = scene_xml.load_bitmap(os.path.join(d, "sky.hdr"))
+    assert t.dtype == np.float32 and t.shape == (1, 3, 3)
+    np.testing.assert_array_equal(t[0, 0], np.float32([128, 64, 32]) * np.float32(2.0 ** -7))
+    np.testing.assert_array_equal(t[0, 1], np.float32([255, 0, 1]))
+    np.testing.assert_array_equal(t[0, 2], np.zeros(3, np.float32))
+    P = np.array([[0, 0, 0], [1, 0, 0], [1, 1, 0]], np.float32)
+    write_obj(os.path.join(d, "tri.obj"), P, np.array([[0, 1, 2]]), uv=P[:, :2])
+    with open(os.path.join(d, "s.xml"), "w") as f:
+        f.write('<scene><bsdf type="diffuse" id="t"><texture type="bitmap" name="reflectance">'
+                '<string name="filename" value="sky.hdr"/></texture></bsdf>'
+                '<shape type="obj"><string name="filename" value="tri.obj"/><ref id="t"/></shape></scene>')
+    spec = scene_xml.load_xml(os.path.join(d, "s.xml"))
+    np.testing.assert_array_equal(spec.textures[0], t)
+
+
+@pytest.mark.parametrize("raw, msg", [
+    (_hdr([[[1, 2, 3, 130]]], header=b"FORMAT=32-bit_rle_xyze\n"), "unsupported HDR format"),
+    (_hdr([[[1, 2, 3, 130]]], res=b"+Y 1 +X 1\n"), "unsupported HDR data layout"),
+    (_hdr([[[1, 2, 3, 130]] * 2], body=b"\x01\x02\x03"), "truncated HDR data"),
+    # an RLE scanline whose length field disagrees with the width
+    (_hdr([[[0, 0, 0, 0]] * 8], body=bytes([2, 2, 0, 9]) + bytes(64)), "invalid decoded scanline length"),
+    # a dump of zero bytes (stb would loop on it) and a run past the scanline's end
+    (_hdr([[[0, 0, 0, 0]] * 8], body=bytes([2, 2, 0, 8, 0])), "corrupt HDR dump"),
+    (_hdr([[[0, 0, 0, 0]] * 8], body=bytes([2, 2, 0, 8, 128 + 9, 5])), "corrupt HDR run"),
+])
+def test_radiance_errors(tmp_path, raw, msg):
+    path = os.path.join(str(tmp_path), "bad.hdr")
+    with open(path, "wb") as f:
+        f.write(raw)
+    with pytest.raises(scene_xml.SceneXmlError, match=msg):
+        scene_xml.load_bitmap(path)
+
+
+def test_images_the_reference_cannot_load_are_refused(tmp_path):
+    from PIL import Image
+    d = str(tmp_path)
+    Image.fromarray(np.arange(16, dtype=np.uint16).reshape(4, 4) * 4000).save(os.path.join(d, "g16.png"))
+    Image.fromarray(np.zeros((4, 4, 3), np.uint8)).save(os.path.join(d, "t.tiff"))
+    for name, msg in [("g16.png", "16-bit PNGs"), ("t.tiff", "TIFF")]:
+        with pytest.raises(scene_xml.SceneXmlError, match=msg):
+            scene_xml.load_bitmap(os.path.join(d, name))
