@@ -280,7 +280,11 @@ int trn_render_grad_noalloc(trn_scene* scene, const trn_camera* camera, const tr
 int trn_viewset_create(trn_scene* scene, int nviews, const trn_view* views, trn_viewset** out);
 int trn_viewset_destroy(trn_viewset* views);
 /* Replace the views of a set (storage grows as needed; a serving loop
- * re-uses one set per scene and phase). */
+ * re-uses one set per scene and phase). The next render call uploads the new
+ * table on its stream from one of four pinned staging slots, so a caller that
+ * changes the views on every call runs up to four calls ahead of the device;
+ * only a growth of the set waits for the uploads in flight. Successive calls
+ * on one set must use one stream (the table is rewritten in stream order). */
 int trn_viewset_update(trn_viewset* views, int nviews, const trn_view* view_array);
 int trn_viewset_num_pixels(const trn_viewset* views, long long* npix);
 /* Allocate the set's round buffers now: the queue of the split integrator
