@@ -107,14 +107,62 @@ class Camera:
                 "width": c.width, "height": c.height}
 
 
+def _host_f32(x) -> torch.Tensor:
+    """A float32 CPU tensor of a tensor (any device), array or sequence."""
+    if isinstance(x, torch.Tensor):
+        return x.detach().to("cpu", torch.float32)
+    return torch.as_tensor(np.asarray(x, np.float32))
+
+
+def rotation_axis_angle(angle, axis, derivative: bool = False) -> torch.Tensor:
+    """CalcRotateAxisAngle (Renderer/Utils.cpp:200-232): the right-handed
+    rotation by `angle` radians about the normalised `axis`, a 3x3 matrix on
+    column vectors, c I + s [k]x + (1 - c) k k^T. With derivative=True its
+    derivative with respect to the angle, -s I + c [k]x + s k k^T."""
+    k = _host_f32(axis).reshape(3)
+    k = k / torch.linalg.vector_norm(k)
+    a = _host_f32(angle).reshape(())
+    s, c = torch.sin(a), torch.cos(a)
+    K = torch.zeros(3, 3)
+    K[0, 1], K[0, 2], K[1, 0], K[1, 2], K[2, 0], K[2, 1] = -k[2], k[1], k[2], -k[0], -k[1], k[0]
+    kk = torch.outer(k, k)
+    eye = torch.eye(3)
+    if derivative:
+        return -s * eye + c * K + s * kk
+    return c * eye + s * K + (1.0 - c) * kk
+
+
 class Shape:
-    """Primitive parameters (Primitive.cpp:374-388)."""
+    """Primitive parameters (Primitive.cpp:374-388), and its rotations
+    (Primitive::Configure, Primitive.cpp:158-189):
+
+    - rotate_matrix (3x3 or 4x4, p' = M p on column vectors) with obj_center c:
+      the fixed pose rotation of multi-pose optimisation, p' = M (p - c) + c.
+      The reference's own pose tensors (pyTensorRay/multi_pose.py:53-64) pack
+      a row-major matrix into its column layout, so a pose built there from
+      `mat` is `mat.reshape(3, 3).T` here.
+    - diff_rotation(axis) with rotate_angle: a differentiable rotation about
+      the world origin, applied after the pose; dL/d(angle) comes back from
+      Scene.get_grads() as "rotation_angle".
+
+    Translation is applied last. The reference applies the pose in object
+    space, before the shape's XML to_world; here meshes are held in world
+    space, so the two agree for shapes without a to_world transform."""
 
     def __init__(self, scene: "Scene", index: int, vstart: int, vcount: int, fcount: int):
         self._scene, self.index = scene, index
         self._vstart, self._vcount, self._fcount = vstart, vcount, fcount
         self.requires_translation_grad = False
         self.requires_vertex_grad = False
+        self.requires_rotation_grad = False
+        self._rotate_matrix = None
+        self._obj_center = None
+        self._rotate_axis = None
+        self._rotate_angle = 0.0
+
+    def _changed(self) -> None:
+        if self._scene is not None:
+            self._scene._dirty = True
 
     @property
     def translation(self) -> torch.Tensor:
@@ -126,11 +174,75 @@ class Shape:
                                                                device=self._scene.device).reshape(3)
         self._scene._dirty = True
 
+    @property
+    def rotate_matrix(self):
+        return self._rotate_matrix
+
+    @rotate_matrix.setter
+    def rotate_matrix(self, m) -> None:
+        if m is not None:
+            m = _host_f32(m)
+            if m.shape not in ((3, 3), (4, 4)):
+                raise RuntimeError("rotate_matrix must be 3x3 or 4x4")
+            m = m[:3, :3].clone()
+        self._rotate_matrix = m
+        self._changed()
+
+    @property
+    def obj_center(self):
+        return self._obj_center
+
+    @obj_center.setter
+    def obj_center(self, c) -> None:
+        self._obj_center = None if c is None else _host_f32(c).reshape(3).clone()
+        self._changed()
+
+    @property
+    def rotate_axis(self):
+        return self._rotate_axis
+
+    @rotate_axis.setter
+    def rotate_axis(self, axis) -> None:
+        self._rotate_axis = None if axis is None else tuple(float(x) for x in _host_f32(axis).reshape(3))
+        self._changed()
+
+    @property
+    def rotate_angle(self) -> float:
+        return self._rotate_angle
+
+    @rotate_angle.setter
+    def rotate_angle(self, a) -> None:
+        self._rotate_angle = float(a)
+        self._changed()
+
     def diff_translation(self) -> None:
         self.requires_translation_grad = True
 
     def diff_all_vertex_pos(self) -> None:
         self.requires_vertex_grad = True
+
+    def diff_rotation(self, rotate_axis) -> None:
+        """Primitive::DiffRotation (Primitive.cpp:379-383): rotate about
+        `rotate_axis` by an angle that starts at 0 and is differentiated."""
+        self.rotate_axis = rotate_axis
+        self.rotate_angle = 0.0
+        self.requires_rotation_grad = True
+
+    def get_obj_center(self) -> torch.Tensor:
+        """Primitive::GetObjCenter (Primitive.cpp:444-450): the centre of the
+        shape's bounding box over its unrotated positions."""
+        p = self._scene._raw_positions[self.vertex_slice()]
+        return (0.5 * (p.min(0).values + p.max(0).values)).cpu()
+
+    def _rotations(self):
+        """(pose matrix or None, centre, rotation matrix or None, its
+        derivative or None), on the CPU."""
+        c = self._obj_center if self._obj_center is not None else torch.zeros(3)
+        if self._rotate_axis is None:
+            return self._rotate_matrix, c, None, None
+        return (self._rotate_matrix, c, rotation_axis_angle(self._rotate_angle, self._rotate_axis),
+                rotation_axis_angle(self._rotate_angle, self._rotate_axis, derivative=True))
+
 
     def get_vertex_count(self) -> int:
         return self._vcount
@@ -140,6 +252,52 @@ class Shape:
 
     def vertex_slice(self) -> slice:
         return slice(self._vstart, self._vstart + self._vcount)
+
+
+def posed_positions(raw: torch.Tensor, shapes: list):
+    """The positions the library transforms (world = these + translation):
+    each shape's raw positions through its pose, p' = M (p - c) + c, then its
+    differentiable rotation, R p'. None when no shape is rotated."""
+    rotated = [s for s in shapes if s._rotate_matrix is not None or s._rotate_axis is not None]
+    if not rotated:
+        return None
+    out = raw.clone()
+    for s in rotated:
+        M, c, R, _ = s._rotations()
+        sl = s.vertex_slice()
+        q = raw[sl]
+        if M is not None:
+            cd = c.to(q.device)
+            q = (q - cd) @ M.to(q.device).T + cd
+        if R is not None:
+            q = q @ R.to(q.device).T
+        out[sl] = q
+    return out
+
+
+def pose_grads(raw: torch.Tensor, grad: torch.Tensor, shapes: list):
+    """Chain rule through posed_positions. `grad` is dL/d(posed positions);
+    returns dL/d(raw positions) (rows of rotated shapes through R and M) and
+    dL/d(rotate_angle) per shape (0 for shapes without diff_rotation)."""
+    out = grad.clone()
+    d_angle = torch.zeros(len(shapes), device=grad.device)
+    for i, s in enumerate(shapes):
+        M, c, R, dR = s._rotations()
+        if M is None and R is None:
+            continue
+        sl = s.vertex_slice()
+        g = grad[sl]
+        q = raw[sl]
+        if M is not None:
+            cd = c.to(q.device)
+            q = (q - cd) @ M.to(q.device).T + cd
+        if R is not None:
+            d_angle[i] = (g * (q @ dR.to(q.device).T)).sum()
+            g = g @ R.to(g.device)
+        if M is not None:
+            g = g @ M.to(g.device)
+        out[sl] = g
+    return out, d_angle
 
 
 class BSDF:
@@ -250,7 +408,10 @@ class Scene:
         st = C.c_void_p(_stream())
         check(self._lib.trn_scene_set_translation(self._h, C.c_void_p(self._translation.data_ptr()), st),
               "trn_scene_set_translation")
-        check(self._lib.trn_scene_set_positions(self._h, C.c_void_p(self._raw_positions.data_ptr()), st),
+        # rotated shapes upload their posed positions (kept alive for the copy)
+        posed = posed_positions(self._raw_positions, self.shapes)
+        self._posed = posed if posed is not None else self._raw_positions
+        check(self._lib.trn_scene_set_positions(self._h, C.c_void_p(self._posed.data_ptr()), st),
               "trn_scene_set_positions")
         if refit:
             check(self._lib.trn_scene_refit(self._h, st), "trn_scene_refit")
@@ -287,7 +448,9 @@ class Scene:
     # -- gradients ---------------------------------------------------------------
     def get_grads(self, clear: bool = True) -> dict:
         """Finish the geometry adjoint and return dL/d(translation per mesh),
-        dL/d(raw vertex positions), dL/d(texels) (get_grad, pybind_utils.h:133-142)."""
+        dL/d(raw vertex positions), dL/d(texels) (get_grad, pybind_utils.h:133-142),
+        and, when a shape asked for it (diff_rotation), dL/d(rotate_angle) per
+        mesh as "rotation_angle"."""
         d = self.device
         gt = torch.zeros(self.num_meshes, 3, device=d)
         gp = torch.zeros(self.num_vertices, 3, device=d)
@@ -295,7 +458,12 @@ class Scene:
         check(self._lib.trn_scene_get_grads(self._h, C.c_void_p(gt.data_ptr()), C.c_void_p(gp.data_ptr()),
                                             C.c_void_p(gx.data_ptr()), int(clear), C.c_void_p(_stream())),
               "trn_scene_get_grads")
-        return {"translation": gt, "positions": gp, "texels": gx[: self.num_texels]}
+        out = {"translation": gt, "positions": gp, "texels": gx[: self.num_texels]}
+        if any(s._rotate_matrix is not None or s._rotate_axis is not None for s in self.shapes):
+            out["positions"], d_angle = pose_grads(self._raw_positions, gp, self.shapes)
+            if any(s.requires_rotation_grad for s in self.shapes):
+                out["rotation_angle"] = d_angle
+        return out
 
     def set_path_cache(self, max_bytes: int) -> None:
         """Bound (bytes; 0 = off; default 16 GiB) on the path records that the

@@ -1,0 +1,97 @@
+"""Shape rotations on the host, on the CPU: the axis-angle matrix of
+CalcRotateAxisAngle (Renderer/Utils.cpp:200-232), the pose and the
+differentiable rotation of Primitive::Configure (Primitive.cpp:158-189) as
+api.posed_positions applies them, and the chain rule of api.pose_grads
+against torch autograd of the same composition."""
+from types import SimpleNamespace
+
+import numpy as np
+import pytest
+import torch
+from scipy.spatial.transform import Rotation
+
+from tensorray_b200 import api
+
+
+def _reference_columns(angle, axis):
+    """The three columns CalcRotateAxisAngle writes (Utils.cpp:210-229)."""
+    x, y, z = np.asarray(axis, np.float64) / np.linalg.norm(axis)
+    s, c = np.sin(angle), np.cos(angle)
+    c0 = [x * x + (1 - x * x) * c, x * y * (1 - c) + z * s, x * z * (1 - c) - y * s]
+    c1 = [x * y * (1 - c) - z * s, y * y + (1 - y * y) * c, y * z * (1 - c) + x * s]
+    c2 = [x * z * (1 - c) + y * s, y * z * (1 - c) - x * s, z * z + (1 - z * z) * c]
+    return np.stack([c0, c1, c2], 1)
+
+
+@pytest.mark.parametrize("angle, axis", [(0.3, (0, 1, 0)), (-1.2, (1, 2, 3)), (2.9, (0.5, -0.2, 0.1))])
+def test_axis_angle_matrix(angle, axis):
+    R = api.rotation_axis_angle(angle, axis).double().numpy()
+    np.testing.assert_allclose(R, _reference_columns(angle, axis), atol=1e-6)   # float32 evaluation
+    rv = np.asarray(axis, np.float64) / np.linalg.norm(axis) * angle
+    np.testing.assert_allclose(R, Rotation.from_rotvec(rv).as_matrix(), atol=1e-6)
+    h = 1e-3
+    fd = (_reference_columns(angle + h, axis) - _reference_columns(angle - h, axis)) / (2 * h)
+    np.testing.assert_allclose(api.rotation_axis_angle(angle, axis, derivative=True).double().numpy(), fd,
+                               atol=1e-5)
+
+
+def _scene_with(raw, sizes):
+    sc = SimpleNamespace(_dirty=False, _raw_positions=raw, device=raw.device)
+    shapes, v = [], 0
+    for i, n in enumerate(sizes):
+        shapes.append(api.Shape(sc, i, v, n, 0))
+        v += n
+    sc.shapes = shapes
+    return sc, shapes
+
+
+def test_unrotated_shapes_upload_their_raw_positions():
+    raw = torch.randn(10, 3)
+    _, shapes = _scene_with(raw, [4, 6])
+    assert api.posed_positions(raw, shapes) is None
+    g = torch.randn(10, 3)
+    gp, da = api.pose_grads(raw, g, shapes)
+    assert torch.equal(gp, g) and torch.equal(da, torch.zeros(2))
+
+
+def test_pose_and_rotation_and_their_chain_rule():
+    torch.manual_seed(0)
+    raw = torch.randn(30, 3, dtype=torch.float32)
+    sc, shapes = _scene_with(raw, [10, 12, 8])
+    M = torch.as_tensor(Rotation.from_rotvec([0.2, -0.7, 0.4]).as_matrix(), dtype=torch.float32)
+    shapes[0].rotate_matrix = M
+    shapes[0].obj_center = shapes[0].get_obj_center()
+    assert sc._dirty
+    shapes[1].diff_rotation((1.0, 0.5, -0.25))
+    shapes[1].rotate_angle = 0.4
+    shapes[2].rotate_matrix = np.eye(4)                   # 4x4 input, identity pose
+    shapes[2].diff_rotation(torch.tensor([0.0, 0.0, 2.0]))
+    posed = api.posed_positions(raw, shapes)
+
+    # the same composition, written out and differentiated by autograd
+    p = raw.clone().requires_grad_(True)
+    th = torch.tensor([0.0, 0.4, 0.0], requires_grad=True)
+    c0 = 0.5 * (raw[:10].min(0).values + raw[:10].max(0).values)
+    parts = [(p[:10] - c0) @ M.T + c0]
+    for sl, i, axis in ((slice(10, 22), 1, (1.0, 0.5, -0.25)), (slice(22, 30), 2, (0.0, 0.0, 1.0))):
+        k = torch.tensor(axis) / torch.linalg.vector_norm(torch.tensor(axis))
+        K = torch.zeros(3, 3)
+        K[0, 1], K[0, 2], K[1, 0], K[1, 2], K[2, 0], K[2, 1] = -k[2], k[1], k[2], -k[0], -k[1], k[0]
+        R = torch.cos(th[i]) * torch.eye(3) + torch.sin(th[i]) * K + (1 - torch.cos(th[i])) * torch.outer(k, k)
+        parts.append(p[sl] @ R.T)
+    world = torch.cat(parts)
+    torch.testing.assert_close(posed, world.detach(), rtol=1e-6, atol=1e-6)
+
+    w = torch.randn(30, 3)
+    (world * w).sum().backward()
+    gp, da = api.pose_grads(raw, w, shapes)
+    torch.testing.assert_close(gp, p.grad, rtol=1e-5, atol=1e-5)
+    torch.testing.assert_close(da[1:], th.grad[1:], rtol=1e-5, atol=1e-5)
+    assert da[0] == 0.0
+
+
+def test_rotate_matrix_checks_its_shape():
+    raw = torch.zeros(3, 3)
+    _, shapes = _scene_with(raw, [3])
+    with pytest.raises(RuntimeError, match="3x3 or 4x4"):
+        shapes[0].rotate_matrix = np.eye(2)
