@@ -250,8 +250,56 @@ class Shape:
     def get_face_count(self) -> int:
         return self._fcount
 
+    def _faces(self) -> np.ndarray:
+        return np.ascontiguousarray(self._scene.spec.meshes[self.index].faces, np.int32).reshape(-1, 3)
+
+    def get_face_indices(self, out=None) -> np.ndarray:
+        """Primitive::GetFaceIndices (Primitive.cpp:419-433): the shape's
+        triangles as vertex indices local to the shape, 3 per face. The
+        reference writes them through a pointer; here they are returned, and
+        copied into `out` (an array or tensor of 3 * faces ints) when given."""
+        f = self._faces().reshape(-1)
+        return _fill(out, f)
+
+    def get_edge_count(self) -> int:
+        """Primitive::GetEdgeCount (Primitive.cpp:400-403): the edges
+        ObjMesh::processEdges finds in the shape's mesh."""
+        return int(len(mesh_edges(self._faces())))
+
+    def get_edge_data(self, out=None) -> np.ndarray:
+        """Primitive::GetEdgeData (Primitive.cpp:435-442): the first vertex of
+        every edge, then the second (2 * edges ints, local to the shape),
+        copied into `out` when given."""
+        e = mesh_edges(self._faces())
+        return _fill(out, np.concatenate([e[:, 0], e[:, 1]]).astype(np.int32))
+
+    def export_mesh(self, filename: str) -> None:
+        """Primitive::ExportMesh (Primitive.cpp:452-469): an OBJ of the shape's
+        unrotated, untranslated positions ("v x y z", 6 significant digits as
+        the reference's stream writes them) and its faces (1-based)."""
+        P = self._scene._raw_positions[self.vertex_slice()].detach().cpu().numpy()
+        F = self._faces()
+        with open(filename, "w") as f:
+            for p in P:
+                f.write("v %g %g %g\n" % (float(p[0]), float(p[1]), float(p[2])))
+            for t in F:
+                f.write("f %d %d %d\n" % (int(t[0]) + 1, int(t[1]) + 1, int(t[2]) + 1))
+
     def vertex_slice(self) -> slice:
         return slice(self._vstart, self._vstart + self._vcount)
+
+
+def _fill(out, values: np.ndarray) -> np.ndarray:
+    """`values`, also copied into `out` (a numpy array or a tensor) when given."""
+    if out is not None:
+        n = out.numel() if isinstance(out, torch.Tensor) else out.size
+        if n != values.size:
+            raise RuntimeError(f"output holds {n} elements, {values.size} needed")
+        if isinstance(out, torch.Tensor):
+            out.view(-1).copy_(torch.from_numpy(values).to(out.dtype))
+        else:
+            out.reshape(-1)[:] = values
+    return values
 
 
 def posed_positions(raw: torch.Tensor, shapes: list):
@@ -326,6 +374,12 @@ class Scene:
             self.load_spec(spec)
 
     # -- construction -------------------------------------------------------
+    def load_file(self, filename: str) -> None:
+        """Scene::LoadFromFile (Scene.cpp:41-44): the reference's XML scene
+        format (scene_xml.load_xml) into this scene; configure() follows."""
+        from . import scene_xml
+        self.load_spec(scene_xml.load_xml(filename))
+
     def load_spec(self, spec: SceneSpec) -> None:
         a = spec.arrays()
         self.spec = spec

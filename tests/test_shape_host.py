@@ -1,8 +1,9 @@
-"""Shape rotations on the host, on the CPU: the axis-angle matrix of
-CalcRotateAxisAngle (Renderer/Utils.cpp:200-232), the pose and the
+"""Shape parameters and accessors on the host, on the CPU: the axis-angle
+matrix of CalcRotateAxisAngle (Renderer/Utils.cpp:200-232), the pose and the
 differentiable rotation of Primitive::Configure (Primitive.cpp:158-189) as
-api.posed_positions applies them, and the chain rule of api.pose_grads
-against torch autograd of the same composition."""
+api.posed_positions applies them, the chain rule of api.pose_grads against
+torch autograd of the same composition, and the face, edge and mesh-export
+accessors of Primitive (Primitive.cpp:400-469)."""
 from types import SimpleNamespace
 
 import numpy as np
@@ -95,3 +96,44 @@ def test_rotate_matrix_checks_its_shape():
     _, shapes = _scene_with(raw, [3])
     with pytest.raises(RuntimeError, match="3x3 or 4x4"):
         shapes[0].rotate_matrix = np.eye(2)
+
+
+def _mesh_scene(tmp_path):
+    """A fake scene holding two meshes (a quad and a tetrahedron)."""
+    from tensorray_b200 import scenes
+    quad = scenes.MeshSpec(np.array([[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0]], np.float32),
+                           np.array([[0, 1, 2], [0, 2, 3]], np.int32))
+    tet = scenes.MeshSpec(np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1.5]], np.float32),
+                          np.array([[0, 2, 1], [0, 1, 3], [0, 3, 2], [1, 2, 3]], np.int32))
+    raw = torch.as_tensor(np.concatenate([quad.positions, tet.positions]))
+    sc = SimpleNamespace(_dirty=False, _raw_positions=raw, device=raw.device,
+                         spec=SimpleNamespace(meshes=[quad, tet]))
+    shapes = [api.Shape(sc, 0, 0, 4, 2), api.Shape(sc, 1, 4, 4, 4)]
+    return sc, shapes
+
+
+def test_face_and_edge_accessors(tmp_path):
+    _, (quad, tet) = _mesh_scene(tmp_path)
+    assert tet.get_face_indices().tolist() == [0, 2, 1, 0, 1, 3, 0, 3, 2, 1, 2, 3]
+    out = torch.zeros(6, dtype=torch.int32)
+    quad.get_face_indices(out)
+    assert out.tolist() == [0, 1, 2, 0, 2, 3]
+    with pytest.raises(RuntimeError, match="needed"):
+        quad.get_face_indices(np.zeros(5, np.int32))
+    # a quad has 5 edges, a closed tetrahedron 6; first vertices, then second
+    assert quad.get_edge_count() == 5 and tet.get_edge_count() == 6
+    ed = np.zeros(12, np.int32)
+    tet.get_edge_data(ed)
+    assert sorted(zip(ed[:6].tolist(), ed[6:].tolist())) == [(0, 1), (0, 2), (0, 3), (1, 2), (1, 3), (2, 3)]
+
+
+def test_export_mesh_writes_what_load_obj_reads(tmp_path):
+    from tensorray_b200 import scenes
+    _, (quad, tet) = _mesh_scene(tmp_path)
+    path = str(tmp_path / "tet.obj")
+    tet.export_mesh(path)
+    text = open(path).read().splitlines()
+    assert text[3] == "v 0 0 1.5" and text[4] == "f 1 3 2"
+    m = scenes.load_obj(path)
+    np.testing.assert_array_equal(m.positions, tet._scene.spec.meshes[1].positions)
+    np.testing.assert_array_equal(m.faces, tet._scene.spec.meshes[1].faces)
