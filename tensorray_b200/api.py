@@ -243,7 +243,6 @@ class Shape:
         return (self._rotate_matrix, c, rotation_axis_angle(self._rotate_angle, self._rotate_axis),
                 rotation_axis_angle(self._rotate_angle, self._rotate_axis, derivative=True))
 
-
     def get_vertex_count(self) -> int:
         return self._vcount
 
