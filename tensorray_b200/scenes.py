@@ -342,10 +342,15 @@ def load_obj(path: str, bsdf: int = 0, smooth: bool = True, light: int = -1,
     1.0f - v in float32 arithmetic (ObjMesh.cpp:73-78), numbers rounded to
     float32 as strtof rounds them, faces of 3 or 4 corners in the forms i,
     i/t, i/t/n, i//n with 1-based or negative (relative) indices, quads split
-    into (0, 1, 2) and (3, 0, 2). Normals (`vn`), smoothing groups and
-    materials are not used by the renderer and are skipped. The reference
-    leaves the texture indices of a quad's second triangle unset; here they
-    follow its position corners. A comment line is skipped whole; the
+    into (0, 1, 2) and (3, 0, 2). Smoothing groups and materials are not
+    used by the renderer and are skipped. Normals (`vn`) are skipped too, and
+    that is a difference: for a smooth mesh whose file has normals, the
+    reference shades with those (per face corner, constant with respect to
+    the vertex positions; Primitive.cpp:113-131, 205-208), while this renderer
+    always uses the area-weighted vertex normals of the positions, which the
+    reference computes when the file has none (Primitive.cpp:323-340). The
+    reference leaves the texture indices of a quad's second triangle unset;
+    here they follow its position corners. A comment line is skipped whole; the
     reference reads the tokens after a lone '#' as commands, so a comment
     such as "# v 1 2 3" would add a vertex there."""
     pos, us, vs, faces, uvf = [], [], [], [], []
