@@ -1,5 +1,4 @@
 """Shared helpers for the parity tests: scenes, oracle cameras, samples."""
-import numpy as np
 import torch
 
 from oracle import tr_oracle as O

@@ -6,7 +6,6 @@ import os
 import re
 
 import numpy as np
-import pytest
 
 from oracle import tr_oracle as O
 

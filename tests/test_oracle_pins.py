@@ -4,7 +4,6 @@ reference's primitive-op goldens."""
 import math
 
 import numpy as np
-import pytest
 import torch
 
 from oracle import tr_oracle as O
