@@ -352,7 +352,10 @@ def load_obj(path: str, bsdf: int = 0, smooth: bool = True, light: int = -1,
     reference leaves the texture indices of a quad's second triangle unset;
     here they follow its position corners. A comment line is skipped whole; the
     reference reads the tokens after a lone '#' as commands, so a comment
-    such as "# v 1 2 3" would add a vertex there."""
+    such as "# v 1 2 3" would add a vertex there. A face line that ends in a
+    blank before a CRLF line end is read as its corners here; the reference
+    takes the carriage return for one more corner that it cannot parse
+    (ObjMesh.cpp:101-135), with an uninitialised index."""
     pos, us, vs, faces, uvf = [], [], [], [], []
     textured = False
     with open(path, "r") as f:

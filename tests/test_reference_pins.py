@@ -239,3 +239,87 @@ def test_fixture_is_what_the_reference_computes(pins, tmp_path):
                                          check=True).stdout)
         for k in CAMERA_KEYS:
             assert _rel(_f32(live[k]), _f32(case["reference"][k])) <= CAMERA_TOL
+
+
+def _random_obj(seed: int) -> str:
+    """A seeded OBJ: 4-40 vertices written with 0-9 decimals, exponents,
+    integers or 17 digits, space or tab separators, optional texture
+    coordinates and normals, comments, blank, 'o', 'g', 's' and 'usemtl'
+    lines, triangles and quads in every corner form, negative indices, and
+    LF or CRLF line ends. With CRLF no line ends in a blank: the reference's
+    face parser would then read the carriage return as one more corner
+    (ObjMesh.cpp:101-135 splits only at ' ', '\\t', '\\n'), an index sscanf
+    cannot parse, which leaves its corner uninitialised."""
+    rng = np.random.default_rng(seed)
+
+    def num():
+        x = rng.normal(0, 2)
+        k = rng.integers(0, 5)
+        if k == 0:
+            return f"{x:.{rng.integers(0, 10)}f}"
+        if k == 1:
+            return f"{x:.{rng.integers(1, 8)}e}"
+        if k == 2:
+            return repr(float(np.float32(x)))
+        if k == 3:
+            return f"{int(x * 10)}"
+        return f"{x:.17g}"
+
+    def sep():
+        return " " if rng.random() < 0.8 else "\t"
+
+    nv = int(rng.integers(4, 40))
+    textured, normals = rng.random() < 0.6, rng.random() < 0.5
+    lines = []
+    for _ in range(nv):
+        lines.append("v" + sep() + sep().join(num() for _ in range(3)))
+        if rng.random() < 0.1:
+            lines.append("# comment words here")
+        if rng.random() < 0.05:
+            lines.append("")
+    for _ in range(nv if textured else 0):
+        lines.append(f"vt {rng.random():.{rng.integers(1, 9)}f} {rng.random():.{rng.integers(1, 9)}f}")
+    for _ in range(nv if normals else 0):
+        lines.append("vn 0 0 1")
+    lines += ["o object", "g group", "s 1", "usemtl material"]
+    for _ in range(int(rng.integers(1, 30))):
+        idx = rng.choice(nv, 3 if rng.random() < 0.6 else 4, replace=False)
+        neg = rng.random() < 0.2
+        corners = []
+        for i in idx:
+            p = str(int(i) - nv) if neg else str(int(i) + 1)
+            t = int(i) + 1
+            corners.append(f"{p}/{t}/{t}" if textured and normals else f"{p}/{t}" if textured
+                           else f"{p}//{t}" if normals else p)
+        lines.append("f " + sep().join(corners) + (" " if rng.random() < 0.2 else ""))
+        if rng.random() < 0.1:
+            lines.append("s off")
+    end = "\n" if rng.random() < 0.9 else "\r\n"
+    if end == "\r\n":
+        lines = [line.rstrip(" \t") for line in lines]
+    return end.join(lines) + end
+
+
+@pytest.mark.skipif(not os.path.exists(PROBE), reason="the reference probe is built only where the reference is")
+def test_random_obj_files_load_as_the_reference_loads_them(tmp_path):
+    """150 seeded OBJ files through the reference's own loader and this one:
+    the same float32 positions and texture coordinates, the same faces
+    (texture indices of a quad's second triangle aside) and edge lists."""
+    for seed in range(150):
+        text = _random_obj(seed)
+        path = tmp_path / f"r{seed}.obj"
+        path.write_bytes(text.encode())
+        r = json.loads(subprocess.run([PROBE, "obj", str(path)], capture_output=True, text=True,
+                                      check=True).stdout)
+        m = scenes.load_obj(str(path))
+        P = _f32(r["positions"]).reshape(-1, 3)
+        assert np.array_equal(m.positions.view(np.uint32), P.view(np.uint32)), seed
+        F = np.asarray(r["face_positions"]).reshape(-1, 3)
+        assert np.array_equal(m.faces, F), seed
+        assert np.array_equal(api.mesh_edges(F), _reference_edges(r)), seed
+        if r["textured"]:
+            assert np.array_equal(m.uvs.view(np.uint32), _f32(r["texcoords"]).reshape(-1, 2).view(np.uint32)), seed
+            keep = np.ones(len(F), bool)
+            keep[_quad_second_rows(text)] = False
+            FT = np.asarray(r["face_texcoords"]).reshape(-1, 3)
+            assert np.array_equal(m.uv_faces[keep], FT[keep]), seed
