@@ -196,7 +196,8 @@ def load_bitmap(path: str) -> np.ndarray:
       replicated, alpha dropped, and each value v becomes powf(v/255, 2.2).
     - Radiance .hdr: linear RGBE (_read_radiance).
     - 16-bit PNGs and other formats are refused, as stb_image 2.02 refuses
-      them.
+      them, and so are colour-mapped TGA images, which it decodes into
+      uninitialised channels.
     - .npy [H, W, 3] arrays are taken as they are (this package's own format
       for generated textures).
 
@@ -218,6 +219,11 @@ def load_bitmap(path: str) -> np.ndarray:
     _require(img.format in _STB_8BIT_FORMATS and img.mode in ("1", "L", "LA", "P", "PA", "RGB", "RGBA"),
              f"{path}: {img.format} {img.mode} images are not loaded (the reference's stb_image 2.02 reads "
              "8-bit JPEG, PNG, BMP, TGA, PNM, GIF and Radiance HDR)")
+    # stb_image 2.02 reads a colour-mapped TGA's palette entries one byte wide
+    # and leaves the other channels uninitialised (stbi__tga_load)
+    _require(not (img.format == "TGA" and img.mode in ("P", "PA")),
+             f"{path}: colour-mapped TGA images are not loaded (the reference's stb_image 2.02 does not "
+             "decode them)")
     a = np.asarray(img.convert("RGB"), np.uint8)
     return np.ascontiguousarray(_gamma_lut()[a])
 

@@ -345,3 +345,68 @@ def test_random_cameras_match_the_reference(tmp_path):
         for k in CAMERA_KEYS:
             for got in (lib_cam[k], ora_cam[k]):
                 assert _rel(got, _f32(r[k])) <= 2e-6, (args, k)
+
+
+def _random_image(rng, i):
+    """A seeded image file the reference's stb_image decodes: 8-bit PNG, BMP,
+    TGA (not colour-mapped), PPM/PGM or GIF in gray, gray+alpha, RGB, RGBA
+    or palette form, or a Radiance file (flat, or run-length encoded where
+    the format allows it, 8 <= width < 32768) with runs, dumps and black
+    pixels. Returns (name, bytes)."""
+    import io
+
+    from PIL import Image
+    if i % 3 < 2:
+        H, W = int(rng.integers(1, 40)), int(rng.integers(1, 40))
+        mode = ["L", "LA", "RGB", "RGBA", "P"][int(rng.integers(0, 5))]
+        fmt = ["PNG", "BMP", "TGA", "PPM", "GIF"][int(rng.integers(0, 5))]
+        ch = {"L": 1, "LA": 2, "RGB": 3, "RGBA": 4, "P": 3}[mode]
+        a = rng.integers(0, 256, (H, W, ch), dtype=np.uint8)
+        img = Image.fromarray(a[:, :, 0] if ch == 1 else a, "RGB" if mode == "P" else mode)
+        if mode == "P" and fmt != "TGA":
+            img = img.convert("P")
+        if (fmt in ("BMP", "PPM") and mode in ("LA", "RGBA")) or (fmt == "PPM" and img.mode == "P"):
+            img = img.convert("RGB")
+        if fmt == "GIF" and img.mode not in ("L", "P"):
+            img = img.convert("P")
+        b = io.BytesIO()
+        img.save(b, fmt)
+        return f"r{i}.{fmt.lower()}", b.getvalue()
+    from tests.golden.make_edx_goldens import _hdr_bytes
+    H, W = int(rng.integers(1, 12)), int(rng.choice([3, 7, 8, 9, 40, 200, 300]))
+    rgbe = rng.integers(0, 256, (H, W, 4), dtype=np.uint8)
+    for j in range(H):
+        for k in range(4):
+            s = int(rng.integers(0, W))
+            rgbe[j, s:min(W, s + int(rng.integers(1, 160))), k] = rng.integers(0, 256)
+    rgbe[..., 3] = np.where(rng.random((H, W)) < 0.1, 0, rgbe[..., 3])
+    return f"r{i}.hdr", _hdr_bytes(rgbe, W >= 8 and rng.random() < 0.8)
+
+
+@pytest.mark.skipif(not os.path.exists(PROBE), reason="the reference probe is built only where the reference is")
+def test_random_images_load_as_the_reference_loads_them(tmp_path):
+    """150 seeded image files through the reference's stb_image and
+    scene_xml.load_bitmap: the same float32 texels (JPEG is not among them:
+    another decoder), or an error from both."""
+    rng = np.random.default_rng(21)
+    for i in range(150):
+        name, raw = _random_image(rng, i)
+        path = tmp_path / name
+        path.write_bytes(raw)
+        r = json.loads(subprocess.run([PROBE, "bitmap", str(path)], capture_output=True, text=True,
+                                      check=True).stdout)
+        if "error" in r:
+            with pytest.raises(scene_xml.SceneXmlError):
+                scene_xml.load_bitmap(str(path))
+            continue
+        ref = _f32(r["texels"]).reshape(r["height"], r["width"], 3)
+        got = scene_xml.load_bitmap(str(path))
+        assert got.shape == ref.shape and np.array_equal(got.view(np.uint32), ref.view(np.uint32)), name
+
+
+def test_colour_mapped_tga_is_refused(tmp_path):
+    from PIL import Image
+    p = tmp_path / "pal.tga"
+    Image.fromarray(np.zeros((4, 4, 3), np.uint8)).convert("P").save(str(p), "TGA")
+    with pytest.raises(scene_xml.SceneXmlError, match="colour-mapped TGA"):
+        scene_xml.load_bitmap(str(p))
