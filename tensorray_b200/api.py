@@ -144,6 +144,9 @@ class Shape:
     - diff_rotation(axis) with rotate_angle: a differentiable rotation about
       the world origin, applied after the pose; dL/d(angle) comes back from
       Scene.get_grads() as "rotation_angle".
+    - vertex_id with vertex_translation: one vertex moved in world space after
+      the rotations (Primitive.cpp:194-199); dL/d(vertex_translation) comes
+      back as "vertex_translation".
 
     Translation is applied last. The reference applies the pose in object
     space, before the shape's XML to_world; here meshes are held in world
@@ -159,6 +162,8 @@ class Shape:
         self._obj_center = None
         self._rotate_axis = None
         self._rotate_angle = 0.0
+        self._vertex_id = -1
+        self._vertex_translation = None
 
     def _changed(self) -> None:
         if self._scene is not None:
@@ -214,6 +219,33 @@ class Shape:
     def rotate_angle(self, a) -> None:
         self._rotate_angle = float(a)
         self._changed()
+
+    @property
+    def vertex_id(self) -> int:
+        return self._vertex_id
+
+    @vertex_id.setter
+    def vertex_id(self, i) -> None:
+        i = int(i)
+        if i >= self._vcount:
+            raise RuntimeError(f"vertex_id {i} is out of range for a shape of {self._vcount} vertices")
+        self._vertex_id = i
+        self._changed()
+
+    @property
+    def vertex_translation(self):
+        return self._vertex_translation
+
+    @vertex_translation.setter
+    def vertex_translation(self, t) -> None:
+        self._vertex_translation = None if t is None else _host_f32(t).reshape(3).clone()
+        self._changed()
+
+    def _moves_vertex(self) -> bool:
+        return self._vertex_id >= 0 and self._vertex_translation is not None
+
+    def _posed(self) -> bool:
+        return self._rotate_matrix is not None or self._rotate_axis is not None or self._moves_vertex()
 
     def diff_translation(self) -> None:
         self.requires_translation_grad = True
@@ -304,12 +336,13 @@ def _fill(out, values: np.ndarray) -> np.ndarray:
 def posed_positions(raw: torch.Tensor, shapes: list):
     """The positions the library transforms (world = these + translation):
     each shape's raw positions through its pose, p' = M (p - c) + c, then its
-    differentiable rotation, R p'. None when no shape is rotated."""
-    rotated = [s for s in shapes if s._rotate_matrix is not None or s._rotate_axis is not None]
-    if not rotated:
+    differentiable rotation, R p', then its one moved vertex. None when no
+    shape is posed."""
+    posed = [s for s in shapes if s._posed()]
+    if not posed:
         return None
     out = raw.clone()
-    for s in rotated:
+    for s in posed:
         M, c, R, _ = s._rotations()
         sl = s.vertex_slice()
         q = raw[sl]
@@ -318,21 +351,28 @@ def posed_positions(raw: torch.Tensor, shapes: list):
             q = (q - cd) @ M.to(q.device).T + cd
         if R is not None:
             q = q @ R.to(q.device).T
+        if s._moves_vertex():
+            q = q.clone()
+            q[s._vertex_id] += s._vertex_translation.to(q.device)
         out[sl] = q
     return out
 
 
 def pose_grads(raw: torch.Tensor, grad: torch.Tensor, shapes: list):
     """Chain rule through posed_positions. `grad` is dL/d(posed positions);
-    returns dL/d(raw positions) (rows of rotated shapes through R and M) and
-    dL/d(rotate_angle) per shape (0 for shapes without diff_rotation)."""
+    returns dL/d(raw positions) (rows of rotated shapes through R and M),
+    dL/d(rotate_angle) per shape (0 for shapes without diff_rotation) and
+    dL/d(vertex_translation) per shape [shapes, 3] (0 where no vertex moves)."""
     out = grad.clone()
     d_angle = torch.zeros(len(shapes), device=grad.device)
+    d_vertex = torch.zeros(len(shapes), 3, device=grad.device)
     for i, s in enumerate(shapes):
         M, c, R, dR = s._rotations()
+        sl = s.vertex_slice()
+        if s._moves_vertex():
+            d_vertex[i] = grad[sl][s._vertex_id]
         if M is None and R is None:
             continue
-        sl = s.vertex_slice()
         g = grad[sl]
         q = raw[sl]
         if M is not None:
@@ -344,7 +384,7 @@ def pose_grads(raw: torch.Tensor, grad: torch.Tensor, shapes: list):
         if M is not None:
             g = g @ M.to(g.device)
         out[sl] = g
-    return out, d_angle
+    return out, d_angle, d_vertex
 
 
 class BSDF:
@@ -502,8 +542,9 @@ class Scene:
     def get_grads(self, clear: bool = True) -> dict:
         """Finish the geometry adjoint and return dL/d(translation per mesh),
         dL/d(raw vertex positions), dL/d(texels) (get_grad, pybind_utils.h:133-142),
-        and, when a shape asked for it (diff_rotation), dL/d(rotate_angle) per
-        mesh as "rotation_angle"."""
+        and, when a shape asked for them, dL/d(rotate_angle) per mesh as
+        "rotation_angle" (diff_rotation) and dL/d(vertex_translation) per mesh
+        as "vertex_translation" (vertex_id)."""
         d = self.device
         gt = torch.zeros(self.num_meshes, 3, device=d)
         gp = torch.zeros(self.num_vertices, 3, device=d)
@@ -512,10 +553,12 @@ class Scene:
                                             C.c_void_p(gx.data_ptr()), int(clear), C.c_void_p(_stream())),
               "trn_scene_get_grads")
         out = {"translation": gt, "positions": gp, "texels": gx[: self.num_texels]}
-        if any(s._rotate_matrix is not None or s._rotate_axis is not None for s in self.shapes):
-            out["positions"], d_angle = pose_grads(self._raw_positions, gp, self.shapes)
+        if any(s._posed() for s in self.shapes):
+            out["positions"], d_angle, d_vertex = pose_grads(self._raw_positions, gp, self.shapes)
             if any(s.requires_rotation_grad for s in self.shapes):
                 out["rotation_angle"] = d_angle
+            if any(s._moves_vertex() for s in self.shapes):
+                out["vertex_translation"] = d_vertex
         return out
 
     def set_path_cache(self, max_bytes: int) -> None:

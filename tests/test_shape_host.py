@@ -51,8 +51,8 @@ def test_unrotated_shapes_upload_their_raw_positions():
     _, shapes = _scene_with(raw, [4, 6])
     assert api.posed_positions(raw, shapes) is None
     g = torch.randn(10, 3)
-    gp, da = api.pose_grads(raw, g, shapes)
-    assert torch.equal(gp, g) and torch.equal(da, torch.zeros(2))
+    gp, da, dv = api.pose_grads(raw, g, shapes)
+    assert torch.equal(gp, g) and torch.equal(da, torch.zeros(2)) and torch.equal(dv, torch.zeros(2, 3))
 
 
 def test_pose_and_rotation_and_their_chain_rule():
@@ -85,10 +85,36 @@ def test_pose_and_rotation_and_their_chain_rule():
 
     w = torch.randn(30, 3)
     (world * w).sum().backward()
-    gp, da = api.pose_grads(raw, w, shapes)
+    gp, da, _ = api.pose_grads(raw, w, shapes)
     torch.testing.assert_close(gp, p.grad, rtol=1e-5, atol=1e-5)
     torch.testing.assert_close(da[1:], th.grad[1:], rtol=1e-5, atol=1e-5)
     assert da[0] == 0.0
+
+
+def test_moved_vertex_and_its_gradient():
+    """vertex_id / vertex_translation (Primitive.cpp:194-199): one vertex moved
+    in world space after the rotations; its gradient is that vertex's."""
+    torch.manual_seed(1)
+    raw = torch.randn(12, 3)
+    sc, shapes = _scene_with(raw, [5, 7])
+    shapes[1].diff_rotation((0.0, 0.0, 1.0))
+    shapes[1].rotate_angle = 0.3
+    shapes[1].vertex_id = 4
+    t = torch.tensor([0.1, -0.2, 0.05])
+    shapes[1].vertex_translation = t
+    posed = api.posed_positions(raw, shapes)
+    R = api.rotation_axis_angle(0.3, (0.0, 0.0, 1.0))
+    expected = raw.clone()
+    expected[5:] = raw[5:] @ R.T
+    expected[5 + 4] += t
+    torch.testing.assert_close(posed, expected)
+    g = torch.randn(12, 3)
+    gp, da, dv = api.pose_grads(raw, g, shapes)
+    torch.testing.assert_close(dv[1], g[9])
+    assert torch.equal(dv[0], torch.zeros(3))
+    torch.testing.assert_close(gp[5:], g[5:] @ R)      # the moved vertex's raw gradient still goes through R
+    with pytest.raises(RuntimeError, match="out of range"):
+        shapes[0].vertex_id = 5
 
 
 def test_rotate_matrix_checks_its_shape():
