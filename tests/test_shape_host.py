@@ -163,3 +163,60 @@ def test_export_mesh_writes_what_load_obj_reads(tmp_path):
     m = scenes.load_obj(path)
     np.testing.assert_array_equal(m.positions, tet._scene.spec.meshes[1].positions)
     np.testing.assert_array_equal(m.faces, tet._scene.spec.meshes[1].faces)
+
+
+class _FakeLib:
+    """Stands in for the library's scene calls: records the positions that
+    configure() uploads and hands get_grads() a fixed position gradient."""
+
+    def __init__(self, nv, grad):
+        self.nv, self.grad, self.uploaded = nv, grad, None
+
+    def trn_scene_get_grads(self, h, gt, gp, gx, clear, st):
+        import ctypes
+        ctypes.memmove(gp.value, self.grad.data_ptr(), self.grad.numel() * 4)
+        return 0
+
+    def trn_scene_set_translation(self, h, t, st):
+        return 0
+
+    def trn_scene_set_positions(self, h, p, st):
+        import ctypes
+        buf = (ctypes.c_float * (3 * self.nv)).from_address(p.value)
+        self.uploaded = torch.tensor(np.frombuffer(buf, np.float32).copy()).reshape(-1, 3)
+        return 0
+
+    def trn_scene_configure(self, h, st):
+        return 0
+
+
+def test_scene_uploads_posed_positions_and_chains_its_gradients(monkeypatch):
+    """Scene.configure uploads the posed positions and Scene.get_grads chains
+    the library's position gradient through the poses, with the angle and
+    moved-vertex gradients only when a shape asks for them."""
+    import ctypes
+    nv = 12
+    torch.manual_seed(2)
+    raw, g = torch.randn(nv, 3), torch.randn(nv, 3)
+    sc = api.Scene.__new__(api.Scene)
+    sc.device, sc._h, sc._dirty = torch.device("cpu"), ctypes.c_void_p(1), True
+    sc.num_meshes, sc.num_vertices, sc.num_texels = 2, nv, 0
+    sc._raw_positions, sc._translation = raw.clone(), torch.zeros(2, 3)
+    sc._lib = _FakeLib(nv, g)
+    monkeypatch.setattr(api, "_stream", lambda: 0)
+
+    sc.shapes = [api.Shape(sc, 0, 0, 5, 0), api.Shape(sc, 1, 5, 7, 0)]
+    sc.configure()
+    assert torch.equal(sc._lib.uploaded, raw)
+    assert sorted(sc.get_grads()) == ["positions", "texels", "translation"]
+
+    sc.shapes[1].diff_rotation((0, 1, 0))
+    sc.shapes[1].rotate_angle = 0.2
+    sc.shapes[0].vertex_id = 2
+    sc.shapes[0].vertex_translation = (0.5, 0.0, 0.0)
+    sc.configure()
+    assert torch.equal(sc._lib.uploaded, api.posed_positions(raw, sc.shapes))
+    out = sc.get_grads()
+    gp, da, dv = api.pose_grads(raw, g, sc.shapes)
+    assert torch.equal(out["positions"], gp) and torch.equal(out["rotation_angle"], da)
+    assert torch.equal(out["vertex_translation"], dv)
