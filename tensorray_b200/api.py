@@ -85,16 +85,39 @@ class RenderOptions:
 
 
 class Camera:
-    """Pinhole sensor (Camera::Init, Camera.cpp:89-103)."""
+    """Pinhole sensor (Camera::Init, Camera.cpp:89-103; the binding,
+    TensorRay.cpp:143-151): Camera() is empty until init(); update(other)
+    copies another camera's pose; resize(width, height) keeps the pose."""
 
-    def __init__(self, pos, target, up, width: int, height: int, fov: float):
+    def __init__(self, pos=None, target=None, up=None, width: int = 0, height: int = 0, fov: float = 35.0):
+        self.c = TrnCamera()
+        self.width = self.height = 0
+        self.pos = self.target = self.up = None
+        self.fov = float(fov)
+        if pos is not None:
+            self.init(pos, target, up, width, height, fov)
+
+    def init(self, pos, target, up, width: int, height: int, fov: float = 35.0) -> None:
+        """Camera::Init with the reference's defaults (fov 35 degrees; clip
+        planes 1 and 1000, Camera.h:115-123)."""
+        c = TrnCamera()
+        f3 = lambda v: (C.c_float * 3)(*[float(x) for x in v])
+        check(_abi.load().trn_camera_init(C.byref(c), f3(pos), f3(target), f3(up), int(width), int(height),
+                                          C.c_float(float(fov))), "trn_camera_init")
+        self.c = c
         self.width, self.height = int(width), int(height)
         self.pos, self.target, self.up, self.fov = tuple(pos), tuple(target), tuple(up), float(fov)
-        self.c = TrnCamera()
-        lib = _abi.load()
-        f3 = lambda v: (C.c_float * 3)(*[float(x) for x in v])
-        check(lib.trn_camera_init(C.byref(self.c), f3(pos), f3(target), f3(up), self.width, self.height,
-                                  C.c_float(self.fov)), "trn_camera_init")
+
+    def update(self, other: "Camera") -> None:
+        """Camera::Update (Camera.h:110-113): this camera takes the other's
+        pose, resolution and field of view."""
+        self.init(other.pos, other.target, other.up, other.width, other.height, other.fov)
+
+    def resize(self, width: int, height: int) -> None:
+        """Camera::Resize (Camera.cpp:105-137): a new resolution, same pose."""
+        if self.pos is None:
+            raise RuntimeError("camera not initialised")
+        self.init(self.pos, self.target, self.up, width, height, self.fov)
 
     def matrices(self) -> dict:
         c = self.c

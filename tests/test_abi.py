@@ -6,6 +6,7 @@ import os
 import re
 
 import numpy as np
+import pytest
 
 from oracle import tr_oracle as O
 
@@ -80,3 +81,24 @@ def test_sample_layout_dims():
     assert api.sample_dims(2, 3) == 12
     assert api.sample_dims(3, 3) == 19
     assert api.sample_slots(4, 8, 8, 4) == 64
+
+
+def test_camera_init_update_resize():
+    """The binding's Camera() / init / update / resize (TensorRay.cpp:143-151)
+    over trn_camera_init: an empty camera takes a pose with init, copies one
+    with update, and keeps its pose through resize."""
+    from tensorray_b200 import api
+    a = api.Camera((0.0, 0.0, 4.0), (0.0, 0.0, 0.0), (0.0, 1.0, 0.0), 256, 128, 45.0)
+    b = api.Camera()
+    assert b.width == 0 and b.pos is None
+    b.update(a)
+    ma, mb = a.matrices(), b.matrices()
+    assert all(np.array_equal(ma[k], mb[k]) for k in ma)
+    b.resize(512, 256)
+    ref = api.Camera((0.0, 0.0, 4.0), (0.0, 0.0, 0.0), (0.0, 1.0, 0.0), 512, 256, 45.0).matrices()
+    assert (b.width, b.height) == (512, 256) and all(np.array_equal(b.matrices()[k], ref[k]) for k in ref)
+    c = api.Camera()
+    c.init((1.0, 2.0, 3.0), (0.0, 0.0, 0.0), (0.0, 1.0, 0.0), 64, 64)
+    assert c.fov == 35.0
+    with pytest.raises(RuntimeError, match="not initialised"):
+        api.Camera().resize(8, 8)
