@@ -539,11 +539,24 @@ class Scene:
         if self._dirty:
             self.configure()
 
-    def get_width(self) -> int:
-        return self.cameras[0].width
+    def get_width(self, i: int = 0) -> int:
+        """Scene::GetImageWidth (Scene.h:127): sensor i's image width."""
+        return self.cameras[i].width
 
-    def get_height(self) -> int:
-        return self.cameras[0].height
+    def get_height(self, i: int = 0) -> int:
+        """Scene::GetImageHeight (Scene.h:128): sensor i's image height."""
+        return self.cameras[i].height
+
+    @property
+    def num_bsdf(self) -> int:
+        """The scene's BSDF count (Scene::mBSDFCount)."""
+        return len(self.bsdfs)
+
+    @property
+    def emitters(self) -> list:
+        """The area lights, one per emitting shape, in shape order
+        (Scene::mLights; the reference binds no methods on them)."""
+        return [s for s, m in zip(self.shapes, self.spec.meshes) if m.light >= 0]
 
     @property
     def handle(self):

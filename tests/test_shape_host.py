@@ -220,3 +220,15 @@ def test_scene_uploads_posed_positions_and_chains_its_gradients(monkeypatch):
     gp, da, dv = api.pose_grads(raw, g, sc.shapes)
     assert torch.equal(out["positions"], gp) and torch.equal(out["rotation_angle"], da)
     assert torch.equal(out["vertex_translation"], dv)
+
+
+def test_scene_accessors_of_the_binding():
+    """get_width(i) / get_height(i) per sensor (Scene.h:127-128), num_bsdf and
+    emitters (TensorRay.cpp:153-163), on a scene object built without a GPU."""
+    sc = api.Scene.__new__(api.Scene)
+    sc.cameras = [SimpleNamespace(width=64, height=32), SimpleNamespace(width=128, height=96)]
+    sc.bsdfs = [object(), object(), object()]
+    sc.spec = SimpleNamespace(meshes=[SimpleNamespace(light=-1), SimpleNamespace(light=0), SimpleNamespace(light=-1)])
+    sc.shapes = ["sphere", "lamp", "ground"]
+    assert (sc.get_width(), sc.get_height(), sc.get_width(1), sc.get_height(1)) == (64, 32, 128, 96)
+    assert sc.num_bsdf == 3 and sc.emitters == ["lamp"]
