@@ -6,6 +6,7 @@ import os
 
 import numpy as np
 import pytest
+import torch
 
 from tensorray_b200 import scene_xml, scenes
 
@@ -173,3 +174,36 @@ def test_images_the_reference_cannot_load_are_refused(tmp_path):
     for name, msg in [("g16.png", "16-bit PNGs"), ("t.tiff", "TIFF")]:
         with pytest.raises(scene_xml.SceneXmlError, match=msg):
             scene_xml.load_bitmap(os.path.join(d, name))
+
+
+class _FakeSceneLib:
+    """The library's scene creation and counts, without a device: records
+    the descriptor's sizes."""
+
+    def trn_scene_create(self, d, out):
+        self.desc = (d._obj.num_vertices, d._obj.num_triangles, d._obj.num_meshes, d._obj.num_bsdfs)
+        return 0
+
+    def trn_scene_counts(self, h, nv, nt, ne, ntex, nm):
+        nv._obj.value, nt._obj.value = self.desc[0], self.desc[1]
+        ne._obj.value, ntex._obj.value, nm._obj.value = 0, 0, self.desc[2]
+        return 0
+
+
+def test_scene_load_file_reads_the_xml(tmp_path):
+    """Scene().load_file(path), as the reference's scripts load a scene
+    (Scene::LoadFromFile, Scene.cpp:41-44), gives the shapes, BSDFs and
+    cameras of scene_xml.load_xml (library calls faked: no GPU here)."""
+    import ctypes
+
+    from tensorray_b200 import api
+    path, ref = config1_xml(str(tmp_path))
+    sc = api.Scene.__new__(api.Scene)
+    sc.device, sc._lib, sc._h, sc._dirty = torch.device("cpu"), _FakeSceneLib(), ctypes.c_void_p(), True
+    sc.shapes, sc.bsdfs, sc.cameras = [], [], []
+    sc.load_file(path)
+    assert sc._lib.desc == (sum(len(m.positions) for m in ref.meshes), sum(len(m.faces) for m in ref.meshes),
+                            len(ref.meshes), len(ref.bsdfs))
+    assert [s.get_vertex_count() for s in sc.shapes] == [len(m.positions) for m in ref.meshes]
+    assert [(c.width, c.height) for c in sc.cameras] == [(c.width, c.height) for c in ref.cameras]
+    assert sc.num_bsdf == len(ref.bsdfs) and sc.get_width(0) == ref.cameras[0].width
