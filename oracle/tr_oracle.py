@@ -31,7 +31,8 @@ Differences that are deliberate and shared with the GPU path:
 Parity status: partly pinned to the reference's own outputs.
   * Pinned by the reference's code: the edge lists (build_edges equals
     ObjMesh::processEdges row for row) and the camera (camera_matrices within
-    1e-6 relative of EDX::Camera and the renderer's derived matrices). The
+    1e-6 relative of EDX::Camera and the renderer's derived matrices on the
+    fixtures, 2e-6 on seeded random cameras). The
     reference's EDXUtil mesh and camera sources are plain C++ and are built
     into oracle/_ref/edx_probe (oracle/edx/Makefile); its outputs on seeded
     inputs are the fixtures in tests/golden/edx_pins.json.
