@@ -5,6 +5,8 @@
 #include <cmath>
 #include <cstdio>
 #include <random>
+#include <string>
+#include <vector>
 using namespace trn;
 
 namespace {
@@ -45,7 +47,40 @@ double rel(const double* a, const double* b, int n) {
 
 }  // namespace
 
-int main() {
+// Mode "eval_inner_vjp IN OUT": int32 n, then n records of 17 float32
+// (type, roughness, spec[3], kd[3], lo[3], li[3], gB[3]) in; n records of 12
+// float32 (B[3], g_lo[3], g_li[3], g_kd[3]) out.
+int run_eval_inner_vjp(const char* in_path, const char* out_path) {
+  FILE* fi = std::fopen(in_path, "rb");
+  if (!fi) return 1;
+  int n = 0;
+  if (std::fread(&n, sizeof n, 1, fi) != 1 || n < 0) return 1;
+  std::vector<float> in((size_t)n * 17), out((size_t)n * 12);
+  if (std::fread(in.data(), sizeof(float), in.size(), fi) != in.size()) return 1;
+  std::fclose(fi);
+  for (int i = 0; i < n; i++) {
+    const float* c = &in[(size_t)i * 17];
+    BsdfDesc b{};
+    b.type = (int)c[0];
+    b.tex = -1;
+    b.roughness = c[1];
+    for (int k = 0; k < 3; k++) b.spec[k] = c[2 + k];
+    const F3 kd(c[5], c[6], c[7]), lo(c[8], c[9], c[10]), li(c[11], c[12], c[13]), gB(c[14], c[15], c[16]);
+    F3 g_lo = F3z(), g_li = F3z(), g_kd = F3z();
+    const F3 B = eval_inner_vjp(b, kd, lo, li, gB, g_lo, g_li, g_kd);
+    const F3 o[4] = {B, g_lo, g_li, g_kd};
+    for (int j = 0; j < 4; j++)
+      for (int k = 0; k < 3; k++) out[(size_t)i * 12 + 3 * j + k] = o[j][k];
+  }
+  FILE* fo = std::fopen(out_path, "wb");
+  if (!fo) return 1;
+  std::fwrite(out.data(), sizeof(float), out.size(), fo);
+  std::fclose(fo);
+  return 0;
+}
+
+int main(int argc, char** argv) {
+  if (argc == 4 && std::string(argv[1]) == "eval_inner_vjp") return run_eval_inner_vjp(argv[2], argv[3]);
   std::mt19937 rng(1);
   std::uniform_real_distribution<float> U(-1.f, 1.f);
   auto rv = [&]() { return F3(U(rng), U(rng), U(rng)); };

@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 
 
 @pytest.fixture(scope="module")
-def harness(tmp_path_factory):
+def harness_exe(tmp_path_factory):
     out = str(tmp_path_factory.mktemp("vjp") / "vjp_harness")
     src = os.path.join(HERE, "native", "vjp_harness.cu")
     scene = os.path.join(build.CSRC, "scene.cu")
@@ -23,7 +23,12 @@ def harness(tmp_path_factory):
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
         pytest.fail("nvcc failed:\n" + res.stderr[-2000:])
-    run = subprocess.run([out], capture_output=True, text=True, timeout=300)
+    return out
+
+
+@pytest.fixture(scope="module")
+def harness(harness_exe):
+    run = subprocess.run([harness_exe], capture_output=True, text=True, timeout=300)
     assert run.returncode == 0, run.stderr
     return {l.split()[0]: (int(l.split()[1]), float(l.split()[2])) for l in run.stdout.strip().splitlines()}
 
@@ -34,3 +39,63 @@ def test_reverse_mode_matches_dual_numbers(harness, name, tol):
     cases, worst = harness[name]
     assert cases > 10000
     assert worst < tol, f"{name}: worst relative error {worst:.3e}"
+
+
+def test_bsdf_adjoint_matches_autograd_of_the_oracle(harness_exe, tmp_path):
+    """eval_inner_vjp, the library's hand-written reverse mode of the BSDF
+    value (Diffuse.cpp:37-41, Microfacet.cpp:37-79), against torch autograd
+    of the oracle's independent restatement (tr_oracle.eval_inner) in float64,
+    on 2000 seeded cases (a tenth with a direction below the horizon).
+
+    Each output (value, gradients with respect to the two local directions
+    and the albedo) is measured by its error relative to the float64 result,
+    and so is the same autograd run in float32. Near grazing directions
+    (cos ~ 1e-3) the gradient's 1/q^2 terms cancel, and both float32
+    computations are then about 1e-4 off. The hand-written adjoint must be as
+    accurate as float32 autograd: its median, 99th percentile and largest
+    error within 2x, 3x and 2x of autograd's (measured: 3.6e-8, 5.2e-6 and
+    1.02e-4 against 3.5e-8, 2.9e-6 and 1.03e-4)."""
+    from types import SimpleNamespace
+
+    import numpy as np
+    import torch
+
+    from oracle import tr_oracle as O
+    rng = np.random.default_rng(4)
+    n = 2000
+    c = np.zeros((n, 17), np.float32)
+    c[:, 0] = rng.integers(0, 2, n)
+    c[:, 1] = rng.uniform(0.05, 1.0, n)
+    c[:, 2:5] = rng.uniform(0, 1, (n, 3))
+    c[:, 5:8] = rng.uniform(0, 1, (n, 3))
+    for cols in (slice(8, 11), slice(11, 14)):
+        v = rng.normal(size=(n, 3))
+        v[:, 2] = np.abs(v[:, 2]) * np.where(rng.random(n) < 0.9, 1.0, -1.0)
+        c[:, cols] = v / np.linalg.norm(v, axis=1, keepdims=True)
+    c[:, 14:17] = rng.normal(size=(n, 3))
+    fi, fo = tmp_path / "in.bin", tmp_path / "out.bin"
+    fi.write_bytes(np.int32(n).tobytes() + c.tobytes())
+    subprocess.run([harness_exe, "eval_inner_vjp", str(fi), str(fo)], check=True, timeout=120)
+    out = np.fromfile(str(fo), np.float32).reshape(n, 12)
+
+    def autograd(i, dtype):
+        b = SimpleNamespace(type=int(c[i, 0]), roughness=float(c[i, 1]),
+                            specular=tuple(float(x) for x in c[i, 2:5]))
+        kd, lo, li = (torch.tensor(c[i:i + 1, a:a + 3], dtype=dtype, requires_grad=True) for a in (5, 8, 11))
+        B = O.eval_inner(b, kd, lo, li)
+        B.backward(torch.tensor(c[i:i + 1, 14:17], dtype=B.dtype))
+        zero = torch.zeros(1, 3, dtype=B.dtype)
+        return [B.detach()[0]] + [(t.grad if t.grad is not None else zero)[0] for t in (lo, li, kd)]
+
+    e_lib, e_f32 = [], []
+    for i in range(n):
+        r64, r32 = autograd(i, torch.float64), autograd(i, torch.float32)
+        for j in range(4):
+            ref = r64[j].numpy()
+            scale = max(np.abs(ref).max(), 1e-6)
+            e_lib.append(np.abs(out[i, 3 * j:3 * j + 3] - ref).max() / scale)
+            e_f32.append(np.abs(r32[j].double().numpy() - ref).max() / scale)
+    e_lib, e_f32 = np.array(e_lib), np.array(e_f32)
+    assert np.median(e_lib) <= 2 * np.median(e_f32) + 1e-9
+    assert np.percentile(e_lib, 99) <= 3 * np.percentile(e_f32, 99)
+    assert e_lib.max() <= 2 * e_f32.max(), (e_lib.max(), e_f32.max())
