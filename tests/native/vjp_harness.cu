@@ -79,8 +79,38 @@ int run_eval_inner_vjp(const char* in_path, const char* out_path) {
   return 0;
 }
 
+// Mode "xdotn_grad IN OUT": int32 n, then n records of 19 float32
+// (org[3], target[3], P0[3], P1[3], P2[3], n[3], W) in; n records of 16
+// float32 (xdotn, g_org[3], g_target[3], g0[3], g1[3], g2[3]) out.
+int run_xdotn_grad(const char* in_path, const char* out_path) {
+  FILE* fi = std::fopen(in_path, "rb");
+  if (!fi) return 1;
+  int n = 0;
+  if (std::fread(&n, sizeof n, 1, fi) != 1 || n < 0) return 1;
+  std::vector<float> in((size_t)n * 19), out((size_t)n * 16);
+  if (std::fread(in.data(), sizeof(float), in.size(), fi) != in.size()) return 1;
+  std::fclose(fi);
+  for (int i = 0; i < n; i++) {
+    const float* c = &in[(size_t)i * 19];
+    const F3 org(c[0], c[1], c[2]), target(c[3], c[4], c[5]), P0(c[6], c[7], c[8]), P1(c[9], c[10], c[11]),
+        P2(c[12], c[13], c[14]), nn(c[15], c[16], c[17]);
+    F3 g[5];
+    xdotn_grad(org, target, P0, P1, P2, nn, c[18], g[0], g[1], g[2], g[3], g[4]);
+    float* o = &out[(size_t)i * 16];
+    o[0] = xdotn<float>(org, target, P0, P1, P2, nn);
+    for (int j = 0; j < 5; j++)
+      for (int k = 0; k < 3; k++) o[1 + 3 * j + k] = g[j][k];
+  }
+  FILE* fo = std::fopen(out_path, "wb");
+  if (!fo) return 1;
+  std::fwrite(out.data(), sizeof(float), out.size(), fo);
+  std::fclose(fo);
+  return 0;
+}
+
 int main(int argc, char** argv) {
   if (argc == 4 && std::string(argv[1]) == "eval_inner_vjp") return run_eval_inner_vjp(argv[2], argv[3]);
+  if (argc == 4 && std::string(argv[1]) == "xdotn_grad") return run_xdotn_grad(argv[2], argv[3]);
   std::mt19937 rng(1);
   std::uniform_real_distribution<float> U(-1.f, 1.f);
   auto rv = [&]() { return F3(U(rng), U(rng), U(rng)); };

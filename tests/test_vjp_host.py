@@ -99,3 +99,60 @@ def test_bsdf_adjoint_matches_autograd_of_the_oracle(harness_exe, tmp_path):
     assert np.median(e_lib) <= 2 * np.median(e_f32) + 1e-9
     assert np.percentile(e_lib, 99) <= 3 * np.percentile(e_f32, 99)
     assert e_lib.max() <= 2 * e_f32.max(), (e_lib.max(), e_f32.max())
+
+
+def test_xdotn_adjoint_matches_autograd_of_the_oracle(harness_exe, tmp_path):
+    """xdotn_grad, the library's reverse mode of the boundary terms' xDotN
+    (RayIntersectAD, Utils.cpp:288-297, then n . (w P0 + u P1 + v P2) with
+    detached vertices), against float64 autograd of the same composition of
+    the oracle's ray_intersect_ad and normalize, on 2000 seeded rays towards
+    random triangles. Value and the gradients with respect to the ray's two
+    points and the three vertices are as accurate as float32 autograd: median,
+    99th percentile and largest error within 2x, 3x and 2x of autograd's
+    (measured: 3.2e-7, 1.2e-4 and 8.2e-3 against 3.6e-7, 1.2e-4 and 8.2e-3;
+    the tail is rays nearly parallel to their triangle)."""
+    import numpy as np
+    import torch
+
+    from oracle import tr_oracle as O
+    rng = np.random.default_rng(8)
+    n = 2000
+    c = np.zeros((n, 19), np.float32)
+    P0 = rng.normal(size=(n, 3))
+    P1, P2 = P0 + rng.normal(size=(n, 3)), P0 + rng.normal(size=(n, 3))
+    bary = rng.dirichlet([1, 1, 1], n)
+    hit = bary[:, :1] * P0 + bary[:, 1:2] * P1 + bary[:, 2:3] * P2
+    org = hit + rng.normal(size=(n, 3)) * 2
+    target = org + (hit - org) * rng.uniform(0.3, 0.9, (n, 1))
+    c[:, 0:3], c[:, 3:6], c[:, 6:9], c[:, 9:12], c[:, 12:15] = org, target, P0, P1, P2
+    nn = rng.normal(size=(n, 3))
+    c[:, 15:18] = nn / np.linalg.norm(nn, axis=1, keepdims=True)
+    c[:, 18] = rng.normal(size=n)
+    fi, fo = tmp_path / "in.bin", tmp_path / "out.bin"
+    fi.write_bytes(np.int32(n).tobytes() + c.tobytes())
+    subprocess.run([harness_exe, "xdotn_grad", str(fi), str(fo)], check=True, timeout=120)
+    out = np.fromfile(str(fo), np.float32).reshape(n, 16)
+
+    def autograd(i, dtype):
+        pts = [torch.tensor(c[i:i + 1, a:a + 3], dtype=dtype, requires_grad=True) for a in (0, 3, 6, 9, 12)]
+        o, tg, p0, p1, p2 = pts
+        u, v = O.ray_intersect_ad(O.normalize(tg - o), o, p0, p1 - p0, p2 - p0)
+        w = 1.0 - u - v
+        u2 = w[:, None] * p0.detach() + u[:, None] * p1.detach() + v[:, None] * p2.detach()
+        x = O.dot(torch.tensor(c[i:i + 1, 15:18], dtype=dtype), u2)
+        (x * float(c[i, 18])).sum().backward()
+        return [x.detach()] + [p.grad[0] for p in pts]
+
+    e_lib, e_f32 = [], []
+    for i in range(n):
+        r64, r32 = autograd(i, torch.float64), autograd(i, torch.float32)
+        got = [out[i, 0:1]] + [out[i, 1 + 3 * j:4 + 3 * j] for j in range(5)]
+        for g, a, b in zip(got, r64, r32):
+            ref = a.numpy()
+            scale = max(np.abs(ref).max(), 1e-6)
+            e_lib.append(np.abs(g - ref).max() / scale)
+            e_f32.append(np.abs(b.double().numpy() - ref).max() / scale)
+    e_lib, e_f32 = np.array(e_lib), np.array(e_f32)
+    assert np.median(e_lib) <= 2 * np.median(e_f32) + 1e-9
+    assert np.percentile(e_lib, 99) <= 3 * np.percentile(e_f32, 99)
+    assert e_lib.max() <= 2 * e_f32.max(), (e_lib.max(), e_f32.max())
