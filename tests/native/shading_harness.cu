@@ -1,6 +1,7 @@
-// Host build of the library's shading functions (test infrastructure). Reads
-// cases from argv[1] and writes the library's values to argv[2], for the
-// comparison with the oracle's restatements in tests/test_shading_host.py.
+// Host build of the library's shading and camera functions (test
+// infrastructure). Reads cases from a file and writes the library's values
+// to another, for the comparison with the oracle's restatements in
+// tests/test_shading_host.py.
 //
 // Input: int32 n, then n records of kIn float32:
 //   type, roughness, spec[3], kd[3], wo[3], wi[3], s0, s1, n[3], ng[3]
@@ -11,6 +12,7 @@
 #include "../../tensorray_b200/csrc/shading.cuh"
 
 #include <cstdio>
+#include <string>
 #include <vector>
 
 using namespace trn;
@@ -20,9 +22,41 @@ constexpr int kIn = 22;
 constexpr int kOut = 19;
 }  // namespace
 
+// Mode "camera IN OUT": int32 n, the CameraDesc bytes (the library's
+// trn_camera, same layout), then n records of 9 float32 (p[3], ng[3], J, qx,
+// qy) in; n records of 10 float32 out: sample_direct (qx, qy, valid, pixel,
+// sensor_val), sensor_ray_dir[3], image_pixel, camera_factor.
+int run_camera(const char* in_path, const char* out_path) {
+  FILE* fi = std::fopen(in_path, "rb");
+  if (!fi) return 1;
+  int n = 0;
+  CameraDesc cam;
+  if (std::fread(&n, sizeof n, 1, fi) != 1 || n < 0 || std::fread(&cam, sizeof cam, 1, fi) != 1) return 1;
+  std::vector<float> in((size_t)n * 9), out((size_t)n * 10);
+  if (std::fread(in.data(), sizeof(float), in.size(), fi) != in.size()) return 1;
+  std::fclose(fi);
+  for (int i = 0; i < n; i++) {
+    const float* c = &in[(size_t)i * 9];
+    float* o = &out[(size_t)i * 10];
+    const F3 p(c[0], c[1], c[2]), ng(c[3], c[4], c[5]);
+    const SensorSample sd = sample_direct(cam, p);
+    o[0] = sd.qx; o[1] = sd.qy; o[2] = sd.valid ? 1.f : 0.f; o[3] = (float)sd.pixel; o[4] = sd.sensor_val;
+    const F3 d = sensor_ray_dir(cam, c[7], c[8]);
+    o[5] = d.x; o[6] = d.y; o[7] = d.z;
+    o[8] = (float)image_pixel(cam, c[7], c[8]);
+    o[9] = camera_factor<float>(cam, p, ng, c[6]);
+  }
+  FILE* fo = std::fopen(out_path, "wb");
+  if (!fo) return 1;
+  std::fwrite(out.data(), sizeof(float), out.size(), fo);
+  std::fclose(fo);
+  return 0;
+}
+
 int main(int argc, char** argv) {
+  if (argc == 4 && std::string(argv[1]) == "camera") return run_camera(argv[2], argv[3]);
   if (argc != 3) {
-    std::fprintf(stderr, "usage: shading_harness IN OUT\n");
+    std::fprintf(stderr, "usage: shading_harness IN OUT | shading_harness camera IN OUT\n");
     return 2;
   }
   FILE* fi = std::fopen(argv[1], "rb");

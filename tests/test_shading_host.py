@@ -10,7 +10,11 @@ directions, roughness from 0.01 to 1 and samples at 0, 1/2 and the ends of
 - eval_inner (Diffuse.cpp:37-41, Microfacet.cpp:37-79) and bsdf_pdf_local
   agree within 1e-6 relative per case: the Fresnel term's exp and a few
   divisions round differently in libm and in torch (largest seen: 2.1e-7 and
-  2.5e-7).
+  2.5e-7);
+- the sensor functions, Camera::sampleDirect (Camera.cpp:399-416), the
+  boundary-ray direction (Camera.cpp:379-397), WriteToImage's pixel
+  (Camera.cpp:418-431) and EvalFilter's factor (Camera.cpp:279-303), agree
+  bit for bit on the library's camera.
 
 The device build of the same functions is checked against the oracle by the
 GPU parity tests; this adds per-function coverage of the edge cases without
@@ -32,20 +36,25 @@ N_BSDF = 1500      # cases that go through the oracle's per-material calls
 
 
 @pytest.fixture(scope="module")
-def harness_out(tmp_path_factory):
-    d = tmp_path_factory.mktemp("shading")
-    exe = str(d / "shading_harness")
+def harness_exe(tmp_path_factory):
+    exe = str(tmp_path_factory.mktemp("shading_exe") / "shading_harness")
     cmd = [build._nvcc(), "-O2", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a",
            "--expt-relaxed-constexpr", os.path.join(HERE, "native", "shading_harness.cu"), "-o", exe]
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
         pytest.fail("nvcc failed:\n" + res.stderr[-2000:])
+    return exe
+
+
+@pytest.fixture(scope="module")
+def harness_out(harness_exe, tmp_path_factory):
+    d = tmp_path_factory.mktemp("shading")
     c = _cases()
     fi, fo = str(d / "in.bin"), str(d / "out.bin")
     with open(fi, "wb") as f:
         f.write(np.int32(N).tobytes())
         f.write(c.tobytes())
-    subprocess.run([exe, fi, fo], check=True, timeout=120)
+    subprocess.run([harness_exe, fi, fo], check=True, timeout=120)
     return c, np.fromfile(fo, np.float32).reshape(N, 19)
 
 
@@ -118,3 +127,30 @@ def test_bsdf_value_pdf_and_visible_normal_sample(harness_out):
             vs = O.vndf_sample(wo, np.float32(c[i, 1]), _t(c[i:i + 1, 14]), _t(c[i:i + 1, 15])).numpy()[0]
             assert _bits_equal(out[i, 9:12], vs), i
     assert worst_eval <= 1e-6 and worst_pdf <= 1e-6, (worst_eval, worst_pdf)
+
+
+def test_sensor_functions_are_bit_identical(harness_exe, tmp_path):
+    from tensorray_b200 import api
+    from tests.helpers import oracle_camera_from
+    rng = np.random.default_rng(3)
+    cam = api.Camera((1.0, 2.0, 5.0), (0.0, 0.5, 0.0), (0.0, 1.0, 0.0), 320, 200, 40.0)
+    oc = oracle_camera_from(cam)
+    n = 20000
+    c = np.zeros((n, 9), np.float32)
+    c[:, 0:3] = rng.normal(0, 2, (n, 3))                       # points in front of and behind the camera
+    ng = rng.normal(size=(n, 3))
+    c[:, 3:6] = ng / np.linalg.norm(ng, axis=1, keepdims=True)
+    c[:, 6] = rng.uniform(0.5, 2, n)
+    c[:, 7:9] = rng.uniform(-0.1, 1.1, (n, 2))                 # sensor coordinates, some off the film
+    fi, fo = tmp_path / "cin.bin", tmp_path / "cout.bin"
+    fi.write_bytes(np.int32(n).tobytes() + bytes(cam.c) + c.tobytes())
+    subprocess.run([harness_exe, "camera", str(fi), str(fo)], check=True, timeout=120)
+    out = np.fromfile(str(fo), np.float32).reshape(n, 10)
+    qx, qy, valid, pixel, sval = O.sample_direct(oc, _t(c[:, 0:3]))
+    assert _bits_equal(out[:, 0], qx.numpy()) and _bits_equal(out[:, 1], qy.numpy())
+    assert np.array_equal(out[:, 2], valid.numpy().astype(np.float32))
+    assert np.array_equal(out[:, 3], pixel.numpy().astype(np.float32))
+    assert _bits_equal(out[:, 4], sval.numpy())
+    assert _bits_equal(out[:, 5:8], O.sensor_ray_dir(oc, _t(c[:, 7]), _t(c[:, 8])).numpy())
+    assert np.array_equal(out[:, 8], O.image_pixel(oc, _t(c[:, 7]), _t(c[:, 8])).numpy().astype(np.float32))
+    assert _bits_equal(out[:, 9], O.camera_factor(oc, _t(c[:, 0:3]), _t(c[:, 3:6]), _t(c[:, 6])).numpy())
