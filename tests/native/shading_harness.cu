@@ -53,10 +53,56 @@ int run_camera(const char* in_path, const char* out_path) {
   return 0;
 }
 
+// Mode "hash IN OUT": int32 n, then n records of 4 uint32 (seed, term, dim,
+// slot) in; n float32 hash_uniform values out.
+int run_hash(const char* in_path, const char* out_path) {
+  FILE* fi = std::fopen(in_path, "rb");
+  if (!fi) return 1;
+  int n = 0;
+  if (std::fread(&n, sizeof n, 1, fi) != 1 || n < 0) return 1;
+  std::vector<uint32_t> in((size_t)n * 4);
+  std::vector<float> out(n);
+  if (std::fread(in.data(), sizeof(uint32_t), in.size(), fi) != in.size()) return 1;
+  std::fclose(fi);
+  for (int i = 0; i < n; i++) out[i] = hash_uniform(in[4 * i], in[4 * i + 1], in[4 * i + 2], in[4 * i + 3]);
+  FILE* fo = std::fopen(out_path, "wb");
+  if (!fo) return 1;
+  std::fwrite(out.data(), sizeof(float), out.size(), fo);
+  std::fclose(fo);
+  return 0;
+}
+
+// Mode "discrete IN OUT": int32 c, c float32 CDF values, int32 m, m float32
+// samples in; m records (int32 index, float32 reused sample) out.
+int run_discrete(const char* in_path, const char* out_path) {
+  FILE* fi = std::fopen(in_path, "rb");
+  if (!fi) return 1;
+  int c = 0, m = 0;
+  if (std::fread(&c, sizeof c, 1, fi) != 1 || c <= 0) return 1;
+  std::vector<float> cdf(c);
+  if (std::fread(cdf.data(), sizeof(float), c, fi) != (size_t)c) return 1;
+  if (std::fread(&m, sizeof m, 1, fi) != 1 || m < 0) return 1;
+  std::vector<float> u(m);
+  if (std::fread(u.data(), sizeof(float), m, fi) != (size_t)m) return 1;
+  std::fclose(fi);
+  FILE* fo = std::fopen(out_path, "wb");
+  if (!fo) return 1;
+  for (int i = 0; i < m; i++) {
+    float reuse = 0.f;
+    const int idx = sample_discrete(cdf.data(), c, u[i], reuse);
+    std::fwrite(&idx, sizeof idx, 1, fo);
+    std::fwrite(&reuse, sizeof reuse, 1, fo);
+  }
+  std::fclose(fo);
+  return 0;
+}
+
 int main(int argc, char** argv) {
   if (argc == 4 && std::string(argv[1]) == "camera") return run_camera(argv[2], argv[3]);
+  if (argc == 4 && std::string(argv[1]) == "hash") return run_hash(argv[2], argv[3]);
+  if (argc == 4 && std::string(argv[1]) == "discrete") return run_discrete(argv[2], argv[3]);
   if (argc != 3) {
-    std::fprintf(stderr, "usage: shading_harness IN OUT | shading_harness camera IN OUT\n");
+    std::fprintf(stderr, "usage: shading_harness IN OUT | shading_harness camera|hash|discrete IN OUT\n");
     return 2;
   }
   FILE* fi = std::fopen(argv[1], "rb");

@@ -14,7 +14,9 @@ directions, roughness from 0.01 to 1 and samples at 0, 1/2 and the ends of
 - the sensor functions, Camera::sampleDirect (Camera.cpp:399-416), the
   boundary-ray direction (Camera.cpp:379-397), WriteToImage's pixel
   (Camera.cpp:418-431) and EvalFilter's factor (Camera.cpp:279-303), agree
-  bit for bit on the library's camera.
+  bit for bit on the library's camera;
+- the counter-hash sampler and discrete sampling with sample reuse agree bit
+  for bit.
 
 The device build of the same functions is checked against the oracle by the
 GPU parity tests; this adds per-function coverage of the edge cases without
@@ -154,3 +156,43 @@ def test_sensor_functions_are_bit_identical(harness_exe, tmp_path):
     assert _bits_equal(out[:, 5:8], O.sensor_ray_dir(oc, _t(c[:, 7]), _t(c[:, 8])).numpy())
     assert np.array_equal(out[:, 8], O.image_pixel(oc, _t(c[:, 7]), _t(c[:, 8])).numpy().astype(np.float32))
     assert _bits_equal(out[:, 9], O.camera_factor(oc, _t(c[:, 0:3]), _t(c[:, 3:6]), _t(c[:, 6])).numpy())
+
+
+def test_sample_sources_are_bit_identical(harness_exe, tmp_path):
+    """The counter-hash sampler every path reads its uniforms from
+    (hash_uniform) over 15,200 (seed, term, dimension, slot) tuples, slots 0
+    and 2^32 - 1 among them; and Distribution1D::SampleDiscrete with
+    ReuseSample (Distribution.cu:37-48, Distribution.cpp:37-43) over CDFs of
+    1-300 entries with zero-weight runs, at random samples, at the CDF's own
+    values and at 0, 1 and the ends of (0, 1)."""
+    rng = np.random.default_rng(5)
+    recs, ref = [], []
+    for _ in range(50):
+        seed, term, dim = (int(x) for x in rng.integers(0, 2 ** 32, 3, dtype=np.uint64))
+        slots = np.concatenate([rng.integers(0, 2 ** 32, 300, dtype=np.uint64),
+                                np.array([0, 1, 2 ** 32 - 1, 2 ** 31], np.uint64)])
+        recs += [(seed, term, dim, int(s)) for s in slots]
+        ref.append(O.hash_uniform(seed, term, dim, slots))
+    recs, ref = np.array(recs, np.uint32), np.concatenate(ref).astype(np.float32)
+    fi, fo = tmp_path / "hin.bin", tmp_path / "hout.bin"
+    fi.write_bytes(np.int32(len(recs)).tobytes() + recs.tobytes())
+    subprocess.run([harness_exe, "hash", str(fi), str(fo)], check=True, timeout=120)
+    assert _bits_equal(np.fromfile(str(fo), np.float32), ref)
+
+    for _ in range(30):
+        n = int(rng.integers(1, 300))
+        f = rng.uniform(0, 1, n).astype(np.float32)
+        f[rng.random(n) < 0.3] = 0
+        f[0] = f[0] if f.sum() > 0 else 1.0
+        cdf, integral = O.cdf_of(torch.as_tensor(f))
+        u = np.concatenate([rng.random(500).astype(np.float32), cdf.numpy()[:50],
+                            np.array([0.0, 1.0, 2 ** -24, 1 - 2 ** -24], np.float32)])
+        fi, fo = tmp_path / "din.bin", tmp_path / "dout.bin"
+        fi.write_bytes(np.int32(n).tobytes() + cdf.numpy().astype(np.float32).tobytes()
+                       + np.int32(len(u)).tobytes() + u.tobytes())
+        subprocess.run([harness_exe, "discrete", str(fi), str(fo)], check=True, timeout=120)
+        raw = np.fromfile(str(fo), np.uint8).reshape(-1, 8)
+        idx = raw[:, :4].copy().view(np.int32).ravel()
+        reuse = raw[:, 4:].copy().view(np.float32).ravel()
+        ri, _, rr = O.sample_discrete(cdf, integral, torch.as_tensor(f), torch.as_tensor(u))
+        assert np.array_equal(idx, ri.numpy()) and _bits_equal(reuse, rr.numpy())
