@@ -108,8 +108,36 @@ int run_xdotn_grad(const char* in_path, const char* out_path) {
   return 0;
 }
 
+// Mode "camera_factor_grad IN OUT": int32 n, the CameraDesc bytes, then n
+// records of 7 float32 (p[3], ng[3], W) in; n records of 7 float32 (g_p[3],
+// g_ng[3], g_J) out.
+int run_camera_factor_grad(const char* in_path, const char* out_path) {
+  FILE* fi = std::fopen(in_path, "rb");
+  if (!fi) return 1;
+  int n = 0;
+  CameraDesc cam;
+  if (std::fread(&n, sizeof n, 1, fi) != 1 || n < 0 || std::fread(&cam, sizeof cam, 1, fi) != 1) return 1;
+  std::vector<float> in((size_t)n * 7), out((size_t)n * 7);
+  if (std::fread(in.data(), sizeof(float), in.size(), fi) != in.size()) return 1;
+  std::fclose(fi);
+  for (int i = 0; i < n; i++) {
+    const float* c = &in[(size_t)i * 7];
+    F3 g_p, g_ng;
+    float g_J = 0.f;
+    camera_factor_grad(cam, F3(c[0], c[1], c[2]), F3(c[3], c[4], c[5]), c[6], g_p, g_ng, g_J);
+    float* o = &out[(size_t)i * 7];
+    o[0] = g_p.x; o[1] = g_p.y; o[2] = g_p.z; o[3] = g_ng.x; o[4] = g_ng.y; o[5] = g_ng.z; o[6] = g_J;
+  }
+  FILE* fo = std::fopen(out_path, "wb");
+  if (!fo) return 1;
+  std::fwrite(out.data(), sizeof(float), out.size(), fo);
+  std::fclose(fo);
+  return 0;
+}
+
 int main(int argc, char** argv) {
   if (argc == 4 && std::string(argv[1]) == "eval_inner_vjp") return run_eval_inner_vjp(argv[2], argv[3]);
+  if (argc == 4 && std::string(argv[1]) == "camera_factor_grad") return run_camera_factor_grad(argv[2], argv[3]);
   if (argc == 4 && std::string(argv[1]) == "xdotn_grad") return run_xdotn_grad(argv[2], argv[3]);
   std::mt19937 rng(1);
   std::uniform_real_distribution<float> U(-1.f, 1.f);
