@@ -135,8 +135,46 @@ int run_camera_factor_grad(const char* in_path, const char* out_path) {
   return 0;
 }
 
+// Mode "factor_vjp IN OUT": int32 n, then n records of 30 float32 (type,
+// roughness, spec[3], xprev[3], x[3], ns[3], kd[3], z[3], nz[3], J, K[3],
+// adj[3]) in; n records of 22 float32 (F[3], g_prev[3], g_x[3], g_ns[3],
+// g_kd[3], g_z[3], g_nz[3], g_J) out.
+int run_factor_vjp(const char* in_path, const char* out_path) {
+  FILE* fi = std::fopen(in_path, "rb");
+  if (!fi) return 1;
+  int n = 0;
+  if (std::fread(&n, sizeof n, 1, fi) != 1 || n < 0) return 1;
+  std::vector<float> in((size_t)n * 30), out((size_t)n * 22);
+  if (std::fread(in.data(), sizeof(float), in.size(), fi) != in.size()) return 1;
+  std::fclose(fi);
+  for (int i = 0; i < n; i++) {
+    const float* c = &in[(size_t)i * 30];
+    BsdfDesc b{};
+    b.type = (int)c[0];
+    b.tex = -1;
+    b.roughness = c[1];
+    for (int k = 0; k < 3; k++) b.spec[k] = c[2 + k];
+    auto v3 = [&](int o) { return F3(c[o], c[o + 1], c[o + 2]); };
+    F3 g[6] = {F3z(), F3z(), F3z(), F3z(), F3z(), F3z()};
+    float gJ = 0.f;
+    const F3 F = factor_vjp(b, true, true, v3(5), v3(8), v3(11), v3(14), v3(17), v3(20), c[23], v3(24), v3(27),
+                            g[0], g[1], g[2], g[3], g[4], g[5], gJ);
+    float* o = &out[(size_t)i * 22];
+    o[0] = F.x; o[1] = F.y; o[2] = F.z;
+    for (int j = 0; j < 6; j++)
+      for (int k = 0; k < 3; k++) o[3 + 3 * j + k] = g[j][k];
+    o[21] = gJ;
+  }
+  FILE* fo = std::fopen(out_path, "wb");
+  if (!fo) return 1;
+  std::fwrite(out.data(), sizeof(float), out.size(), fo);
+  std::fclose(fo);
+  return 0;
+}
+
 int main(int argc, char** argv) {
   if (argc == 4 && std::string(argv[1]) == "eval_inner_vjp") return run_eval_inner_vjp(argv[2], argv[3]);
+  if (argc == 4 && std::string(argv[1]) == "factor_vjp") return run_factor_vjp(argv[2], argv[3]);
   if (argc == 4 && std::string(argv[1]) == "camera_factor_grad") return run_camera_factor_grad(argv[2], argv[3]);
   if (argc == 4 && std::string(argv[1]) == "xdotn_grad") return run_xdotn_grad(argv[2], argv[3]);
   std::mt19937 rng(1);

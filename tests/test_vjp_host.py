@@ -204,3 +204,82 @@ def test_camera_factor_adjoint_matches_autograd_of_the_oracle(harness_exe, tmp_p
     assert np.median(e_lib) <= 2 * np.median(e_f32) + 1e-9
     assert np.percentile(e_lib, 99) <= 3 * np.percentile(e_f32, 99)
     assert e_lib.max() <= 2 * e_f32.max(), (e_lib.max(), e_f32.max())
+
+
+def test_path_factor_adjoint_matches_autograd_of_the_oracle(harness_exe, tmp_path):
+    """factor_vjp, the library's reverse mode of the NEE / continuation factor
+    of EvalRadianceDirect (Integrator.cpp:186-267),
+    F = B(kd, wo, wi) |ns.wi| |nz.wi| / d^2 J K with the BSDF in the frame
+    coordinate_system builds around the unnormalised shading normal, against
+    float64 autograd of the same factor composed from the oracle's
+    coordinate_system, bsdf_eval, normalize and dot, on 2000 seeded diffuse
+    and GGX vertices. Value and the gradients with respect to the previous
+    vertex, the vertex, the shading normal, the albedo, the next point, its
+    normal and J are as accurate as float32 autograd: median, 99th percentile
+    and largest error within 2x, 3x and 2x of autograd's (measured: 1.6e-7,
+    6.6e-6 and 2.8e-3 against 1.6e-7, 6.7e-6 and 2.5e-2)."""
+    from types import SimpleNamespace
+
+    import numpy as np
+    import torch
+
+    from oracle import tr_oracle as O
+    rng = np.random.default_rng(12)
+    n = 2000
+
+    def unit(m):
+        v = rng.normal(size=(m, 3))
+        return v / np.linalg.norm(v, axis=1, keepdims=True)
+
+    c = np.zeros((n, 30), np.float32)
+    c[:, 0] = (np.arange(n) % 3 != 0).astype(np.float32)
+    c[:, 1] = rng.uniform(0.1, 0.9, n)
+    c[:, 2:5] = [0.04, 0.05, 0.5]
+    ns = unit(n) * 0.3 + np.array([0.0, 1.0, 0.0])
+    nsu = ns / np.linalg.norm(ns, axis=1, keepdims=True)
+    ns = nsu * rng.uniform(0.9, 1.0, (n, 1))                      # unnormalised shading normals
+    x = rng.uniform(-1, 1, (n, 3))
+    c[:, 5:8] = x + (nsu + unit(n) * 0.8) * rng.uniform(1, 2, (n, 1))
+    c[:, 8:11], c[:, 11:14] = x, ns
+    c[:, 14:17] = [0.3, 0.5, 0.7]
+    c[:, 17:20] = x + (nsu + unit(n) * 0.8) * rng.uniform(0.5, 2.5, (n, 1))
+    c[:, 20:23] = unit(n)
+    c[:, 23] = rng.uniform(0.5, 1.5, n)
+    c[:, 24:27] = rng.uniform(0.1, 10, (n, 3))
+    c[:, 27:30] = rng.normal(size=(n, 3))
+    fi, fo = tmp_path / "in.bin", tmp_path / "out.bin"
+    fi.write_bytes(np.int32(n).tobytes() + c.tobytes())
+    subprocess.run([harness_exe, "factor_vjp", str(fi), str(fo)], check=True, timeout=120)
+    out = np.fromfile(str(fo), np.float32).reshape(n, 22)
+
+    def autograd(i, dtype):
+        b = SimpleNamespace(type=int(c[i, 0]), roughness=float(c[i, 1]), specular=tuple(float(v) for v in c[i, 2:5]))
+        xp, xx, nsv, kd, zz, nz = (torch.tensor(c[i:i + 1, a:a + 3], dtype=dtype, requires_grad=True)
+                                   for a in (5, 8, 11, 14, 17, 20))
+        J = torch.tensor(c[i:i + 1, 23], dtype=dtype, requires_grad=True)
+        wo = -O.normalize(xx - xp)
+        t, bb = O.coordinate_system(nsv)
+        wi = zz - xx
+        d2 = O.dot(wi, wi)
+        wi = wi / torch.sqrt(d2)[:, None]
+        G = O.dot(nz, -wi).abs() / d2
+        bv = O.bsdf_eval(b, (t, bb, nsv), None, kd, wo, wi, False) * O.dot(nsv, wi).abs()[:, None]
+        F = bv * (J * G)[:, None] * torch.tensor(c[i:i + 1, 24:27], dtype=dtype)
+        (F * torch.tensor(c[i:i + 1, 27:30], dtype=dtype)).sum().backward()
+        zero = torch.zeros(1, 3, dtype=dtype)
+        return [F.detach()[0]] + [(q.grad if q.grad is not None else zero)[0]
+                                  for q in (xp, xx, nsv, kd, zz, nz)] + [J.grad]
+
+    e_lib, e_f32 = [], []
+    for i in range(n):
+        r64, r32 = autograd(i, torch.float64), autograd(i, torch.float32)
+        got = [out[i, 0:3]] + [out[i, 3 + 3 * j:6 + 3 * j] for j in range(6)] + [out[i, 21:22]]
+        for g, a, b in zip(got, r64, r32):
+            ref = a.numpy()
+            scale = max(np.abs(ref).max(), 1e-6)
+            e_lib.append(np.abs(g - ref).max() / scale)
+            e_f32.append(np.abs(b.double().numpy() - ref).max() / scale)
+    e_lib, e_f32 = np.array(e_lib), np.array(e_f32)
+    assert np.median(e_lib) <= 2 * np.median(e_f32) + 1e-9
+    assert np.percentile(e_lib, 99) <= 3 * np.percentile(e_f32, 99)
+    assert e_lib.max() <= 2 * e_f32.max(), (e_lib.max(), e_f32.max())
