@@ -47,31 +47,21 @@ double rel(const double* a, const double* b, int n) {
 
 }  // namespace
 
-// Mode "eval_inner_vjp IN OUT": int32 n, then n records of 17 float32
-// (type, roughness, spec[3], kd[3], lo[3], li[3], gB[3]) in; n records of 12
-// float32 (B[3], g_lo[3], g_li[3], g_kd[3]) out.
-int run_eval_inner_vjp(const char* in_path, const char* out_path) {
+// File-driven modes: int32 n, `header_bytes` of header (copied to `header`),
+// then n records of in_w float32; writes n records of out_w float32 that
+// `body(in, out)` fills.
+template <class Body>
+int run_records(const char* in_path, const char* out_path, int in_w, int out_w, void* header, size_t header_bytes,
+                Body&& body) {
   FILE* fi = std::fopen(in_path, "rb");
   if (!fi) return 1;
   int n = 0;
   if (std::fread(&n, sizeof n, 1, fi) != 1 || n < 0) return 1;
-  std::vector<float> in((size_t)n * 17), out((size_t)n * 12);
+  if (header_bytes && std::fread(header, header_bytes, 1, fi) != 1) return 1;
+  std::vector<float> in((size_t)n * in_w), out((size_t)n * out_w, 0.f);
   if (std::fread(in.data(), sizeof(float), in.size(), fi) != in.size()) return 1;
   std::fclose(fi);
-  for (int i = 0; i < n; i++) {
-    const float* c = &in[(size_t)i * 17];
-    BsdfDesc b{};
-    b.type = (int)c[0];
-    b.tex = -1;
-    b.roughness = c[1];
-    for (int k = 0; k < 3; k++) b.spec[k] = c[2 + k];
-    const F3 kd(c[5], c[6], c[7]), lo(c[8], c[9], c[10]), li(c[11], c[12], c[13]), gB(c[14], c[15], c[16]);
-    F3 g_lo = F3z(), g_li = F3z(), g_kd = F3z();
-    const F3 B = eval_inner_vjp(b, kd, lo, li, gB, g_lo, g_li, g_kd);
-    const F3 o[4] = {B, g_lo, g_li, g_kd};
-    for (int j = 0; j < 4; j++)
-      for (int k = 0; k < 3; k++) out[(size_t)i * 12 + 3 * j + k] = o[j][k];
-  }
+  for (int i = 0; i < n; i++) body(&in[(size_t)i * in_w], &out[(size_t)i * out_w]);
   FILE* fo = std::fopen(out_path, "wb");
   if (!fo) return 1;
   std::fwrite(out.data(), sizeof(float), out.size(), fo);
@@ -79,97 +69,73 @@ int run_eval_inner_vjp(const char* in_path, const char* out_path) {
   return 0;
 }
 
-// Mode "xdotn_grad IN OUT": int32 n, then n records of 19 float32
-// (org[3], target[3], P0[3], P1[3], P2[3], n[3], W) in; n records of 16
-// float32 (xdotn, g_org[3], g_target[3], g0[3], g1[3], g2[3]) out.
+BsdfDesc bsdf_of(const float* c) {
+  BsdfDesc b{};
+  b.type = (int)c[0];
+  b.tex = -1;
+  b.roughness = c[1];
+  for (int k = 0; k < 3; k++) b.spec[k] = c[2 + k];
+  return b;
+}
+
+// Mode "eval_inner_vjp IN OUT": records of 17 float32 (type, roughness,
+// spec[3], kd[3], lo[3], li[3], gB[3]) in; 12 float32 (B[3], g_lo[3], g_li[3],
+// g_kd[3]) out.
+int run_eval_inner_vjp(const char* in_path, const char* out_path) {
+  return run_records(in_path, out_path, 17, 12, nullptr, 0, [](const float* c, float* o) {
+    const BsdfDesc b = bsdf_of(c);
+    const F3 kd(c[5], c[6], c[7]), lo(c[8], c[9], c[10]), li(c[11], c[12], c[13]), gB(c[14], c[15], c[16]);
+    F3 g_lo = F3z(), g_li = F3z(), g_kd = F3z();
+    const F3 r[4] = {eval_inner_vjp(b, kd, lo, li, gB, g_lo, g_li, g_kd), g_lo, g_li, g_kd};
+    for (int j = 0; j < 4; j++)
+      for (int k = 0; k < 3; k++) o[3 * j + k] = r[j][k];
+  });
+}
+
+// Mode "xdotn_grad IN OUT": records of 19 float32 (org[3], target[3], P0[3],
+// P1[3], P2[3], n[3], W) in; 16 float32 (xdotn, g_org[3], g_target[3], g0[3],
+// g1[3], g2[3]) out.
 int run_xdotn_grad(const char* in_path, const char* out_path) {
-  FILE* fi = std::fopen(in_path, "rb");
-  if (!fi) return 1;
-  int n = 0;
-  if (std::fread(&n, sizeof n, 1, fi) != 1 || n < 0) return 1;
-  std::vector<float> in((size_t)n * 19), out((size_t)n * 16);
-  if (std::fread(in.data(), sizeof(float), in.size(), fi) != in.size()) return 1;
-  std::fclose(fi);
-  for (int i = 0; i < n; i++) {
-    const float* c = &in[(size_t)i * 19];
+  return run_records(in_path, out_path, 19, 16, nullptr, 0, [](const float* c, float* o) {
     const F3 org(c[0], c[1], c[2]), target(c[3], c[4], c[5]), P0(c[6], c[7], c[8]), P1(c[9], c[10], c[11]),
         P2(c[12], c[13], c[14]), nn(c[15], c[16], c[17]);
     F3 g[5];
     xdotn_grad(org, target, P0, P1, P2, nn, c[18], g[0], g[1], g[2], g[3], g[4]);
-    float* o = &out[(size_t)i * 16];
     o[0] = xdotn<float>(org, target, P0, P1, P2, nn);
     for (int j = 0; j < 5; j++)
       for (int k = 0; k < 3; k++) o[1 + 3 * j + k] = g[j][k];
-  }
-  FILE* fo = std::fopen(out_path, "wb");
-  if (!fo) return 1;
-  std::fwrite(out.data(), sizeof(float), out.size(), fo);
-  std::fclose(fo);
-  return 0;
+  });
 }
 
-// Mode "camera_factor_grad IN OUT": int32 n, the CameraDesc bytes, then n
-// records of 7 float32 (p[3], ng[3], W) in; n records of 7 float32 (g_p[3],
-// g_ng[3], g_J) out.
+// Mode "camera_factor_grad IN OUT": the CameraDesc bytes after n, then
+// records of 7 float32 (p[3], ng[3], W) in; 7 float32 (g_p[3], g_ng[3], g_J)
+// out.
 int run_camera_factor_grad(const char* in_path, const char* out_path) {
-  FILE* fi = std::fopen(in_path, "rb");
-  if (!fi) return 1;
-  int n = 0;
   CameraDesc cam;
-  if (std::fread(&n, sizeof n, 1, fi) != 1 || n < 0 || std::fread(&cam, sizeof cam, 1, fi) != 1) return 1;
-  std::vector<float> in((size_t)n * 7), out((size_t)n * 7);
-  if (std::fread(in.data(), sizeof(float), in.size(), fi) != in.size()) return 1;
-  std::fclose(fi);
-  for (int i = 0; i < n; i++) {
-    const float* c = &in[(size_t)i * 7];
+  return run_records(in_path, out_path, 7, 7, &cam, sizeof cam, [&cam](const float* c, float* o) {
     F3 g_p, g_ng;
     float g_J = 0.f;
     camera_factor_grad(cam, F3(c[0], c[1], c[2]), F3(c[3], c[4], c[5]), c[6], g_p, g_ng, g_J);
-    float* o = &out[(size_t)i * 7];
     o[0] = g_p.x; o[1] = g_p.y; o[2] = g_p.z; o[3] = g_ng.x; o[4] = g_ng.y; o[5] = g_ng.z; o[6] = g_J;
-  }
-  FILE* fo = std::fopen(out_path, "wb");
-  if (!fo) return 1;
-  std::fwrite(out.data(), sizeof(float), out.size(), fo);
-  std::fclose(fo);
-  return 0;
+  });
 }
 
-// Mode "factor_vjp IN OUT": int32 n, then n records of 30 float32 (type,
-// roughness, spec[3], xprev[3], x[3], ns[3], kd[3], z[3], nz[3], J, K[3],
-// adj[3]) in; n records of 22 float32 (F[3], g_prev[3], g_x[3], g_ns[3],
-// g_kd[3], g_z[3], g_nz[3], g_J) out.
+// Mode "factor_vjp IN OUT": records of 30 float32 (type, roughness, spec[3],
+// xprev[3], x[3], ns[3], kd[3], z[3], nz[3], J, K[3], adj[3]) in; 22 float32
+// (F[3], g_prev[3], g_x[3], g_ns[3], g_kd[3], g_z[3], g_nz[3], g_J) out.
 int run_factor_vjp(const char* in_path, const char* out_path) {
-  FILE* fi = std::fopen(in_path, "rb");
-  if (!fi) return 1;
-  int n = 0;
-  if (std::fread(&n, sizeof n, 1, fi) != 1 || n < 0) return 1;
-  std::vector<float> in((size_t)n * 30), out((size_t)n * 22);
-  if (std::fread(in.data(), sizeof(float), in.size(), fi) != in.size()) return 1;
-  std::fclose(fi);
-  for (int i = 0; i < n; i++) {
-    const float* c = &in[(size_t)i * 30];
-    BsdfDesc b{};
-    b.type = (int)c[0];
-    b.tex = -1;
-    b.roughness = c[1];
-    for (int k = 0; k < 3; k++) b.spec[k] = c[2 + k];
-    auto v3 = [&](int o) { return F3(c[o], c[o + 1], c[o + 2]); };
+  return run_records(in_path, out_path, 30, 22, nullptr, 0, [](const float* c, float* o) {
+    const BsdfDesc b = bsdf_of(c);
+    auto v3 = [&](int k) { return F3(c[k], c[k + 1], c[k + 2]); };
     F3 g[6] = {F3z(), F3z(), F3z(), F3z(), F3z(), F3z()};
     float gJ = 0.f;
     const F3 F = factor_vjp(b, true, true, v3(5), v3(8), v3(11), v3(14), v3(17), v3(20), c[23], v3(24), v3(27),
                             g[0], g[1], g[2], g[3], g[4], g[5], gJ);
-    float* o = &out[(size_t)i * 22];
     o[0] = F.x; o[1] = F.y; o[2] = F.z;
     for (int j = 0; j < 6; j++)
       for (int k = 0; k < 3; k++) o[3 + 3 * j + k] = g[j][k];
     o[21] = gJ;
-  }
-  FILE* fo = std::fopen(out_path, "wb");
-  if (!fo) return 1;
-  std::fwrite(out.data(), sizeof(float), out.size(), fo);
-  std::fclose(fo);
-  return 0;
+  });
 }
 
 int main(int argc, char** argv) {
